@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""bench.py — SNAP atom-steps/s (E+F) on B200: adjoint vs plain dB/dr path; LJ pairs/s.
+
+Workload (default `snap_j8`): SNAP twojmax=8, two species (weights 1.0/0.5, radii
+0.5/0.45, rcutfac 5.0, switching on), BCC a=3.2 A 30^3 cells = 54,000 atoms, periodic,
+species 70/30 and jitter N(0, 0.12 A) from seed 4, per-species beta ~ N(0, 1e-2).
+A step is one energy + forces evaluation of all atoms, neighbor build included.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is the adjoint path's atom-steps/s with inputs resident in HBM, timed with CUDA
+events on the launching stream, L2 flushed (256 MiB write) before every step, max over
+ranks.  `e2e` is the same metric through the host-pointer C-ABI call
+(ipg_snap_energy_forces) with pinned host buffers: the H2D copy of positions/species/
+beta and the D2H copy of E, W and F are inside the timed region.  The plain dB/dr path
+and the pair workloads (LJ 1000 atoms, the 5-term linear combination over 32,000 atoms)
+are measured in the same run and reported as extra keys.  With --gpus N > 1 (torchrun)
+every rank evaluates its own copy of the workload (weak scaling, no collective in the
+data path).  `--impl reference` times the reference algorithm's CPU restatement
+(oracle/, OpenMP over all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "interatomicpotentials.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "SNAP atom-steps/s (E+F, 1 B200): adjoint vs plain dB/dr path; LJ pairs/s"
+UNIT = "atom-steps/s"
+WORKLOAD = ("snap_j8: SNAP twojmax=8 (55 components), 2 species (weights 1.0/0.5, radii 0.5/0.45, "
+            "rcutfac 5.0, switching on), BCC a=3.2 A 30^3 = 54,000 atoms, periodic, jitter N(0,0.12 A), "
+            "adjoint-Y energy+forces (neighbor build included)")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def oracle_sample_rate(system, prm, beta, target_s):
+    """The oracle (reference algorithm, C++/OpenMP) on the first M centre atoms of the
+    workload, M sized for about `target_s` seconds.  Returns (atom-steps/s, M, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    orc = oracle.Snap(prm["twojmax"], prm["radii"], prm["weight"], prm["rcutfac"], prm["rmin0"], prm["rfac0"],
+                      switch=prm.get("switch_flag", False))
+    sp = np.array([prm["species"].index(s) for s in system.symbols], np.int32)
+    args = (system.positions, sp, system.L, beta, 0.0)
+    m = 64
+    t0 = time.perf_counter()
+    orc.energy_forces(*args, mode="plain", i0=0, i1=m)
+    dt = time.perf_counter() - t0
+    m = int(min(len(system), max(64, m * target_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    orc.energy_forces(*args, mode="plain", i0=0, i1=m)
+    dt = time.perf_counter() - t0
+    return m / dt, m, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from ipg import workloads as W
+    system, prm, beta = W.snap_j8()
+    cores = cpu_count()
+    for _ in range(args.warmup):
+        oracle_sample_rate(system, prm, beta, 0.5)
+    rates, ms, secs = [], 0, 0.0
+    for _ in range(args.steps):
+        r, m, dt = oracle_sample_rate(system, prm, beta, 3.0)
+        rates.append(r)
+        ms, secs = m, secs + dt
+    value = float(np.median(rates))
+    sample = (f"first {ms} of the 54,000 centre atoms per step (plain dB/dr path as in compute_all_descriptors, "
+              f"contracted with beta), {cores} OpenMP threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * len(system) / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "n_atoms": len(system)},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="size of the CPU-baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and pair-workload lines")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import ipg
+    from ipg import flops as FL
+    from ipg import workloads as W
+    from ipg._lib import SNAP_ADJOINT, SNAP_PLAIN, lib
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    system, prm, beta = W.snap_j8()
+    n = len(system)
+    snap = ipg.SNAP(n, prm["twojmax"], prm["species"], prm["rcutfac"], prm["rmin0"], prm["rfac0"], prm["radii"],
+                    prm["weight"], switch_flag=True, ctx=ipg.Context(local))
+    ctx = snap.ctx
+    ctx.set_stream(stream.cuda_stream)
+    K = len(snap)
+    nsp = len(prm["species"])
+    sp_host = snap.species_ids(system)
+    beta_b = snap.beta_blocks(beta)
+    npairs = len(ipg.neighborlist_snap(system, snap, ctx=ctx)._j)
+
+    pos_d = torch.tensor(system.positions, device=dev)
+    sp_d = torch.tensor(sp_host, device=dev)
+    E_d = torch.zeros(1, dtype=torch.float64, device=dev)
+    F_d = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    W_d = torch.zeros(6, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    L = system.L
+    vp = C.c_void_p
+
+    def step(mode):
+        ctx.check(lib().ipg_snap_energy_forces_dev(snap.handle, n, vp(pos_d.data_ptr()), vp(sp_d.data_ptr()),
+                                                   L.ctypes.data_as(vp), beta_b.ctypes.data_as(vp), 0.0, mode,
+                                                   vp(E_d.data_ptr()), vp(F_d.data_ptr()), vp(W_d.data_ptr())))
+
+    def timed(fn, steps, kernel_timing=False):
+        for _ in range(args.warmup):
+            fn()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if kernel_timing:
+            ctx.timing(True)
+            for k in ("snap_atom", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
+                ctx.timing_read(k)
+        l0 = ctx.launch_count()
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        launches = ctx.launch_count() - l0
+        kt = {}
+        if kernel_timing:
+            for k in ("snap_atom", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
+                kt[k] = ctx.timing_read(k)
+            ctx.timing(False)
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = t.item()
+        return ms, launches, kt
+
+    with ClockSampler(local) as clk:
+        ms_adj, launches, kt = timed(lambda: step(SNAP_ADJOINT), args.steps, kernel_timing=True)
+    clocks = clk.summary()
+    value = world * n * args.steps / (ms_adj * 1e-3)
+
+    # e2e through the host-pointer C-ABI call, pinned host buffers
+    pos_h = torch.from_numpy(system.positions.copy()).pin_memory()
+    sp_h = torch.from_numpy(sp_host.copy()).pin_memory()
+    F_h = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    E_h = np.zeros(1)
+    W_h = np.zeros(6)
+
+    def step_e2e():
+        ctx.check(lib().ipg_snap_energy_forces(snap.handle, n, vp(pos_h.data_ptr()), vp(sp_h.data_ptr()),
+                                               L.ctypes.data_as(vp), beta_b.ctypes.data_as(vp), 0.0, SNAP_ADJOINT,
+                                               E_h.ctypes.data_as(vp), vp(F_h.data_ptr()), W_h.ctypes.data_as(vp)))
+
+    ms_e2e, _, _ = timed(step_e2e, args.steps)
+    e2e = {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int(24 * n + 4 * n + 8 * nsp * K), "d2h_bytes_per_step": int(24 * n + 8 * 8)}
+
+    # roofline of the dominant kernel (the fused per-atom SNAP kernel, FP64 pipe)
+    probe = C.CDLL(os.path.join(ROOT, "interatomicpotentials.jl_b200", "ipg", "libipg_probe.so"))
+    probe.ipg_probe_fp64_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    tf = C.c_double()
+    probe.ipg_probe_fp64_peak(local, 5, C.byref(tf), None)
+    fp64_peak = tf.value
+    ka_ms, ka_n = kt.get("snap_atom", (0.0, 0))
+    flops_launch = FL.snap_atom_kernel(prm["twojmax"], n, npairs, "adjoint")
+    achieved = flops_launch / (ka_ms / max(ka_n, 1) * 1e-3) / 1e12 if ka_n else None
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": (achieved / fp64_peak) if achieved else None, "traffic": None,
+                "kernel": "k_snap_atom<adjoint>", "peak_source": "measured DFMA probe (libipg_probe.so), this run",
+                "flops_per_launch": flops_launch, "avg_launch_ms": ka_ms / max(ka_n, 1)}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_adj / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "n_atoms": n, "n_pairs": npairs, "twojmax": prm["twojmax"],
+                       "path": "adjoint", "l2": "flushed before every step (256 MiB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": roofline, "clocks": clocks, "e2e": e2e, "gpu_launches": int(launches),
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items() if v[1]}}
+
+    if not args.no_extras:
+        ms_plain, _, ktp = timed(lambda: step(SNAP_PLAIN), max(2, args.steps // 2), kernel_timing=True)
+        plain_value = world * n * max(2, args.steps // 2) / (ms_plain * 1e-3)
+        line["plain_value"] = plain_value
+        line["adjoint_over_plain"] = value / plain_value
+        line["plain_kernel_ms_per_step"] = {k: v[0] / max(2, args.steps // 2) for k, v in ktp.items() if v[1]}
+        pair = {}
+        for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000())):
+            pairs = sum(len(x) for x in ipg.neighborlist(s2, p2.get_rcutoff(), ctx=ctx).j)
+            terms = ipg.empirical.empirical_terms(p2)
+            idx = {s: k for k, s in enumerate(s2.unique_symbols())}
+            arr = (ipg._lib.PairTerm * len(terms))()
+            for q, (c, pp) in enumerate(terms):
+                arr[q] = pp.term(idx, c)
+            p_d = torch.tensor(s2.positions, device=dev)
+            s_d = torch.tensor(np.array([idx[s] for s in s2.symbols], np.int32), device=dev)
+            f_d = torch.zeros((len(s2), 3), dtype=torch.float64, device=dev)
+            L2 = s2.L
+
+            def pstep():
+                ctx.check(lib().ipg_pair_eval_dev(ctx.handle, len(s2), vp(p_d.data_ptr()), vp(s_d.data_ptr()),
+                                                  L2.ctypes.data_as(vp), C.cast(arr, vp), len(terms),
+                                                  vp(E_d.data_ptr()), vp(f_d.data_ptr()), vp(W_d.data_ptr()), 7))
+            ms_p, _, _ = timed(pstep, args.steps)
+            # pairs/s counts every term's half pairs, as the reference evaluates them
+            term_pairs = pairs * len(terms)
+            pair[name] = {"pairs_per_s": world * term_pairs * args.steps / (ms_p * 1e-3), "ms_per_step":
+                          ms_p / args.steps, "n_atoms": len(s2), "half_pairs": pairs, "terms": len(terms)}
+        line["lj_pairs_per_s"] = pair
+
+    if rank == 0 and world == 1:
+        rate, m, dt = oracle_sample_rate(system, prm, beta_b, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cpu_count(), "kind": "port",
+                                "sample": f"first {m} of {n} centre atoms, plain dB/dr path, {dt:.1f} s, "
+                                          f"{cpu_count()} OpenMP threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.set_stream(None)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

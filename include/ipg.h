@@ -1,0 +1,232 @@
+/* ipg.h — C ABI of libipg.so, the B200 (sm_100a) force-field evaluation library.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an int status
+ * (IPG_OK = 0, negative = error) and never aborts.  Details of the last error of a
+ * context are available from ipg_last_error().
+ *
+ * Each declaration names the reference (cesmix-mit/InteratomicPotentials.jl v0.3.2)
+ * interface it replaces, as file:line within that project.
+ *
+ * Conventions
+ *  - Positions and forces are AoS: x0 y0 z0 x1 y1 z1 ... (Julia Vector{SVector{3,Float64}}
+ *    reinterpreted as a flat Float64 array).
+ *  - L[3] is the orthorhombic box diagonal; INFINITY marks an open (non-periodic) axis,
+ *    as in src/nnlist.jl:29 and src/BasisSystems/SNAP/utilities/utl.jl:64.
+ *  - Species are 0-based int32 ids.  For pair terms they index the 64-bit species mask;
+ *    for SNAP they index snap.species.
+ *  - Units: the pair API takes atomic units (bohr, hartree), like the reference
+ *    internals after austrip; the SNAP API takes the caller's length unit, like the
+ *    reference's ustrip.
+ *  - Host-pointer entry points copy inputs to the device and results back before they
+ *    return.  *_dev entry points take device pointers and run on the context's stream
+ *    (set with ipg_set_stream); they synchronise that stream before returning.
+ *  - Ownership: the caller owns every buffer it passes.  The library owns the device
+ *    scratch inside a context and grows it on demand.
+ *  - Threading: one context per host thread; calls on distinct contexts are independent.
+ */
+#ifndef IPG_H
+#define IPG_H
+
+#include <stdint.h>
+
+#if defined(IPG_BUILD) && defined(__GNUC__)
+#define IPG_API __attribute__((visibility("default")))
+#else
+#define IPG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define IPG_OK 0
+#define IPG_ERR_ARG (-1)          /* invalid argument (null pointer, bad size or flag)   */
+#define IPG_ERR_CUDA (-2)         /* CUDA runtime error                                  */
+#define IPG_ERR_NOMEM (-3)        /* device allocation failed                            */
+#define IPG_ERR_CAPACITY (-4)     /* a device-side capacity was exceeded                 */
+#define IPG_ERR_TIMEOUT (-5)      /* a bounded device wait ran out                       */
+#define IPG_ERR_NONFINITE (-6)    /* NaN or Inf in positions                             */
+#define IPG_ERR_SPECIES (-7)      /* species id out of range                             */
+#define IPG_ERR_UNSUPPORTED (-8)  /* valid in the reference but not built here           */
+#define IPG_ERR_NODEVICE (-9)     /* no CUDA device (or not an sm_100 device)            */
+
+/* ---- opaque handles ------------------------------------------------------------------ */
+typedef struct ipg_ctx ipg_ctx;
+typedef struct ipg_nlist ipg_nlist;
+typedef struct ipg_snap ipg_snap;
+
+/* ---- context ------------------------------------------------------------------------- */
+/* Creates a context on CUDA device `device` with its own non-blocking stream. */
+IPG_API int ipg_create(int device, ipg_ctx** out);
+IPG_API int ipg_destroy(ipg_ctx* ctx);
+/* Message of the last error on ctx ("" if none).  Valid until the next call on ctx. */
+IPG_API const char* ipg_last_error(const ipg_ctx* ctx);
+/* Upper bound, in milliseconds, for every bounded device-side wait (default 2000). */
+IPG_API int ipg_set_timeout_ms(ipg_ctx* ctx, uint32_t ms);
+/* Runs subsequent *_dev calls on `stream` (a cudaStream_t, or NULL for the context's own). */
+IPG_API int ipg_set_stream(ipg_ctx* ctx, void* stream);
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+IPG_API int ipg_version(void);
+/* Number of kernels this context has launched so far (for launch accounting).
+ * Instrumentation with no counterpart in the reference. */
+IPG_API int ipg_launch_count(const ipg_ctx* ctx, int64_t* out);
+/* Per-kernel device timing (instrumentation with no counterpart in the reference):
+ * when enabled, the dominant kernels are bracketed by CUDA events on the context's
+ * stream.  ipg_timing_read returns the summed milliseconds and launch count recorded
+ * under `kernel` ("snap_atom", "snap_contract", "snap_gather", "pair_eval",
+ * "neighbor") since the last read, and resets them. */
+IPG_API int ipg_timing_enable(ipg_ctx* ctx, int on);
+IPG_API int ipg_timing_read(ipg_ctx* ctx, const char* kernel, double* total_ms, int64_t* launches);
+
+/* ---- neighbor lists -------------------------------------------------------------------
+ * Replaces neighborlist(s, rcut) (src/nnlist.jl:23-46) and neighborlist(A, snap)
+ * (src/BasisSystems/SNAP/utilities/utl.jl:38-101).
+ *
+ * mode IPG_NLIST_HALF: pairs (i, j > i) whose Distances.PeriodicEuclidean distance is
+ *   <= cut[0]; r = x_i - x_j under minimum image (get_displacement, src/nnlist.jl:18-21).
+ * mode IPG_NLIST_FULL: pairs (i, j != i) with |r|^2 <= cut[s_i * nspecies + s_j] and
+ *   r = x_j - x_i (utl.jl:87-89); the candidate radius is sqrt(max cut) — or, with
+ *   IPG_NLIST_LITERAL_SQRT, the reference's literal sqrt(sqrt(max cut)) (utl.jl:81).
+ * Within each atom the neighbors are sorted by index (inrange(..., true), utl.jl:81). */
+#define IPG_NLIST_HALF 0
+#define IPG_NLIST_FULL 1
+#define IPG_NLIST_LITERAL_SQRT 0x100
+IPG_API int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
+                       int32_t nspecies, const double* cut, int32_t mode, ipg_nlist** out);
+IPG_API int ipg_nlist_size(const ipg_nlist* nl, int64_t* npairs);
+/* offsets [n+1], j [npairs] (0-based), r [3*npairs]; any may be NULL. */
+IPG_API int ipg_nlist_export(const ipg_nlist* nl, int64_t* offsets, int32_t* j, double* r);
+IPG_API int ipg_nlist_free(ipg_nlist* nl);
+
+/* ---- empirical pair potentials ---------------------------------------------------------
+ * One ipg_pair_term is one EmpiricalPotential; a list of terms with coefficients is a
+ * LinearCombinationPotential (src/mixed/linear_combination_potential.jl:7-39).  Each
+ * term keeps its own cutoff and species filter (src/types/empirical_potential.jl:26-43:
+ * a pair counts when BOTH species are in the term's set).
+ * params by kind (all atomic units):
+ *   IPG_PAIR_LJ      eps, sigma                   src/empirical/lj.jl:35-36
+ *   IPG_PAIR_BM      A, rho, sigma, C, D          src/empirical/bm.jl:38-39
+ *   IPG_PAIR_COUL    q1, q2                       src/empirical/coulomb.jl:36-37
+ *   IPG_PAIR_MORSE   D, alpha, sigma              src/empirical/morse.jl:36-39
+ *   IPG_PAIR_ZBL     Z1, Z2, e                    src/empirical/zbl.jl:27-36
+ *   IPG_PAIR_MOCK_R2 seed  (E = seed R^2, f = seed R^2 r; test/mocks.jl:22-34)            */
+#define IPG_PAIR_LJ 1
+#define IPG_PAIR_BM 2
+#define IPG_PAIR_COUL 3
+#define IPG_PAIR_MORSE 4
+#define IPG_PAIR_ZBL 5
+#define IPG_PAIR_MOCK_R2 6
+#define IPG_MAX_PAIR_TERMS 16
+typedef struct ipg_pair_term {
+  int32_t kind;
+  int32_t reserved;
+  double coeff;          /* linear-combination coefficient                           */
+  double rcut;           /* get_rcutoff(p)                                           */
+  uint64_t species_mask; /* bit s set <=> species s in get_species(p); ~0 = missing  */
+  double params[8];
+} ipg_pair_term;
+
+/* What to compute (bit flags). */
+#define IPG_WANT_E 1u
+#define IPG_WANT_F 2u
+#define IPG_WANT_W 4u
+
+/* energy_and_force / potential_energy / force / virial_stress for an EmpiricalPotential
+ * or a LinearCombinationPotential (empirical_potential.jl:49-77,
+ * linear_combination_potential.jl:27-39).  E [1], F [3n], W6 [6] = [xx,yy,zz,zy,zx,yx]
+ * (empirical_potential.jl:63-64); outputs not selected by `flags` may be NULL. */
+IPG_API int ipg_pair_eval(ipg_ctx* ctx, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                  const ipg_pair_term* terms, int32_t nterms, double* E, double* F, double* W6, uint32_t flags);
+IPG_API int ipg_pair_eval_dev(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
+                      const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
+                      uint32_t flags);
+
+/* ---- SNAP -------------------------------------------------------------------------------
+ * ipg_snap_params mirrors SNAP{S,T} (src/BasisSystems/SNAP/types/types.jl:8-25).
+ * chem_flag is not built (IPG_ERR_UNSUPPORTED).  wselfall_flag has no effect without
+ * chem_flag (compute_ui.jl:142, compute_b.jl:134-155 with one element).               */
+#define IPG_MAX_SNAP_SPECIES 8
+typedef struct ipg_snap_params {
+  int32_t twojmax;
+  int32_t nspecies;
+  double rcutfac;
+  double rmin0;
+  double rfac0;
+  double radii[IPG_MAX_SNAP_SPECIES];
+  double weight[IPG_MAX_SNAP_SPECIES];
+  int32_t chem_flag;
+  int32_t bzero_flag;
+  int32_t bnorm_flag;
+  int32_t switch_flag;
+  int32_t wselfall_flag;
+  int32_t literal_sqrt_radius; /* reproduce utl.jl:81's sqrt(cutmax) search radius */
+} ipg_snap_params;
+
+/* Builds the prebuilt tables of initialize_prebuilt_arrays (prebuilt_arrays.jl:48-247)
+ * and uploads them.  The ctx must outlive the handle. */
+IPG_API int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out);
+IPG_API int ipg_snap_destroy(ipg_snap* snap);
+/* K = length(snap) = get_num_snap_coeffs (utl.jl:8-25). */
+IPG_API int ipg_snap_ncoeff(const ipg_snap* snap, int32_t* K);
+
+/* compute_local_descriptors / compute_force_descriptors / compute_all_descriptors
+ * (src/BasisSystems/SNAP/snap.jl:103-124, 126-167, 226-285; the force descriptors follow
+ * compute_all_descriptors' row indexing, snap.jl:261).
+ *   B  [n][K]
+ *   dB [n][K*nspecies][3]   (each atom's 3 x (K*nspecies) matrix, column-major)
+ *   W  [K*nspecies][6]      (6 x (K*nspecies), column-major; absolute positions as in
+ *                            snap.jl:267-281)                                          */
+#define IPG_DESC_B 1u
+#define IPG_DESC_DB 2u
+#define IPG_DESC_W 4u
+IPG_API int ipg_snap_descriptors(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                         double* B, double* dB, double* W, uint32_t what);
+
+/* potential_energy / force / energy_and_force / virial_stress of LBasisPotential over
+ * SNAP (src/BasisPotentials/basis_potentials.jl:14-57, linear_potential.jl:20-49):
+ *   E = beta0 + sum_i beta[s_i] . B_i,  F_k = sum_blocks dB_k[:, block] . beta[block],
+ *   W6 = W . beta.
+ * beta is [nspecies][K] (one block per centre species; the reference's single K-vector
+ * is every block equal).  mode IPG_SNAP_PLAIN materialises every per-neighbor dB/dr
+ * and contracts it; IPG_SNAP_ADJOINT accumulates Y = d(beta.B)/dU per atom and
+ * contracts dU/dr with Y per neighbor (design of compute_yi.jl / compute_dij.jl).     */
+#define IPG_SNAP_PLAIN 0
+#define IPG_SNAP_ADJOINT 1
+IPG_API int ipg_snap_energy_forces(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                           const double* beta, double beta0, int32_t mode, double* E, double* F, double* W6);
+IPG_API int ipg_snap_energy_forces_dev(ipg_snap* snap, int64_t n, const double* d_pos, const int32_t* d_species,
+                               const double L[3], const double* beta, double beta0, int32_t mode, double* d_E,
+                               double* d_F, double* d_W6);
+
+/* Vector-Jacobian product of (E, F) with respect to beta (the pullback of the
+ * ChainRulesCore.rrule for potential_energy / force):
+ *   gbeta[s][k] = gE * sum_{i: s_i=s} B_i[k] + sum_atoms gF_atom . dB_atom[:, block s][k],
+ *   gbeta0 = gE.  gF [3n] may be NULL (energy-only pullback).                          */
+IPG_API int ipg_snap_vjp_beta(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                      double gE, const double* gF, double* gbeta, double* gbeta0);
+
+/* ---- batched SNAP ------------------------------------------------------------------------
+ * Many configurations at once: atoms of configuration c are atom_offsets[c] ..
+ * atom_offsets[c+1]-1 of the flattened arrays; L is [nconfig][3].  Per-configuration
+ * energies E [nconfig] (each with beta0) and virials W6 [nconfig][6]; forces [3 n_total].
+ * With graph != 0 the whole evaluation is captured once into a CUDA graph per shape and
+ * replayed on later calls with the same atom counts.                                    */
+IPG_API int ipg_snap_batch_energy_forces(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
+                                 const int32_t* species, const double* L, const double* beta, double beta0,
+                                 int32_t mode, double* E, double* F, double* W6);
+IPG_API int ipg_snap_batch_energy_forces_dev(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets,
+                                     const double* d_pos, const int32_t* d_species, const double* L,
+                                     const double* beta, double beta0, int32_t mode, int32_t graph, double* d_E,
+                                     double* d_F, double* d_W6);
+/* Force-matching loss over a batch, L = sum_atoms |F - F_ref|^2, with its gradient with
+ * respect to beta [nspecies][K] (gradient of beta0 is 0).  F_ref [3 n_total].         */
+IPG_API int ipg_snap_batch_loss_grad(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
+                             const int32_t* species, const double* L, const double* beta, double beta0,
+                             const double* F_ref, double* loss, double* gbeta);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IPG_H */

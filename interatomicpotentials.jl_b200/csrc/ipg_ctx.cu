@@ -1,0 +1,278 @@
+// ipg_ctx.cu — context lifetime, error reporting, device scratch, status word, scan.
+#include <cstdarg>
+
+#include "ipg_internal.cuh"
+
+int ipg_fail(ipg_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return code;
+}
+
+int ipg_cuda_check(ipg_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return IPG_OK;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return ipg_fail(ctx, IPG_ERR_NOMEM, "%s: %s", what, cudaGetErrorString(e));
+  }
+  return ipg_fail(ctx, IPG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int ipg_scratch(ipg_ctx* ctx, const char* name, size_t bytes, void** out) {
+  DevBuf& b = ctx->bufs[name];
+  if (b.cap < bytes) {
+    if (b.p) {
+      // The stream may still use the old buffer.
+      CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+      CUDA_RET(ctx, cudaFree(b.p));
+      b.p = nullptr;
+      b.cap = 0;
+    }
+    size_t cap = bytes + bytes / 8 + 256;
+    cudaError_t e = cudaMalloc(&b.p, cap);
+    if (e != cudaSuccess) {
+      b.p = nullptr;
+      cudaGetLastError();
+      return ipg_fail(ctx, IPG_ERR_NOMEM, "device allocation of %zu bytes for '%s' failed", cap, name);
+    }
+    b.cap = cap;
+  }
+  *out = b.p;
+  return IPG_OK;
+}
+
+int ipg_status_reset(ipg_ctx* ctx) {
+  CUDA_RET(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+  return IPG_OK;
+}
+
+int ipg_sync(ipg_ctx* ctx) {
+  CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  return IPG_OK;
+}
+
+int ipg_status_check(ipg_ctx* ctx, const char* what) {
+  CUDA_RET(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  int st = *ctx->h_status;
+  if (st == IPG_ERR_CAPACITY) return ipg_fail(ctx, st, "%s: device capacity exceeded", what);
+  if (st == IPG_ERR_TIMEOUT) return ipg_fail(ctx, st, "%s: bounded device wait timed out", what);
+  if (st == IPG_ERR_NONFINITE) return ipg_fail(ctx, st, "%s: non-finite position", what);
+  if (st == IPG_ERR_SPECIES) return ipg_fail(ctx, st, "%s: species id out of range", what);
+  if (st != IPG_OK) return ipg_fail(ctx, st, "%s: device status %d", what, st);
+  return IPG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Kernel timing: event pairs per kernel name, resolved when read.
+int ipg_timing_mark(ipg_ctx* ctx, const char* name, bool start) {
+  if (!ctx->timing) return IPG_OK;
+  cudaEvent_t e;
+  if (!ctx->event_pool.empty()) {
+    e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+  } else {
+    CUDA_RET(ctx, cudaEventCreate(&e));
+  }
+  CUDA_RET(ctx, cudaEventRecord(e, ctx->stream));
+  auto& t = ctx->timed[name];
+  t.ev.push_back(e);
+  if (!start) t.launches++;
+  return IPG_OK;
+}
+
+static int timing_resolve(ipg_ctx* ctx) {
+  for (auto& kv : ctx->timed) {
+    auto& t = kv.second;
+    for (size_t q = 0; q + 1 < t.ev.size(); q += 2) {
+      CUDA_RET(ctx, cudaEventSynchronize(t.ev[q + 1]));
+      float ms = 0.f;
+      CUDA_RET(ctx, cudaEventElapsedTime(&ms, t.ev[q], t.ev[q + 1]));
+      t.ms += ms;
+      ctx->event_pool.push_back(t.ev[q]);
+      ctx->event_pool.push_back(t.ev[q + 1]);
+    }
+    t.ev.clear();
+  }
+  return IPG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Exclusive scan, three phases: per-block scan (2048 items per block), scan of block
+// sums (recursive), add block offsets.
+namespace {
+constexpr int SCAN_T = 512;
+constexpr int SCAN_PER = 4;
+constexpr int SCAN_BLOCK = SCAN_T * SCAN_PER;
+
+__global__ void k_scan_block(const int64_t* __restrict__ in, int64_t* __restrict__ out, int64_t n,
+                             int64_t* __restrict__ bsum) {
+  __shared__ int64_t wsum[SCAN_T / 32];
+  int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK + (int64_t)threadIdx.x * SCAN_PER;
+  int64_t v[SCAN_PER];
+  int64_t run = 0;
+#pragma unroll
+  for (int q = 0; q < SCAN_PER; q++) {
+    int64_t idx = base + q;
+    int64_t x = idx < n ? in[idx] : 0;
+    v[q] = run;
+    run += x;
+  }
+  // inclusive warp scan of per-thread totals
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int64_t incl = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int64_t s = lane < SCAN_T / 32 ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t t = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += t;
+    }
+    if (lane < SCAN_T / 32) wsum[lane] = s;
+  }
+  __syncthreads();
+  int64_t excl = incl - run + (w > 0 ? wsum[w - 1] : 0);
+#pragma unroll
+  for (int q = 0; q < SCAN_PER; q++) {
+    int64_t idx = base + q;
+    if (idx < n) out[idx] = excl + v[q];
+  }
+  if (threadIdx.x == SCAN_T - 1) bsum[blockIdx.x] = excl + run;
+}
+
+__global__ void k_scan_add(int64_t* __restrict__ out, int64_t n, const int64_t* __restrict__ boff) {
+  int64_t idx = (int64_t)blockIdx.x * SCAN_BLOCK + threadIdx.x;
+  int64_t add = boff[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < SCAN_PER; q++, idx += SCAN_T)
+    if (idx < n) out[idx] += add;
+}
+}  // namespace
+
+static int scan_level(ipg_ctx* ctx, const int64_t* in, int64_t* out, int64_t n, int depth) {
+  int64_t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  if (nb < 1) nb = 1;
+  char name[32];
+  snprintf(name, sizeof(name), "scan_bsum%d", depth);
+  int64_t* bsum;
+  IPG_RET(scratch(ctx, name, (size_t)nb + 1, &bsum));
+  IPG_LAUNCH(ctx, k_scan_block, (unsigned)nb, SCAN_T, 0, in, out, n, bsum);
+  if (nb > 1) {
+    IPG_RET(scan_level(ctx, bsum, bsum, nb, depth + 1));
+    IPG_LAUNCH(ctx, k_scan_add, (unsigned)nb, SCAN_T, 0, out, n, bsum);
+  }
+  return IPG_OK;
+}
+
+int ipg_scan_i64(ipg_ctx* ctx, const int64_t* in, int64_t* out, int64_t n_plus_1) {
+  if (n_plus_1 <= 0) return IPG_OK;
+  return scan_level(ctx, in, out, n_plus_1, 0);
+}
+
+// ---------------------------------------------------------------------------------
+extern "C" {
+
+int ipg_version(void) { return 100; }
+
+int ipg_create(int device, ipg_ctx** out) {
+  if (!out) return IPG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return IPG_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return IPG_ERR_ARG;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return IPG_ERR_CUDA;
+  if (prop.major != 10) return IPG_ERR_NODEVICE;  // built for sm_100a only
+  ipg_ctx* ctx = new ipg_ctx();
+  ctx->device = device;
+  ctx->num_sms = prop.multiProcessorCount;
+  int dev0 = 0;
+  cudaGetDevice(&dev0);
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_status, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return IPG_ERR_CUDA;
+  }
+  ctx->stream = ctx->own_stream;
+  cudaMemset(ctx->d_status, 0, sizeof(int));
+  cudaDeviceSynchronize();
+  *out = ctx;
+  return IPG_OK;
+}
+
+int ipg_destroy(ipg_ctx* ctx) {
+  if (!ctx) return IPG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->bufs)
+    if (kv.second.p) cudaFree(kv.second.p);
+  for (auto& kv : ctx->timed)
+    for (cudaEvent_t e : kv.second.ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return IPG_OK;
+}
+
+const char* ipg_last_error(const ipg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int ipg_set_timeout_ms(ipg_ctx* ctx, uint32_t ms) {
+  if (!ctx || ms == 0) return IPG_ERR_ARG;
+  ctx->timeout_ms = ms;
+  return IPG_OK;
+}
+
+int ipg_set_stream(ipg_ctx* ctx, void* stream) {
+  if (!ctx) return IPG_ERR_ARG;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return IPG_OK;
+}
+
+int ipg_timing_enable(ipg_ctx* ctx, int on) {
+  if (!ctx) return IPG_ERR_ARG;
+  if (!on) IPG_RET(timing_resolve(ctx));
+  ctx->timing = on != 0;
+  return IPG_OK;
+}
+
+int ipg_timing_read(ipg_ctx* ctx, const char* kernel, double* total_ms, int64_t* launches) {
+  if (!ctx || !kernel) return IPG_ERR_ARG;
+  IPG_RET(timing_resolve(ctx));
+  auto it = ctx->timed.find(kernel);
+  if (total_ms) *total_ms = it == ctx->timed.end() ? 0.0 : it->second.ms;
+  if (launches) *launches = it == ctx->timed.end() ? 0 : it->second.launches;
+  if (it != ctx->timed.end()) {
+    it->second.ms = 0.0;
+    it->second.launches = 0;
+  }
+  return IPG_OK;
+}
+
+int ipg_launch_count(const ipg_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return IPG_ERR_ARG;
+  *out = ctx->launches;
+  return IPG_OK;
+}
+
+}  // extern "C"

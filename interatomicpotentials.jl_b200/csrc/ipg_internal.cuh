@@ -1,0 +1,217 @@
+// ipg_internal.cuh — shared definitions of the libipg CUDA sources (sm_100a, FP64).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "ipg.h"
+
+// ----------------------------------------------------------------------------------
+// Context: one CUDA stream, named growable device scratch buffers, a device status
+// word that kernels raise instead of trapping, and the last error message.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct ipg_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  uint32_t timeout_ms = 2000;
+  int64_t launches = 0;
+  int* d_status = nullptr;  // device status word (IPG_OK or a negative code)
+  int* h_status = nullptr;  // pinned mirror
+  std::map<std::string, DevBuf> bufs;
+  std::map<std::string, std::vector<char>> hbufs;
+  // optional per-kernel device timing (ipg_timing_enable / ipg_timing_read)
+  bool timing = false;
+  struct Timed {
+    std::vector<cudaEvent_t> ev;  // start/stop pairs
+    double ms = 0.0;
+    int64_t launches = 0;
+  };
+  std::map<std::string, Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+// Records a start/stop event pair around a launch when timing is enabled.
+int ipg_timing_mark(ipg_ctx* ctx, const char* name, bool start);
+
+// Status propagation: every internal function returns int.
+#define IPG_RET(x)            \
+  do {                        \
+    int _st = (x);            \
+    if (_st != IPG_OK) return _st; \
+  } while (0)
+
+int ipg_fail(ipg_ctx* ctx, int code, const char* fmt, ...);
+int ipg_cuda_check(ipg_ctx* ctx, cudaError_t e, const char* what);
+
+#define CUDA_RET(ctx, call) IPG_RET(ipg_cuda_check((ctx), (call), #call))
+
+// Named device scratch: grows (never shrinks) to at least `bytes`.
+int ipg_scratch(ipg_ctx* ctx, const char* name, size_t bytes, void** out);
+template <class T>
+int scratch(ipg_ctx* ctx, const char* name, size_t count, T** out) {
+  void* p = nullptr;
+  IPG_RET(ipg_scratch(ctx, name, count * sizeof(T) + 16, &p));
+  *out = static_cast<T*>(p);
+  return IPG_OK;
+}
+// Named pinned host staging buffer.
+template <class T>
+T* host_scratch(ipg_ctx* ctx, const char* name, size_t count) {
+  auto& v = ctx->hbufs[name];
+  if (v.size() < count * sizeof(T)) v.resize(count * sizeof(T));
+  return reinterpret_cast<T*>(v.data());
+}
+
+// Kernel launch with accounting and error check.
+#define IPG_LAUNCH(ctx, kernel, grid, block, smem, ...)                                          \
+  do {                                                                                           \
+    kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                             \
+    (ctx)->launches++;                                                                           \
+    IPG_RET(ipg_cuda_check((ctx), cudaGetLastError(), #kernel));                                 \
+  } while (0)
+
+// As IPG_LAUNCH, bracketed by timing events named `name` when timing is enabled.
+#define IPG_TIMED_LAUNCH(ctx, name, kernel, grid, block, smem, ...) \
+  do {                                                             \
+    IPG_RET(ipg_timing_mark((ctx), (name), true));                 \
+    IPG_LAUNCH(ctx, kernel, grid, block, smem, __VA_ARGS__);       \
+    IPG_RET(ipg_timing_mark((ctx), (name), false));                \
+  } while (0)
+
+// Resets the device status word (async) and reads it back after a sync.
+int ipg_status_reset(ipg_ctx* ctx);
+int ipg_status_check(ipg_ctx* ctx, const char* what);
+int ipg_sync(ipg_ctx* ctx);
+
+// Exclusive scan of n+1 int64 values (in[n] must be 0): out[k] = sum_{q<k} in[q];
+// out[n] is the total.  `out` may alias `in`.
+int ipg_scan_i64(ipg_ctx* ctx, const int64_t* in, int64_t* out, int64_t n_plus_1);
+
+// Sets device status to `code` (first error wins).
+__device__ __forceinline__ void dev_raise(int* status, int code) { atomicCAS(status, 0, code); }
+
+// ----------------------------------------------------------------------------------
+// Minimum-image arithmetic of the reference, reproduced bit for bit (no FMA contraction).
+// Julia mod(x, y) for y > 0 finite (the sign of the result follows y).
+__device__ __forceinline__ double jl_mod_dev(double x, double L) {
+  double r = (x >= 0.0 && x < L) ? x : fmod(x, L);
+  if (r == 0.0) return 0.0;
+  if (r < 0.0) r = __dadd_rn(r, L);
+  return r;
+}
+// src/nnlist.jl:18-21 get_displacement (one axis); L = +inf marks an open axis.
+__device__ __forceinline__ double disp_axis_dev(double L, double x, double y) {
+  double dx = __dsub_rn(x, y);
+  if (isinf(L)) return dx;
+  double d = jl_mod_dev(dx, L);
+  return (__dmul_rn(2.0, d) < L) ? d : __dsub_rn(d, L);
+}
+// Distances.jl PeriodicEuclidean, one axis: min(mod(|a-b|, L), L - mod(|a-b|, L)).
+__device__ __forceinline__ double pe_axis_dev(double L, double a, double b) {
+  double s1 = fabs(__dsub_rn(a, b));
+  if (isinf(L)) return s1;
+  double s2 = (s1 < L) ? s1 : fmod(s1, L);
+  double s3 = __dsub_rn(L, s2);
+  return s2 < s3 ? s2 : s3;
+}
+__device__ __forceinline__ double sumsq3_dev(double a, double b, double c) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
+}
+
+// ----------------------------------------------------------------------------------
+// Cell lists (ipg_nlist.cu).  Configurations are independent boxes; atoms of config c are
+// [atom_off[c], atom_off[c+1]).  Each configuration owns its own cell grid.
+struct ConfGrid {
+  double L[3];   // box diagonal, +inf on open axes
+  double lo[3];  // grid origin
+  double cs[3];  // cell edge (>= search radius on every axis with more than one cell)
+  int nc[3];     // cells per axis
+  int pad;
+  int64_t cell_off;  // first global cell id of this configuration
+  int64_t atom_off;
+  int64_t natoms;
+};
+
+struct CellList {
+  int nconf = 0;
+  int64_t n = 0;
+  int64_t ncells = 0;
+  double radius = 0.0;
+  ConfGrid* d_grid = nullptr;      // [nconf]
+  std::vector<ConfGrid> h_grid;    // host copy
+  int32_t* d_conf = nullptr;       // [n] configuration of each atom
+  int64_t* d_cell_start = nullptr; // [ncells+1]
+  int32_t* d_cell_atoms = nullptr; // [n] atom ids in cell order (ascending inside a cell)
+  int32_t* d_slot_of = nullptr;    // [n] slot of each atom
+  double4* d_spos = nullptr;       // [n] positions in slot order (w = species as double)
+};
+
+// Builds the cell list for `radius` (prefix selects the scratch buffers used).
+int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d_pos, const int32_t* d_species,
+                    int nconf, const int64_t* h_atom_off, const double* h_L, double radius, CellList& cl);
+
+// Materialised pair list in CSR form over atoms (original order), neighbors ascending.
+struct PairList {
+  int64_t n = 0;
+  int64_t npairs = 0;
+  int64_t* d_off = nullptr;  // [n+1]
+  int32_t* d_j = nullptr;    // [npairs]
+  double* d_r = nullptr;     // [npairs][3]
+  int64_t* d_in_off = nullptr;  // [n+1]   transpose: pairs whose neighbor is atom k
+  int64_t* d_in_pair = nullptr; // [npairs]
+};
+
+// mode: IPG_NLIST_HALF (cut[0] = rcut) or IPG_NLIST_FULL (cut = nsp*nsp cutsq), with
+// IPG_NLIST_LITERAL_SQRT optionally or-ed in.  want_transpose builds d_in_off/d_in_pair.
+int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl);
+
+// Device helper: the distinct neighbor-cell coordinates along one axis (<= 3).
+__device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {
+  int cnt = 0;
+  for (int d = -1; d <= 1; d++) {
+    int k = c + d;
+    if (per) {
+      k = (k % nc + nc) % nc;
+    } else if (k < 0 || k >= nc) {
+      continue;
+    }
+    bool dup = false;
+    for (int q = 0; q < cnt; q++) dup |= (out[q] == k);
+    if (!dup) out[cnt++] = k;
+  }
+  return cnt;
+}
+__device__ __forceinline__ void cell_coords(const ConfGrid& g, double x, double y, double z, int* c) {
+  double p[3] = {x, y, z};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    double w = isinf(g.L[a]) ? p[a] - g.lo[a] : p[a] - g.L[a] * floor(p[a] / g.L[a]);
+    int k = (int)floor(w / g.cs[a]);
+    k = k < 0 ? 0 : k;
+    k = k > g.nc[a] - 1 ? g.nc[a] - 1 : k;
+    c[a] = k;
+  }
+}
+
+// ----------------------------------------------------------------------------------
+// Small device reductions.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}

@@ -1,0 +1,489 @@
+// ipg_nlist.cu — cell-list neighbor build (replaces the BallTree + PeriodicEuclidean
+// search of src/nnlist.jl:23-46 and src/BasisSystems/SNAP/utilities/utl.jl:38-101).
+//
+// Pipeline (all on the context's stream):
+//   k_extent       per-configuration min/max of open axes (only when an axis is open)
+//   k_cell_count   cell id per atom + histogram
+//   scan           cell_start
+//   k_cell_fill    scatter atom ids into their cells
+//   k_cell_sort    sort each cell ascending (deterministic slot order), slot_of, spos
+// and, for a materialised list:
+//   k_pair_count / scan / k_pair_emit / k_pair_sort, optionally the transpose.
+// Membership is decided per candidate with the reference's own arithmetic
+// (PeriodicEuclidean distance, get_displacement), so any cell edge >= the search radius
+// proposes every pair exactly once.
+#include <algorithm>
+
+#include "ipg_internal.cuh"
+
+namespace {
+
+__global__ void k_extent(const double* __restrict__ pos, const ConfGrid* __restrict__ grid, double* __restrict__ ext) {
+  // one block per configuration; ext[c*6 + a] = min, ext[c*6 + 3 + a] = max
+  const ConfGrid g = grid[blockIdx.x];
+  __shared__ double smin[3][32], smax[3][32];
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = threadIdx.x; i < g.natoms; i += blockDim.x) {
+    const double* p = pos + 3 * (g.atom_off + i);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      mn[a] = fmin(mn[a], p[a]);
+      mx[a] = fmax(mx[a], p[a]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[a] = fmin(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+      mx[a] = fmax(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+    }
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int a = 0; a < 3; a++) {
+      smin[a][w] = mn[a];
+      smax[a][w] = mx[a];
+    }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    int a = threadIdx.x;
+    double m = INFINITY, M = -INFINITY;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
+      m = fmin(m, smin[a][q]);
+      M = fmax(M, smax[a][q]);
+    }
+    ext[blockIdx.x * 6 + a] = m;
+    ext[blockIdx.x * 6 + 3 + a] = M;
+  }
+}
+
+__global__ void k_cell_count(int64_t n, const double* __restrict__ pos, const int32_t* __restrict__ species, int nsp,
+                             const ConfGrid* __restrict__ grid, int nconf, int32_t* __restrict__ conf,
+                             int32_t* __restrict__ cell_of, int64_t* __restrict__ count, int* status) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // configuration by binary search over atom offsets
+  int lo = 0, hi = nconf - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (grid[mid].atom_off <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const ConfGrid& g = grid[lo];
+  double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+    dev_raise(status, IPG_ERR_NONFINITE);
+    x = y = z = 0.0;
+  }
+  if (species && (species[i] < 0 || species[i] >= nsp)) dev_raise(status, IPG_ERR_SPECIES);
+  int c[3];
+  cell_coords(g, x, y, z, c);
+  int64_t cell = g.cell_off + ((int64_t)c[2] * g.nc[1] + c[1]) * g.nc[0] + c[0];
+  conf[i] = lo;
+  cell_of[i] = (int32_t)cell;
+  atomicAdd((unsigned long long*)&count[cell], 1ull);
+}
+
+__global__ void k_cell_fill(int64_t n, const int32_t* __restrict__ cell_of, const int64_t* __restrict__ cell_start,
+                            int64_t* __restrict__ fill, int32_t* __restrict__ cell_atoms) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t c = cell_of[i];
+  unsigned long long q = atomicAdd((unsigned long long*)&fill[c], 1ull);
+  cell_atoms[cell_start[c] + (int64_t)q] = (int32_t)i;
+}
+
+__global__ void k_cell_sort(int64_t ncells, const int64_t* __restrict__ cell_start, int32_t* __restrict__ cell_atoms) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  int64_t s = cell_start[c], e = cell_start[c + 1];
+  for (int64_t a = s + 1; a < e; a++) {
+    int32_t v = cell_atoms[a];
+    int64_t b = a - 1;
+    while (b >= s && cell_atoms[b] > v) {
+      cell_atoms[b + 1] = cell_atoms[b];
+      b--;
+    }
+    cell_atoms[b + 1] = v;
+  }
+}
+
+__global__ void k_cell_gather(int64_t n, const int32_t* __restrict__ cell_atoms, const double* __restrict__ pos,
+                              const int32_t* __restrict__ species, int32_t* __restrict__ slot_of,
+                              double4* __restrict__ spos) {
+  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int32_t i = cell_atoms[s];
+  slot_of[i] = (int32_t)s;
+  spos[s] = make_double4(pos[3 * (int64_t)i], pos[3 * (int64_t)i + 1], pos[3 * (int64_t)i + 2],
+                         species ? (double)species[i] : 0.0);
+}
+
+// ---------------------------------------------------------------------------------
+// Pair tests.  HALF: nnlist.jl:39-44.  FULL: utl.jl:81-93.
+struct PairTest {
+  int mode;          // IPG_NLIST_HALF / IPG_NLIST_FULL
+  int literal;       // utl.jl:81 literal search radius
+  int nsp;
+  double rcut;       // HALF: cutoff; FULL: candidate radius (cutmax or sqrt(cutmax))
+  double cutsq[64];  // FULL: [nsp][nsp], nsp <= 8
+};
+
+// Returns true when (i, j) belongs to the list; r receives the stored displacement.
+__device__ __forceinline__ bool pair_ok(const PairTest& t, const double* L, int32_t i, double4 xi, int32_t j,
+                                        double4 xj, double* r) {
+  if (t.mode == IPG_NLIST_HALF) {
+    if (j <= i) return false;
+  } else if (j == i) {
+    return false;
+  }
+  double s0 = pe_axis_dev(L[0], xi.x, xj.x);
+  double s1 = pe_axis_dev(L[1], xi.y, xj.y);
+  double s2 = pe_axis_dev(L[2], xi.z, xj.z);
+  if (sqrt(sumsq3_dev(s0, s1, s2)) > t.rcut) return false;
+  r[0] = disp_axis_dev(L[0], xi.x, xj.x);
+  r[1] = disp_axis_dev(L[1], xi.y, xj.y);
+  r[2] = disp_axis_dev(L[2], xi.z, xj.z);
+  if (t.mode == IPG_NLIST_HALF) return true;
+  r[0] = -r[0];
+  r[1] = -r[1];
+  r[2] = -r[2];
+  double rsq = sumsq3_dev(r[0], r[1], r[2]);
+  return rsq <= t.cutsq[(int)xi.w * t.nsp + (int)xj.w];
+}
+
+template <bool EMIT>
+__global__ void k_pair_walk(int64_t n, PairTest t, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ conf,
+                            const int64_t* __restrict__ cell_start, const int32_t* __restrict__ cell_atoms,
+                            const double4* __restrict__ spos, int64_t* __restrict__ cnt,
+                            const int64_t* __restrict__ off, int32_t* __restrict__ outj, double* __restrict__ outr) {
+  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int32_t i = cell_atoms[s];
+  double4 xi = spos[s];
+  const ConfGrid g = grid[conf[i]];
+  int c[3];
+  cell_coords(g, xi.x, xi.y, xi.z, c);
+  int sx[3], sy[3], sz[3];
+  int nx = stencil_axis(c[0], g.nc[0], !isinf(g.L[0]), sx);
+  int ny = stencil_axis(c[1], g.nc[1], !isinf(g.L[1]), sy);
+  int nz = stencil_axis(c[2], g.nc[2], !isinf(g.L[2]), sz);
+  int64_t k = 0, base = EMIT ? off[i] : 0;
+  for (int a = 0; a < nz; a++)
+    for (int b = 0; b < ny; b++)
+      for (int d = 0; d < nx; d++) {
+        int64_t cell = g.cell_off + ((int64_t)sz[a] * g.nc[1] + sy[b]) * g.nc[0] + sx[d];
+        int64_t e = cell_start[cell + 1];
+        for (int64_t q = cell_start[cell]; q < e; q++) {
+          int32_t j = cell_atoms[q];
+          double r[3];
+          if (pair_ok(t, g.L, i, xi, j, spos[q], r)) {
+            if (EMIT) {
+              outj[base + k] = j;
+              outr[3 * (base + k)] = r[0];
+              outr[3 * (base + k) + 1] = r[1];
+              outr[3 * (base + k) + 2] = r[2];
+            }
+            k++;
+          }
+        }
+      }
+  if (!EMIT) cnt[i] = k;
+}
+
+// Sorts each atom's list by neighbor index (insertion sort; lists are short).
+__global__ void k_pair_sort(int64_t n, const int64_t* __restrict__ off, int32_t* __restrict__ j,
+                            double* __restrict__ r) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t s = off[i], e = off[i + 1];
+  for (int64_t a = s + 1; a < e; a++) {
+    int32_t v = j[a];
+    double r0 = r[3 * a], r1 = r[3 * a + 1], r2 = r[3 * a + 2];
+    int64_t b = a - 1;
+    while (b >= s && j[b] > v) {
+      j[b + 1] = j[b];
+      r[3 * (b + 1)] = r[3 * b];
+      r[3 * (b + 1) + 1] = r[3 * b + 1];
+      r[3 * (b + 1) + 2] = r[3 * b + 2];
+      b--;
+    }
+    j[b + 1] = v;
+    r[3 * (b + 1)] = r0;
+    r[3 * (b + 1) + 1] = r1;
+    r[3 * (b + 1) + 2] = r2;
+  }
+}
+
+// Transpose: for every atom k, the pairs p whose neighbor is k, in ascending p.
+__global__ void k_in_count(int64_t np, const int32_t* __restrict__ j, int64_t* __restrict__ cnt) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  atomicAdd((unsigned long long*)&cnt[j[p]], 1ull);
+}
+__global__ void k_in_fill(int64_t np, const int32_t* __restrict__ j, const int64_t* __restrict__ in_off,
+                          int64_t* __restrict__ fill, int64_t* __restrict__ in_pair) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  int32_t k = j[p];
+  unsigned long long q = atomicAdd((unsigned long long*)&fill[k], 1ull);
+  in_pair[in_off[k] + (int64_t)q] = p;
+}
+__global__ void k_in_sort(int64_t n, const int64_t* __restrict__ in_off, int64_t* __restrict__ in_pair) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int64_t s = in_off[k], e = in_off[k + 1];
+  for (int64_t a = s + 1; a < e; a++) {
+    int64_t v = in_pair[a];
+    int64_t b = a - 1;
+    while (b >= s && in_pair[b] > v) {
+      in_pair[b + 1] = in_pair[b];
+      b--;
+    }
+    in_pair[b + 1] = v;
+  }
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+}  // namespace
+
+int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d_pos, const int32_t* d_species,
+                    int nconf, const int64_t* h_atom_off, const double* h_L, double radius, CellList& cl) {
+  std::string pre(prefix);
+  cl.nconf = nconf;
+  cl.n = n;
+  cl.radius = radius;
+  cl.h_grid.assign(nconf, ConfGrid());
+  bool any_open = false;
+  for (int c = 0; c < nconf; c++) {
+    ConfGrid& g = cl.h_grid[c];
+    g.atom_off = h_atom_off[c];
+    g.natoms = h_atom_off[c + 1] - h_atom_off[c];
+    for (int a = 0; a < 3; a++) {
+      double L = h_L[3 * c + a];
+      if (!(L > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "box length L[%d] of configuration %d must be > 0", a, c);
+      g.L[a] = std::isinf(L) ? INFINITY : L;
+      any_open |= std::isinf(L);
+    }
+  }
+  IPG_RET(scratch(ctx, (pre + "grid").c_str(), nconf, &cl.d_grid));
+  std::vector<double> ext(6 * (size_t)nconf, 0.0);
+  if (any_open && n > 0) {
+    CUDA_RET(ctx, cudaMemcpyAsync(cl.d_grid, cl.h_grid.data(), sizeof(ConfGrid) * nconf, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    double* d_ext;
+    IPG_RET(scratch(ctx, (pre + "ext").c_str(), 6 * (size_t)nconf, &d_ext));
+    IPG_LAUNCH(ctx, k_extent, nconf, 256, 0, d_pos, cl.d_grid, d_ext);
+    CUDA_RET(ctx, cudaMemcpyAsync(ext.data(), d_ext, sizeof(double) * 6 * nconf, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  const double rc = radius * (1.0 + 1e-9);
+  int64_t cell_total = 0;
+  for (int c = 0; c < nconf; c++) {
+    ConfGrid& g = cl.h_grid[c];
+    int64_t tot = 1;
+    double e3[3];
+    for (int a = 0; a < 3; a++) {
+      double lo = 0.0, e = g.L[a];
+      if (std::isinf(g.L[a])) {
+        lo = ext[6 * c + a];
+        e = ext[6 * c + 3 + a] - lo;
+        if (!(e >= 0.0) || !std::isfinite(e)) {  // empty config or non-finite input
+          lo = 0.0;
+          e = 0.0;
+        }
+      }
+      g.lo[a] = lo;
+      e3[a] = e;
+      int nc = 1;
+      if (rc > 0.0 && std::isfinite(rc) && e > 0.0) nc = (int)std::max(1.0, std::min(std::floor(e / rc), 1024.0));
+      g.nc[a] = nc;
+      tot *= nc;
+    }
+    while (tot > std::max<int64_t>(64, 8 * g.natoms)) {  // keep the grid proportional to the atoms
+      int a = (g.nc[0] >= g.nc[1] && g.nc[0] >= g.nc[2]) ? 0 : (g.nc[1] >= g.nc[2] ? 1 : 2);
+      tot /= g.nc[a];
+      g.nc[a] = std::max(1, g.nc[a] / 2);
+      tot *= g.nc[a];
+    }
+    for (int a = 0; a < 3; a++) g.cs[a] = e3[a] > 0.0 ? e3[a] / g.nc[a] : 1.0;
+    g.cell_off = cell_total;
+    cell_total += tot;
+  }
+  if (cell_total >= (int64_t)INT32_MAX) return ipg_fail(ctx, IPG_ERR_CAPACITY, "too many cells");
+  cl.ncells = cell_total;
+  CUDA_RET(ctx, cudaMemcpyAsync(cl.d_grid, cl.h_grid.data(), sizeof(ConfGrid) * nconf, cudaMemcpyHostToDevice,
+                                ctx->stream));
+  int64_t *count, *fill;
+  int32_t* cell_of;
+  IPG_RET(scratch(ctx, (pre + "conf").c_str(), n, &cl.d_conf));
+  IPG_RET(scratch(ctx, (pre + "cell_of").c_str(), n, &cell_of));
+  IPG_RET(scratch(ctx, (pre + "cell_start").c_str(), cell_total + 1, &cl.d_cell_start));
+  IPG_RET(scratch(ctx, (pre + "cell_fill").c_str(), cell_total + 1, &fill));
+  IPG_RET(scratch(ctx, (pre + "cell_atoms").c_str(), n, &cl.d_cell_atoms));
+  IPG_RET(scratch(ctx, (pre + "slot_of").c_str(), n, &cl.d_slot_of));
+  IPG_RET(scratch(ctx, (pre + "spos").c_str(), n, &cl.d_spos));
+  count = cl.d_cell_start;
+  CUDA_RET(ctx, cudaMemsetAsync(count, 0, sizeof(int64_t) * (cell_total + 1), ctx->stream));
+  CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (cell_total + 1), ctx->stream));
+  if (n == 0) return IPG_OK;
+  IPG_LAUNCH(ctx, k_cell_count, nblk(n, 256), 256, 0, n, d_pos, d_species, 64, cl.d_grid, nconf, cl.d_conf, cell_of,
+             count, ctx->d_status);
+  IPG_RET(ipg_scan_i64(ctx, count, cl.d_cell_start, cell_total + 1));
+  IPG_LAUNCH(ctx, k_cell_fill, nblk(n, 256), 256, 0, n, cell_of, cl.d_cell_start, fill, cl.d_cell_atoms);
+  IPG_LAUNCH(ctx, k_cell_sort, nblk(cell_total, 128), 128, 0, cell_total, cl.d_cell_start, cl.d_cell_atoms);
+  IPG_LAUNCH(ctx, k_cell_gather, nblk(n, 256), 256, 0, n, cl.d_cell_atoms, d_pos, d_species, cl.d_slot_of, cl.d_spos);
+  return IPG_OK;
+}
+
+int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl) {
+  (void)d_species;
+  std::string pre(prefix);
+  PairTest t;
+  memset(&t, 0, sizeof(t));
+  t.mode = mode & 0xff;
+  t.literal = (mode & IPG_NLIST_LITERAL_SQRT) ? 1 : 0;
+  t.nsp = nsp;
+  if (t.mode == IPG_NLIST_HALF) {
+    t.rcut = h_cut[0];
+  } else {
+    if (nsp < 1 || nsp > 8) return ipg_fail(ctx, IPG_ERR_ARG, "nspecies must be in 1..8 for a full list");
+    double cutmax2 = 0.0;
+    for (int q = 0; q < nsp * nsp; q++) {
+      t.cutsq[q] = h_cut[q];
+      cutmax2 = std::max(cutmax2, h_cut[q]);
+    }
+    double cutmax = std::sqrt(cutmax2);
+    t.rcut = t.literal ? std::sqrt(cutmax) : cutmax;
+  }
+  int64_t n = cl.n;
+  pl.n = n;
+  int64_t* cnt;
+  IPG_RET(scratch(ctx, (pre + "off").c_str(), n + 1, &pl.d_off));
+  cnt = pl.d_off;
+  CUDA_RET(ctx, cudaMemsetAsync(cnt, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+  if (n > 0)
+    IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+               cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
+  IPG_RET(ipg_scan_i64(ctx, cnt, pl.d_off, n + 1));
+  CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  if (pl.npairs >= (int64_t)1 << 40) return ipg_fail(ctx, IPG_ERR_CAPACITY, "pair count overflow");
+  IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
+  IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
+  if (n > 0) {
+    IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+               cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
+    IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
+  }
+  if (want_transpose) {
+    int64_t* fill;
+    IPG_RET(scratch(ctx, (pre + "in_off").c_str(), n + 1, &pl.d_in_off));
+    IPG_RET(scratch(ctx, (pre + "in_fill").c_str(), n + 1, &fill));
+    IPG_RET(scratch(ctx, (pre + "in_pair").c_str(), pl.npairs + 1, &pl.d_in_pair));
+    CUDA_RET(ctx, cudaMemsetAsync(pl.d_in_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+    CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+    if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.npairs, pl.d_j, pl.d_in_off);
+    IPG_RET(ipg_scan_i64(ctx, pl.d_in_off, pl.d_in_off, n + 1));
+    if (pl.npairs > 0) {
+      IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.npairs, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
+      IPG_LAUNCH(ctx, k_in_sort, nblk(n, 128), 128, 0, n, pl.d_in_off, pl.d_in_pair);
+    }
+  }
+  return IPG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+struct ipg_nlist {
+  int64_t n = 0, npairs = 0;
+  std::vector<int64_t> off;
+  std::vector<int32_t> j;
+  std::vector<double> r;
+};
+
+extern "C" {
+
+int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
+                       int32_t nspecies, const double* cut, int32_t mode, ipg_nlist** out) {
+  if (!ctx || !out || n < 0 || (n > 0 && !pos) || !L || !cut) return IPG_ERR_ARG;
+  if (n >= INT32_MAX) return ipg_fail(ctx, IPG_ERR_ARG, "n too large");
+  int base = mode & 0xff;
+  if (base != IPG_NLIST_HALF && base != IPG_NLIST_FULL) return ipg_fail(ctx, IPG_ERR_ARG, "bad mode");
+  if (base == IPG_NLIST_FULL && !species) return ipg_fail(ctx, IPG_ERR_ARG, "full list needs species");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  for (int64_t k = 0; k < 3 * n; k++)
+    if (!std::isfinite(pos[k])) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite position");
+  if (species)
+    for (int64_t k = 0; k < n; k++)
+      if (species[k] < 0 || species[k] >= std::max(1, (int)nspecies))
+        return ipg_fail(ctx, IPG_ERR_SPECIES, "species id out of range");
+  double *d_pos;
+  int32_t* d_sp = nullptr;
+  IPG_RET(scratch(ctx, "nl_in_pos", 3 * (size_t)n + 3, &d_pos));
+  if (n) CUDA_RET(ctx, cudaMemcpyAsync(d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  if (species) {
+    IPG_RET(scratch(ctx, "nl_in_sp", (size_t)n + 1, &d_sp));
+    if (n) CUDA_RET(ctx, cudaMemcpyAsync(d_sp, species, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  IPG_RET(ipg_status_reset(ctx));
+  int64_t aoff[2] = {0, n};
+  double radius;
+  if (base == IPG_NLIST_HALF) {
+    radius = cut[0];
+  } else {
+    double m = 0.0;
+    for (int q = 0; q < nspecies * nspecies; q++) m = std::max(m, cut[q]);
+    radius = std::sqrt(m);
+    if (mode & IPG_NLIST_LITERAL_SQRT) radius = std::sqrt(radius);
+  }
+  if (!(radius >= 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "cutoff must be >= 0");
+  CellList cl;
+  IPG_RET(ipg_build_cells(ctx, "nl_", n, d_pos, d_sp, 1, aoff, L, radius, cl));
+  PairList pl;
+  IPG_RET(ipg_build_pairs(ctx, "nl_", cl, d_sp, std::max(1, (int)nspecies), cut, mode, false, pl));
+  IPG_RET(ipg_status_check(ctx, "ipg_neighbor_build"));
+  ipg_nlist* nl = new ipg_nlist();
+  nl->n = n;
+  nl->npairs = pl.npairs;
+  nl->off.resize(n + 1);
+  nl->j.resize(pl.npairs);
+  nl->r.resize(3 * pl.npairs);
+  CUDA_RET(ctx, cudaMemcpyAsync(nl->off.data(), pl.d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  if (pl.npairs) {
+    CUDA_RET(ctx, cudaMemcpyAsync(nl->j.data(), pl.d_j, sizeof(int32_t) * pl.npairs, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_RET(ctx, cudaMemcpyAsync(nl->r.data(), pl.d_r, sizeof(double) * 3 * pl.npairs, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  }
+  int st = ipg_sync(ctx);
+  if (st) {
+    delete nl;
+    return st;
+  }
+  *out = nl;
+  return IPG_OK;
+}
+
+int ipg_nlist_size(const ipg_nlist* nl, int64_t* npairs) {
+  if (!nl || !npairs) return IPG_ERR_ARG;
+  *npairs = nl->npairs;
+  return IPG_OK;
+}
+
+int ipg_nlist_export(const ipg_nlist* nl, int64_t* offsets, int32_t* j, double* r) {
+  if (!nl) return IPG_ERR_ARG;
+  if (offsets) memcpy(offsets, nl->off.data(), sizeof(int64_t) * (nl->n + 1));
+  if (j && nl->npairs) memcpy(j, nl->j.data(), sizeof(int32_t) * nl->npairs);
+  if (r && nl->npairs) memcpy(r, nl->r.data(), sizeof(double) * 3 * nl->npairs);
+  return IPG_OK;
+}
+
+int ipg_nlist_free(ipg_nlist* nl) {
+  if (!nl) return IPG_ERR_ARG;
+  delete nl;
+  return IPG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,333 @@
+// ipg_pair.cu — fused multi-term empirical pair potentials.
+//
+// Replaces, for every term of a LinearCombinationPotential at once, the per-term
+// neighbor build + pair loop of src/types/empirical_potential.jl:20-67 with one walk of
+// the cell list at the largest cutoff.  One thread owns one atom (cell-sorted order, so a
+// warp reads the same neighbor cells), visits every candidate once, and applies each
+// term's own cutoff (PeriodicEuclidean distance <= rcut_t, as the term's own neighbor
+// list would) and species filter (both species in the term's set,
+// empirical_potential.jl:26-43).  Each atom sums its full neighbor set, so forces need no
+// atomics; the half-list energy and virial are recovered as 1/2 of the directed sums.
+// For j < i the displacement is the negated reference displacement of the stored half
+// pair (i.e. -get_displacement(x_j, x_i)), so every force term equals the reference's
+// term bit for bit; only the order of summation differs.
+#include "ipg_internal.cuh"
+
+namespace {
+
+struct PairTermDev {
+  int kind;
+  int pad;
+  double coeff, rcut;
+  unsigned long long mask;
+  double p[8];  // kind-specific precomputed constants (see prepare_terms)
+};
+
+struct PairTerms {
+  int nterms;
+  double rcut_max;
+  PairTermDev t[IPG_MAX_PAIR_TERMS];
+};
+
+__constant__ PairTerms c_terms;
+
+// ZBL screening coefficients, src/empirical/zbl.jl:27-28.
+__constant__ double c_zbl_c[4] = {0.18175, 0.50986, 0.28022, 0.02817};
+__constant__ double c_zbl_a[4] = {3.19980, 0.94229, 0.40290, 0.20162};
+
+// V(R) and g(R) (force = g r) of one term.
+__device__ __forceinline__ void term_eval(const PairTermDev& t, double R, double& V, double& g) {
+  switch (t.kind) {
+    case IPG_PAIR_LJ: {  // lj.jl:35-36; p = eps, sigma, 4eps, 24eps
+      double s = t.p[1] / R;
+      double s2 = s * s;
+      double s6 = s2 * s2 * s2;
+      double s12 = s6 * s6;
+      V = t.p[2] * (s12 - s6);
+      g = t.p[3] * (2.0 * s12 - s6) / (R * R);
+      break;
+    }
+    case IPG_PAIR_BM: {  // bm.jl:38-39; p = A, rho, sigma, C, D
+      double ex = t.p[0] * exp((t.p[2] - R) / t.p[1]);
+      double c = t.p[3] / R, d = t.p[4] / R;
+      double c2 = c * c, d2 = d * d;
+      double c6 = c2 * c2 * c2, d8 = (d2 * d2) * (d2 * d2);
+      V = ex + c6 - d8;
+      g = ex / (t.p[1] * R) + (c6 - d8) / (R * R);
+      break;
+    }
+    case IPG_PAIR_COUL: {  // coulomb.jl:36-37; p = q1, q2, k_e q1 q2
+      V = t.p[2] / R;
+      g = t.p[2] / (R * R * R);
+      break;
+    }
+    case IPG_PAIR_MORSE: {  // morse.jl:36-39; p = D, alpha, sigma
+      double e = exp(-t.p[1] * (R - t.p[2]));
+      double om = 1.0 - e;
+      V = t.p[0] * om * om;
+      g = 2.0 * t.p[0] * t.p[1] * om * e / R;
+      break;
+    }
+    case IPG_PAIR_ZBL: {  // zbl.jl:29-36; p = Z1, Z2, e, coeff = Z1 Z2 e^2, dden, ln(e)
+      double d = R / t.p[4];
+      double phi = 0.0, dphi = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        double ek = exp(-c_zbl_a[k] * d * t.p[5]);  // e^(-a_k d) with base e = p[2]
+        phi += c_zbl_c[k] * ek;
+        dphi += c_zbl_a[k] * c_zbl_c[k] * ek;
+      }
+      dphi = -dphi;
+      V = t.p[3] * phi / R;
+      g = t.p[3] * (phi + d * dphi) / (R * R * R);
+      break;
+    }
+    case IPG_PAIR_MOCK_R2: {  // test/mocks.jl:29-34; p = seed
+      V = R * R * t.p[0];
+      g = R * R * t.p[0];
+      break;
+    }
+    default:
+      V = 0.0;
+      g = 0.0;
+  }
+}
+
+constexpr int PAIR_T = 128;
+
+__global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid* __restrict__ grid,
+                                                      const int64_t* __restrict__ cell_start,
+                                                      const int32_t* __restrict__ cell_atoms,
+                                                      const double4* __restrict__ spos, double* __restrict__ F,
+                                                      double* __restrict__ partial, int* status) {
+  __shared__ double red[PAIR_T / 32][7];
+  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // E, W[6]
+  if (s < n) {
+    int32_t i = cell_atoms[s];
+    double4 xi = spos[s];
+    int si = (int)xi.w;
+    const ConfGrid g = grid[0];
+    int c[3];
+    cell_coords(g, xi.x, xi.y, xi.z, c);
+    int sx[3], sy[3], sz[3];
+    int nx = stencil_axis(c[0], g.nc[0], !isinf(g.L[0]), sx);
+    int ny = stencil_axis(c[1], g.nc[1], !isinf(g.L[1]), sy);
+    int nz = stencil_axis(c[2], g.nc[2], !isinf(g.L[2]), sz);
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    const int nt = c_terms.nterms;
+    const double rmax = c_terms.rcut_max;
+    for (int a = 0; a < nz; a++)
+      for (int b = 0; b < ny; b++)
+        for (int d = 0; d < nx; d++) {
+          int64_t cell = ((int64_t)sz[a] * g.nc[1] + sy[b]) * g.nc[0] + sx[d];
+          int64_t e = cell_start[cell + 1];
+          for (int64_t q = cell_start[cell]; q < e; q++) {
+            int32_t j = cell_atoms[q];
+            if (j == i) continue;
+            double4 xj = spos[q];
+            double p0 = pe_axis_dev(g.L[0], xi.x, xj.x);
+            double p1 = pe_axis_dev(g.L[1], xi.y, xj.y);
+            double p2 = pe_axis_dev(g.L[2], xi.z, xj.z);
+            double dist = sqrt(sumsq3_dev(p0, p1, p2));
+            if (dist > rmax) continue;
+            int sj = (int)xj.w;
+            double r0, r1, r2;
+            if (j > i) {
+              r0 = disp_axis_dev(g.L[0], xi.x, xj.x);
+              r1 = disp_axis_dev(g.L[1], xi.y, xj.y);
+              r2 = disp_axis_dev(g.L[2], xi.z, xj.z);
+            } else {
+              r0 = -disp_axis_dev(g.L[0], xj.x, xi.x);
+              r1 = -disp_axis_dev(g.L[1], xj.y, xi.y);
+              r2 = -disp_axis_dev(g.L[2], xj.z, xi.z);
+            }
+            double R = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+            double V = 0.0, gsum = 0.0;
+            for (int t = 0; t < nt; t++) {
+              const PairTermDev& T = c_terms.t[t];
+              if (dist > T.rcut) continue;
+              if (!((T.mask >> si) & 1ull) || !((T.mask >> sj) & 1ull)) continue;
+              double v, gg;
+              term_eval(T, R, v, gg);
+              V += T.coeff * v;
+              gsum += T.coeff * gg;
+            }
+            double fx = gsum * r0, fy = gsum * r1, fz = gsum * r2;
+            f0 += fx;
+            f1 += fy;
+            f2 += fz;
+            acc[0] += 0.5 * V;
+            // empirical_potential.jl:63-64: r * f' -> [xx, yy, zz, zy, zx, yx]
+            acc[1] += 0.5 * r0 * fx;
+            acc[2] += 0.5 * r1 * fy;
+            acc[3] += 0.5 * r2 * fz;
+            acc[4] += 0.5 * r2 * fy;
+            acc[5] += 0.5 * r2 * fx;
+            acc[6] += 0.5 * r1 * fx;
+          }
+        }
+    if (F) {
+      F[3 * (int64_t)i] = f0;
+      F[3 * (int64_t)i + 1] = f1;
+      F[3 * (int64_t)i + 2] = f2;
+    }
+  }
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    double v = warp_sum(acc[k]);
+    if (lane == 0) red[w][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double v = 0.0;
+    for (int q = 0; q < PAIR_T / 32; q++) v += red[q][threadIdx.x];
+    partial[(int64_t)blockIdx.x * 7 + threadIdx.x] = v;
+  }
+}
+
+// Deterministic final reduction of per-block partials: one block, fixed order.
+__global__ void k_reduce_partials(int64_t nblocks, int width, const double* __restrict__ partial,
+                                  double* __restrict__ out) {
+  __shared__ double sm[256];
+  for (int k = 0; k < width; k++) {
+    double v = 0.0;
+    for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x) v += partial[b * width + k];
+    sm[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = sm[0];
+    __syncthreads();
+  }
+}
+
+int prepare_terms(ipg_ctx* ctx, const ipg_pair_term* terms, int nterms, PairTerms& pt) {
+  memset(&pt, 0, sizeof(pt));
+  if (nterms < 0 || nterms > IPG_MAX_PAIR_TERMS)
+    return ipg_fail(ctx, IPG_ERR_ARG, "nterms must be in 0..%d", IPG_MAX_PAIR_TERMS);
+  pt.nterms = nterms;
+  pt.rcut_max = 0.0;
+  for (int k = 0; k < nterms; k++) {
+    const ipg_pair_term& s = terms[k];
+    PairTermDev& d = pt.t[k];
+    d.kind = s.kind;
+    d.coeff = s.coeff;
+    d.rcut = s.rcut;
+    d.mask = s.species_mask;
+    if (!(s.rcut >= 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "term %d: rcut must be >= 0", k);
+    if (std::isinf(s.rcut)) return ipg_fail(ctx, IPG_ERR_ARG, "term %d: rcut must be finite", k);
+    pt.rcut_max = std::max(pt.rcut_max, s.rcut);
+    for (int q = 0; q < 8; q++) d.p[q] = s.params[q];
+    switch (s.kind) {
+      case IPG_PAIR_LJ:
+        d.p[2] = 4.0 * s.params[0];
+        d.p[3] = 24.0 * s.params[0];
+        break;
+      case IPG_PAIR_BM:
+      case IPG_PAIR_MORSE:
+      case IPG_PAIR_MOCK_R2:
+        break;
+      case IPG_PAIR_COUL:
+        d.p[2] = 1.0 * s.params[0] * s.params[1];  // k_e = 1 (src/constants.jl:7)
+        break;
+      case IPG_PAIR_ZBL: {
+        double Z1 = s.params[0], Z2 = s.params[1], e = s.params[2];
+        d.p[3] = 1.0 * Z1 * Z2 * e * e;                                     // _zbl_coeff
+        d.p[4] = 0.8854 * 0.529 / (std::pow(Z1, 0.23) + std::pow(Z2, 0.23));  // _zbl_d divisor
+        d.p[5] = std::log(e);
+        if (!(e > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "term %d: ZBL e must be > 0", k);
+        break;
+      }
+      default:
+        return ipg_fail(ctx, IPG_ERR_ARG, "term %d: unknown kind %d", k, s.kind);
+    }
+  }
+  return IPG_OK;
+}
+
+int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
+                     const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
+                     uint32_t flags) {
+  PairTerms pt;
+  IPG_RET(prepare_terms(ctx, terms, nterms, pt));
+  CUDA_RET(ctx, cudaMemcpyToSymbolAsync(c_terms, &pt, sizeof(pt), 0, cudaMemcpyHostToDevice, ctx->stream));
+  IPG_RET(ipg_status_reset(ctx));
+  int64_t aoff[2] = {0, n};
+  CellList cl;
+  IPG_RET(ipg_build_cells(ctx, "pair_", n, d_pos, d_species, 1, aoff, L, pt.rcut_max, cl));
+  int64_t nb = std::max<int64_t>(1, (n + PAIR_T - 1) / PAIR_T);
+  double *partial, *red;
+  IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
+  IPG_RET(scratch(ctx, "pair_red", 8, &red));
+  IPG_TIMED_LAUNCH(ctx, "pair_eval", k_pair_eval, (unsigned)nb, PAIR_T, 0, n, cl.d_grid, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos,
+             (flags & IPG_WANT_F) ? d_F : nullptr, partial, ctx->d_status);
+  IPG_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, nb, 7, partial, red);
+  if ((flags & IPG_WANT_E) && d_E)
+    CUDA_RET(ctx, cudaMemcpyAsync(d_E, red, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if ((flags & IPG_WANT_W) && d_W6)
+    CUDA_RET(ctx, cudaMemcpyAsync(d_W6, red + 1, 6 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  return IPG_OK;
+}
+
+int check_pair_args(ipg_ctx* ctx, int64_t n, const void* pos, const void* species, const double* L,
+                    const ipg_pair_term* terms, int32_t nterms, const void* E, const void* F, const void* W6,
+                    uint32_t flags) {
+  if (!ctx) return IPG_ERR_ARG;
+  if (n < 0 || n >= INT32_MAX) return ipg_fail(ctx, IPG_ERR_ARG, "n out of range");
+  if ((n > 0 && (!pos || !species)) || !L || (nterms > 0 && !terms))
+    return ipg_fail(ctx, IPG_ERR_ARG, "null input pointer");
+  if ((flags & IPG_WANT_E) && !E) return ipg_fail(ctx, IPG_ERR_ARG, "E requested but NULL");
+  if ((flags & IPG_WANT_F) && !F && n > 0) return ipg_fail(ctx, IPG_ERR_ARG, "F requested but NULL");
+  if ((flags & IPG_WANT_W) && !W6) return ipg_fail(ctx, IPG_ERR_ARG, "W6 requested but NULL");
+  return IPG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipg_pair_eval(ipg_ctx* ctx, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                  const ipg_pair_term* terms, int32_t nterms, double* E, double* F, double* W6, uint32_t flags) {
+  IPG_RET(check_pair_args(ctx, n, pos, species, L, terms, nterms, E, F, W6, flags));
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  for (int64_t k = 0; k < 3 * n; k++)
+    if (!std::isfinite(pos[k])) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite position");
+  for (int64_t k = 0; k < n; k++)
+    if (species[k] < 0 || species[k] >= 64) return ipg_fail(ctx, IPG_ERR_SPECIES, "species id out of range 0..63");
+  double *d_pos, *d_out;
+  int32_t* d_sp;
+  IPG_RET(scratch(ctx, "pair_in_pos", 3 * (size_t)n + 3, &d_pos));
+  IPG_RET(scratch(ctx, "pair_in_sp", (size_t)n + 1, &d_sp));
+  IPG_RET(scratch(ctx, "pair_out", 3 * (size_t)n + 8, &d_out));
+  if (n) {
+    CUDA_RET(ctx, cudaMemcpyAsync(d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_RET(ctx, cudaMemcpyAsync(d_sp, species, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  // d_out layout: [E, W6 (6), pad, F (3n)]
+  IPG_RET(pair_eval_device(ctx, n, d_pos, d_sp, L, terms, nterms, d_out, d_out + 8, d_out + 1,
+                           flags | IPG_WANT_E | IPG_WANT_W));
+  std::vector<double> head(8);
+  CUDA_RET(ctx, cudaMemcpyAsync(head.data(), d_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if ((flags & IPG_WANT_F) && n)
+    CUDA_RET(ctx, cudaMemcpyAsync(F, d_out + 8, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  IPG_RET(ipg_status_check(ctx, "ipg_pair_eval"));
+  if (flags & IPG_WANT_E) *E = head[0];
+  if (flags & IPG_WANT_W) memcpy(W6, head.data() + 1, 6 * sizeof(double));
+  return IPG_OK;
+}
+
+int ipg_pair_eval_dev(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
+                      const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
+                      uint32_t flags) {
+  IPG_RET(check_pair_args(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags));
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(pair_eval_device(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags));
+  IPG_RET(ipg_status_check(ctx, "ipg_pair_eval_dev"));
+  return IPG_OK;
+}
+
+}  // extern "C"

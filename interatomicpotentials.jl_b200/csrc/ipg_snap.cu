@@ -1,0 +1,1309 @@
+// ipg_snap.cu — SNAP bispectrum pipeline on sm_100a (FP64).
+//
+// One thread block owns one centre atom at a time (persistent grid-stride loop) and
+// keeps everything of that atom in shared memory:
+//   phase 1  Utot = wself*I + sum_j sfac*w_j*U(r_ij)      (compute_ui.jl:5-175)
+//            warps take neighbors, lanes take the entries of one level of the Wigner
+//            recursion; per-warp partial sums are reduced across warps in fixed order.
+//   phase 2  Z = CG (Utot x Utot) CG                       (compute_z.jl:1-62)
+//            threads take Z entries; Utot is read from shared memory.
+//   phase 3  B, E_i = beta[s_i] . B_i                       (compute_b.jl:67-157)
+//   phase 4  Y = d(beta.B)/dU  (adjoint mode only)          (design of compute_yi.jl)
+//   phase 5  per neighbor: U and dU/dr recomputed level by level, then
+//            adjoint: dE_i/dr_ij = 2 sum Re(conj(dU) Y)    (design of compute_dij.jl)
+//            plain:   dB_i/dr_ij, 3 CG-symmetry terms       (compute_b.jl:166-404),
+//                     written out per directed pair (the materialised dB/dr)
+//            vjp:     V_i = sum_j (g_i - g_j) . dU_ij, then dB-contraction with Z.
+// The per-pair results are scattered to atoms by a gather over the CSR list and its
+// transpose, so every reduction is in a fixed order (bitwise reproducible).
+#include <algorithm>
+
+#include "ipg_snap.cuh"
+
+namespace {
+
+enum SnapMode { MODE_DESC = 0, MODE_ADJ = 1, MODE_PLAIN = 2, MODE_VJP = 3 };
+
+struct SnapIO {
+  int64_t n;
+  const int64_t* off;       // [n+1] neighbor CSR
+  const int32_t* nbr;       // [np]
+  const double* rij;        // [np][3]  x_j - x_i
+  const int32_t* species;   // [n]
+  double* Ei;               // [n] beta[s_i].B_i (without beta0)
+  double* B;                // [n][K] or null
+  double* fvec;             // [np][3]  adjoint dE_i/dr_ij
+  double* dbl;              // [np][K][3] plain dB_i/dr_ij
+  const double* g;          // [n][3] VJP cotangent of forces
+  double gE;                // VJP cotangent of energy
+  double* gpart;            // [gridDim][nsp*K] VJP partials
+  int* status;
+};
+
+__device__ __forceinline__ double2 cmul_conj(double2 a, double2 v) {  // conj(a) * v
+  return make_double2(a.x * v.x + a.y * v.y, a.x * v.y - a.y * v.x);
+}
+
+__device__ __forceinline__ double sfac_of(const SnapDev& S, double r, double rcut) {  // compute_ui.jl:350-364
+  if (!S.switch_flag) return 1.0;
+  if (r <= S.rmin0) return 1.0;
+  if (r > rcut) return 0.0;
+  return 0.5 * (cos((r - S.rmin0) * (M_PI / (rcut - S.rmin0))) + 1.0);
+}
+__device__ __forceinline__ double dsfac_of(const SnapDev& S, double r, double rcut) {  // compute_ui.jl:366-380
+  if (!S.switch_flag) return 0.0;
+  if (r <= S.rmin0) return 0.0;
+  double rcutfac = M_PI / (rcut - S.rmin0);
+  return -0.5 * (sin((r - S.rmin0) * rcutfac) * rcutfac);
+}
+
+// Number of weight-1 half-plane entries of level l (rows 2mb < l, plus ma < l/2 of the
+// middle row for even l); the middle element of an even level has weight 1/2.
+__device__ __forceinline__ int nfull_of(int l) { return ((l + 1) / 2) * (l + 1) + ((l & 1) ? 0 : l / 2); }
+
+// Per-pair geometry for the derivative recursion (compute_duidrj, compute_ui.jl:328-347
+// and the prologue of compute_duarray, :191-216).
+struct PairGeom {
+  double2 a, b;
+  double2 da[3], db[3];
+  double u[3];
+  double sfac, dsfac;
+};
+
+__device__ __forceinline__ void geom_du(const SnapDev& S, double x, double y, double z, double rcut, double wj,
+                                        PairGeom& G) {
+  double rsq = x * x + y * y + z * z;
+  double r = sqrt(rsq);
+  double rscale0 = S.rfac0 * M_PI / (rcut - S.rmin0);
+  double theta0 = (r - S.rmin0) * rscale0;
+  double sn, cs;
+  sincos(theta0, &sn, &cs);
+  double z0 = r * cs / sn;
+  double dz0dr = z0 / r - (r * rscale0) * (rsq + z0 * z0) / rsq;
+  double rinv = 1.0 / r;
+  G.u[0] = x * rinv;
+  G.u[1] = y * rinv;
+  G.u[2] = z * rinv;
+  double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+  G.a = make_double2(z0 * r0inv, -z * r0inv);
+  G.b = make_double2(y * r0inv, -x * r0inv);
+  double dr0invdr = -r0inv * r0inv * r0inv * (r + z0 * dz0dr);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double dr0 = dr0invdr * G.u[k];
+    double dz0 = dz0dr * G.u[k];
+    G.da[k] = make_double2(dz0 * r0inv + z0 * dr0, -z * dr0);
+    G.db[k] = make_double2(y * dr0, -x * dr0);
+  }
+  G.da[2].y += -r0inv;
+  G.db[0].y += -r0inv;
+  G.db[1].x += r0inv;
+  G.sfac = sfac_of(S, r, rcut) * wj;
+  G.dsfac = dsfac_of(S, r, rcut) * wj;
+}
+
+// One level of the Wigner recursion (compute_ui.jl:66-101, derivative :224-267) for
+// `ncomp` components (1: U only; 4: U and dU/dx, dU/dy, dU/dz), lanes over
+// (component, entry).  prev holds level j-1 rows 0..j/2 (row length j), cur receives
+// level j rows 0..j/2 (row length j+1) and, for odd j, the mirrored row (j+1)/2
+// (inversion symmetry, compute_ui.jl:105-125).  Buffers are [comp][ext_max].
+__device__ __forceinline__ void wigner_level(const SnapDev& S, const double* rpq, int j, int ncomp,
+                                             const PairGeom& G, const double2* __restrict__ prev,
+                                             double2* __restrict__ cur, int lane) {
+  const int J2 = S.J + 2;
+  const int em = S.ext_max;
+  const int nrec = (j / 2 + 1) * (j + 1);
+  for (int t = lane; t < ncomp * nrec; t += 32) {
+    int comp = t / nrec;
+    int e = t - comp * nrec;
+    int mb = e / (j + 1);
+    int ma = e - mb * (j + 1);
+    double2 dA = make_double2(0.0, 0.0), dB = make_double2(0.0, 0.0);
+    if (comp == 1) { dA = G.da[0]; dB = G.db[0]; }
+    if (comp == 2) { dA = G.da[1]; dB = G.db[1]; }
+    if (comp == 3) { dA = G.da[2]; dB = G.db[2]; }
+    double2 res = make_double2(0.0, 0.0);
+    if (ma > 0) {  // -rootpq[ma][j-mb] * conj(b) * u_{j-1}[mb][ma-1]
+      double rp = rpq[ma * J2 + (j - mb)];
+      double2 v = prev[mb * j + ma - 1];
+      double2 t1 = cmul_conj(G.b, v);
+      if (comp) {
+        double2 dv = prev[comp * em + mb * j + ma - 1];
+        double2 t2 = cmul_conj(dB, v);
+        double2 t3 = cmul_conj(G.b, dv);
+        t1 = make_double2(t2.x + t3.x, t2.y + t3.y);
+      }
+      res = make_double2(-rp * t1.x, -rp * t1.y);
+    }
+    if (ma < j) {  // + rootpq[j-ma][j-mb] * conj(a) * u_{j-1}[mb][ma]
+      double rp = rpq[(j - ma) * J2 + (j - mb)];
+      double2 v = prev[mb * j + ma];
+      double2 t1 = cmul_conj(G.a, v);
+      if (comp) {
+        double2 dv = prev[comp * em + mb * j + ma];
+        double2 t2 = cmul_conj(dA, v);
+        double2 t3 = cmul_conj(G.a, dv);
+        t1 = make_double2(t2.x + t3.x, t2.y + t3.y);
+      }
+      res.x += rp * t1.x;
+      res.y += rp * t1.y;
+    }
+    cur[comp * em + e] = res;
+  }
+  __syncwarp();
+  if (j & 1) {  // u[R][c] = (-1)^(c+R) conj(u[j-R][j-c]),  R = (j+1)/2
+    const int R = (j + 1) / 2;
+    for (int t = lane; t < ncomp * (j + 1); t += 32) {
+      int comp = t / (j + 1);
+      int c = t - comp * (j + 1);
+      double2 src = cur[comp * em + (j - R) * (j + 1) + (j - c)];
+      double sg = ((c + R) & 1) ? -1.0 : 1.0;
+      cur[comp * em + R * (j + 1) + c] = make_double2(sg * src.x, -sg * src.y);
+    }
+    __syncwarp();
+  }
+}
+
+// Shared-memory layout (doubles, 16-byte aligned blocks).
+struct SmemLayout {
+  size_t ut, zs, ys, bs, rpq, lv, duf, gacc, total;
+};
+
+__host__ __device__ inline size_t al16(size_t x) { return (x + 1) & ~size_t(1); }  // in doubles
+
+__host__ __device__ inline SmemLayout smem_layout(const SnapDev& S, int nwarps, int mode) {
+  SmemLayout L;
+  size_t o = 0;
+  L.ut = o;
+  o += al16(2 * (size_t)S.idxu_max);
+  L.zs = o;  // Z; phase 1 reuses it for the per-warp partial sums of Utot
+  const size_t zsz = 2 * (size_t)S.idxz_max, usz = 2 * (size_t)nwarps * S.u_half;
+  o += al16(zsz > usz ? zsz : usz);
+  L.ys = o;  // Y (adjoint) or V (vjp)
+  o += al16(2 * (size_t)S.u_half);
+  L.bs = o;
+  o += al16((size_t)S.K);
+  L.rpq = o;
+  o += al16((size_t)(S.J + 2) * (S.J + 2));
+  L.lv = o;  // per warp: 2 levels x 4 components x ext_max complex
+  o += al16((size_t)nwarps * 2 * 4 * 2 * S.ext_max);
+  L.duf = o;  // plain: per-warp dU/dr [3][u_half]; vjp: per-warp partial V [u_half]
+  if (mode == MODE_PLAIN) o += al16((size_t)nwarps * 2 * 3 * S.u_half);
+  if (mode == MODE_VJP) o += al16((size_t)nwarps * 2 * S.u_half);
+  L.gacc = o;
+  if (mode == MODE_VJP) o += al16((size_t)S.nsp * S.K);
+  L.total = o * sizeof(double);
+  return L;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapDev S, SnapIO io) {
+  extern __shared__ double smem[];
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const SmemLayout L = smem_layout(S, nwarps, MODE);
+  double2* ut = reinterpret_cast<double2*>(smem + L.ut);
+  double2* zs = reinterpret_cast<double2*>(smem + L.zs);
+  double2* ys = reinterpret_cast<double2*>(smem + L.ys);
+  double* bs = smem + L.bs;
+  double* rpq = smem + L.rpq;
+  double2* lvw = reinterpret_cast<double2*>(smem + L.lv) + (size_t)warp * 2 * 4 * S.ext_max;
+  double2* lv0 = lvw;
+  double2* lv1 = lvw + 4 * S.ext_max;
+  double* gacc = smem + L.gacc;
+  const int J = S.J, K = S.K, uh = S.u_half;
+
+  for (int q = threadIdx.x; q < (J + 2) * (J + 2); q += blockDim.x) rpq[q] = S.rootpq[q];
+  if (MODE == MODE_VJP)
+    for (int q = threadIdx.x; q < S.nsp * K; q += blockDim.x) gacc[q] = 0.0;
+  __syncthreads();
+
+  for (int64_t i = blockIdx.x; i < io.n; i += gridDim.x) {
+    const int64_t beg = io.off[i], end = io.off[i + 1];
+    const int si = io.species[i];
+
+    // ---------------- phase 1: Utot (half plane) ----------------
+    double2* upart = zs;  // [nwarps][u_half]
+    for (int q = threadIdx.x; q < nwarps * uh; q += blockDim.x) upart[q] = make_double2(0.0, 0.0);
+    __syncthreads();
+    {
+      double2* up = upart + (size_t)warp * uh;
+      for (int64_t p = beg + warp; p < end; p += nwarps) {
+        const double x = io.rij[3 * p], y = io.rij[3 * p + 1], z = io.rij[3 * p + 2];
+        const int sj = io.species[io.nbr[p]];
+        const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;  // runtime_arrays.jl:50
+        const double rsq = x * x + y * y + z * z;
+        const double r = sqrt(rsq);
+        const double theta0 = (r - S.rmin0) * S.rfac0 * M_PI / (rcut - S.rmin0);
+        const double z0 = r / tan(theta0);
+        const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+        PairGeom G;
+        G.a = make_double2(r0inv * z0, -r0inv * z);
+        G.b = make_double2(r0inv * y, -r0inv * x);
+        const double sw = sfac_of(S, r, rcut) * S.weight[sj];
+        double2* prev = lv0;
+        double2* cur = lv1;
+        if (lane == 0) {
+          prev[0] = make_double2(1.0, 0.0);
+          up[0].x += sw;
+        }
+        __syncwarp();
+        for (int j = 1; j <= J; j++) {
+          wigner_level(S, rpq, j, 1, G, prev, cur, lane);
+          const int nrec = (j / 2 + 1) * (j + 1);
+          double2* upj = up + S.half_block[j];
+          for (int e = lane; e < nrec; e += 32) {
+            double2 v = cur[e];
+            upj[e].x += sw * v.x;
+            upj[e].y += sw * v.y;
+          }
+          __syncwarp();
+          double2* t = prev;
+          prev = cur;
+          cur = t;
+        }
+      }
+    }
+    __syncthreads();
+    // cross-warp sum (fixed order) + wself diagonal + inversion-symmetric fill
+    for (int h = threadIdx.x; h < uh; h += blockDim.x) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int w = 0; w < nwarps; w++) {
+        double2 v = upart[(size_t)w * uh + h];
+        s.x += v.x;
+        s.y += v.y;
+      }
+      int j = 0;
+      while (j < J && S.half_block[j + 1] <= h) j++;
+      int e = h - S.half_block[j];
+      int mb = e / (j + 1), ma = e - mb * (j + 1);
+      if (ma == mb) s.x += S.wself;
+      const int ub = S.idxu_block[j];
+      const bool middle = (2 * mb == j);
+      if (middle && ma > mb) continue;  // written as the mirror of ma' = j - ma
+      ut[ub + mb * (j + 1) + ma] = s;
+      if (!(middle && ma == mb)) {
+        double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+        ut[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * s.x, -sg * s.y);
+      }
+    }
+    __syncthreads();
+
+    // ---------------- phase 2: Z ----------------
+    for (int jjz = threadIdx.x; jjz < S.idxz_max; jjz += blockDim.x) {
+      const ZDev q = S.idxz[jjz];
+      const double* cgb = S.cglist + q.cgoff;
+      const int j1 = q.j1, j2 = q.j2;
+      double zr = 0.0, zi = 0.0;
+      int i1 = q.u1base, i2 = q.u2base, icgb = q.icgb0;
+      for (int ib = 0; ib < q.nb; ib++) {
+        double sr = 0.0, sim = 0.0;
+        int icga = q.icga0;
+        for (int ia = 0; ia < q.na; ia++) {
+          const double2 u1 = ut[i1 + ia];
+          const double2 u2 = ut[i2 - ia];
+          const double c = __ldg(cgb + icga);
+          sr += c * (u1.x * u2.x - u1.y * u2.y);
+          sim += c * (u1.x * u2.y + u1.y * u2.x);
+          icga += j2;
+        }
+        const double cb = __ldg(cgb + icgb);
+        zr += cb * sr;
+        zi += cb * sim;
+        i1 += j1 + 1;
+        i2 -= j2 + 1;
+        icgb += j2;
+      }
+      if (S.bnorm_flag) {
+        zr /= (q.j + 1);
+        zi /= (q.j + 1);
+      }
+      zs[jjz] = make_double2(zr, zi);
+    }
+    __syncthreads();
+
+    // ---------------- phase 3: B and E_i ----------------
+    for (int b = threadIdx.x; b < K; b += blockDim.x) {
+      const DBDev d = S.db[b];
+      const int l = d.l[0], z0 = d.z0[0], u0 = S.idxu_block[l];
+      const int nf = nfull_of(l);
+      double s = 0.0;
+      for (int e = 0; e < nf; e++) {
+        double2 u = ut[u0 + e], zz = zs[z0 + e];
+        s += u.x * zz.x + u.y * zz.y;
+      }
+      if (!(l & 1)) {
+        int e = (l / 2) * (l + 1) + l / 2;
+        double2 u = ut[u0 + e], zz = zs[z0 + e];
+        s += 0.5 * (u.x * zz.x + u.y * zz.y);
+      }
+      double Bv = 2.0 * s - (S.bzero_flag ? S.bzero[l] : 0.0);
+      bs[b] = Bv;
+      if (io.B) io.B[i * K + b] = Bv;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double e = 0.0;
+      const double* bt = S.beta + (size_t)si * K;
+      for (int b = lane; b < K; b += 32) e += bt[b] * bs[b];
+      e = warp_sum(e);
+      if (lane == 0) io.Ei[i] = e;
+    }
+
+    if (MODE == MODE_DESC) {
+      __syncthreads();
+      continue;
+    }
+
+    // ---------------- phase 4: Y (adjoint) / zero V (vjp) ----------------
+    if (MODE == MODE_ADJ) {
+      const double* yc = S.ycoef + (size_t)si * S.idxz_max;
+      for (int h = threadIdx.x; h < uh; h += blockDim.x) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
+          int jjz = S.y_jjz[q];
+          double c = yc[jjz];
+          double2 zz = zs[jjz];
+          s.x += c * zz.x;
+          s.y += c * zz.y;
+        }
+        ys[h] = s;
+      }
+    }
+    double2* vall = reinterpret_cast<double2*>(smem + L.duf);  // VJP: [nwarps][u_half]
+    if (MODE == MODE_VJP)
+      for (int q = threadIdx.x; q < nwarps * uh; q += blockDim.x) vall[q] = make_double2(0.0, 0.0);
+    __syncthreads();
+
+    // ---------------- phase 5: per-neighbor derivatives ----------------
+    double2* dufw = reinterpret_cast<double2*>(smem + L.duf) + (size_t)warp * 3 * uh;  // [3][u_half]
+    double2* vw = vall + (size_t)warp * uh;
+    double gi[3] = {0.0, 0.0, 0.0};
+    if (MODE == MODE_VJP) {
+      gi[0] = io.g[3 * i];
+      gi[1] = io.g[3 * i + 1];
+      gi[2] = io.g[3 * i + 2];
+    }
+    for (int64_t p = beg + warp; p < end; p += nwarps) {
+      const int32_t jn = io.nbr[p];
+      const int sj = io.species[jn];
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+      PairGeom G;
+      geom_du(S, io.rij[3 * p], io.rij[3 * p + 1], io.rij[3 * p + 2], rcut, S.weight[sj], G);
+      double gv[3] = {0.0, 0.0, 0.0};
+      if (MODE == MODE_VJP) {
+        gv[0] = gi[0] - io.g[3 * jn];
+        gv[1] = gi[1] - io.g[3 * jn + 1];
+        gv[2] = gi[2] - io.g[3 * jn + 2];
+      }
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+      double2* prev = lv0;
+      double2* cur = lv1;
+      const int em = S.ext_max;
+      for (int j = 0; j <= J; j++) {
+        if (j == 0) {
+          if (lane < 4) cur[lane * em] = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
+          __syncwarp();
+        } else {
+          wigner_level(S, rpq, j, 4, G, prev, cur, lane);
+        }
+        const int nrec = (j / 2 + 1) * (j + 1);
+        const int hb = S.half_block[j];
+        if (MODE == MODE_ADJ) {
+          const int nf = nfull_of(j);
+          const int emid = (j & 1) ? -1 : (j / 2) * (j + 1) + j / 2;
+          for (int e = lane; e < nrec; e += 32) {
+            double w = (e < nf) ? 1.0 : (e == emid ? 0.5 : 0.0);
+            if (w == 0.0) continue;
+            double2 u = cur[e];
+            double2 Y = ys[hb + e];
+            double2 d0 = cur[em + e], d1 = cur[2 * em + e], d2 = cur[3 * em + e];
+            acc0 += w * ((G.dsfac * u.x * G.u[0] + G.sfac * d0.x) * Y.x + (G.dsfac * u.y * G.u[0] + G.sfac * d0.y) * Y.y);
+            acc1 += w * ((G.dsfac * u.x * G.u[1] + G.sfac * d1.x) * Y.x + (G.dsfac * u.y * G.u[1] + G.sfac * d1.y) * Y.y);
+            acc2 += w * ((G.dsfac * u.x * G.u[2] + G.sfac * d2.x) * Y.x + (G.dsfac * u.y * G.u[2] + G.sfac * d2.y) * Y.y);
+          }
+        } else if (MODE == MODE_PLAIN) {
+          for (int e = lane; e < nrec; e += 32) {
+            double2 u = cur[e];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              double2 d = cur[(k + 1) * em + e];
+              dufw[k * uh + hb + e] = make_double2(G.dsfac * u.x * G.u[k] + G.sfac * d.x,
+                                                   G.dsfac * u.y * G.u[k] + G.sfac * d.y);
+            }
+          }
+        } else if (MODE == MODE_VJP) {
+          for (int e = lane; e < nrec; e += 32) {
+            double2 u = cur[e];
+            double vx = 0.0, vy = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              double2 d = cur[(k + 1) * em + e];
+              vx += gv[k] * (G.dsfac * u.x * G.u[k] + G.sfac * d.x);
+              vy += gv[k] * (G.dsfac * u.y * G.u[k] + G.sfac * d.y);
+            }
+            vw[hb + e].x += vx;  // this lane owns entry e of this warp's partial
+            vw[hb + e].y += vy;
+          }
+        }
+        __syncwarp();
+        double2* t = prev;
+        prev = cur;
+        cur = t;
+      }
+      if (MODE == MODE_ADJ) {
+        acc0 = warp_sum(acc0);
+        acc1 = warp_sum(acc1);
+        acc2 = warp_sum(acc2);
+        if (lane == 0) {
+          io.fvec[3 * p] = 2.0 * acc0;
+          io.fvec[3 * p + 1] = 2.0 * acc1;
+          io.fvec[3 * p + 2] = 2.0 * acc2;
+        }
+      } else if (MODE == MODE_PLAIN) {
+        double* out = io.dbl + (size_t)p * K * 3;
+        for (int t = lane; t < 3 * K; t += 32) {
+          const int b = t / 3, k = t - 3 * b;
+          const DBDev d = S.db[b];
+          double tot = 0.0;
+#pragma unroll
+          for (int term = 0; term < 3; term++) {
+            const int l = d.l[term], z0 = d.z0[term], hb = S.half_block[l];
+            const int nf = nfull_of(l);
+            const double2* du = dufw + k * uh + hb;
+            double s = 0.0;
+            for (int e = 0; e < nf; e++) {
+              double2 a = du[e], zz = zs[z0 + e];
+              s += a.x * zz.x + a.y * zz.y;
+            }
+            if (!(l & 1)) {
+              int e = (l / 2) * (l + 1) + l / 2;
+              double2 a = du[e], zz = zs[z0 + e];
+              s += 0.5 * (a.x * zz.x + a.y * zz.y);
+            }
+            tot += d.fac[term] * s;
+          }
+          out[t] = 2.0 * tot;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+
+    if (MODE == MODE_VJP) {
+      // V = sum of the per-warp partials (fixed order)
+      double2* vpart = ys;
+      for (int h = threadIdx.x; h < uh; h += blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        for (int w = 0; w < nwarps; w++) {
+          v.x += vall[(size_t)w * uh + h].x;
+          v.y += vall[(size_t)w * uh + h].y;
+        }
+        vpart[h] = v;
+      }
+      __syncthreads();
+      // gbeta[s_i][b] += gE * B_i[b] + 2 sum_terms fac * sum_half Re(conj(V) Z)
+      for (int b = threadIdx.x; b < K; b += blockDim.x) {
+        const DBDev d = S.db[b];
+        double tot = 0.0;
+        for (int term = 0; term < 3; term++) {
+          const int l = d.l[term], z0 = d.z0[term], hb = S.half_block[l];
+          const int nf = nfull_of(l);
+          double s = 0.0;
+          for (int e = 0; e < nf; e++) {
+            double2 a = vpart[hb + e], zz = zs[z0 + e];
+            s += a.x * zz.x + a.y * zz.y;
+          }
+          if (!(l & 1)) {
+            int e = (l / 2) * (l + 1) + l / 2;
+            double2 a = vpart[hb + e], zz = zs[z0 + e];
+            s += 0.5 * (a.x * zz.x + a.y * zz.y);
+          }
+          tot += d.fac[term] * s;
+        }
+        gacc[(size_t)si * K + b] += 2.0 * tot + io.gE * bs[b];
+      }
+      __syncthreads();
+    }
+  }
+  if (MODE == MODE_VJP) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < S.nsp * K; q += blockDim.x) io.gpart[(size_t)blockIdx.x * S.nsp * K + q] = gacc[q];
+  }
+}
+
+// Plain path contraction: f_p = dB_i/dr_ij . beta[s_i] from the materialised dB/dr.
+__global__ void k_snap_contract(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ species,
+                                const double* __restrict__ dbl, const double* __restrict__ beta, int K,
+                                double* __restrict__ fvec) {
+  // one warp per atom; lanes over (pair, component) rows
+  int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const double* bt = beta + (size_t)species[i] * K;
+  for (int64_t p = off[i]; p < off[i + 1]; p++) {
+    const double* d = dbl + (size_t)p * K * 3;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int b = lane; b < K; b += 32) {
+      double bb = bt[b];
+      a0 += d[3 * b] * bb;
+      a1 += d[3 * b + 1] * bb;
+      a2 += d[3 * b + 2] * bb;
+    }
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    if (lane == 0) {
+      fvec[3 * p] = a0;
+      fvec[3 * p + 1] = a1;
+      fvec[3 * p + 2] = a2;
+    }
+  }
+}
+
+// F_k = sum_{p in out(k)} f_p - sum_{q in in(k)} f_q; per-atom virial contribution
+// w6[k] = sum_{p in out(k)} f_p (x) (x_k - x_j(p)) with absolute positions
+// (snap.jl:292-306 contracted with beta): [xx, yy, zz, yz, xz, xy] as in the reference.
+__global__ void k_snap_gather(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ nbr,
+                              const int64_t* __restrict__ in_off, const int64_t* __restrict__ in_pair,
+                              const double* __restrict__ fvec, const double* __restrict__ pos,
+                              double* __restrict__ F, double* __restrict__ w6) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  const double xk = pos[3 * k], yk = pos[3 * k + 1], zk = pos[3 * k + 2];
+  for (int64_t p = off[k]; p < off[k + 1]; p++) {
+    double a = fvec[3 * p], b = fvec[3 * p + 1], c = fvec[3 * p + 2];
+    f0 += a;
+    f1 += b;
+    f2 += c;
+    int64_t jn = nbr[p];
+    double dx = xk - pos[3 * jn], dy = yk - pos[3 * jn + 1], dz = zk - pos[3 * jn + 2];
+    w[0] += a * dx;
+    w[1] += b * dy;
+    w[2] += c * dz;
+    w[3] += b * dz;
+    w[4] += a * dz;
+    w[5] += a * dy;
+  }
+  for (int64_t q = in_off[k]; q < in_off[k + 1]; q++) {
+    int64_t p = in_pair[q];
+    f0 -= fvec[3 * p];
+    f1 -= fvec[3 * p + 1];
+    f2 -= fvec[3 * p + 2];
+  }
+  if (F) {
+    F[3 * k] = f0;
+    F[3 * k + 1] = f1;
+    F[3 * k + 2] = f2;
+  }
+  if (w6)
+    for (int c = 0; c < 6; c++) w6[6 * k + c] = w[c];
+}
+
+// Per-configuration sums (fixed order): E[c] = beta0 + sum Ei, W6[c] = sum w6.
+__global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ atom_off, const double* __restrict__ Ei,
+                              const double* __restrict__ w6, double beta0, double* __restrict__ E,
+                              double* __restrict__ W6) {
+  __shared__ double sm[7][128];
+  int c = blockIdx.x;
+  if (c >= nconf) return;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t i = atom_off[c] + threadIdx.x; i < atom_off[c + 1]; i += blockDim.x) {
+    acc[0] += Ei ? Ei[i] : 0.0;
+    if (w6)
+      for (int q = 0; q < 6; q++) acc[1 + q] += w6[6 * i + q];
+  }
+  for (int q = 0; q < 7; q++) sm[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int q = 0; q < 7; q++) sm[q][threadIdx.x] += sm[q][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (E) E[c] = beta0 + sm[0][0];
+    if (W6)
+      for (int q = 0; q < 6; q++) W6[6 * c + q] = sm[1 + q][0];
+  }
+}
+
+// Per-atom force descriptors: dB_k[block s][b][c] = sum_{p in out(k), s_k = s} dbl_p -
+// sum_{q in in(k), s_owner(q) = s} dbl_q   (snap.jl:289-290).  One thread per (atom, b*3+c).
+__global__ void k_snap_dB_atoms(int64_t n, int K, int nsp, const int64_t* __restrict__ off,
+                                const int64_t* __restrict__ in_off, const int64_t* __restrict__ in_pair,
+                                const int32_t* __restrict__ owner, const int32_t* __restrict__ species,
+                                const double* __restrict__ dbl, double* __restrict__ dB) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t k = t / (3 * K);
+  int bc = (int)(t - k * 3 * K);
+  if (k >= n) return;
+  double acc[IPG_MAX_SNAP_SPECIES];
+#pragma unroll
+  for (int s = 0; s < IPG_MAX_SNAP_SPECIES; s++) acc[s] = 0.0;
+  const int sk = species[k];
+  double own = 0.0;
+  for (int64_t p = off[k]; p < off[k + 1]; p++) own += dbl[(size_t)p * 3 * K + bc];
+#pragma unroll
+  for (int s = 0; s < IPG_MAX_SNAP_SPECIES; s++)
+    if (s == sk) acc[s] += own;
+  for (int64_t q = in_off[k]; q < in_off[k + 1]; q++) {
+    int64_t p = in_pair[q];
+    int so = species[owner[p]];
+    double v = dbl[(size_t)p * 3 * K + bc];
+#pragma unroll
+    for (int s = 0; s < IPG_MAX_SNAP_SPECIES; s++)
+      if (s == so) acc[s] -= v;
+  }
+  const int b = bc / 3, c = bc - 3 * b;
+  for (int s = 0; s < nsp; s++) dB[((size_t)k * K * nsp + (size_t)s * K + b) * 3 + c] = acc[s];
+}
+
+__global__ void k_pair_owner(int64_t n, const int64_t* __restrict__ off, int32_t* __restrict__ owner) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int64_t p = off[i]; p < off[i + 1]; p++) owner[p] = (int32_t)i;
+}
+
+// Virial descriptors W[block s][b][6] = sum over pairs of dB_i/dr_ij (x) (x_i - x_j)
+// (snap.jl:292-306), per-block partials [grid][nsp*K*6].  Thread per component b,
+// atoms strided over blocks.
+__global__ void k_snap_W_desc(int64_t n, int K, int nsp, const int64_t* __restrict__ off,
+                              const int32_t* __restrict__ nbr, const int32_t* __restrict__ species,
+                              const double* __restrict__ pos, const double* __restrict__ dbl,
+                              double* __restrict__ part) {
+  extern __shared__ double wsm[];  // [nsp][K][6]
+  for (int q = threadIdx.x; q < nsp * K * 6; q += blockDim.x) wsm[q] = 0.0;
+  __syncthreads();
+  for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const int s = species[i];
+    const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+    for (int b = threadIdx.x; b < K; b += blockDim.x) {
+      double w[6] = {0, 0, 0, 0, 0, 0};
+      for (int64_t p = off[i]; p < off[i + 1]; p++) {
+        const double* d = dbl + ((size_t)p * K + b) * 3;
+        int64_t jn = nbr[p];
+        double dx = xi - pos[3 * jn], dy = yi - pos[3 * jn + 1], dz = zi - pos[3 * jn + 2];
+        w[0] += d[0] * dx;
+        w[1] += d[1] * dy;
+        w[2] += d[2] * dz;
+        w[3] += d[1] * dz;
+        w[4] += d[0] * dz;
+        w[5] += d[0] * dy;
+      }
+      for (int c = 0; c < 6; c++) wsm[((size_t)s * K + b) * 6 + c] += w[c];
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nsp * K * 6; q += blockDim.x) part[(size_t)blockIdx.x * nsp * K * 6 + q] = wsm[q];
+}
+
+__global__ void k_sum_partials(int64_t nblocks, int width, const double* __restrict__ part, double* __restrict__ out,
+                               double scale_add_base) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= width) return;
+  double s = scale_add_base;
+  for (int64_t b = 0; b < nblocks; b++) s += part[b * width + q];
+  out[q] = s;
+}
+
+// ycoef[s][z] = y_mult[z] * beta[s][y_jjb[z]]
+__global__ void k_ycoef(int nsp, int nz, int K, const double* __restrict__ ymult, const int32_t* __restrict__ yjjb,
+                        const double* __restrict__ beta, double* __restrict__ ycoef) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nsp * nz) return;
+  int s = t / nz, z = t - s * nz;
+  ycoef[t] = ymult[z] * beta[(size_t)s * K + yjjb[z]];
+}
+
+// Elementwise loss pieces: g = 2 (F - F_ref), per-atom |F - F_ref|^2.
+__global__ void k_loss_grad(int64_t n, const double* __restrict__ F, const double* __restrict__ Fref,
+                            double* __restrict__ g, double* __restrict__ li) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int c = 0; c < 3; c++) {
+    double d = F[3 * i + c] - Fref[3 * i + c];
+    g[3 * i + c] = 2.0 * d;
+    s += d * d;
+  }
+  li[i] = s;
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+struct ipg_snap {
+  ipg_ctx* ctx = nullptr;
+  ipg_snap_params p;
+  SnapHost h;
+  SnapDev dev;
+  void* d_tables = nullptr;
+  double* d_ymult = nullptr;
+  int32_t* d_yjjb = nullptr;
+  std::vector<double> cutsq;
+  double radius = 0.0;
+  int threads = 128;
+  int blocks_per_sm = 0;  // 0 = occupancy-derived
+  std::vector<double> beta_host;  // last uploaded beta
+};
+
+namespace {
+
+int upload_tables(ipg_snap* s) {
+  ipg_ctx* ctx = s->ctx;
+  SnapHost& h = s->h;
+  // one allocation: rootpq | cglist | ymult (doubles), idxz | db (structs), y_off | y_jjz | yjjb (ints)
+  auto pad = [](size_t b) { return (b + 255) & ~size_t(255); };
+  size_t o_rpq = 0;
+  size_t o_cg = o_rpq + pad(h.rootpq.size() * 8);
+  size_t o_ym = o_cg + pad(h.cglist.size() * 8);
+  size_t o_z = o_ym + pad(h.y_mult.size() * 8);
+  size_t o_db = o_z + pad(h.idxz.size() * sizeof(ZDev));
+  size_t o_yoff = o_db + pad(h.db.size() * sizeof(DBDev));
+  size_t o_yjjz = o_yoff + pad(h.y_off.size() * 4);
+  size_t o_yjjb = o_yjjz + pad(h.y_jjz.size() * 4);
+  size_t total = o_yjjb + pad(h.y_jjb.size() * 4);
+  CUDA_RET(ctx, cudaMalloc(&s->d_tables, total));
+  char* b = static_cast<char*>(s->d_tables);
+  std::vector<char> hostbuf(total, 0);
+  memcpy(hostbuf.data() + o_rpq, h.rootpq.data(), h.rootpq.size() * 8);
+  memcpy(hostbuf.data() + o_cg, h.cglist.data(), h.cglist.size() * 8);
+  memcpy(hostbuf.data() + o_ym, h.y_mult.data(), h.y_mult.size() * 8);
+  memcpy(hostbuf.data() + o_z, h.idxz.data(), h.idxz.size() * sizeof(ZDev));
+  memcpy(hostbuf.data() + o_db, h.db.data(), h.db.size() * sizeof(DBDev));
+  memcpy(hostbuf.data() + o_yoff, h.y_off.data(), h.y_off.size() * 4);
+  memcpy(hostbuf.data() + o_yjjz, h.y_jjz.data(), h.y_jjz.size() * 4);
+  memcpy(hostbuf.data() + o_yjjb, h.y_jjb.data(), h.y_jjb.size() * 4);
+  CUDA_RET(ctx, cudaMemcpy(b, hostbuf.data(), total, cudaMemcpyHostToDevice));
+  SnapDev& d = s->dev;
+  memset(&d, 0, sizeof(d));
+  d.J = h.J;
+  d.nsp = s->p.nspecies;
+  d.K = h.idxb_max;
+  d.idxu_max = h.idxu_max;
+  d.idxz_max = h.idxz_max;
+  d.u_half = h.u_half;
+  d.ext_max = h.ext_max;
+  d.idxcg_max = h.idxcg_max;
+  d.switch_flag = s->p.switch_flag;
+  d.bzero_flag = s->p.bzero_flag;
+  d.bnorm_flag = s->p.bnorm_flag;
+  d.rcutfac = s->p.rcutfac;
+  d.rmin0 = s->p.rmin0;
+  d.rfac0 = s->p.rfac0;
+  d.wself = 1.0;
+  for (int q = 0; q < s->p.nspecies; q++) {
+    d.radii[q] = s->p.radii[q];
+    d.weight[q] = s->p.weight[q];
+  }
+  for (int j = 0; j <= h.J; j++) {
+    d.idxu_block[j] = h.idxu_block[j];
+    d.bzero[j] = h.bzero[j];
+  }
+  for (int j = 0; j <= h.J + 1; j++) d.half_block[j] = h.half_block[j];
+  d.rootpq = reinterpret_cast<const double*>(b + o_rpq);
+  d.cglist = reinterpret_cast<const double*>(b + o_cg);
+  d.idxz = reinterpret_cast<const ZDev*>(b + o_z);
+  d.db = reinterpret_cast<const DBDev*>(b + o_db);
+  d.y_off = reinterpret_cast<const int32_t*>(b + o_yoff);
+  d.y_jjz = reinterpret_cast<const int32_t*>(b + o_yjjz);
+  s->d_ymult = reinterpret_cast<double*>(b + o_ym);
+  s->d_yjjb = reinterpret_cast<int32_t*>(b + o_yjjb);
+  return IPG_OK;
+}
+
+template <int MODE>
+int launch_atoms(ipg_snap* s, const SnapDev& dev, const SnapIO& io, int64_t natoms, int64_t* grid_used) {
+  ipg_ctx* ctx = s->ctx;
+  const int threads = s->threads;
+  SmemLayout L = smem_layout(dev, threads / 32, MODE);
+  size_t smem = L.total;
+  if (smem > 227 * 1024)
+    return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "twojmax %d needs %zu bytes of shared memory per block", dev.J, smem);
+  CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_atom<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = s->blocks_per_sm;
+  if (per_sm <= 0) {
+    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_atom<MODE>, threads, smem));
+    per_sm = std::max(1, per_sm);
+  }
+  int64_t grid = std::min<int64_t>(std::max<int64_t>(natoms, 1), (int64_t)ctx->num_sms * per_sm);
+  if (grid_used) *grid_used = grid;
+  IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_atom<MODE>, (unsigned)grid, threads, smem, dev, io);
+  return IPG_OK;
+}
+
+int set_beta(ipg_snap* s, const double* beta, SnapDev& dev) {
+  ipg_ctx* ctx = s->ctx;
+  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  double *d_beta, *d_ycoef;
+  IPG_RET(scratch(ctx, "snap_beta", (size_t)nsp * K, &d_beta));
+  IPG_RET(scratch(ctx, "snap_ycoef", (size_t)nsp * s->h.idxz_max, &d_ycoef));
+  std::vector<double> b(beta ? beta : nullptr, beta ? beta + (size_t)nsp * K : nullptr);
+  if (!beta) b.assign((size_t)nsp * K, 0.0);
+  double* hb = host_scratch<double>(ctx, "snap_beta_h", b.size());
+  memcpy(hb, b.data(), b.size() * 8);
+  CUDA_RET(ctx, cudaMemcpyAsync(d_beta, hb, b.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  IPG_LAUNCH(ctx, k_ycoef, nblk((int64_t)nsp * s->h.idxz_max, 256), 256, 0, nsp, s->h.idxz_max, K, s->d_ymult,
+             s->d_yjjb, d_beta, d_ycoef);
+  dev.beta = d_beta;
+  dev.ycoef = d_ycoef;
+  return IPG_OK;
+}
+
+int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
+                         const int64_t* h_atom_off, const double* h_L, PairList& pl);
+
+// Neighbor build for a set of configurations (device positions).
+int snap_neighbors(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
+                   const int64_t* h_atom_off, const double* h_L, PairList& pl) {
+  IPG_RET(ipg_timing_mark(s->ctx, "neighbor", true));
+  int st = snap_neighbors_inner(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl);
+  if (st) return st;
+  return ipg_timing_mark(s->ctx, "neighbor", false);
+}
+
+int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
+                         const int64_t* h_atom_off, const double* h_L, PairList& pl) {
+  CellList cl;
+  IPG_RET(ipg_build_cells(s->ctx, "snap_", n, d_pos, d_species, nconf, h_atom_off, h_L, s->radius, cl));
+  int mode = IPG_NLIST_FULL | (s->p.literal_sqrt_radius ? IPG_NLIST_LITERAL_SQRT : 0);
+  IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl));
+  return IPG_OK;
+}
+
+struct EvalOut {
+  double* E = nullptr;   // [nconf] device
+  double* F = nullptr;   // [3n] device
+  double* W6 = nullptr;  // [nconf][6] device
+  double* B = nullptr;   // [n][K] device
+  double* dB = nullptr;  // [n][K*nsp][3] device
+  double* Wd = nullptr;  // [K*nsp][6] device
+};
+
+// Energy / forces / descriptors for device inputs.  mode: MODE_DESC (B/E only), MODE_ADJ,
+// MODE_PLAIN.  Writes device outputs; does not synchronise.
+int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
+              const int64_t* h_atom_off, const double* h_L, const double* beta, double beta0, int mode,
+              const EvalOut& out) {
+  ipg_ctx* ctx = s->ctx;
+  SnapDev dev = s->dev;
+  IPG_RET(set_beta(s, beta, dev));
+  PairList pl;
+  IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl));
+  const int K = dev.K, nsp = dev.nsp;
+  const int64_t np = pl.npairs;
+  double *Ei, *fvec = nullptr, *dbl = nullptr, *w6 = nullptr;
+  IPG_RET(scratch(ctx, "snap_Ei", (size_t)n + 1, &Ei));
+  SnapIO io;
+  memset(&io, 0, sizeof(io));
+  io.n = n;
+  io.off = pl.d_off;
+  io.nbr = pl.d_j;
+  io.rij = pl.d_r;
+  io.species = d_species;
+  io.Ei = Ei;
+  io.B = out.B;
+  io.status = ctx->d_status;
+  const bool need_plain = (mode == MODE_PLAIN) || out.dB || out.Wd;
+  if (mode == MODE_ADJ) {
+    IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
+    io.fvec = fvec;
+    if (n) IPG_RET(launch_atoms<MODE_ADJ>(s, dev, io, n, nullptr));
+  } else if (need_plain) {
+    IPG_RET(scratch(ctx, "snap_dbl", (size_t)np * K * 3 + 3, &dbl));
+    io.dbl = dbl;
+    if (n) IPG_RET(launch_atoms<MODE_PLAIN>(s, dev, io, n, nullptr));
+    if (out.F || out.W6) {
+      IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
+      if (n) IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, dbl, dev.beta, K, fvec);
+    }
+  } else {
+    if (n) IPG_RET(launch_atoms<MODE_DESC>(s, dev, io, n, nullptr));
+  }
+  if (out.W6) IPG_RET(scratch(ctx, "snap_w6", 6 * (size_t)n + 6, &w6));
+  if ((out.F || out.W6) && fvec && n)
+    IPG_TIMED_LAUNCH(ctx, "snap_gather", k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off, pl.d_in_pair, fvec, d_pos,
+               out.F, w6);
+  if (out.E || out.W6) {
+    int64_t* d_aoff;
+    IPG_RET(scratch(ctx, "snap_aoff", (size_t)nconf + 1, &d_aoff));
+    int64_t* h = host_scratch<int64_t>(ctx, "snap_aoff_h", nconf + 1);
+    memcpy(h, h_atom_off, sizeof(int64_t) * (nconf + 1));
+    CUDA_RET(ctx, cudaMemcpyAsync(d_aoff, h, sizeof(int64_t) * (nconf + 1), cudaMemcpyHostToDevice, ctx->stream));
+    IPG_LAUNCH(ctx, k_conf_reduce, nconf, 128, 0, nconf, d_aoff, Ei, w6, beta0, out.E, out.W6);
+  }
+  if (out.dB && n) {
+    int32_t* owner;
+    IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
+    IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
+    IPG_LAUNCH(ctx, k_snap_dB_atoms, nblk(n * 3 * K, 128), 128, 0, n, K, nsp, pl.d_off, pl.d_in_off, pl.d_in_pair,
+               owner, d_species, dbl, out.dB);
+  }
+  if (out.Wd) {
+    const int width = nsp * K * 6;
+    int64_t grid = std::min<int64_t>(std::max<int64_t>(n, 1), 2 * ctx->num_sms);
+    double* part;
+    IPG_RET(scratch(ctx, "snap_wpart", (size_t)grid * width, &part));
+    size_t sm = (size_t)width * 8;
+    if (sm > 48 * 1024)
+      CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_W_desc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IPG_LAUNCH(ctx, k_snap_W_desc, (unsigned)grid, 64, sm, n, K, nsp, pl.d_off, pl.d_j, d_species, d_pos, dbl, part);
+    IPG_LAUNCH(ctx, k_sum_partials, nblk(width, 128), 128, 0, grid, width, part, out.Wd, 0.0);
+  }
+  return IPG_OK;
+}
+
+int check_common(ipg_snap* s, int64_t n, const void* pos, const void* species, const double* L) {
+  if (!s) return IPG_ERR_ARG;
+  if (n < 0 || n >= INT32_MAX) return ipg_fail(s->ctx, IPG_ERR_ARG, "n out of range");
+  if (n > 0 && (!pos || !species)) return ipg_fail(s->ctx, IPG_ERR_ARG, "null positions or species");
+  if (!L) return ipg_fail(s->ctx, IPG_ERR_ARG, "null box");
+  return IPG_OK;
+}
+
+int check_host_inputs(ipg_snap* s, int64_t n, const double* pos, const int32_t* species) {
+  for (int64_t k = 0; k < 3 * n; k++)
+    if (!std::isfinite(pos[k])) return ipg_fail(s->ctx, IPG_ERR_NONFINITE, "non-finite position");
+  for (int64_t k = 0; k < n; k++)
+    if (species[k] < 0 || species[k] >= s->p.nspecies) return ipg_fail(s->ctx, IPG_ERR_SPECIES, "species id out of range");
+  return IPG_OK;
+}
+
+int upload_inputs(ipg_snap* s, int64_t n, const double* pos, const int32_t* species, double** d_pos,
+                  int32_t** d_sp) {
+  ipg_ctx* ctx = s->ctx;
+  IPG_RET(scratch(ctx, "snap_in_pos", 3 * (size_t)n + 3, d_pos));
+  IPG_RET(scratch(ctx, "snap_in_sp", (size_t)n + 1, d_sp));
+  if (n) {
+    CUDA_RET(ctx, cudaMemcpyAsync(*d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_RET(ctx, cudaMemcpyAsync(*d_sp, species, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  return IPG_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+extern "C" {
+
+int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out) {
+  if (!ctx || !params || !out) return IPG_ERR_ARG;
+  *out = nullptr;
+  const ipg_snap_params& p = *params;
+  if (p.twojmax < 0 || p.twojmax > SNAP_MAX_J)
+    return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "twojmax must be in 0..%d", SNAP_MAX_J);
+  if (p.nspecies < 1 || p.nspecies > IPG_MAX_SNAP_SPECIES)
+    return ipg_fail(ctx, IPG_ERR_ARG, "nspecies must be in 1..%d", IPG_MAX_SNAP_SPECIES);
+  if (p.chem_flag != p.bnorm_flag)  // snap.jl:10-13
+    return ipg_fail(ctx, IPG_ERR_ARG, "chem_flag and bnorm_flag should be the same");
+  if (p.chem_flag) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "chem_flag is not built");
+  if (!(p.rcutfac > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "rcutfac must be > 0");
+  for (int q = 0; q < p.nspecies; q++)
+    if (!(p.radii[q] > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "radii must be > 0");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  ipg_snap* s = new ipg_snap();
+  s->ctx = ctx;
+  s->p = p;
+  if (snap_build_tables(p, s->h) != IPG_OK) {
+    delete s;
+    return ipg_fail(ctx, IPG_ERR_ARG, "bad SNAP parameters");
+  }
+  int st = upload_tables(s);
+  if (st) {
+    delete s;
+    return st;
+  }
+  // cutoffs, utl.jl:41-56
+  const int ns = p.nspecies;
+  s->cutsq.assign(ns * ns, 0.0);
+  double cutmax = 0.0;
+  for (int a = 0; a < ns; a++) {
+    double cut = 2.0 * p.radii[a] * p.rcutfac;
+    cutmax = std::max(cutmax, cut);
+    s->cutsq[a * ns + a] = cut * cut;
+    for (int b = a + 1; b < ns; b++) {
+      double c = (p.radii[a] + p.radii[b]) * p.rcutfac;
+      s->cutsq[a * ns + b] = c * c;
+      s->cutsq[b * ns + a] = c * c;
+    }
+  }
+  s->radius = p.literal_sqrt_radius ? std::sqrt(cutmax) : cutmax;
+  *out = s;
+  return IPG_OK;
+}
+
+int ipg_snap_destroy(ipg_snap* s) {
+  if (!s) return IPG_ERR_ARG;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  if (s->d_tables) cudaFree(s->d_tables);
+  delete s;
+  return IPG_OK;
+}
+
+int ipg_snap_ncoeff(const ipg_snap* s, int32_t* K) {
+  if (!s || !K) return IPG_ERR_ARG;
+  *K = s->h.idxb_max;
+  return IPG_OK;
+}
+
+int ipg_snap_descriptors(ipg_snap* s, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                         double* B, double* dB, double* W, uint32_t what) {
+  IPG_RET(check_common(s, n, pos, species, L));
+  ipg_ctx* ctx = s->ctx;
+  if (((what & IPG_DESC_B) && !B) || ((what & IPG_DESC_DB) && !dB && n) || ((what & IPG_DESC_W) && !W))
+    return ipg_fail(ctx, IPG_ERR_ARG, "requested descriptor output is NULL");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  IPG_RET(ipg_status_reset(ctx));
+  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  EvalOut o;
+  double *dB_d = nullptr, *B_d = nullptr, *W_d = nullptr;
+  if (what & IPG_DESC_B) IPG_RET(scratch(ctx, "snap_out_B", (size_t)n * K + 1, &B_d));
+  if (what & IPG_DESC_DB) IPG_RET(scratch(ctx, "snap_out_dB", (size_t)n * K * nsp * 3 + 1, &dB_d));
+  if (what & IPG_DESC_W) IPG_RET(scratch(ctx, "snap_out_W", (size_t)K * nsp * 6 + 1, &W_d));
+  o.B = B_d;
+  o.dB = dB_d;
+  o.Wd = W_d;
+  int64_t aoff[2] = {0, n};
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, nullptr, 0.0, MODE_DESC, o));
+  if (B_d && n) CUDA_RET(ctx, cudaMemcpyAsync(B, B_d, sizeof(double) * n * K, cudaMemcpyDeviceToHost, ctx->stream));
+  if (dB_d && n)
+    CUDA_RET(ctx, cudaMemcpyAsync(dB, dB_d, sizeof(double) * n * K * nsp * 3, cudaMemcpyDeviceToHost, ctx->stream));
+  if (W_d) {
+    if (n) CUDA_RET(ctx, cudaMemcpyAsync(W, W_d, sizeof(double) * K * nsp * 6, cudaMemcpyDeviceToHost, ctx->stream));
+    else memset(W, 0, sizeof(double) * K * nsp * 6);
+  }
+  return ipg_status_check(ctx, "ipg_snap_descriptors");
+}
+
+int ipg_snap_energy_forces_dev(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species,
+                               const double L[3], const double* beta, double beta0, int32_t mode, double* d_E,
+                               double* d_F, double* d_W6) {
+  IPG_RET(check_common(s, n, d_pos, d_species, L));
+  ipg_ctx* ctx = s->ctx;
+  if (mode != IPG_SNAP_PLAIN && mode != IPG_SNAP_ADJOINT) return ipg_fail(ctx, IPG_ERR_ARG, "bad mode");
+  if (!beta) return ipg_fail(ctx, IPG_ERR_ARG, "null beta");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(ipg_status_reset(ctx));
+  EvalOut o;
+  o.E = d_E;
+  o.F = d_F;
+  o.W6 = d_W6;
+  int64_t aoff[2] = {0, n};
+  IPG_RET(snap_eval(s, n, d_pos, d_species, 1, aoff, L, beta, beta0,
+                    mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN, o));
+  return ipg_status_check(ctx, "ipg_snap_energy_forces_dev");
+}
+
+int ipg_snap_energy_forces(ipg_snap* s, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                           const double* beta, double beta0, int32_t mode, double* E, double* F, double* W6) {
+  IPG_RET(check_common(s, n, pos, species, L));
+  ipg_ctx* ctx = s->ctx;
+  if (mode != IPG_SNAP_PLAIN && mode != IPG_SNAP_ADJOINT) return ipg_fail(ctx, IPG_ERR_ARG, "bad mode");
+  if (!beta) return ipg_fail(ctx, IPG_ERR_ARG, "null beta");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  IPG_RET(ipg_status_reset(ctx));
+  double* d_out;  // [E, W6(6), pad, F(3n)]
+  IPG_RET(scratch(ctx, "snap_out_EF", 3 * (size_t)n + 8, &d_out));
+  EvalOut o;
+  o.E = d_out;
+  o.W6 = d_out + 1;
+  o.F = F ? d_out + 8 : nullptr;
+  int64_t aoff[2] = {0, n};
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, beta0, mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN,
+                    o));
+  double head[8];
+  CUDA_RET(ctx, cudaMemcpyAsync(head, d_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (F && n) CUDA_RET(ctx, cudaMemcpyAsync(F, d_out + 8, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  IPG_RET(ipg_status_check(ctx, "ipg_snap_energy_forces"));
+  if (E) *E = head[0];
+  if (W6) memcpy(W6, head + 1, 6 * sizeof(double));
+  return IPG_OK;
+}
+
+}  // extern "C"
+
+// Entry points that need the VJP kernel and batching live below, sharing the helpers.
+namespace {
+
+// gbeta = sum over blocks of the VJP partials (device), for device inputs already
+// resident.  g = cotangent of forces [3n] (device), gE scalar.
+int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
+                    const int64_t* h_atom_off, const double* h_L, const double* beta, double gE, const double* d_g,
+                    double* d_gbeta) {
+  ipg_ctx* ctx = s->ctx;
+  SnapDev dev = s->dev;
+  IPG_RET(set_beta(s, beta, dev));
+  PairList pl;
+  IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl));
+  const int K = dev.K, nsp = dev.nsp;
+  double* Ei;
+  IPG_RET(scratch(ctx, "snap_Ei", (size_t)n + 1, &Ei));
+  SnapIO io;
+  memset(&io, 0, sizeof(io));
+  io.n = n;
+  io.off = pl.d_off;
+  io.nbr = pl.d_j;
+  io.rij = pl.d_r;
+  io.species = d_species;
+  io.Ei = Ei;
+  io.g = d_g;
+  io.gE = gE;
+  io.status = ctx->d_status;
+  int threads = s->threads;
+  SmemLayout L = smem_layout(dev, threads / 32, MODE_VJP);
+  int per_sm = 1;
+  CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_atom<MODE_VJP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_atom<MODE_VJP>, threads, L.total));
+  int64_t grid = std::min<int64_t>(std::max<int64_t>(n, 1), (int64_t)ctx->num_sms * std::max(1, per_sm));
+  double* gpart;
+  IPG_RET(scratch(ctx, "snap_gpart", (size_t)grid * nsp * K, &gpart));
+  io.gpart = gpart;
+  if (n) {
+    IPG_RET(launch_atoms<MODE_VJP>(s, dev, io, n, &grid));
+    IPG_LAUNCH(ctx, k_sum_partials, nblk((int64_t)nsp * K, 128), 128, 0, grid, nsp * K, gpart, d_gbeta, 0.0);
+  } else {
+    CUDA_RET(ctx, cudaMemsetAsync(d_gbeta, 0, sizeof(double) * nsp * K, ctx->stream));
+  }
+  return IPG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipg_snap_vjp_beta(ipg_snap* s, int64_t n, const double* pos, const int32_t* species, const double L[3], double gE,
+                      const double* gF, double* gbeta, double* gbeta0) {
+  IPG_RET(check_common(s, n, pos, species, L));
+  ipg_ctx* ctx = s->ctx;
+  if (!gbeta) return ipg_fail(ctx, IPG_ERR_ARG, "null gbeta");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  IPG_RET(ipg_status_reset(ctx));
+  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  double *d_g, *d_gb;
+  IPG_RET(scratch(ctx, "snap_vjp_g", 3 * (size_t)n + 3, &d_g));
+  IPG_RET(scratch(ctx, "snap_vjp_gb", (size_t)nsp * K, &d_gb));
+  if (n) {
+    if (gF) CUDA_RET(ctx, cudaMemcpyAsync(d_g, gF, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+    else CUDA_RET(ctx, cudaMemsetAsync(d_g, 0, sizeof(double) * 3 * n, ctx->stream));
+  }
+  int64_t aoff[2] = {0, n};
+  std::vector<double> zero_beta((size_t)nsp * K, 0.0);
+  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, 1, aoff, L, zero_beta.data(), gE, d_g, d_gb));
+  CUDA_RET(ctx, cudaMemcpyAsync(gbeta, d_gb, sizeof(double) * nsp * K, cudaMemcpyDeviceToHost, ctx->stream));
+  IPG_RET(ipg_status_check(ctx, "ipg_snap_vjp_beta"));
+  if (gbeta0) *gbeta0 = gE;
+  return IPG_OK;
+}
+
+int ipg_snap_batch_energy_forces_dev(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* d_pos,
+                                     const int32_t* d_species, const double* L, const double* beta, double beta0,
+                                     int32_t mode, int32_t graph, double* d_E, double* d_F, double* d_W6) {
+  if (!s || nconfig < 1 || !atom_offsets || !L || !beta) return s ? ipg_fail(s->ctx, IPG_ERR_ARG, "bad batch args") : IPG_ERR_ARG;
+  ipg_ctx* ctx = s->ctx;
+  if (mode != IPG_SNAP_PLAIN && mode != IPG_SNAP_ADJOINT) return ipg_fail(ctx, IPG_ERR_ARG, "bad mode");
+  if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
+  for (int c = 0; c < nconfig; c++)
+    if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
+  (void)graph;
+  int64_t n = atom_offsets[nconfig];
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(ipg_status_reset(ctx));
+  EvalOut o;
+  o.E = d_E;
+  o.F = d_F;
+  o.W6 = d_W6;
+  IPG_RET(snap_eval(s, n, d_pos, d_species, nconfig, atom_offsets, L, beta, beta0,
+                    mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN, o));
+  return ipg_status_check(ctx, "ipg_snap_batch_energy_forces_dev");
+}
+
+int ipg_snap_batch_energy_forces(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
+                                 const int32_t* species, const double* L, const double* beta, double beta0,
+                                 int32_t mode, double* E, double* F, double* W6) {
+  if (!s || nconfig < 1 || !atom_offsets || !L || !beta) return s ? ipg_fail(s->ctx, IPG_ERR_ARG, "bad batch args") : IPG_ERR_ARG;
+  ipg_ctx* ctx = s->ctx;
+  if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
+  for (int c = 0; c < nconfig; c++)
+    if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
+  int64_t n = atom_offsets[nconfig];
+  IPG_RET(check_common(s, n, pos, species, L));
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  double* d_out;  // [E(nconf), W6(6 nconf), F(3n)]
+  IPG_RET(scratch(ctx, "snap_out_batch", 7 * (size_t)nconfig + 3 * (size_t)n + 2, &d_out));
+  IPG_RET(ipg_status_reset(ctx));
+  EvalOut o;
+  o.E = d_out;
+  o.W6 = d_out + nconfig;
+  o.F = F ? d_out + 7 * nconfig : nullptr;
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, beta0,
+                    mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN, o));
+  if (E) CUDA_RET(ctx, cudaMemcpyAsync(E, d_out, sizeof(double) * nconfig, cudaMemcpyDeviceToHost, ctx->stream));
+  if (W6) CUDA_RET(ctx, cudaMemcpyAsync(W6, d_out + nconfig, sizeof(double) * 6 * nconfig, cudaMemcpyDeviceToHost, ctx->stream));
+  if (F && n) CUDA_RET(ctx, cudaMemcpyAsync(F, d_out + 7 * nconfig, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return ipg_status_check(ctx, "ipg_snap_batch_energy_forces");
+}
+
+int ipg_snap_batch_loss_grad(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
+                             const int32_t* species, const double* L, const double* beta, double beta0,
+                             const double* F_ref, double* loss, double* gbeta) {
+  if (!s || nconfig < 1 || !atom_offsets || !L || !beta || !F_ref || !loss || !gbeta)
+    return s ? ipg_fail(s->ctx, IPG_ERR_ARG, "bad batch args") : IPG_ERR_ARG;
+  ipg_ctx* ctx = s->ctx;
+  if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
+  for (int c = 0; c < nconfig; c++)
+    if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
+  int64_t n = atom_offsets[nconfig];
+  IPG_RET(check_common(s, n, pos, species, L));
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  double *d_F, *d_Fref, *d_g, *d_li, *d_gb, *d_l;
+  IPG_RET(scratch(ctx, "loss_F", 3 * (size_t)n + 3, &d_F));
+  IPG_RET(scratch(ctx, "loss_Fref", 3 * (size_t)n + 3, &d_Fref));
+  IPG_RET(scratch(ctx, "loss_g", 3 * (size_t)n + 3, &d_g));
+  IPG_RET(scratch(ctx, "loss_li", (size_t)n + 1, &d_li));
+  IPG_RET(scratch(ctx, "loss_gb", (size_t)nsp * K, &d_gb));
+  IPG_RET(scratch(ctx, "loss_l", 1, &d_l));
+  if (n) CUDA_RET(ctx, cudaMemcpyAsync(d_Fref, F_ref, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  IPG_RET(ipg_status_reset(ctx));
+  EvalOut o;
+  o.F = d_F;
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, beta0, MODE_ADJ, o));
+  if (n) {
+    IPG_LAUNCH(ctx, k_loss_grad, nblk(n, 256), 256, 0, n, d_F, d_Fref, d_g, d_li);
+    IPG_LAUNCH(ctx, k_sum_partials, 1, 32, 0, n, 1, d_li, d_l, 0.0);
+  } else {
+    CUDA_RET(ctx, cudaMemsetAsync(d_l, 0, sizeof(double), ctx->stream));
+  }
+  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, 0.0, d_g, d_gb));
+  CUDA_RET(ctx, cudaMemcpyAsync(gbeta, d_gb, sizeof(double) * nsp * K, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_RET(ctx, cudaMemcpyAsync(loss, d_l, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  (void)beta0;
+  return ipg_status_check(ctx, "ipg_snap_batch_loss_grad");
+}
+
+}  // extern "C"

@@ -1,0 +1,58 @@
+// ipg_snap.cuh — SNAP tables and device-side descriptor of a SNAP basis.
+#pragma once
+
+#include "ipg_internal.cuh"
+
+// One Z entry (one (j1, j2, j, ma, mb) of the idxz list, prebuilt_arrays.jl:183-216),
+// with the start offsets of its CG double sum precomputed.
+struct ZDev {
+  int16_t j1, j2, j, na, nb, pad;
+  int32_t u1base;  // idxu_block[j1] + (j1+1)*mb1min + ma1min
+  int32_t u2base;  // idxu_block[j2] + (j2+1)*mb2max + ma2max
+  int32_t icga0;   // ma1min*(j2+1) + ma2max
+  int32_t icgb0;   // mb1min*(j2+1) + mb2max
+  int32_t cgoff;   // idxcg_block[j1][j2][j]
+};
+
+// One bispectrum component (j1, j2, j) and the three half-plane sums of its
+// derivative (compute_b.jl:207-400): level l[t], first Z index z0[t], factor fac[t].
+struct DBDev {
+  int32_t l[3];
+  int32_t z0[3];
+  double fac[3];
+};
+
+constexpr int SNAP_MAX_J = 12;
+
+struct SnapDev {
+  int J, nsp, K, idxu_max, idxz_max, u_half, ext_max, idxcg_max;
+  int switch_flag, bzero_flag, bnorm_flag, pad;
+  double rcutfac, rmin0, rfac0, wself;
+  double radii[IPG_MAX_SNAP_SPECIES], weight[IPG_MAX_SNAP_SPECIES];
+  int idxu_block[SNAP_MAX_J + 2];
+  int half_block[SNAP_MAX_J + 2];
+  double bzero[SNAP_MAX_J + 1];
+  const double* rootpq;  // [(J+2)*(J+2)]
+  const double* cglist;  // [idxcg_max]
+  const ZDev* idxz;      // [idxz_max]
+  const DBDev* db;       // [K]
+  const int32_t* y_off;  // [u_half+1]  CSR: Z entries feeding each half-plane Y entry
+  const int32_t* y_jjz;  // [idxz_max]
+  const double* ycoef;   // [nsp][idxz_max] multiplicity * factor * beta (set per beta)
+  const double* beta;    // [nsp][K]
+};
+
+struct SnapHost {
+  int J = 0, idxu_max = 0, idxz_max = 0, idxb_max = 0, idxcg_max = 0, u_half = 0, ext_max = 0;
+  std::vector<int> idxu_block, half_block, idxcg_block, idxz_block, idxb_block;
+  std::vector<int> idxb;  // 3 per component
+  std::vector<ZDev> idxz;
+  std::vector<int> zjju_half;  // half-plane index of each Z entry
+  std::vector<DBDev> db;
+  std::vector<double> cglist, rootpq, bzero;
+  std::vector<int32_t> y_off, y_jjz;
+  std::vector<int32_t> y_jjb;     // component whose beta scales each Z entry in Y
+  std::vector<double> y_mult;     // multiplicity * (j1+1)/(j+1) factor of each Z entry
+};
+
+int snap_build_tables(const ipg_snap_params& p, SnapHost& h);

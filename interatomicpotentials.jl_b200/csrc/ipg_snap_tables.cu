@@ -1,0 +1,196 @@
+// ipg_snap_tables.cpp — host construction of the SNAP index and Clebsch–Gordan tables.
+//
+// The tables are those of initialize_prebuilt_arrays
+// (src/BasisSystems/SNAP/types/prebuilt_arrays.jl:48-321): the same enumeration order of
+// (j1 >= j2, j = |j1-j2|..min(J, j1+j2) step 2) blocks, the same CG coefficients (factorial
+// sums, :250-312) and sqrt(p/q) roots (:314-321), because the descriptors are defined by
+// that ordering.  Derived tables (half-plane offsets, the Y gather list, the dB term list)
+// are new and serve the CUDA kernels.
+#include <cmath>
+
+#include "ipg_snap.cuh"
+
+namespace {
+
+// Factorials as long double (64-bit mantissa): exact wherever the reference's Int64
+// products are exact (twojmax <= 8), and free of Int64 overflow beyond that.
+long double fact(int n) {
+  long double f = 1.0L;
+  for (int k = 2; k <= n; k++) f *= k;
+  return f;
+}
+
+// prebuilt_arrays.jl:250-257
+double delta_cg(int j1, int j2, int j) {
+  long double den = fact((j1 + j2 + j) / 2 + 1);
+  long double num = fact((j1 + j2 - j) / 2) * fact((j1 - j2 + j) / 2) * fact((-j1 + j2 + j) / 2);
+  return std::sqrt((double)num / (double)den);
+}
+
+}  // namespace
+
+int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
+  const int J = p.twojmax;
+  if (J < 0 || J > SNAP_MAX_J) return IPG_ERR_ARG;
+  const int jd = J + 1;
+  h.J = J;
+  auto blk = [jd](int a, int b, int c) { return (a * jd + b) * jd + c; };
+  h.idxcg_block.assign(jd * jd * jd, -1);
+  h.idxz_block.assign(jd * jd * jd, -1);
+  h.idxb_block.assign(jd * jd * jd, -1);
+  h.idxu_block.assign(jd, 0);
+  h.half_block.assign(jd + 1, 0);
+
+  int cnt = 0;
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2) {
+        h.idxcg_block[blk(j1, j2, j)] = cnt;
+        cnt += (j1 + 1) * (j2 + 1);
+      }
+  h.idxcg_max = cnt;
+
+  cnt = 0;
+  for (int j = 0; j <= J; j++) {
+    h.idxu_block[j] = cnt;
+    cnt += (j + 1) * (j + 1);
+  }
+  h.idxu_max = cnt;
+
+  // half plane: rows mb = 0..j/2 of every level
+  cnt = 0;
+  h.ext_max = 1;
+  for (int j = 0; j <= J; j++) {
+    h.half_block[j] = cnt;
+    cnt += (j / 2 + 1) * (j + 1);
+    h.ext_max = std::max(h.ext_max, ((j + 1) / 2 + 1) * (j + 1));
+  }
+  h.half_block[jd] = cnt;
+  h.u_half = cnt;
+
+  h.idxb.clear();
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2)
+        if (j >= j1) {
+          h.idxb_block[blk(j1, j2, j)] = (int)h.idxb.size() / 3;
+          h.idxb.push_back(j1);
+          h.idxb.push_back(j2);
+          h.idxb.push_back(j);
+        }
+  h.idxb_max = (int)h.idxb.size() / 3;
+
+  h.idxz.clear();
+  h.zjju_half.clear();
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2) {
+        h.idxz_block[blk(j1, j2, j)] = (int)h.idxz.size();
+        for (int mb = 0; 2 * mb <= j; mb++)
+          for (int ma = 0; ma <= j; ma++) {
+            int ma1min = std::max(0, (2 * ma - j - j2 + j1) / 2);
+            int ma2max = (2 * ma - j - (2 * ma1min - j1) + j2) / 2;
+            int na = std::min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
+            int mb1min = std::max(0, (2 * mb - j - j2 + j1) / 2);
+            int mb2max = (2 * mb - j - (2 * mb1min - j1) + j2) / 2;
+            int nb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
+            ZDev z;
+            z.j1 = (int16_t)j1;
+            z.j2 = (int16_t)j2;
+            z.j = (int16_t)j;
+            z.na = (int16_t)na;
+            z.nb = (int16_t)nb;
+            z.pad = 0;
+            z.u1base = h.idxu_block[j1] + (j1 + 1) * mb1min + ma1min;
+            z.u2base = h.idxu_block[j2] + (j2 + 1) * mb2max + ma2max;
+            z.icga0 = ma1min * (j2 + 1) + ma2max;
+            z.icgb0 = mb1min * (j2 + 1) + mb2max;
+            z.cgoff = h.idxcg_block[blk(j1, j2, j)];
+            h.idxz.push_back(z);
+            h.zjju_half.push_back(h.half_block[j] + (j + 1) * mb + ma);
+          }
+      }
+  h.idxz_max = (int)h.idxz.size();
+
+  h.rootpq.assign((J + 2) * (J + 2), 0.0);
+  for (int a = 1; a <= J; a++)
+    for (int b = 1; b <= J; b++) h.rootpq[a * (J + 2) + b] = std::sqrt((double)a / (double)b);
+
+  h.cglist.assign(h.idxcg_max, 0.0);
+  int idx = 0;
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2)
+        for (int m1 = 0; m1 <= j1; m1++) {
+          int aa2 = 2 * m1 - j1;
+          for (int m2 = 0; m2 <= j2; m2++, idx++) {
+            int bb2 = 2 * m2 - j2;
+            int m = (aa2 + bb2 + j) / 2;
+            if (m < 0 || m > j) continue;
+            double sum = 0.0;
+            int zmin = std::max(0, std::max(-(j - j2 + aa2) / 2, -(j - j1 - bb2) / 2));
+            int zmax = std::min((j1 + j2 - j) / 2, std::min((j1 - aa2) / 2, (j2 + bb2) / 2));
+            for (int z = zmin; z <= zmax; z++) {
+              long double den = fact(z) * fact((j1 + j2 - j) / 2 - z) * fact((j1 - aa2) / 2 - z) * fact((j2 + bb2) / 2 - z) *
+                            fact((j - j2 + aa2) / 2 + z) * fact((j - j1 - bb2) / 2 + z);
+              sum += ((z % 2 == 0) ? 1.0 : -1.0) / (double)den;
+            }
+            int cc2 = 2 * m - j;
+            long double sf = fact((j1 + aa2) / 2) * fact((j1 - aa2) / 2) * fact((j2 + bb2) / 2) * fact((j2 - bb2) / 2) *
+                         fact((j + cc2) / 2) * fact((j - cc2) / 2) * (long double)(j + 1);
+            h.cglist[idx] = sum * delta_cg(j1, j2, j) * std::sqrt((double)sf);
+          }
+        }
+
+  // bzero (prebuilt_arrays.jl:52-63); wself = 1
+  h.bzero.assign(jd, 0.0);
+  if (p.bzero_flag)
+    for (int j = 0; j <= J; j++) h.bzero[j] = p.bnorm_flag ? 1.0 : (double)(j + 1);
+
+  // dB terms (compute_b.jl:207-400): Z(j1,j2,j) on level j, (j+1)/(j1+1) Z(j,j2,j1) on
+  // level j1, (j+1)/(j2+1) Z(j,j1,j2) on level j2 (factors dropped when bnorm_flag).
+  h.db.resize(h.idxb_max);
+  for (int b = 0; b < h.idxb_max; b++) {
+    int j1 = h.idxb[3 * b], j2 = h.idxb[3 * b + 1], j = h.idxb[3 * b + 2];
+    DBDev& d = h.db[b];
+    d.l[0] = j;
+    d.z0[0] = h.idxz_block[blk(j1, j2, j)];
+    d.fac[0] = 1.0;
+    d.l[1] = j1;
+    d.z0[1] = h.idxz_block[blk(j, j2, j1)];
+    d.fac[1] = p.bnorm_flag ? 1.0 : (j + 1) / (j1 + 1.0);
+    d.l[2] = j2;
+    d.z0[2] = h.idxz_block[blk(j, j1, j2)];
+    d.fac[2] = p.bnorm_flag ? 1.0 : (j + 1) / (j2 + 1.0);
+  }
+
+  // Y = d(beta . B)/dU (design of compute_yi.jl:86-118): each Z entry (J1,J2,J,ma,mb)
+  // feeds Y(J,ma,mb) with weight beta[jjb] times multiplicity and (J1+1)/(J+1).
+  h.y_jjb.assign(h.idxz_max, 0);
+  h.y_mult.assign(h.idxz_max, 0.0);
+  for (int z = 0; z < h.idxz_max; z++) {
+    int j1 = h.idxz[z].j1, j2 = h.idxz[z].j2, j = h.idxz[z].j;
+    int jjb;
+    double mult;
+    if (j >= j1) {
+      jjb = h.idxb_block[blk(j1, j2, j)];
+      mult = (j1 == j) ? ((j2 == j) ? 3.0 : 2.0) : 1.0;
+    } else if (j >= j2) {
+      jjb = h.idxb_block[blk(j, j2, j1)];
+      mult = (j2 == j) ? 2.0 : 1.0;
+    } else {
+      jjb = h.idxb_block[blk(j2, j, j1)];
+      mult = 1.0;
+    }
+    if (!p.bnorm_flag && j1 > j) mult *= (j1 + 1) / (j + 1.0);
+    h.y_jjb[z] = jjb;
+    h.y_mult[z] = mult;
+  }
+  h.y_off.assign(h.u_half + 1, 0);
+  for (int z = 0; z < h.idxz_max; z++) h.y_off[h.zjju_half[z] + 1]++;
+  for (int q = 0; q < h.u_half; q++) h.y_off[q + 1] += h.y_off[q];
+  h.y_jjz.assign(h.idxz_max, 0);
+  std::vector<int32_t> fill(h.y_off.begin(), h.y_off.end() - 1);
+  for (int z = 0; z < h.idxz_max; z++) h.y_jjz[fill[h.zjju_half[z]]++] = z;
+  return IPG_OK;
+}

@@ -1,0 +1,65 @@
+"""Batched SNAP (many configurations per launch) and the force-matching loss gradient."""
+import numpy as np
+import pytest
+
+import oracle
+import ipg
+from ipg import workloads as W
+from conftest import TOL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch():
+    systems = W.batch512(nconf=24, nmin=32, nmax=400)
+    prm = W.snap_j8_params()
+    snap = ipg.SNAP(1, prm["twojmax"], prm["species"], prm["rcutfac"], prm["rmin0"], prm["rfac0"], prm["radii"],
+                    prm["weight"], switch_flag=True)
+    orc = oracle.Snap(prm["twojmax"], prm["radii"], prm["weight"], prm["rcutfac"], prm["rmin0"], prm["rfac0"],
+                      switch=True)
+    beta = np.random.default_rng(5).normal(0, 1e-2, (2, len(snap)))
+    return systems, snap, orc, beta
+
+
+@pytest.mark.parametrize("mode", ["adjoint", "plain"])
+def test_batch_matches_single_and_oracle(batch, mode):
+    systems, snap, orc, beta = batch
+    E, F, Wv = snap.batch_energy_forces(systems, beta, 0.1, mode=mode)
+    off = np.concatenate([[0], np.cumsum([len(s) for s in systems])])
+    for c, s in enumerate(systems):
+        eo, fo, wo = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.1)
+        assert abs(E[c] - eo) <= TOL * abs(eo)
+        assert rel_err(F[off[c]:off[c + 1]], fo) <= TOL
+        assert rel_err(Wv[c], wo) <= TOL
+        if c < 3:
+            e1, f1, w1 = snap.energy_forces(s, beta, 0.1, mode=mode)
+            assert abs(E[c] - e1) <= 1e-13 * abs(e1)
+            assert rel_err(F[off[c]:off[c + 1]], f1) <= 1e-13
+
+
+def test_loss_gradient(batch):
+    systems, snap, orc, beta = batch
+    rng = np.random.default_rng(6)
+    beta_ref = beta + rng.normal(0, 1e-3, beta.shape)
+    _, Fref, _ = snap.batch_energy_forces(systems, beta_ref, 0.0)
+    Fref = Fref + rng.normal(0, 0.01, Fref.shape)
+    loss, g = snap.batch_loss_grad(systems, beta, Fref)
+    _, F, _ = snap.batch_energy_forces(systems, beta, 0.0)
+    assert abs(loss - np.sum((F - Fref) ** 2)) <= 1e-12 * loss
+    # oracle: dL/dbeta = sum_k 2 (F_k - Fref_k) . dF_k/dbeta, per configuration
+    off = np.concatenate([[0], np.cumsum([len(s) for s in systems])])
+    go = np.zeros_like(g)
+    for c, s in enumerate(systems):
+        gF = 2.0 * (F[off[c]:off[c + 1]] - Fref[off[c]:off[c + 1]])
+        gb, _ = orc.vjp_beta(s.positions, snap.species_ids(s), s.L, 0.0, gF)
+        go += gb
+    assert rel_err(g, go) <= TOL
+    # L is quadratic in beta: central differences are exact up to rounding
+    h = 1e-4
+    for (s_, k) in [(0, 0), (1, 7), (0, 54)]:
+        bp = beta.copy(); bp[s_, k] += h
+        bm = beta.copy(); bm[s_, k] -= h
+        lp = snap.batch_loss_grad(systems, bp, Fref)[0]
+        lm = snap.batch_loss_grad(systems, bm, Fref)[0]
+        assert abs((lp - lm) / (2 * h) - g[s_, k]) <= 1e-6 * np.abs(g).max()

@@ -1,0 +1,220 @@
+"""GPU SNAP vs the oracle (restatement of src/BasisSystems/SNAP/**), FP64, 1e-10 relative.
+
+SNAP has no stored reference outputs (its tests compare against live LAMMPS and are
+disabled, test/runtests.jl:46-50), so besides oracle parity the tests pin known
+answers: the isolated-atom bispectrum, rotation/permutation invariance, sum of forces,
+finite differences of the energy, and adjoint == plain.
+"""
+import numpy as np
+import pytest
+from scipy.spatial.transform import Rotation
+
+import oracle
+import ipg
+from ipg import workloads as W
+from conftest import TOL, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def make(prm, **kw):
+    """GPU SNAP and oracle SNAP with the same parameters."""
+    p = dict(prm)
+    p.update(kw)
+    snap = ipg.SNAP(1, p["twojmax"], p["species"], p["rcutfac"], p["rmin0"], p["rfac0"], p["radii"], p["weight"],
+                    bzero_flag=p.get("bzero_flag", False), switch_flag=p.get("switch_flag", False),
+                    literal_sqrt_radius=p.get("literal", False))
+    orc = oracle.Snap(p["twojmax"], p["radii"], p["weight"], p["rcutfac"], p["rmin0"], p["rfac0"],
+                      bzero=p.get("bzero_flag", False), bnorm=False, switch=p.get("switch_flag", False),
+                      literal_sqrt=p.get("literal", False))
+    return snap, orc
+
+
+def fixture_system(golden, tag):
+    return ipg.System(golden[f"snap_{tag}_pos"], list(golden[f"snap_{tag}_symbols"]), golden[f"snap_{tag}_box"],
+                      (False, False, False))
+
+
+def fixture_params(golden, tag):
+    return dict(twojmax=int(golden[f"snap_{tag}_twojmax"]), species=list(golden[f"snap_{tag}_species"]),
+                rcutfac=float(golden[f"snap_{tag}_rcutfac"]), rmin0=0.0, rfac0=float(golden[f"snap_{tag}_rfac0"]),
+                radii=list(golden[f"snap_{tag}_radii"]), weight=list(golden[f"snap_{tag}_weight"]))
+
+
+def check_descriptors(s, snap, orc):
+    B, dB, Wd = ipg.compute_all_descriptors(s, snap)
+    Bo, dBo, Wo = orc.descriptors(s.positions, snap.species_ids(s), s.L)
+    assert rel_err(B, Bo) <= TOL
+    assert rel_err(dB, dBo.transpose(0, 2, 1)) <= TOL
+    assert rel_err(Wd, Wo.T) <= TOL
+    assert rel_err(ipg.compute_local_descriptors(s, snap), Bo) <= TOL
+    assert rel_err(ipg.compute_force_descriptors(s, snap), dBo.transpose(0, 2, 1)) <= TOL
+    return B, dB, Wd
+
+
+@pytest.mark.parametrize("tag", ["single", "multi"])
+@pytest.mark.parametrize("literal", [False, True])
+def test_reference_fixture_3atoms(golden, tag, literal):
+    """test/SNAP/snap_test_{single,multi}_element.jl inputs (all pairs inside sqrt(cutmax))."""
+    s = fixture_system(golden, tag)
+    prm = fixture_params(golden, tag)
+    snap, orc = make(prm, literal=literal)
+    check_descriptors(s, snap, orc)
+
+
+@pytest.mark.parametrize("flags", [dict(), dict(bzero_flag=True), dict(switch_flag=True)])
+def test_fixture_flags(golden, flags):
+    s = fixture_system(golden, "multi")
+    snap, orc = make(fixture_params(golden, "multi"), **flags)
+    check_descriptors(s, snap, orc)
+
+
+def test_isolated_atom_closed_form():
+    """Utot = wself*I gives B(j1,j2,j) = j+1 (and 0 with bzero)."""
+    for J in (2, 4, 6, 8):
+        snap = ipg.SNAP(1, J, ["X"], 1.0, 0.0, 0.99363, [0.5], [1.0])
+        s = ipg.System([[0.0, 0.0, 0.0]], ["X"], [10.0] * 3, (False, False, False))
+        B = ipg.compute_local_descriptors(s, snap)[0]
+        orc = oracle.Snap(J, [0.5], [1.0], 1.0, 0.0, 0.99363)
+        jj = orc.index_tables()["idxb"][:, 2]
+        np.testing.assert_allclose(B, (jj + 1).astype(float), rtol=1e-13, atol=0)
+        snap0 = ipg.SNAP(1, J, ["X"], 1.0, 0.0, 0.99363, [0.5], [1.0], bzero_flag=True)
+        assert np.all(np.abs(ipg.compute_local_descriptors(s, snap0)) <= 1e-12)
+
+
+@pytest.mark.parametrize("J", [2, 3, 5, 6, 8, 10])
+def test_random_cluster_all_J(J):
+    rng = np.random.default_rng(J)
+    pos = rng.uniform(0, 6, (24, 3))
+    s = ipg.System(pos, list(np.where(rng.random(24) < 0.5, "A", "B")), [6.0] * 3, (True, True, False))
+    snap, orc = make(dict(twojmax=J, species=["A", "B"], rcutfac=2.0, rmin0=0.2, rfac0=0.97, radii=[1.0, 0.8],
+                          weight=[1.0, 0.7], switch_flag=True))
+    check_descriptors(s, snap, orc)
+
+
+def test_snap_j6_config_plain_parity():
+    """Config 3 (twojmax 6, BCC 16^3 = 8192 atoms): E and F through the plain dB/dr path."""
+    s, prm, beta = W.snap_j6()
+    snap, orc = make(prm)
+    e, f, w = snap.energy_forces(s, beta, 0.0, mode="plain")
+    eo, fo, wo = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.0, mode="plain")
+    assert abs(e - eo) <= TOL * abs(eo)
+    assert rel_err(f, fo) <= TOL
+    assert rel_err(w, wo) <= TOL
+    ea, fa, wa = snap.energy_forces(s, beta, 0.0, mode="adjoint")
+    assert abs(ea - eo) <= TOL * abs(eo)
+    assert rel_err(fa, fo) <= TOL
+    assert rel_err(wa, wo) <= TOL
+
+
+@pytest.mark.parametrize("mode", ["plain", "adjoint"])
+def test_snap_j8_two_species_parity(mode):
+    """Config 4 at reduced size (BCC 8^3 = 1024 atoms), per-species beta blocks."""
+    s, prm, beta = W.snap_j8(cells=8)
+    snap, orc = make(prm)
+    e, f, w = snap.energy_forces(s, beta, 0.25, mode=mode)
+    eo, fo, wo = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.25, mode="plain")
+    assert abs(e - eo) <= TOL * abs(eo)
+    assert rel_err(f, fo) <= TOL
+    assert rel_err(w, wo) <= TOL
+    assert np.abs(f.sum(0)).max() <= 1e-12 * np.abs(f).max()
+
+
+def test_snap_j8_full_size_adjoint_equals_plain():
+    """Config 4 at full size (54,000 atoms): adjoint and plain forces agree, sum F = 0."""
+    s, prm, beta = W.snap_j8()
+    snap, _ = make(prm)
+    e1, f1, w1 = snap.energy_forces(s, beta, 0.0, mode="plain")
+    e2, f2, w2 = snap.energy_forces(s, beta, 0.0, mode="adjoint")
+    assert abs(e1 - e2) <= TOL * abs(e1)
+    assert rel_err(f2, f1) <= TOL
+    assert rel_err(w2, w1) <= TOL
+    assert np.abs(f2.sum(0)).max() <= 1e-11 * np.abs(f2).max()
+
+
+def test_fd_forces_j8():
+    """Central differences (h = 1e-5 A) of E against F on a subset of atoms."""
+    s, prm, beta = W.snap_j8(cells=4)
+    snap, _ = make(prm)
+    _, f, _ = snap.energy_forces(s, beta, mode="adjoint")
+    rng = np.random.default_rng(0)
+    h = 1e-5
+    for a in rng.choice(len(s), 8, replace=False):
+        for c in range(3):
+            pp = s.positions.copy(); pp[a, c] += h
+            pm = s.positions.copy(); pm[a, c] -= h
+            ep = snap.energy_forces(ipg.System(pp, s.symbols, s.box), beta)[0]
+            em = snap.energy_forces(ipg.System(pm, s.symbols, s.box), beta)[0]
+            assert abs(-(ep - em) / (2 * h) - f[a, c]) <= 1e-7 * np.abs(f).max()
+
+
+def test_rotation_and_permutation_invariance():
+    rng = np.random.default_rng(3)
+    pos = rng.normal(0, 1.5, (30, 3))
+    sym = list(np.where(rng.random(30) < 0.5, "A", "B"))
+    snap, _ = make(dict(twojmax=8, species=["A", "B"], rcutfac=3.0, rmin0=0.0, rfac0=0.99363, radii=[1.0, 0.9],
+                        weight=[1.0, 0.6], switch_flag=True))
+    s = ipg.System(pos, sym, [100.0] * 3, (False, False, False))
+    B = ipg.compute_local_descriptors(s, snap)
+    R = Rotation.random(random_state=4).as_matrix()
+    B2 = ipg.compute_local_descriptors(ipg.System(pos @ R.T, sym, [100.0] * 3, (False, False, False)), snap)
+    assert rel_err(B2, B) <= 1e-12
+    perm = rng.permutation(30)
+    B3 = ipg.compute_local_descriptors(ipg.System(pos[perm], [sym[k] for k in perm], [100.0] * 3,
+                                                  (False, False, False)), snap)
+    assert rel_err(B3, B[perm]) <= 1e-13
+
+
+def test_vjp_beta_matches_oracle():
+    s, prm, beta = W.snap_j8(cells=3)
+    snap, orc = make(prm)
+    rng = np.random.default_rng(1)
+    gF = rng.normal(size=(len(s), 3))
+    gb, gb0 = snap.vjp_beta(s, 0.7, gF)
+    gbo, gbo0 = orc.vjp_beta(s.positions, snap.species_ids(s), s.L, 0.7, gF)
+    assert rel_err(gb, gbo) <= TOL
+    assert gb0 == 0.7
+
+
+def test_deterministic_bitwise():
+    s, prm, beta = W.snap_j8(cells=5)
+    snap, _ = make(prm)
+    r1 = snap.energy_forces(s, beta, mode="adjoint")
+    r2 = snap.energy_forces(s, beta, mode="adjoint")
+    assert r1[0] == r2[0] and np.array_equal(r1[1], r2[1])
+
+
+def test_species_out_of_range_rejected():
+    snap = ipg.SNAP(1, 4, ["A"], 1.0, 0.0, 0.99, [1.0], [1.0])
+    s = ipg.System([[0, 0, 0], [1, 0, 0]], ["A", "A"], [5.0] * 3)
+    lib = ipg._lib.lib()
+    import ctypes as C
+    sp = np.array([0, 3], np.int32)
+    B = np.zeros((2, len(snap)))
+    st = lib.ipg_snap_descriptors(snap.handle, 2, s.positions.ctypes.data_as(C.c_void_p),
+                                  sp.ctypes.data_as(C.c_void_p), s.L.ctypes.data_as(C.c_void_p),
+                                  B.ctypes.data_as(C.c_void_p), None, None, 1)
+    assert st == -7
+
+
+def test_chem_flag_unsupported():
+    with pytest.raises(ipg.IPGError) as e:
+        ipg.SNAP(1, 4, ["A"], 1.0, 0.0, 0.99, [1.0], [1.0], chem_flag=True, bnorm_flag=True)
+    assert e.value.status == -8
+
+
+def test_lbasis_potential_api():
+    """LBasisPotential with the reference's single K-vector beta (linear_potential.jl:20-35)."""
+    s, prm, _ = W.snap_j6(cells=4)
+    snap, orc = make(prm)
+    beta = np.random.default_rng(2).normal(0, 1e-2, len(snap))
+    lbp = ipg.LBasisPotential(beta, [0.5], snap)
+    e = ipg.potential_energy(s, lbp)
+    B = ipg.compute_local_descriptors(s, snap)
+    assert abs(e - (0.5 + B.sum(0) @ beta)) <= 1e-12 * abs(e)
+    ef = ipg.energy_and_force(s, lbp)
+    dB = ipg.compute_force_descriptors(s, snap)
+    assert rel_err(ef.f, dB @ beta) <= TOL
+    assert abs(ef.e - e) <= 1e-12 * abs(e)
+    Wd = ipg.compute_virial_descriptors(s, snap)
+    assert rel_err(ipg.virial_stress(s, lbp), Wd @ beta) <= TOL
