@@ -121,14 +121,17 @@ def oracle_sample_rate(system, prm, beta, target_s):
                       switch=prm.get("switch_flag", False))
     sp = np.array([prm["species"].index(s) for s in system.symbols], np.int32)
     args = (system.positions, sp, system.L, beta, 0.0)
-    m = 64
-    t0 = time.perf_counter()
-    orc.energy_forces(*args, mode="plain", i0=0, i1=m)
-    dt = time.perf_counter() - t0
-    m = int(min(len(system), max(64, m * target_s / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    orc.energy_forces(*args, mode="plain", i0=0, i1=m)
-    dt = time.perf_counter() - t0
+    # the neighbor build of the whole system is a fixed cost; calibrate the per-atom cost
+    # from two sample sizes, then time one sample of about target_s seconds
+    def run(m):
+        t0 = time.perf_counter()
+        orc.energy_forces(*args, mode="plain", i0=0, i1=m)
+        return time.perf_counter() - t0
+
+    t_a, t_b = run(64), run(256)
+    per_atom = max((t_b - t_a) / 192.0, 1e-7)
+    m = int(min(len(system), max(256, target_s / per_atom)))
+    dt = run(m)
     return m / dt, m, dt
 
 
@@ -165,6 +168,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="size of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and pair-workload lines")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--cells", type=int, default=30, help="BCC cells per axis (30 -> 54,000 atoms); smaller "
+                    "values give the small cases used for profiling")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -193,7 +199,7 @@ def main():
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    system, prm, beta = W.snap_j8()
+    system, prm, beta = W.snap_j8(cells=args.cells)
     n = len(system)
     snap = ipg.SNAP(n, prm["twojmax"], prm["species"], prm["rcutfac"], prm["rmin0"], prm["rfac0"], prm["radii"],
                     prm["weight"], switch_flag=True, ctx=ipg.Context(local))
@@ -328,7 +334,7 @@ def main():
                           ms_p / args.steps, "n_atoms": len(s2), "half_pairs": pairs, "terms": len(terms)}
         line["lj_pairs_per_s"] = pair
 
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         rate, m, dt = oracle_sample_rate(system, prm, beta_b, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cpu_count(), "kind": "port",
                                 "sample": f"first {m} of {n} centre atoms, plain dB/dr path, {dt:.1f} s, "

@@ -161,8 +161,9 @@ struct CellList {
 };
 
 // Builds the cell list for `radius` (prefix selects the scratch buffers used).
+// Species ids outside [0, nsp) raise IPG_ERR_SPECIES in the device status word.
 int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d_pos, const int32_t* d_species,
-                    int nconf, const int64_t* h_atom_off, const double* h_L, double radius, CellList& cl);
+                    int nsp, int nconf, const int64_t* h_atom_off, const double* h_L, double radius, CellList& cl);
 
 // Materialised pair list in CSR form over atoms (original order), neighbors ascending.
 struct PairList {

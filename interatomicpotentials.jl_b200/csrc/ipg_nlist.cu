@@ -108,14 +108,15 @@ __global__ void k_cell_sort(int64_t ncells, const int64_t* __restrict__ cell_sta
 }
 
 __global__ void k_cell_gather(int64_t n, const int32_t* __restrict__ cell_atoms, const double* __restrict__ pos,
-                              const int32_t* __restrict__ species, int32_t* __restrict__ slot_of,
+                              const int32_t* __restrict__ species, int nsp, int32_t* __restrict__ slot_of,
                               double4* __restrict__ spos) {
   int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int32_t i = cell_atoms[s];
   slot_of[i] = (int32_t)s;
-  spos[s] = make_double4(pos[3 * (int64_t)i], pos[3 * (int64_t)i + 1], pos[3 * (int64_t)i + 2],
-                         species ? (double)species[i] : 0.0);
+  int sp = species ? species[i] : 0;
+  sp = sp < 0 ? 0 : (sp > nsp - 1 ? nsp - 1 : sp);  // bad ids were reported by k_cell_count
+  spos[s] = make_double4(pos[3 * (int64_t)i], pos[3 * (int64_t)i + 1], pos[3 * (int64_t)i + 2], (double)sp);
 }
 
 // ---------------------------------------------------------------------------------
@@ -248,7 +249,7 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (
 }  // namespace
 
 int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d_pos, const int32_t* d_species,
-                    int nconf, const int64_t* h_atom_off, const double* h_L, double radius, CellList& cl) {
+                    int nsp, int nconf, const int64_t* h_atom_off, const double* h_L, double radius, CellList& cl) {
   std::string pre(prefix);
   cl.nconf = nconf;
   cl.n = n;
@@ -327,12 +328,13 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
   CUDA_RET(ctx, cudaMemsetAsync(count, 0, sizeof(int64_t) * (cell_total + 1), ctx->stream));
   CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (cell_total + 1), ctx->stream));
   if (n == 0) return IPG_OK;
-  IPG_LAUNCH(ctx, k_cell_count, nblk(n, 256), 256, 0, n, d_pos, d_species, 64, cl.d_grid, nconf, cl.d_conf, cell_of,
+  IPG_LAUNCH(ctx, k_cell_count, nblk(n, 256), 256, 0, n, d_pos, d_species, nsp, cl.d_grid, nconf, cl.d_conf, cell_of,
              count, ctx->d_status);
   IPG_RET(ipg_scan_i64(ctx, count, cl.d_cell_start, cell_total + 1));
   IPG_LAUNCH(ctx, k_cell_fill, nblk(n, 256), 256, 0, n, cell_of, cl.d_cell_start, fill, cl.d_cell_atoms);
   IPG_LAUNCH(ctx, k_cell_sort, nblk(cell_total, 128), 128, 0, cell_total, cl.d_cell_start, cl.d_cell_atoms);
-  IPG_LAUNCH(ctx, k_cell_gather, nblk(n, 256), 256, 0, n, cl.d_cell_atoms, d_pos, d_species, cl.d_slot_of, cl.d_spos);
+  IPG_LAUNCH(ctx, k_cell_gather, nblk(n, 256), 256, 0, n, cl.d_cell_atoms, d_pos, d_species, nsp, cl.d_slot_of,
+             cl.d_spos);
   return IPG_OK;
 }
 
@@ -439,7 +441,7 @@ int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double 
   }
   if (!(radius >= 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "cutoff must be >= 0");
   CellList cl;
-  IPG_RET(ipg_build_cells(ctx, "nl_", n, d_pos, d_sp, 1, aoff, L, radius, cl));
+  IPG_RET(ipg_build_cells(ctx, "nl_", n, d_pos, d_sp, std::max(1, (int)nspecies), 1, aoff, L, radius, cl));
   PairList pl;
   IPG_RET(ipg_build_pairs(ctx, "nl_", cl, d_sp, std::max(1, (int)nspecies), cut, mode, false, pl));
   IPG_RET(ipg_status_check(ctx, "ipg_neighbor_build"));

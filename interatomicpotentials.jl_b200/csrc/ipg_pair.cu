@@ -258,7 +258,7 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
   IPG_RET(ipg_status_reset(ctx));
   int64_t aoff[2] = {0, n};
   CellList cl;
-  IPG_RET(ipg_build_cells(ctx, "pair_", n, d_pos, d_species, 1, aoff, L, pt.rcut_max, cl));
+  IPG_RET(ipg_build_cells(ctx, "pair_", n, d_pos, d_species, 64, 1, aoff, L, pt.rcut_max, cl));
   int64_t nb = std::max<int64_t>(1, (n + PAIR_T - 1) / PAIR_T);
   double *partial, *red;
   IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));

@@ -40,6 +40,10 @@ struct SnapIO {
   int* status;
 };
 
+// Species ids are validated by the neighbor build (status word); clamping here keeps a
+// bad id from indexing the per-species tables.
+__device__ __forceinline__ int clamp_sp(int s, int nsp) { return s < 0 ? 0 : (s >= nsp ? nsp - 1 : s); }
+
 __device__ __forceinline__ double2 cmul_conj(double2 a, double2 v) {  // conj(a) * v
   return make_double2(a.x * v.x + a.y * v.y, a.x * v.y - a.y * v.x);
 }
@@ -220,7 +224,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
 
   for (int64_t i = blockIdx.x; i < io.n; i += gridDim.x) {
     const int64_t beg = io.off[i], end = io.off[i + 1];
-    const int si = io.species[i];
+    const int si = clamp_sp(io.species[i], S.nsp);
 
     // ---------------- phase 1: Utot (half plane) ----------------
     double2* upart = zs;  // [nwarps][u_half]
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
       double2* up = upart + (size_t)warp * uh;
       for (int64_t p = beg + warp; p < end; p += nwarps) {
         const double x = io.rij[3 * p], y = io.rij[3 * p + 1], z = io.rij[3 * p + 2];
-        const int sj = io.species[io.nbr[p]];
+        const int sj = clamp_sp(io.species[io.nbr[p]], S.nsp);
         const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;  // runtime_arrays.jl:50
         const double rsq = x * x + y * y + z * z;
         const double r = sqrt(rsq);
@@ -386,7 +390,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
     }
     for (int64_t p = beg + warp; p < end; p += nwarps) {
       const int32_t jn = io.nbr[p];
-      const int sj = io.species[jn];
+      const int sj = clamp_sp(io.species[jn], S.nsp);
       const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
       PairGeom G;
       geom_du(S, io.rij[3 * p], io.rij[3 * p + 1], io.rij[3 * p + 2], rcut, S.weight[sj], G);
@@ -534,13 +538,13 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
 
 // Plain path contraction: f_p = dB_i/dr_ij . beta[s_i] from the materialised dB/dr.
 __global__ void k_snap_contract(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ species,
-                                const double* __restrict__ dbl, const double* __restrict__ beta, int K,
+                                int nsp, const double* __restrict__ dbl, const double* __restrict__ beta, int K,
                                 double* __restrict__ fvec) {
   // one warp per atom; lanes over (pair, component) rows
   int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (i >= n) return;
-  const double* bt = beta + (size_t)species[i] * K;
+  const double* bt = beta + (size_t)clamp_sp(species[i], nsp) * K;
   for (int64_t p = off[i]; p < off[i + 1]; p++) {
     const double* d = dbl + (size_t)p * K * 3;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
@@ -677,7 +681,7 @@ __global__ void k_snap_W_desc(int64_t n, int K, int nsp, const int64_t* __restri
   for (int q = threadIdx.x; q < nsp * K * 6; q += blockDim.x) wsm[q] = 0.0;
   __syncthreads();
   for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
-    const int s = species[i];
+    const int s = clamp_sp(species[i], nsp);
     const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
     for (int b = threadIdx.x; b < K; b += blockDim.x) {
       double w[6] = {0, 0, 0, 0, 0, 0};
@@ -869,7 +873,8 @@ int snap_neighbors(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d
 int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
                          const int64_t* h_atom_off, const double* h_L, PairList& pl) {
   CellList cl;
-  IPG_RET(ipg_build_cells(s->ctx, "snap_", n, d_pos, d_species, nconf, h_atom_off, h_L, s->radius, cl));
+  IPG_RET(ipg_build_cells(s->ctx, "snap_", n, d_pos, d_species, s->p.nspecies, nconf, h_atom_off, h_L, s->radius,
+                          cl));
   int mode = IPG_NLIST_FULL | (s->p.literal_sqrt_radius ? IPG_NLIST_LITERAL_SQRT : 0);
   IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl));
   return IPG_OK;
@@ -919,7 +924,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     if (n) IPG_RET(launch_atoms<MODE_PLAIN>(s, dev, io, n, nullptr));
     if (out.F || out.W6) {
       IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
-      if (n) IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, dbl, dev.beta, K, fvec);
+      if (n) IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, nsp, dbl, dev.beta, K,
+                               fvec);
     }
   } else {
     if (n) IPG_RET(launch_atoms<MODE_DESC>(s, dev, io, n, nullptr));
