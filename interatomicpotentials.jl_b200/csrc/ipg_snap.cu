@@ -19,10 +19,13 @@
 #include <algorithm>
 
 #include "ipg_snap.cuh"
+#include "ipg_snap_chain.cuh"
 
 namespace {
 
 enum SnapMode { MODE_DESC = 0, MODE_ADJ = 1, MODE_PLAIN = 2, MODE_VJP = 3 };
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
 struct SnapIO {
   int64_t n;
@@ -37,6 +40,7 @@ struct SnapIO {
   const double* g;          // [n][3] VJP cotangent of forces
   double gE;                // VJP cotangent of energy
   double* gpart;            // [gridDim][nsp*K] VJP partials
+  double2* yout;            // [n][u_half] adjoint: weighted Y written out for the pair kernel
   int* status;
 };
 
@@ -372,7 +376,18 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
           s.y += c * zz.y;
         }
         ys[h] = s;
+        if (io.yout) {  // half-plane weight folded in: 1, 1/2 on the middle element, 0 beyond
+          int j = 0;
+          while (j < J && S.half_block[j + 1] <= h) j++;
+          const int e = h - S.half_block[j], mb = e / (j + 1), ma = e - mb * (j + 1);
+          const double w = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
+          io.yout[(size_t)i * uh + h] = make_double2(w * s.x, w * s.y);
+        }
       }
+    }
+    if (MODE == MODE_ADJ && io.yout) {  // the per-neighbor part runs in k_snap_pair_adj
+      __syncthreads();
+      continue;
     }
     double2* vall = reinterpret_cast<double2*>(smem + L.duf);  // VJP: [nwarps][u_half]
     if (MODE == MODE_VJP)
@@ -536,6 +551,67 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
   }
 }
 
+// Adjoint per-neighbor kernel: one thread per (directed pair, chain MB); see
+// ipg_snap_chain.cuh.  part[p][MB][3] = chain MB's share of dE_i/dr_ij.
+template <int J, int MB>
+__global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ SnapDev S, int64_t np,
+                                                       const int32_t* __restrict__ owner,
+                                                       const int32_t* __restrict__ nbr, const double* __restrict__ rij,
+                                                       const int32_t* __restrict__ species,
+                                                       const double2* __restrict__ Yw, double* __restrict__ part) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int i = owner[p];
+  const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
+  const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+  PairGeom PG;
+  geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+  snapchain::Geom G;
+  G.a = PG.a;
+  G.b = PG.b;
+  G.sfac = PG.sfac;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    G.da[k] = PG.da[k];
+    G.db[k] = PG.db[k];
+    G.dsu[k] = PG.dsfac * PG.u[k];
+  }
+  double S0, Sk[3];
+  snapchain::chain_adjoint<J, MB>(G, Yw + (size_t)i * S.u_half, S0, Sk);
+  constexpr int NCH = J / 2 + 1;
+  double* out = part + ((size_t)p * NCH + MB) * 3;
+#pragma unroll
+  for (int k = 0; k < 3; k++) out[k] = 2.0 * (G.dsu[k] * S0 + G.sfac * Sk[k]);
+}
+
+constexpr int PAIR_CHAIN_MAX_J = 10;  // twojmax handled by the register-chain kernel
+
+template <int J, int MB>
+int launch_chain(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int32_t* owner, const int32_t* nbr,
+                 const double* rij, const int32_t* species, const double2* Yw, double* part) {
+  if constexpr (MB <= J / 2) {
+    const int T = 128;
+    IPG_TIMED_LAUNCH(ctx, "snap_pair", (k_snap_pair_adj<J, MB>), nblk(np, T), T, 0, S, np, owner, nbr, rij, species,
+                     Yw, part);
+    return launch_chain<J, MB + 1>(ctx, S, np, owner, nbr, rij, species, Yw, part);
+  }
+  return IPG_OK;
+}
+
+int launch_pair_adj(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int32_t* owner, const int32_t* nbr,
+                    const double* rij, const int32_t* species, const double2* Yw, double* part) {
+  if (np == 0) return IPG_OK;
+  switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_chain<JJ, 0>(ctx, S, np, owner, nbr, rij, species, Yw, part);
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
+  }
+}
+
 // Plain path contraction: f_p = dB_i/dr_ij . beta[s_i] from the materialised dB/dr.
 __global__ void k_snap_contract(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ species,
                                 int nsp, const double* __restrict__ dbl, const double* __restrict__ beta, int K,
@@ -570,7 +646,7 @@ __global__ void k_snap_contract(int64_t n, const int64_t* __restrict__ off, cons
 // (snap.jl:292-306 contracted with beta): [xx, yy, zz, yz, xz, xy] as in the reference.
 __global__ void k_snap_gather(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ nbr,
                               const int64_t* __restrict__ in_off, const int64_t* __restrict__ in_pair,
-                              const double* __restrict__ fvec, const double* __restrict__ pos,
+                              const double* __restrict__ fvec, int nch, const double* __restrict__ pos,
                               double* __restrict__ F, double* __restrict__ w6) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -578,7 +654,13 @@ __global__ void k_snap_gather(int64_t n, const int64_t* __restrict__ off, const 
   double w[6] = {0, 0, 0, 0, 0, 0};
   const double xk = pos[3 * k], yk = pos[3 * k + 1], zk = pos[3 * k + 2];
   for (int64_t p = off[k]; p < off[k + 1]; p++) {
-    double a = fvec[3 * p], b = fvec[3 * p + 1], c = fvec[3 * p + 2];
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int q = 0; q < nch; q++) {  // the chains' shares of this pair, in fixed order
+      const double* fv = fvec + ((size_t)p * nch + q) * 3;
+      a += fv[0];
+      b += fv[1];
+      c += fv[2];
+    }
     f0 += a;
     f1 += b;
     f2 += c;
@@ -593,9 +675,16 @@ __global__ void k_snap_gather(int64_t n, const int64_t* __restrict__ off, const 
   }
   for (int64_t q = in_off[k]; q < in_off[k + 1]; q++) {
     int64_t p = in_pair[q];
-    f0 -= fvec[3 * p];
-    f1 -= fvec[3 * p + 1];
-    f2 -= fvec[3 * p + 2];
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int r = 0; r < nch; r++) {
+      const double* fv = fvec + ((size_t)p * nch + r) * 3;
+      a += fv[0];
+      b += fv[1];
+      c += fv[2];
+    }
+    f0 -= a;
+    f1 -= b;
+    f2 -= c;
   }
   if (F) {
     F[3 * k] = f0;
@@ -735,8 +824,6 @@ __global__ void k_loss_grad(int64_t n, const double* __restrict__ F, const doubl
   li[i] = s;
 }
 
-inline unsigned nblk(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
-
 }  // namespace
 
 // ---------------------------------------------------------------------------------
@@ -752,6 +839,7 @@ struct ipg_snap {
   double radius = 0.0;
   int threads = 128;
   int blocks_per_sm = 0;  // 0 = occupancy-derived
+  bool generic_adjoint = false;  // force the in-block per-neighbor adjoint (testing)
   std::vector<double> beta_host;  // last uploaded beta
 };
 
@@ -914,7 +1002,22 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   io.B = out.B;
   io.status = ctx->d_status;
   const bool need_plain = (mode == MODE_PLAIN) || out.dB || out.Wd;
-  if (mode == MODE_ADJ) {
+  int nch = 1;
+  if (mode == MODE_ADJ && dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint) {
+    // per-atom kernel writes the weighted Y; the register-chain kernel does the neighbors
+    nch = dev.J / 2 + 1;
+    double2* yout;
+    int32_t* owner;
+    IPG_RET(scratch(ctx, "snap_yout", (size_t)n * dev.u_half + 1, &yout));
+    IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
+    IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np * nch + 3, &fvec));
+    io.yout = yout;
+    if (n) {
+      IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
+      IPG_RET(launch_atoms<MODE_ADJ>(s, dev, io, n, nullptr));
+      IPG_RET(launch_pair_adj(ctx, dev, np, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+    }
+  } else if (mode == MODE_ADJ) {
     IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
     io.fvec = fvec;
     if (n) IPG_RET(launch_atoms<MODE_ADJ>(s, dev, io, n, nullptr));
@@ -932,8 +1035,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   }
   if (out.W6) IPG_RET(scratch(ctx, "snap_w6", 6 * (size_t)n + 6, &w6));
   if ((out.F || out.W6) && fvec && n)
-    IPG_TIMED_LAUNCH(ctx, "snap_gather", k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off, pl.d_in_pair, fvec, d_pos,
-               out.F, w6);
+    IPG_TIMED_LAUNCH(ctx, "snap_gather", k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off,
+                     pl.d_in_pair, fvec, nch, d_pos, out.F, w6);
   if (out.E || out.W6) {
     int64_t* d_aoff;
     IPG_RET(scratch(ctx, "snap_aoff", (size_t)nconf + 1, &d_aoff));
@@ -1023,6 +1126,19 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
     delete s;
     return st;
   }
+  {  // rootpq table of the register-chain kernel (independent of twojmax)
+    constexpr int R = snapchain::RPQ_STRIDE;
+    double t[R * R] = {};
+    for (int a = 1; a < R; a++)
+      for (int b = 1; b < R; b++) t[a * R + b] = std::sqrt((double)a / (double)b);
+    cudaError_t e = cudaMemcpyToSymbol(snapchain::c_rpq, t, sizeof(t));
+    if (e != cudaSuccess) {
+      cudaFree(s->d_tables);
+      delete s;
+      return ipg_cuda_check(ctx, e, "rootpq upload");
+    }
+  }
+  if (const char* g = getenv("IPG_GENERIC_ADJOINT")) s->generic_adjoint = g[0] == '1';
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);

@@ -1,0 +1,166 @@
+// ipg_snap_chain.cuh — per-neighbor Wigner U / dU recursion held in registers.
+//
+// The recursion of compute_uarray / compute_duarray (compute_ui.jl:50-129, 186-326)
+// builds row mb of level j from row mb of level j-1 only:
+//   u_j[ma][mb] = rootpq[j-ma][j-mb] conj(a) u_{j-1}[ma][mb]
+//               - rootpq[ma][j-mb]   conj(b) u_{j-1}[ma-1][mb]
+// (and its derivative with respect to r_ij).  So the half plane (mb <= j/2) splits into
+// J/2+1 independent "chains", chain mb being row mb of levels 2mb..J.  Chain mb starts
+// from row mb of level 2mb-1, which is the inversion-symmetric mirror of row mb-1 of
+// that level (compute_ui.jl:105-125): u[R][c] = (-1)^(c+R) conj(u[j-R][j-c]).  A thread
+// therefore computes one chain of one neighbor entirely in registers: a short
+// "staircase" (chain k over levels 2k+1, 2k+2 for k < mb) reaches the chain's start,
+// then the chain runs to level J.  With twojmax a template parameter every index is a
+// compile-time constant: no shared memory, no integer division, no divergence.
+//
+// The adjoint contraction (design of compute_dij.jl:5-74) is folded into the chain:
+//   dE_i/dr_ij[k] = 2 sum_e w_e Re(conj(dsfac u_e uhat_k + sfac du_e[k]) Y_e)
+//                 = 2 (dsfac uhat_k S0 + sfac S_k),
+//   S0 = sum_e Re(conj(u_e) Yw_e),  S_k = sum_e Re(conj(du_e[k]) Yw_e),
+// where Yw = w Y carries the half-plane weights (1, 1/2 on the middle element of even
+// levels, 0 beyond it).
+#pragma once
+
+#include "ipg_snap.cuh"
+
+namespace snapchain {
+
+constexpr int RPQ_STRIDE = SNAP_MAX_J + 2;
+// rootpq[p][q] = sqrt(p/q) (prebuilt_arrays.jl:314-321), one table for every twojmax.
+__constant__ double c_rpq[RPQ_STRIDE * RPQ_STRIDE];
+
+constexpr int half_block(int j) { return j <= 0 ? 0 : half_block(j - 1) + ((j - 1) / 2 + 1) * j; }
+
+template <int J>
+struct Chain {
+  double2 u[J + 1];
+  double2 d[3][J + 1];
+};
+
+struct Geom {
+  double2 a, b;
+  double2 da[3], db[3];
+  double sfac, dsu[3];  // dsu[k] = dsfac * uhat_k
+};
+
+__device__ __forceinline__ double2 conjmul(double2 a, double2 v) {  // conj(a) * v
+  return make_double2(a.x * v.x + a.y * v.y, a.x * v.y - a.y * v.x);
+}
+
+// Row mb: level j-1 -> level j, in place (descending ma keeps the old values needed).
+template <int J, int j, int mb>
+__device__ __forceinline__ void advance(Chain<J>& s, const Geom& G) {
+#pragma unroll
+  for (int ma = j; ma >= 0; --ma) {
+    double2 nu = make_double2(0.0, 0.0);
+    double2 nd[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) nd[k] = make_double2(0.0, 0.0);
+    if (ma > 0) {
+      const double rp = c_rpq[ma * RPQ_STRIDE + (j - mb)];
+      const double2 v = s.u[ma - 1];
+      const double2 t = conjmul(G.b, v);
+      nu.x = -rp * t.x;
+      nu.y = -rp * t.y;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const double2 t1 = conjmul(G.db[k], v);
+        const double2 t2 = conjmul(G.b, s.d[k][ma - 1]);
+        nd[k].x = -rp * (t1.x + t2.x);
+        nd[k].y = -rp * (t1.y + t2.y);
+      }
+    }
+    if (ma < j) {
+      const double rp = c_rpq[(j - ma) * RPQ_STRIDE + (j - mb)];
+      const double2 v = s.u[ma];
+      const double2 t = conjmul(G.a, v);
+      nu.x += rp * t.x;
+      nu.y += rp * t.y;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const double2 t1 = conjmul(G.da[k], v);
+        const double2 t2 = conjmul(G.a, s.d[k][ma]);
+        nd[k].x += rp * (t1.x + t2.x);
+        nd[k].y += rp * (t1.y + t2.y);
+      }
+    }
+    s.u[ma] = nu;
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][ma] = nd[k];
+  }
+}
+
+// Row (j+1)/2 of an odd level from row (j-1)/2 by inversion symmetry.
+template <int J, int j>
+__device__ __forceinline__ void mirror(Chain<J>& s) {
+  constexpr int R = (j + 1) / 2;
+  double2 tu[j + 1];
+  double2 td[3][j + 1];
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    tu[c] = s.u[j - c];
+#pragma unroll
+    for (int k = 0; k < 3; k++) td[k][c] = s.d[k][j - c];
+  }
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+    s.u[c] = make_double2(sg * tu[c].x, -sg * tu[c].y);
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][c] = make_double2(sg * td[k][c].x, -sg * td[k][c].y);
+  }
+}
+
+// Staircase: chain k from level 2k to 2k+1, mirror, chain k+1 to level 2k+2.
+template <int J, int k, int MB>
+__device__ __forceinline__ void staircase(Chain<J>& s, const Geom& G) {
+  if constexpr (k < MB) {
+    advance<J, 2 * k + 1, k>(s, G);
+    mirror<J, 2 * k + 1>(s);
+    advance<J, 2 * k + 2, k + 1>(s, G);
+    staircase<J, k + 1, MB>(s, G);
+  }
+}
+
+template <int J, int j, int mb>
+__device__ __forceinline__ void contract(const Chain<J>& s, const double2* __restrict__ Yw, double& S0, double* S) {
+  constexpr int base = half_block(j) + mb * (j + 1);
+  constexpr int last = (2 * mb == j) ? mb : j;  // middle row of an even level stops at ma = j/2
+#pragma unroll
+  for (int ma = 0; ma <= last; ma++) {
+    const double2 y = Yw[base + ma];
+    S0 += s.u[ma].x * y.x + s.u[ma].y * y.y;
+#pragma unroll
+    for (int k = 0; k < 3; k++) S[k] += s.d[k][ma].x * y.x + s.d[k][ma].y * y.y;
+  }
+}
+
+template <int J, int j, int MB>
+__device__ __forceinline__ void run_levels(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, double& S0,
+                                           double* S) {
+  if constexpr (j <= J) {
+    advance<J, j, MB>(s, G);
+    contract<J, j, MB>(s, Yw, S0, S);
+    run_levels<J, j + 1, MB>(s, G, Yw, S0, S);
+  }
+}
+
+// Chain MB of one neighbor: returns S0 and S[3].
+template <int J, int MB>
+__device__ __forceinline__ void chain_adjoint(const Geom& G, const double2* __restrict__ Yw, double& S0, double* S) {
+  Chain<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);  // level 0
+  staircase<J, 0, MB>(s, G);
+  S0 = 0.0;
+  S[0] = S[1] = S[2] = 0.0;
+  contract<J, 2 * MB, MB>(s, Yw, S0, S);
+  run_levels<J, 2 * MB + 1, MB>(s, G, Yw, S0, S);
+}
+
+}  // namespace snapchain

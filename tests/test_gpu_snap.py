@@ -218,3 +218,24 @@ def test_lbasis_potential_api():
     assert abs(ef.e - e) <= 1e-12 * abs(e)
     Wd = ipg.compute_virial_descriptors(s, snap)
     assert rel_err(ipg.virial_stress(s, lbp), Wd @ beta) <= TOL
+
+
+@pytest.mark.parametrize("J", [4, 7, 8, 11, 12])
+def test_adjoint_paths_agree(J, monkeypatch):
+    """twojmax <= 10 runs the register-chain kernel, larger twojmax (or IPG_GENERIC_ADJOINT=1)
+    the in-block per-neighbor loop; both must equal the plain dB/dr path and the oracle."""
+    rng = np.random.default_rng(100 + J)
+    pos = rng.uniform(0, 7, (40, 3))
+    s = ipg.System(pos, list(np.where(rng.random(40) < 0.6, "A", "B")), [7.0] * 3)
+    prm = dict(twojmax=J, species=["A", "B"], rcutfac=2.2, rmin0=0.1, rfac0=0.98, radii=[1.0, 0.8],
+               weight=[1.0, 0.7], switch_flag=True)
+    snap, orc = make(prm)
+    beta = rng.normal(0, 1e-2, (2, len(snap)))
+    eo, fo, wo = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.0)
+    for generic in ("0", "1"):
+        monkeypatch.setenv("IPG_GENERIC_ADJOINT", generic)
+        snap2, _ = make(prm)
+        e, f, w = snap2.energy_forces(s, beta, 0.0, mode="adjoint")
+        assert abs(e - eo) <= TOL * abs(eo)
+        assert rel_err(f, fo) <= TOL, generic
+        assert rel_err(w, wo) <= TOL
