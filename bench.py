@@ -233,7 +233,7 @@ def main():
         torch.cuda.synchronize()
         if kernel_timing:
             ctx.timing(True)
-            for k in ("snap_atom", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
+            for k in ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
                 ctx.timing_read(k)
         l0 = ctx.launch_count()
         evs = []
@@ -251,7 +251,7 @@ def main():
         launches = ctx.launch_count() - l0
         kt = {}
         if kernel_timing:
-            for k in ("snap_atom", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
+            for k in ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
                 kt[k] = ctx.timing_read(k)
             ctx.timing(False)
         if dist:

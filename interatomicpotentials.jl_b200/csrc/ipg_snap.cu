@@ -41,8 +41,15 @@ struct SnapIO {
   double gE;                // VJP cotangent of energy
   double* gpart;            // [gridDim][nsp*K] VJP partials
   double2* yout;            // [n][u_half] adjoint: weighted Y written out for the pair kernel
+  const double2* utot_in;   // [n][idxu_max] Utot from k_snap_utot (phase 1 skipped) or null
   int* status;
 };
+
+// Whether the per-atom kernel needs the per-warp level buffers (its own phase 1 or the
+// in-block per-neighbor phase 5).
+__host__ __device__ inline bool needs_levels(int mode, bool has_utot, bool has_yout) {
+  return !(has_utot && (mode == MODE_DESC || (mode == MODE_ADJ && has_yout)));
+}
 
 // Species ids are validated by the neighbor build (status word); clamping here keeps a
 // bad id from indexing the per-species tables.
@@ -179,7 +186,7 @@ struct SmemLayout {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 1) & ~size_t(1); }  // in doubles
 
-__host__ __device__ inline SmemLayout smem_layout(const SnapDev& S, int nwarps, int mode) {
+__host__ __device__ inline SmemLayout smem_layout(const SnapDev& S, int nwarps, int mode, bool levels) {
   SmemLayout L;
   size_t o = 0;
   L.ut = o;
@@ -194,7 +201,7 @@ __host__ __device__ inline SmemLayout smem_layout(const SnapDev& S, int nwarps, 
   L.rpq = o;
   o += al16((size_t)(S.J + 2) * (S.J + 2));
   L.lv = o;  // per warp: 2 levels x 4 components x ext_max complex
-  o += al16((size_t)nwarps * 2 * 4 * 2 * S.ext_max);
+  if (levels) o += al16((size_t)nwarps * 2 * 4 * 2 * S.ext_max);
   L.duf = o;  // plain: per-warp dU/dr [3][u_half]; vjp: per-warp partial V [u_half]
   if (mode == MODE_PLAIN) o += al16((size_t)nwarps * 2 * 3 * S.u_half);
   if (mode == MODE_VJP) o += al16((size_t)nwarps * 2 * S.u_half);
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
   extern __shared__ double smem[];
   const int nwarps = blockDim.x >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const SmemLayout L = smem_layout(S, nwarps, MODE);
+  const SmemLayout L = smem_layout(S, nwarps, MODE, needs_levels(MODE, io.utot_in != nullptr, io.yout != nullptr));
   double2* ut = reinterpret_cast<double2*>(smem + L.ut);
   double2* zs = reinterpret_cast<double2*>(smem + L.zs);
   double2* ys = reinterpret_cast<double2*>(smem + L.ys);
@@ -231,6 +238,11 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
     const int si = clamp_sp(io.species[i], S.nsp);
 
     // ---------------- phase 1: Utot (half plane) ----------------
+    if (io.utot_in) {  // computed by k_snap_utot
+      const double2* src = io.utot_in + (size_t)i * S.idxu_max;
+      for (int q = threadIdx.x; q < S.idxu_max; q += blockDim.x) ut[q] = src[q];
+      __syncthreads();
+    } else {
     double2* upart = zs;  // [nwarps][u_half]
     for (int q = threadIdx.x; q < nwarps * uh; q += blockDim.x) upart[q] = make_double2(0.0, 0.0);
     __syncthreads();
@@ -296,6 +308,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
       }
     }
     __syncthreads();
+    }  // phase 1
 
     // ---------------- phase 2: Z ----------------
     for (int jjz = threadIdx.x; jjz < S.idxz_max; jjz += blockDim.x) {
@@ -548,6 +561,81 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
   if (MODE == MODE_VJP) {
     __syncthreads();
     for (int q = threadIdx.x; q < S.nsp * K; q += blockDim.x) io.gpart[(size_t)blockIdx.x * S.nsp * K + q] = gacc[q];
+  }
+}
+
+// Utot of every atom (compute_ui.jl:5-175) from the register chains: one block per atom
+// (grid-stride), warp w runs chain w for 32 neighbors at a time and reduces it over the
+// lanes (fixed order); the block then writes the full matrix (wself on the diagonal,
+// the other half by inversion symmetry) to utot[i][idxu_max].
+template <int J>
+__global__ void __launch_bounds__((J / 2 + 1) * 32) k_snap_utot(const __grid_constant__ SnapDev S, int64_t n,
+                                                               const int64_t* __restrict__ off,
+                                                               const int32_t* __restrict__ nbr,
+                                                               const double* __restrict__ rij,
+                                                               const int32_t* __restrict__ species,
+                                                               double2* __restrict__ utot) {
+  constexpr int UH = snapchain::half_block(J + 1);
+  __shared__ double2 acc[UH];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+    for (int h = threadIdx.x; h < UH; h += blockDim.x) acc[h] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const int si = clamp_sp(species[i], S.nsp);
+    const int64_t beg = off[i], end = off[i + 1];
+    for (int64_t p0 = beg; p0 < end; p0 += 32) {
+      const int64_t p = p0 + lane;
+      double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);
+      double sw = 0.0;  // idle lanes contribute zero
+      if (p < end) {
+        const double x = rij[3 * p], y = rij[3 * p + 1], z = rij[3 * p + 2];
+        const int sj = clamp_sp(species[nbr[p]], S.nsp);
+        const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;  // runtime_arrays.jl:50
+        const double r = sqrt(x * x + y * y + z * z);
+        const double theta0 = (r - S.rmin0) * S.rfac0 * M_PI / (rcut - S.rmin0);
+        const double z0 = r / tan(theta0);
+        const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+        a = make_double2(r0inv * z0, -r0inv * z);
+        b = make_double2(r0inv * y, -r0inv * x);
+        sw = sfac_of(S, r, rcut) * S.weight[sj];
+      }
+      snapchain::chain_utot_dispatch<J, 0>(warp, a, b, sw, acc, lane);
+    }
+    __syncthreads();
+    double2* ut = utot + (size_t)i * S.idxu_max;
+    for (int h = threadIdx.x; h < UH; h += blockDim.x) {
+      int j = 0;
+      while (j < J && S.half_block[j + 1] <= h) j++;
+      const int e = h - S.half_block[j], mb = e / (j + 1), ma = e - mb * (j + 1);
+      double2 s = acc[h];
+      if (ma == mb) s.x += S.wself;
+      const int ub = S.idxu_block[j];
+      const bool middle = (2 * mb == j);
+      if (middle && ma > mb) continue;  // written as the mirror of ma' = j - ma
+      ut[ub + mb * (j + 1) + ma] = s;
+      if (!(middle && ma == mb)) {
+        const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+        ut[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * s.x, -sg * s.y);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
+                const double* rij, const int32_t* species, double2* utot) {
+  if (n == 0) return IPG_OK;
+  const int64_t grid = std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
+  switch (S.J) {
+#define IPG_J(JJ)                                                                                             \
+  case JJ:                                                                                                    \
+    IPG_TIMED_LAUNCH(ctx, "snap_utot", k_snap_utot<JJ>, (unsigned)grid, (JJ / 2 + 1) * 32, 0, S, n, off, nbr, \
+                     rij, species, utot);                                                                     \
+    return IPG_OK;
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
   }
 }
 
@@ -911,8 +999,9 @@ int upload_tables(ipg_snap* s) {
 template <int MODE>
 int launch_atoms(ipg_snap* s, const SnapDev& dev, const SnapIO& io, int64_t natoms, int64_t* grid_used) {
   ipg_ctx* ctx = s->ctx;
-  const int threads = s->threads;
-  SmemLayout L = smem_layout(dev, threads / 32, MODE);
+  const bool levels = needs_levels(MODE, io.utot_in != nullptr, io.yout != nullptr);
+  const int threads = levels ? s->threads : 256;
+  SmemLayout L = smem_layout(dev, threads / 32, MODE, levels);
   size_t smem = L.total;
   if (smem > 227 * 1024)
     return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "twojmax %d needs %zu bytes of shared memory per block", dev.J, smem);
@@ -1002,8 +1091,15 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   io.B = out.B;
   io.status = ctx->d_status;
   const bool need_plain = (mode == MODE_PLAIN) || out.dB || out.Wd;
+  const bool chains = dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
+  if (chains && n) {  // Utot from the register-chain kernel
+    double2* utot;
+    IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
+    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot));
+    io.utot_in = utot;
+  }
   int nch = 1;
-  if (mode == MODE_ADJ && dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint) {
+  if (mode == MODE_ADJ && chains) {
     // per-atom kernel writes the weighted Y; the register-chain kernel does the neighbors
     nch = dev.J / 2 + 1;
     double2* yout;
@@ -1284,8 +1380,14 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
   io.g = d_g;
   io.gE = gE;
   io.status = ctx->d_status;
+  if (dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && n) {
+    double2* utot;
+    IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
+    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot));
+    io.utot_in = utot;
+  }
   int threads = s->threads;
-  SmemLayout L = smem_layout(dev, threads / 32, MODE_VJP);
+  SmemLayout L = smem_layout(dev, threads / 32, MODE_VJP, true);
   int per_sm = 1;
   CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_atom<MODE_VJP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
   CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_atom<MODE_VJP>, threads, L.total));

@@ -164,3 +164,106 @@ __device__ __forceinline__ void chain_adjoint(const Geom& G, const double2* __re
 }
 
 }  // namespace snapchain
+
+namespace snapchain {
+
+// ---- U only (Utot accumulation) ------------------------------------------------------
+template <int J>
+struct ChainU {
+  double2 u[J + 1];
+};
+
+template <int J, int j, int mb>
+__device__ __forceinline__ void advance_u(ChainU<J>& s, double2 a, double2 b) {
+#pragma unroll
+  for (int ma = j; ma >= 0; --ma) {
+    double2 nu = make_double2(0.0, 0.0);
+    if (ma > 0) {
+      const double rp = c_rpq[ma * RPQ_STRIDE + (j - mb)];
+      const double2 t = conjmul(b, s.u[ma - 1]);
+      nu.x = -rp * t.x;
+      nu.y = -rp * t.y;
+    }
+    if (ma < j) {
+      const double rp = c_rpq[(j - ma) * RPQ_STRIDE + (j - mb)];
+      const double2 t = conjmul(a, s.u[ma]);
+      nu.x += rp * t.x;
+      nu.y += rp * t.y;
+    }
+    s.u[ma] = nu;
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void mirror_u(ChainU<J>& s) {
+  constexpr int R = (j + 1) / 2;
+  double2 tu[j + 1];
+#pragma unroll
+  for (int c = 0; c <= j; c++) tu[c] = s.u[j - c];
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+    s.u[c] = make_double2(sg * tu[c].x, -sg * tu[c].y);
+  }
+}
+
+template <int J, int k, int MB>
+__device__ __forceinline__ void staircase_u(ChainU<J>& s, double2 a, double2 b) {
+  if constexpr (k < MB) {
+    advance_u<J, 2 * k + 1, k>(s, a, b);
+    mirror_u<J, 2 * k + 1>(s);
+    advance_u<J, 2 * k + 2, k + 1>(s, a, b);
+    staircase_u<J, k + 1, MB>(s, a, b);
+  }
+}
+
+// Adds the warp-wide sum of sw * row mb of level j into acc[half_block(j) + mb*(j+1) + ma]
+// (lane 0 writes; the calling warp owns these entries).
+template <int J, int j, int mb>
+__device__ __forceinline__ void reduce_row(const ChainU<J>& s, double sw, double2* __restrict__ acc, int lane) {
+  constexpr int base = half_block(j) + mb * (j + 1);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    double x = sw * s.u[ma].x, y = sw * s.u[ma].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      y += __shfl_xor_sync(0xffffffffu, y, o);
+    }
+    if (lane == 0) {
+      acc[base + ma].x += x;
+      acc[base + ma].y += y;
+    }
+  }
+}
+
+template <int J, int j, int MB>
+__device__ __forceinline__ void run_levels_u(ChainU<J>& s, double2 a, double2 b, double sw, double2* acc, int lane) {
+  if constexpr (j <= J) {
+    advance_u<J, j, MB>(s, a, b);
+    reduce_row<J, j, MB>(s, sw, acc, lane);
+    run_levels_u<J, j + 1, MB>(s, a, b, sw, acc, lane);
+  }
+}
+
+// Chain MB of one neighbor per lane (sw = 0 on idle lanes), reduced over the warp.
+template <int J, int MB>
+__device__ __forceinline__ void chain_utot(double2 a, double2 b, double sw, double2* acc, int lane) {
+  ChainU<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) s.u[c] = make_double2(0.0, 0.0);
+  s.u[0] = make_double2(1.0, 0.0);
+  staircase_u<J, 0, MB>(s, a, b);
+  reduce_row<J, 2 * MB, MB>(s, sw, acc, lane);
+  run_levels_u<J, 2 * MB + 1, MB>(s, a, b, sw, acc, lane);
+}
+
+template <int J, int MB>
+__device__ __forceinline__ void chain_utot_dispatch(int mb, double2 a, double2 b, double sw, double2* acc, int lane) {
+  if constexpr (MB <= J / 2) {
+    if (mb == MB) chain_utot<J, MB>(a, b, sw, acc, lane);
+    else chain_utot_dispatch<J, MB + 1>(mb, a, b, sw, acc, lane);
+  }
+}
+
+}  // namespace snapchain

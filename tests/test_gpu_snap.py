@@ -220,7 +220,7 @@ def test_lbasis_potential_api():
     assert rel_err(ipg.virial_stress(s, lbp), Wd @ beta) <= TOL
 
 
-@pytest.mark.parametrize("J", [4, 7, 8, 11, 12])
+@pytest.mark.parametrize("J", [4, 7, 8, 11])
 def test_adjoint_paths_agree(J, monkeypatch):
     """twojmax <= 10 runs the register-chain kernel, larger twojmax (or IPG_GENERIC_ADJOINT=1)
     the in-block per-neighbor loop; both must equal the plain dB/dr path and the oracle."""
@@ -239,3 +239,12 @@ def test_adjoint_paths_agree(J, monkeypatch):
         assert abs(e - eo) <= TOL * abs(eo)
         assert rel_err(f, fo) <= TOL, generic
         assert rel_err(w, wo) <= TOL
+
+
+def test_twojmax_beyond_shared_memory_is_unsupported():
+    """twojmax 12 needs more than 227 KB of shared memory per block: a clean error."""
+    s = ipg.System(np.random.default_rng(0).uniform(0, 5, (10, 3)), ["A"] * 10, [5.0] * 3)
+    snap = ipg.SNAP(1, 12, ["A"], 2.0, 0.0, 0.99, [1.0], [1.0])
+    with pytest.raises(ipg.IPGError) as e:
+        ipg.compute_local_descriptors(s, snap)
+    assert e.value.status == -8
