@@ -23,7 +23,10 @@
 
 namespace {
 
-enum SnapMode { MODE_DESC = 0, MODE_ADJ = 1, MODE_PLAIN = 2, MODE_VJP = 3 };
+// MODE_ADJY: the adjoint per-atom part alone (Z, weighted Y out, E from Y); the
+// per-neighbor part runs in k_snap_pair_adj.  MODE_ADJ: the whole adjoint in one block
+// (twojmax beyond the register-chain kernels).
+enum SnapMode { MODE_DESC = 0, MODE_ADJ = 1, MODE_PLAIN = 2, MODE_VJP = 3, MODE_ADJY = 4 };
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
@@ -48,7 +51,7 @@ struct SnapIO {
 // Whether the per-atom kernel needs the per-warp level buffers (its own phase 1 or the
 // in-block per-neighbor phase 5).
 __host__ __device__ inline bool needs_levels(int mode, bool has_utot, bool has_yout) {
-  return !(has_utot && (mode == MODE_DESC || (mode == MODE_ADJ && has_yout)));
+  return !(has_utot && (mode == MODE_DESC || mode == MODE_ADJY || (mode == MODE_ADJ && has_yout)));
 }
 
 // Species ids are validated by the neighbor build (status word); clamping here keeps a
@@ -311,7 +314,8 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
     }  // phase 1
 
     // ---------------- phase 2: Z ----------------
-    for (int jjz = threadIdx.x; jjz < S.idxz_max; jjz += blockDim.x) {
+    for (int t = threadIdx.x; t < S.idxz_max; t += blockDim.x) {
+      const int jjz = S.zperm[t];
       const ZDev q = S.idxz[jjz];
       const double* cgb = S.cglist + q.cgoff;
       const int j1 = q.j1, j2 = q.j2;
@@ -342,6 +346,44 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
       zs[jjz] = make_double2(zr, zi);
     }
     __syncthreads();
+
+    if (MODE == MODE_ADJY) {
+      // Y' = w Y (half-plane weights folded in) out, and E_i from Y: B is cubic in U, so
+      // beta.B = (2/3) sum_h w_h Re(conj(U_h) Y_h) (Euler's theorem), minus beta.bzero.
+      __shared__ double red[32];
+      const double* yc = S.ycoef + (size_t)si * S.idxz_max;
+      double e = 0.0;
+      for (int h = threadIdx.x; h < uh; h += blockDim.x) {
+        int j = 0;
+        while (j < J && S.half_block[j + 1] <= h) j++;
+        const int ee = h - S.half_block[j], mb = ee / (j + 1), ma = ee - mb * (j + 1);
+        const double w = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
+        double2 y = make_double2(0.0, 0.0);
+        if (w != 0.0)
+          for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
+            const int jjz = S.y_jjz[q];
+            const double c = yc[jjz];
+            const double2 zz = zs[jjz];
+            y.x += c * zz.x;
+            y.y += c * zz.y;
+          }
+        y.x *= w;
+        y.y *= w;
+        io.yout[(size_t)i * uh + h] = y;
+        const double2 u = ut[S.idxu_block[j] + ee];
+        e += u.x * y.x + u.y * y.y;
+      }
+      e = warp_sum(e);
+      if (lane == 0) red[warp] = e;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < nwarps; w++) t += red[w];
+        io.Ei[i] = (2.0 / 3.0) * t + S.ebias[si];
+      }
+      __syncthreads();
+      continue;
+    }
 
     // ---------------- phase 3: B and E_i ----------------
     for (int b = threadIdx.x; b < K; b += blockDim.x) {
@@ -564,74 +606,58 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
   }
 }
 
-// Utot of every atom (compute_ui.jl:5-175) from the register chains: one block per atom
-// (grid-stride), warp w runs chain w for 32 neighbors at a time and reduces it over the
-// lanes (fixed order); the block then writes the full matrix (wself on the diagonal,
-// the other half by inversion symmetry) to utot[i][idxu_max].
-template <int J>
-__global__ void __launch_bounds__((J / 2 + 1) * 32) k_snap_utot(const __grid_constant__ SnapDev S, int64_t n,
-                                                               const int64_t* __restrict__ off,
-                                                               const int32_t* __restrict__ nbr,
-                                                               const double* __restrict__ rij,
-                                                               const int32_t* __restrict__ species,
-                                                               double2* __restrict__ utot) {
-  constexpr int UH = snapchain::half_block(J + 1);
-  __shared__ double2 acc[UH];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
-    for (int h = threadIdx.x; h < UH; h += blockDim.x) acc[h] = make_double2(0.0, 0.0);
-    __syncthreads();
-    const int si = clamp_sp(species[i], S.nsp);
-    const int64_t beg = off[i], end = off[i + 1];
-    for (int64_t p0 = beg; p0 < end; p0 += 32) {
-      const int64_t p = p0 + lane;
-      double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);
-      double sw = 0.0;  // idle lanes contribute zero
-      if (p < end) {
-        const double x = rij[3 * p], y = rij[3 * p + 1], z = rij[3 * p + 2];
-        const int sj = clamp_sp(species[nbr[p]], S.nsp);
-        const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;  // runtime_arrays.jl:50
-        const double r = sqrt(x * x + y * y + z * z);
-        const double theta0 = (r - S.rmin0) * S.rfac0 * M_PI / (rcut - S.rmin0);
-        const double z0 = r / tan(theta0);
-        const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
-        a = make_double2(r0inv * z0, -r0inv * z);
-        b = make_double2(r0inv * y, -r0inv * x);
-        sw = sfac_of(S, r, rcut) * S.weight[sj];
-      }
-      snapchain::chain_utot_dispatch<J, 0>(warp, a, b, sw, acc, lane);
+// Utot of every atom (compute_ui.jl:5-175) from the register chains: one launch per
+// chain MB, one warp per atom, lanes over neighbors (32 at a time).  Each chain's rows
+// (and their mirrors) are disjoint, so the launches write disjoint entries of
+// utot[i][idxu_max]; the per-entry sums over lanes are warp reductions in fixed order.
+template <int J, int MB>
+__global__ void __launch_bounds__(128) k_snap_utot(const __grid_constant__ SnapDev S, int64_t n,
+                                                  const int64_t* __restrict__ off, const int32_t* __restrict__ nbr,
+                                                  const double* __restrict__ rij,
+                                                  const int32_t* __restrict__ species, double2* __restrict__ utot) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= n) return;  // warp-uniform
+  const int si = clamp_sp(species[i], S.nsp);
+  const int64_t beg = off[i], end = off[i + 1];
+  double2* ut = utot + (size_t)i * S.idxu_max;
+  for (int64_t p0 = beg; p0 < (end > beg ? end : beg + 1); p0 += 32) {
+    const int64_t p = p0 + lane;
+    double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);
+    double sw = 0.0;  // idle lanes contribute zero
+    if (p < end) {
+      const double x = rij[3 * p], y = rij[3 * p + 1], z = rij[3 * p + 2];
+      const int sj = clamp_sp(species[nbr[p]], S.nsp);
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;  // runtime_arrays.jl:50
+      const double r = sqrt(x * x + y * y + z * z);
+      const double theta0 = (r - S.rmin0) * S.rfac0 * M_PI / (rcut - S.rmin0);
+      const double z0 = r / tan(theta0);
+      const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+      a = make_double2(r0inv * z0, -r0inv * z);
+      b = make_double2(r0inv * y, -r0inv * x);
+      sw = sfac_of(S, r, rcut) * S.weight[sj];
     }
-    __syncthreads();
-    double2* ut = utot + (size_t)i * S.idxu_max;
-    for (int h = threadIdx.x; h < UH; h += blockDim.x) {
-      int j = 0;
-      while (j < J && S.half_block[j + 1] <= h) j++;
-      const int e = h - S.half_block[j], mb = e / (j + 1), ma = e - mb * (j + 1);
-      double2 s = acc[h];
-      if (ma == mb) s.x += S.wself;
-      const int ub = S.idxu_block[j];
-      const bool middle = (2 * mb == j);
-      if (middle && ma > mb) continue;  // written as the mirror of ma' = j - ma
-      ut[ub + mb * (j + 1) + ma] = s;
-      if (!(middle && ma == mb)) {
-        const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
-        ut[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * s.x, -sg * s.y);
-      }
-    }
-    __syncthreads();
+    snapchain::chain_utot_emit<J, MB>(a, b, sw, ut, lane, p0 == beg, S.wself);
   }
+}
+
+template <int J, int MB>
+int launch_utot_chains(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
+                       const double* rij, const int32_t* species, double2* utot) {
+  if constexpr (MB <= J / 2) {
+    IPG_TIMED_LAUNCH(ctx, "snap_utot", (k_snap_utot<J, MB>), nblk(n, 4), 128, 0, S, n, off, nbr, rij, species, utot);
+    return launch_utot_chains<J, MB + 1>(ctx, S, n, off, nbr, rij, species, utot);
+  }
+  return IPG_OK;
 }
 
 int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
                 const double* rij, const int32_t* species, double2* utot) {
   if (n == 0) return IPG_OK;
-  const int64_t grid = std::min<int64_t>(n, (int64_t)ctx->num_sms * 16);
   switch (S.J) {
-#define IPG_J(JJ)                                                                                             \
-  case JJ:                                                                                                    \
-    IPG_TIMED_LAUNCH(ctx, "snap_utot", k_snap_utot<JJ>, (unsigned)grid, (JJ / 2 + 1) * 32, 0, S, n, off, nbr, \
-                     rij, species, utot);                                                                     \
-    return IPG_OK;
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_utot_chains<JJ, 0>(ctx, S, n, off, nbr, rij, species, utot);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
 #undef IPG_J
     default:
@@ -946,7 +972,8 @@ int upload_tables(ipg_snap* s) {
   size_t o_yoff = o_db + pad(h.db.size() * sizeof(DBDev));
   size_t o_yjjz = o_yoff + pad(h.y_off.size() * 4);
   size_t o_yjjb = o_yjjz + pad(h.y_jjz.size() * 4);
-  size_t total = o_yjjb + pad(h.y_jjb.size() * 4);
+  size_t o_zperm = o_yjjb + pad(h.y_jjb.size() * 4);
+  size_t total = o_zperm + pad(h.zperm.size() * 4);
   CUDA_RET(ctx, cudaMalloc(&s->d_tables, total));
   char* b = static_cast<char*>(s->d_tables);
   std::vector<char> hostbuf(total, 0);
@@ -958,6 +985,7 @@ int upload_tables(ipg_snap* s) {
   memcpy(hostbuf.data() + o_yoff, h.y_off.data(), h.y_off.size() * 4);
   memcpy(hostbuf.data() + o_yjjz, h.y_jjz.data(), h.y_jjz.size() * 4);
   memcpy(hostbuf.data() + o_yjjb, h.y_jjb.data(), h.y_jjb.size() * 4);
+  memcpy(hostbuf.data() + o_zperm, h.zperm.data(), h.zperm.size() * 4);
   CUDA_RET(ctx, cudaMemcpy(b, hostbuf.data(), total, cudaMemcpyHostToDevice));
   SnapDev& d = s->dev;
   memset(&d, 0, sizeof(d));
@@ -991,6 +1019,7 @@ int upload_tables(ipg_snap* s) {
   d.db = reinterpret_cast<const DBDev*>(b + o_db);
   d.y_off = reinterpret_cast<const int32_t*>(b + o_yoff);
   d.y_jjz = reinterpret_cast<const int32_t*>(b + o_yjjz);
+  d.zperm = reinterpret_cast<const int32_t*>(b + o_zperm);
   s->d_ymult = reinterpret_cast<double*>(b + o_ym);
   s->d_yjjb = reinterpret_cast<int32_t*>(b + o_yjjb);
   return IPG_OK;
@@ -1032,6 +1061,11 @@ int set_beta(ipg_snap* s, const double* beta, SnapDev& dev) {
              s->d_yjjb, d_beta, d_ycoef);
   dev.beta = d_beta;
   dev.ycoef = d_ycoef;
+  for (int q = 0; q < nsp; q++) {  // -beta[s] . bzero[j(k)] (compute_b.jl:134-155)
+    double t = 0.0;
+    for (int k = 0; k < K; k++) t += b[(size_t)q * K + k] * s->h.bzero[s->h.idxb[3 * k + 2]];
+    dev.ebias[q] = -t;
+  }
   return IPG_OK;
 }
 
@@ -1110,7 +1144,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     io.yout = yout;
     if (n) {
       IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
-      IPG_RET(launch_atoms<MODE_ADJ>(s, dev, io, n, nullptr));
+      IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
       IPG_RET(launch_pair_adj(ctx, dev, np, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
     }
   } else if (mode == MODE_ADJ) {

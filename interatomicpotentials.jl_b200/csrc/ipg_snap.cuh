@@ -40,6 +40,8 @@ struct SnapDev {
   const int32_t* y_jjz;  // [idxz_max]
   const double* ycoef;   // [nsp][idxz_max] multiplicity * factor * beta (set per beta)
   const double* beta;    // [nsp][K]
+  const int32_t* zperm;  // [idxz_max] Z entries ordered by loop shape (nb, na)
+  double ebias[IPG_MAX_SNAP_SPECIES];  // -beta[s] . bzero (energy shift of bzero_flag)
 };
 
 struct SnapHost {
@@ -53,6 +55,7 @@ struct SnapHost {
   std::vector<int32_t> y_off, y_jjz;
   std::vector<int32_t> y_jjb;     // component whose beta scales each Z entry in Y
   std::vector<double> y_mult;     // multiplicity * (j1+1)/(j+1) factor of each Z entry
+  std::vector<int32_t> zperm;     // Z entries sorted by (nb, na): equal trip counts per warp
 };
 
 int snap_build_tables(const ipg_snap_params& p, SnapHost& h);

@@ -267,3 +267,62 @@ __device__ __forceinline__ void chain_utot_dispatch(int mb, double2 a, double2 b
 }
 
 }  // namespace snapchain
+
+namespace snapchain {
+
+constexpr int u_block(int j) { return j * (j + 1) * (2 * j + 1) / 6; }  // idxu_block[j]
+
+// Writes the warp-wide sum of sw * (row mb of level j) into the full Utot matrix: the
+// entry itself and its inversion-symmetric mirror (compute_ui.jl:105-125); wself on the
+// diagonal at the first neighbor chunk (zero_uarraytot, compute_ui.jl:131-152), later
+// chunks accumulate.  Only lane 0 writes; the warp owns this atom's row mb entries.
+template <int J, int j, int mb>
+__device__ __forceinline__ void emit_row(const ChainU<J>& s, double sw, double2* __restrict__ ut, int lane,
+                                         bool first, double wself) {
+  constexpr int ub = u_block(j);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (2 * mb == j && ma > mb) continue;  // middle row: these are mirrors of ma' = j - ma
+    double x = sw * s.u[ma].x, y = sw * s.u[ma].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      y += __shfl_xor_sync(0xffffffffu, y, o);
+    }
+    if (lane == 0) {
+      const int e = ub + mb * (j + 1) + ma;
+      double2 v = first ? make_double2(ma == mb ? wself : 0.0, 0.0) : ut[e];
+      v.x += x;
+      v.y += y;
+      ut[e] = v;
+      if (!(2 * mb == j && ma == mb)) {
+        const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+        ut[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * v.x, -sg * v.y);
+      }
+    }
+  }
+}
+
+template <int J, int j, int MB>
+__device__ __forceinline__ void run_levels_emit(ChainU<J>& s, double2 a, double2 b, double sw, double2* ut,
+                                                int lane, bool first, double wself) {
+  if constexpr (j <= J) {
+    advance_u<J, j, MB>(s, a, b);
+    emit_row<J, j, MB>(s, sw, ut, lane, first, wself);
+    run_levels_emit<J, j + 1, MB>(s, a, b, sw, ut, lane, first, wself);
+  }
+}
+
+template <int J, int MB>
+__device__ __forceinline__ void chain_utot_emit(double2 a, double2 b, double sw, double2* ut, int lane, bool first,
+                                                double wself) {
+  ChainU<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) s.u[c] = make_double2(0.0, 0.0);
+  s.u[0] = make_double2(1.0, 0.0);
+  staircase_u<J, 0, MB>(s, a, b);
+  emit_row<J, 2 * MB, MB>(s, sw, ut, lane, first, wself);
+  run_levels_emit<J, 2 * MB + 1, MB>(s, a, b, sw, ut, lane, first, wself);
+}
+
+}  // namespace snapchain

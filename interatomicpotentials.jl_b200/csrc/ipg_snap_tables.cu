@@ -6,6 +6,7 @@
 // sums, :250-312) and sqrt(p/q) roots (:314-321), because the descriptors are defined by
 // that ordering.  Derived tables (half-plane offsets, the Y gather list, the dB term list)
 // are new and serve the CUDA kernels.
+#include <algorithm>
 #include <cmath>
 
 #include "ipg_snap.cuh"
@@ -189,6 +190,14 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
   h.y_off.assign(h.u_half + 1, 0);
   for (int z = 0; z < h.idxz_max; z++) h.y_off[h.zjju_half[z] + 1]++;
   for (int q = 0; q < h.u_half; q++) h.y_off[q + 1] += h.y_off[q];
+  // Z entries in order of their loop shape, so that the threads of a warp that take
+  // consecutive entries run identical (nb, na) trip counts
+  h.zperm.resize(h.idxz_max);
+  for (int z = 0; z < h.idxz_max; z++) h.zperm[z] = z;
+  std::stable_sort(h.zperm.begin(), h.zperm.end(), [&](int a, int b) {
+    const ZDev &p = h.idxz[a], &q = h.idxz[b];
+    return p.nb != q.nb ? p.nb < q.nb : p.na < q.na;
+  });
   h.y_jjz.assign(h.idxz_max, 0);
   std::vector<int32_t> fill(h.y_off.begin(), h.y_off.end() - 1);
   for (int z = 0; z < h.idxz_max; z++) h.y_jjz[fill[h.zjju_half[z]]++] = z;
