@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
           }
         y.x *= w;
         y.y *= w;
-        io.yout[(size_t)i * uh + h] = y;
+        io.yout[(size_t)h * io.n + i] = y;
         const double2 u = ut[S.idxu_block[j] + ee];
         e += u.x * y.x + u.y * y.y;
       }
@@ -431,18 +431,7 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
           s.y += c * zz.y;
         }
         ys[h] = s;
-        if (io.yout) {  // half-plane weight folded in: 1, 1/2 on the middle element, 0 beyond
-          int j = 0;
-          while (j < J && S.half_block[j + 1] <= h) j++;
-          const int e = h - S.half_block[j], mb = e / (j + 1), ma = e - mb * (j + 1);
-          const double w = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
-          io.yout[(size_t)i * uh + h] = make_double2(w * s.x, w * s.y);
-        }
       }
-    }
-    if (MODE == MODE_ADJ && io.yout) {  // the per-neighbor part runs in k_snap_pair_adj
-      __syncthreads();
-      continue;
     }
     double2* vall = reinterpret_cast<double2*>(smem + L.duf);  // VJP: [nwarps][u_half]
     if (MODE == MODE_VJP)
@@ -665,10 +654,96 @@ int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, c
   }
 }
 
+
+// Adjoint per-atom part, "atoms in lanes": a block takes YS_ATOMS atoms, keeps their
+// Utot in shared memory as [entry][atom] and every lane walks the same Z entries for its
+// own atom, so table and Clebsch-Gordan loads are warp-uniform broadcasts and the Utot
+// reads are conflict-free.  Warp w owns a cost-balanced set of half-plane entries h and
+// accumulates Y_h = sum_{Z entries of h} coef * Z in registers (design of
+// compute_yi.jl:23-121), then writes Y'_h = w_h Y_h to yout[h][atom] and adds
+// Re(conj(U_h) Y'_h) to the atom's energy: E_i = (2/3) sum_h Re(conj(U_h) Y'_h) - beta.bzero
+// (B is cubic in U).
+__global__ void __launch_bounds__(YS_WARPS * 32, 1) k_snap_yatoms(const __grid_constant__ SnapDev S, int64_t n,
+                                                                  const int32_t* __restrict__ species,
+                                                                  const double2* __restrict__ utot,
+                                                                  double2* __restrict__ yout, double* __restrict__ Ei) {
+  extern __shared__ double2 us[];  // [idxu_max][YS_ATOMS]
+  __shared__ double esum[YS_WARPS][YS_ATOMS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int U = S.idxu_max;
+  for (int64_t a0 = (int64_t)blockIdx.x * YS_ATOMS; a0 < n; a0 += (int64_t)gridDim.x * YS_ATOMS) {
+    const int na_blk = (int)((n - a0) < YS_ATOMS ? (n - a0) : YS_ATOMS);
+    for (int idx = threadIdx.x; idx < U * YS_ATOMS; idx += blockDim.x) {
+      const int q = idx / YS_ATOMS, l = idx - q * YS_ATOMS;
+      us[idx] = l < na_blk ? utot[(size_t)(a0 + l) * U + q] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int64_t atom = a0 + lane;
+    const bool valid = lane < na_blk;
+    const int si = valid ? clamp_sp(species[atom], S.nsp) : 0;
+    const double* yc = S.ycoef + (size_t)si * S.idxz_max;
+    double e = 0.0;
+    for (int hh = S.ysched_off[warp]; hh < S.ysched_off[warp + 1]; hh++) {
+      const int h = S.ysched_h[hh];
+      double yr = 0.0, yi = 0.0;
+      for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
+        const int jjz = S.y_jjz[q];
+        const ZDev z = S.idxz[jjz];
+        const double* cgb = S.cglist + z.cgoff;
+        const int j1 = z.j1, j2 = z.j2;
+        double zr = 0.0, zi = 0.0;
+        const double2* p1 = us + (size_t)z.u1base * YS_ATOMS + lane;
+        const double2* p2 = us + (size_t)z.u2base * YS_ATOMS + lane;
+        int icgb = z.icgb0;
+        for (int ib = 0; ib < z.nb; ib++) {
+          double sr = 0.0, sim = 0.0;
+          int icga = z.icga0;
+          for (int ia = 0; ia < z.na; ia++) {
+            const double2 u1 = p1[ia * YS_ATOMS];
+            const double2 u2 = p2[-ia * YS_ATOMS];
+            const double c = __ldg(cgb + icga);
+            sr += c * (u1.x * u2.x - u1.y * u2.y);
+            sim += c * (u1.x * u2.y + u1.y * u2.x);
+            icga += j2;
+          }
+          const double cb = __ldg(cgb + icgb);
+          zr += cb * sr;
+          zi += cb * sim;
+          p1 += (j1 + 1) * YS_ATOMS;
+          p2 -= (j2 + 1) * YS_ATOMS;
+          icgb += j2;
+        }
+        if (S.bnorm_flag) {
+          zr /= (z.j + 1);
+          zi /= (z.j + 1);
+        }
+        const double c = yc[jjz];
+        yr += c * zr;
+        yi += c * zi;
+      }
+      const double w = S.ysched_w[hh];
+      yr *= w;
+      yi *= w;
+      if (valid) yout[(size_t)h * n + atom] = make_double2(yr, yi);
+      const double2 u = us[(size_t)S.u_of_h[h] * YS_ATOMS + lane];
+      e += u.x * yr + u.y * yi;
+    }
+    esum[warp][lane] = e;
+    __syncthreads();
+    if (warp == 0 && valid) {
+      double t = 0.0;
+      for (int w = 0; w < YS_WARPS; w++) t += esum[w][lane];
+      Ei[atom] = (2.0 / 3.0) * t + S.ebias[si];
+    }
+    __syncthreads();
+  }
+}
+
 // Adjoint per-neighbor kernel: one thread per (directed pair, chain MB); see
-// ipg_snap_chain.cuh.  part[p][MB][3] = chain MB's share of dE_i/dr_ij.
+// ipg_snap_chain.cuh.  Yw is the weighted Y as [h][natoms]; part[p][MB][3] = chain MB's
+// share of dE_i/dr_ij.
 template <int J, int MB>
-__global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ SnapDev S, int64_t np,
+__global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ SnapDev S, int64_t np, int64_t natoms,
                                                        const int32_t* __restrict__ owner,
                                                        const int32_t* __restrict__ nbr, const double* __restrict__ rij,
                                                        const int32_t* __restrict__ species,
@@ -691,7 +766,7 @@ __global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ S
     G.dsu[k] = PG.dsfac * PG.u[k];
   }
   double S0, Sk[3];
-  snapchain::chain_adjoint<J, MB>(G, Yw + (size_t)i * S.u_half, S0, Sk);
+  snapchain::chain_adjoint<J, MB>(G, Yw + i, natoms, S0, Sk);
   constexpr int NCH = J / 2 + 1;
   double* out = part + ((size_t)p * NCH + MB) * 3;
 #pragma unroll
@@ -701,24 +776,24 @@ __global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ S
 constexpr int PAIR_CHAIN_MAX_J = 10;  // twojmax handled by the register-chain kernel
 
 template <int J, int MB>
-int launch_chain(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int32_t* owner, const int32_t* nbr,
-                 const double* rij, const int32_t* species, const double2* Yw, double* part) {
+int launch_chain(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+                 const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
   if constexpr (MB <= J / 2) {
     const int T = 128;
-    IPG_TIMED_LAUNCH(ctx, "snap_pair", (k_snap_pair_adj<J, MB>), nblk(np, T), T, 0, S, np, owner, nbr, rij, species,
-                     Yw, part);
-    return launch_chain<J, MB + 1>(ctx, S, np, owner, nbr, rij, species, Yw, part);
+    IPG_TIMED_LAUNCH(ctx, "snap_pair", (k_snap_pair_adj<J, MB>), nblk(np, T), T, 0, S, np, natoms, owner, nbr, rij,
+                     species, Yw, part);
+    return launch_chain<J, MB + 1>(ctx, S, np, natoms, owner, nbr, rij, species, Yw, part);
   }
   return IPG_OK;
 }
 
-int launch_pair_adj(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int32_t* owner, const int32_t* nbr,
-                    const double* rij, const int32_t* species, const double2* Yw, double* part) {
+int launch_pair_adj(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+                    const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
   if (np == 0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return launch_chain<JJ, 0>(ctx, S, np, owner, nbr, rij, species, Yw, part);
+    return launch_chain<JJ, 0>(ctx, S, np, natoms, owner, nbr, rij, species, Yw, part);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
 #undef IPG_J
     default:
@@ -973,7 +1048,11 @@ int upload_tables(ipg_snap* s) {
   size_t o_yjjz = o_yoff + pad(h.y_off.size() * 4);
   size_t o_yjjb = o_yjjz + pad(h.y_jjz.size() * 4);
   size_t o_zperm = o_yjjb + pad(h.y_jjb.size() * 4);
-  size_t total = o_zperm + pad(h.zperm.size() * 4);
+  size_t o_yso = o_zperm + pad(h.zperm.size() * 4);
+  size_t o_ysh = o_yso + pad(h.ysched_off.size() * 4);
+  size_t o_ysw = o_ysh + pad(h.ysched_h.size() * 4);
+  size_t o_uoh = o_ysw + pad(h.ysched_w.size() * 8);
+  size_t total = o_uoh + pad(h.u_of_h.size() * 4);
   CUDA_RET(ctx, cudaMalloc(&s->d_tables, total));
   char* b = static_cast<char*>(s->d_tables);
   std::vector<char> hostbuf(total, 0);
@@ -986,6 +1065,10 @@ int upload_tables(ipg_snap* s) {
   memcpy(hostbuf.data() + o_yjjz, h.y_jjz.data(), h.y_jjz.size() * 4);
   memcpy(hostbuf.data() + o_yjjb, h.y_jjb.data(), h.y_jjb.size() * 4);
   memcpy(hostbuf.data() + o_zperm, h.zperm.data(), h.zperm.size() * 4);
+  memcpy(hostbuf.data() + o_yso, h.ysched_off.data(), h.ysched_off.size() * 4);
+  memcpy(hostbuf.data() + o_ysh, h.ysched_h.data(), h.ysched_h.size() * 4);
+  memcpy(hostbuf.data() + o_ysw, h.ysched_w.data(), h.ysched_w.size() * 8);
+  memcpy(hostbuf.data() + o_uoh, h.u_of_h.data(), h.u_of_h.size() * 4);
   CUDA_RET(ctx, cudaMemcpy(b, hostbuf.data(), total, cudaMemcpyHostToDevice));
   SnapDev& d = s->dev;
   memset(&d, 0, sizeof(d));
@@ -1020,6 +1103,10 @@ int upload_tables(ipg_snap* s) {
   d.y_off = reinterpret_cast<const int32_t*>(b + o_yoff);
   d.y_jjz = reinterpret_cast<const int32_t*>(b + o_yjjz);
   d.zperm = reinterpret_cast<const int32_t*>(b + o_zperm);
+  d.ysched_off = reinterpret_cast<const int32_t*>(b + o_yso);
+  d.ysched_h = reinterpret_cast<const int32_t*>(b + o_ysh);
+  d.ysched_w = reinterpret_cast<const double*>(b + o_ysw);
+  d.u_of_h = reinterpret_cast<const int32_t*>(b + o_uoh);
   s->d_ymult = reinterpret_cast<double*>(b + o_ym);
   s->d_yjjb = reinterpret_cast<int32_t*>(b + o_yjjb);
   return IPG_OK;
@@ -1144,8 +1231,19 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     io.yout = yout;
     if (n) {
       IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
-      IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
-      IPG_RET(launch_pair_adj(ctx, dev, np, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+      const size_t ysm = (size_t)dev.idxu_max * YS_ATOMS * sizeof(double2);
+      if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
+        CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yatoms, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
+        int per_sm = 1;
+        CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yatoms, YS_WARPS * 32, ysm));
+        const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
+        const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
+        IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
+                         io.utot_in, yout, Ei);
+      } else {
+        IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
+      }
+      IPG_RET(launch_pair_adj(ctx, dev, np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
     }
   } else if (mode == MODE_ADJ) {
     IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));

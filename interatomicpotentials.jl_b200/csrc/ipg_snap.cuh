@@ -23,6 +23,8 @@ struct DBDev {
 };
 
 constexpr int SNAP_MAX_J = 12;
+constexpr int YS_WARPS = 8;     // warps of the atoms-in-lanes Y kernel
+constexpr int YS_ATOMS = 32;    // atoms per block of that kernel (one per lane)
 
 struct SnapDev {
   int J, nsp, K, idxu_max, idxz_max, u_half, ext_max, idxcg_max;
@@ -41,6 +43,12 @@ struct SnapDev {
   const double* ycoef;   // [nsp][idxz_max] multiplicity * factor * beta (set per beta)
   const double* beta;    // [nsp][K]
   const int32_t* zperm;  // [idxz_max] Z entries ordered by loop shape (nb, na)
+  // Y schedule of the atoms-in-lanes kernel: warp w owns half-plane entries
+  // ysched_h[ysched_off[w] .. ysched_off[w+1]) (cost-balanced), ysched_w their weights
+  const int32_t* ysched_off;  // [YS_WARPS+1]
+  const int32_t* ysched_h;
+  const double* ysched_w;
+  const int32_t* u_of_h;      // [u_half] index of half-plane entry h in the full Utot
   double ebias[IPG_MAX_SNAP_SPECIES];  // -beta[s] . bzero (energy shift of bzero_flag)
 };
 
@@ -56,6 +64,8 @@ struct SnapHost {
   std::vector<int32_t> y_jjb;     // component whose beta scales each Z entry in Y
   std::vector<double> y_mult;     // multiplicity * (j1+1)/(j+1) factor of each Z entry
   std::vector<int32_t> zperm;     // Z entries sorted by (nb, na): equal trip counts per warp
+  std::vector<int32_t> ysched_off, ysched_h, u_of_h;
+  std::vector<double> ysched_w;
 };
 
 int snap_build_tables(const ipg_snap_params& p, SnapHost& h);

@@ -122,13 +122,15 @@ __device__ __forceinline__ void staircase(Chain<J>& s, const Geom& G) {
   }
 }
 
+// Yw points at this atom's entry of h = 0 in the [h][atom] array; ys is the h stride.
 template <int J, int j, int mb>
-__device__ __forceinline__ void contract(const Chain<J>& s, const double2* __restrict__ Yw, double& S0, double* S) {
+__device__ __forceinline__ void contract(const Chain<J>& s, const double2* __restrict__ Yw, int64_t ys, double& S0,
+                                         double* S) {
   constexpr int base = half_block(j) + mb * (j + 1);
   constexpr int last = (2 * mb == j) ? mb : j;  // middle row of an even level stops at ma = j/2
 #pragma unroll
   for (int ma = 0; ma <= last; ma++) {
-    const double2 y = Yw[base + ma];
+    const double2 y = Yw[(base + ma) * ys];
     S0 += s.u[ma].x * y.x + s.u[ma].y * y.y;
 #pragma unroll
     for (int k = 0; k < 3; k++) S[k] += s.d[k][ma].x * y.x + s.d[k][ma].y * y.y;
@@ -136,18 +138,19 @@ __device__ __forceinline__ void contract(const Chain<J>& s, const double2* __res
 }
 
 template <int J, int j, int MB>
-__device__ __forceinline__ void run_levels(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, double& S0,
-                                           double* S) {
+__device__ __forceinline__ void run_levels(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, int64_t ys,
+                                           double& S0, double* S) {
   if constexpr (j <= J) {
     advance<J, j, MB>(s, G);
-    contract<J, j, MB>(s, Yw, S0, S);
-    run_levels<J, j + 1, MB>(s, G, Yw, S0, S);
+    contract<J, j, MB>(s, Yw, ys, S0, S);
+    run_levels<J, j + 1, MB>(s, G, Yw, ys, S0, S);
   }
 }
 
 // Chain MB of one neighbor: returns S0 and S[3].
 template <int J, int MB>
-__device__ __forceinline__ void chain_adjoint(const Geom& G, const double2* __restrict__ Yw, double& S0, double* S) {
+__device__ __forceinline__ void chain_adjoint(const Geom& G, const double2* __restrict__ Yw, int64_t ys, double& S0,
+                                              double* S) {
   Chain<J> s;
 #pragma unroll
   for (int c = 0; c <= J; c++) {
@@ -159,8 +162,8 @@ __device__ __forceinline__ void chain_adjoint(const Geom& G, const double2* __re
   staircase<J, 0, MB>(s, G);
   S0 = 0.0;
   S[0] = S[1] = S[2] = 0.0;
-  contract<J, 2 * MB, MB>(s, Yw, S0, S);
-  run_levels<J, 2 * MB + 1, MB>(s, G, Yw, S0, S);
+  contract<J, 2 * MB, MB>(s, Yw, ys, S0, S);
+  run_levels<J, 2 * MB + 1, MB>(s, G, Yw, ys, S0, S);
 }
 
 }  // namespace snapchain

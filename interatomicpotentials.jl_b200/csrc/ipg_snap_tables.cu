@@ -198,6 +198,44 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
     const ZDev &p = h.idxz[a], &q = h.idxz[b];
     return p.nb != q.nb ? p.nb < q.nb : p.na < q.na;
   });
+  // Y schedule: every half-plane entry with nonzero weight goes to one of YS_WARPS warps,
+  // longest first to the least loaded warp (cost = inner terms of its Z entries)
+  {
+    h.u_of_h.assign(h.u_half, 0);
+    std::vector<std::pair<double, int>> cost;  // (cost, h)
+    std::vector<double> wgt(h.u_half, 0.0);
+    std::vector<double> hc(h.u_half, 0.0);
+    for (int z = 0; z < h.idxz_max; z++) hc[h.zjju_half[z]] += h.idxz[z].nb * (2.0 + h.idxz[z].na) + 2.0;
+    for (int j = 0; j <= J; j++)
+      for (int mb = 0; 2 * mb <= j; mb++)
+        for (int ma = 0; ma <= j; ma++) {
+          const int hh = h.half_block[j] + mb * (j + 1) + ma;
+          h.u_of_h[hh] = h.idxu_block[j] + mb * (j + 1) + ma;
+          wgt[hh] = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
+          if (wgt[hh] != 0.0) cost.push_back({hc[hh], hh});
+        }
+    std::stable_sort(cost.begin(), cost.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+      return a.first > b.first;
+    });
+    std::vector<std::vector<int>> bins(YS_WARPS);
+    std::vector<double> load(YS_WARPS, 0.0);
+    for (auto& c : cost) {
+      int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      bins[w].push_back(c.second);
+      load[w] += c.first;
+    }
+    h.ysched_off.assign(YS_WARPS + 1, 0);
+    h.ysched_h.clear();
+    h.ysched_w.clear();
+    for (int w = 0; w < YS_WARPS; w++) {
+      std::sort(bins[w].begin(), bins[w].end());
+      for (int hh : bins[w]) {
+        h.ysched_h.push_back(hh);
+        h.ysched_w.push_back(wgt[hh]);
+      }
+      h.ysched_off[w + 1] = (int)h.ysched_h.size();
+    }
+  }
   h.y_jjz.assign(h.idxz_max, 0);
   std::vector<int32_t> fill(h.y_off.begin(), h.y_off.end() - 1);
   for (int z = 0; z < h.idxz_max; z++) h.y_jjz[fill[h.zjju_half[z]]++] = z;
