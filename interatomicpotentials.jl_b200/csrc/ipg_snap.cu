@@ -655,6 +655,37 @@ int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, c
 }
 
 
+// One Z entry (compute_z.jl:8-57) for the calling lane's atom, with na a compile-time
+// constant: the na Clebsch-Gordan factors of the inner sum are the same for every ib
+// (icga restarts at icga0), so they are loaded once; the inner sum is fully unrolled.
+template <int NA>
+__device__ __forceinline__ double2 zitem_lanes(const ZDev& z, const double* __restrict__ cgb,
+                                               const double2* __restrict__ p1, const double2* __restrict__ p2) {
+  double ca[NA];
+#pragma unroll
+  for (int ia = 0; ia < NA; ia++) ca[ia] = __ldg(cgb + z.icga0 + ia * z.j2);
+  const int s1 = (z.j1 + 1) * YS_ATOMS, s2 = (z.j2 + 1) * YS_ATOMS;
+  double zr = 0.0, zi = 0.0;
+  int icgb = z.icgb0;
+  for (int ib = 0; ib < z.nb; ib++) {
+    double sr = 0.0, sim = 0.0;
+#pragma unroll
+    for (int ia = 0; ia < NA; ia++) {
+      const double2 u1 = p1[ia * YS_ATOMS];
+      const double2 u2 = p2[-ia * YS_ATOMS];
+      sr += ca[ia] * (u1.x * u2.x - u1.y * u2.y);
+      sim += ca[ia] * (u1.x * u2.y + u1.y * u2.x);
+    }
+    const double cb = __ldg(cgb + icgb);
+    zr += cb * sr;
+    zi += cb * sim;
+    p1 += s1;
+    p2 -= s2;
+    icgb += z.j2;
+  }
+  return make_double2(zr, zi);
+}
+
 // Adjoint per-atom part, "atoms in lanes": a block takes YS_ATOMS atoms, keeps their
 // Utot in shared memory as [entry][atom] and every lane walks the same Z entries for its
 // own atom, so table and Clebsch-Gordan loads are warp-uniform broadcasts and the Utot
@@ -689,30 +720,20 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 1) k_snap_yatoms(const __grid_c
       for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
         const int jjz = S.y_jjz[q];
         const ZDev z = S.idxz[jjz];
-        const double* cgb = S.cglist + z.cgoff;
-        const int j1 = z.j1, j2 = z.j2;
-        double zr = 0.0, zi = 0.0;
         const double2* p1 = us + (size_t)z.u1base * YS_ATOMS + lane;
         const double2* p2 = us + (size_t)z.u2base * YS_ATOMS + lane;
-        int icgb = z.icgb0;
-        for (int ib = 0; ib < z.nb; ib++) {
-          double sr = 0.0, sim = 0.0;
-          int icga = z.icga0;
-          for (int ia = 0; ia < z.na; ia++) {
-            const double2 u1 = p1[ia * YS_ATOMS];
-            const double2 u2 = p2[-ia * YS_ATOMS];
-            const double c = __ldg(cgb + icga);
-            sr += c * (u1.x * u2.x - u1.y * u2.y);
-            sim += c * (u1.x * u2.y + u1.y * u2.x);
-            icga += j2;
-          }
-          const double cb = __ldg(cgb + icgb);
-          zr += cb * sr;
-          zi += cb * sim;
-          p1 += (j1 + 1) * YS_ATOMS;
-          p2 -= (j2 + 1) * YS_ATOMS;
-          icgb += j2;
+        double2 zz;
+        switch (z.na) {  // warp-uniform: every lane walks the same Z entry
+#define IPG_NA(NA) \
+  case NA:         \
+    zz = zitem_lanes<NA>(z, S.cglist + z.cgoff, p1, p2); \
+    break;
+          IPG_NA(1) IPG_NA(2) IPG_NA(3) IPG_NA(4) IPG_NA(5) IPG_NA(6) IPG_NA(7) IPG_NA(8) IPG_NA(9) IPG_NA(10)
+#undef IPG_NA
+          default:
+            zz = make_double2(0.0, 0.0);
         }
+        double zr = zz.x, zi = zz.y;
         if (S.bnorm_flag) {
           zr /= (z.j + 1);
           zi /= (z.j + 1);
