@@ -655,33 +655,61 @@ int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, c
 }
 
 
-// One Z entry (compute_z.jl:8-57) for the calling lane's atom, with na a compile-time
-// constant: the na Clebsch-Gordan factors of the inner sum are the same for every ib
-// (icga restarts at icga0), so they are loaded once; the inner sum is fully unrolled.
+// The inner CG sum of one ib for the calling lane's atom: sum_ia ca[ia] u1[ia] u2[ia]
+// with u1 = U(j1, mb1, ma1min + ia) and u2 = U(j2, mb2, ma2max - ia).  Only rows
+// mb <= j/2 are stored (the half plane, [h][atom]); a row beyond it is read from its
+// mirror, U[j][mb][ma] = (-1)^(ma+mb) conj(U[j][j-mb][j-ma]) (compute_ui.jl:105-125):
+// its sign alternates with ia (folded into the FMAs) and its conjugate flips the sign of
+// the imaginary part.  M1, M2 say which of the two rows is mirrored.
+template <int NA, bool M1, bool M2>
+__device__ __forceinline__ void zrow_lanes(const double* ca, const double2* __restrict__ p1,
+                                           const double2* __restrict__ p2, double& sr, double& sim) {
+  constexpr int d1 = M1 ? -YS_ATOMS : YS_ATOMS;  // step of ma1 in storage
+  constexpr int d2 = M2 ? YS_ATOMS : -YS_ATOMS;  // step of ma2 in storage
+#pragma unroll
+  for (int ia = 0; ia < NA; ia++) {
+    const double2 v1 = p1[ia * d1];
+    const double2 v2 = p2[ia * d2];
+    const double u1y = M1 ? -v1.y : v1.y;
+    const double u2y = M2 ? -v2.y : v2.y;
+    // alternating sign of a single mirrored row; two mirrored rows: signs cancel per ia
+    const double c = (M1 != M2 && (ia & 1)) ? -ca[ia] : ca[ia];
+    sr += c * (v1.x * v2.x - u1y * u2y);
+    sim += c * (v1.x * u2y + u1y * v2.x);
+  }
+}
+
+// One Z entry (compute_z.jl:8-57) for the calling lane's atom, na a compile-time
+// constant.  The na CG factors of the inner sum are the same for every ib (icga restarts
+// at icga0), so they are loaded once.
 template <int NA>
 __device__ __forceinline__ double2 zitem_lanes(const ZDev& z, const double* __restrict__ cgb,
-                                               const double2* __restrict__ p1, const double2* __restrict__ p2) {
+                                               const double2* __restrict__ uh, const int* __restrict__ hblk,
+                                               int mb1min, int ma1min, int mb2max, int ma2max) {
   double ca[NA];
 #pragma unroll
   for (int ia = 0; ia < NA; ia++) ca[ia] = __ldg(cgb + z.icga0 + ia * z.j2);
-  const int s1 = (z.j1 + 1) * YS_ATOMS, s2 = (z.j2 + 1) * YS_ATOMS;
+  const int j1 = z.j1, j2 = z.j2;
   double zr = 0.0, zi = 0.0;
   int icgb = z.icgb0;
   for (int ib = 0; ib < z.nb; ib++) {
+    const int mb1 = mb1min + ib, mb2 = mb2max - ib;
+    const bool m1 = 2 * mb1 > j1, m2 = 2 * mb2 > j2;
+    const int r1 = m1 ? j1 - mb1 : mb1, c1 = m1 ? j1 - ma1min : ma1min;
+    const int r2 = m2 ? j2 - mb2 : mb2, c2 = m2 ? j2 - ma2max : ma2max;
+    const double2* p1 = uh + (size_t)(hblk[j1] + r1 * (j1 + 1) + c1) * YS_ATOMS;
+    const double2* p2 = uh + (size_t)(hblk[j2] + r2 * (j2 + 1) + c2) * YS_ATOMS;
     double sr = 0.0, sim = 0.0;
-#pragma unroll
-    for (int ia = 0; ia < NA; ia++) {
-      const double2 u1 = p1[ia * YS_ATOMS];
-      const double2 u2 = p2[-ia * YS_ATOMS];
-      sr += ca[ia] * (u1.x * u2.x - u1.y * u2.y);
-      sim += ca[ia] * (u1.x * u2.y + u1.y * u2.x);
-    }
-    const double cb = __ldg(cgb + icgb);
+    if (!m1 && !m2) zrow_lanes<NA, false, false>(ca, p1, p2, sr, sim);
+    else if (m1 && !m2) zrow_lanes<NA, true, false>(ca, p1, p2, sr, sim);
+    else if (!m1 && m2) zrow_lanes<NA, false, true>(ca, p1, p2, sr, sim);
+    else zrow_lanes<NA, true, true>(ca, p1, p2, sr, sim);
+    // sign of the ia = 0 term of the mirrored row(s): (-1)^(ma+mb)
+    const int par = (m1 ? (ma1min + mb1) : 0) + (m2 ? (ma2max + mb2) : 0);
+    const double cb = (par & 1) ? -__ldg(cgb + icgb) : __ldg(cgb + icgb);
     zr += cb * sr;
     zi += cb * sim;
-    p1 += s1;
-    p2 -= s2;
-    icgb += z.j2;
+    icgb += j2;
   }
   return make_double2(zr, zi);
 }
@@ -694,19 +722,19 @@ __device__ __forceinline__ double2 zitem_lanes(const ZDev& z, const double* __re
 // compute_yi.jl:23-121), then writes Y'_h = w_h Y_h to yout[h][atom] and adds
 // Re(conj(U_h) Y'_h) to the atom's energy: E_i = (2/3) sum_h Re(conj(U_h) Y'_h) - beta.bzero
 // (B is cubic in U).
-__global__ void __launch_bounds__(YS_WARPS * 32, 1) k_snap_yatoms(const __grid_constant__ SnapDev S, int64_t n,
+__global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yatoms(const __grid_constant__ SnapDev S, int64_t n,
                                                                   const int32_t* __restrict__ species,
                                                                   const double2* __restrict__ utot,
                                                                   double2* __restrict__ yout, double* __restrict__ Ei) {
-  extern __shared__ double2 us[];  // [idxu_max][YS_ATOMS]
+  extern __shared__ double2 us[];  // half plane of Utot: [u_half][YS_ATOMS]
   __shared__ double esum[YS_WARPS][YS_ATOMS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int U = S.idxu_max;
+  const int U = S.idxu_max, UH = S.u_half;
   for (int64_t a0 = (int64_t)blockIdx.x * YS_ATOMS; a0 < n; a0 += (int64_t)gridDim.x * YS_ATOMS) {
     const int na_blk = (int)((n - a0) < YS_ATOMS ? (n - a0) : YS_ATOMS);
-    for (int idx = threadIdx.x; idx < U * YS_ATOMS; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < UH * YS_ATOMS; idx += blockDim.x) {
       const int q = idx / YS_ATOMS, l = idx - q * YS_ATOMS;
-      us[idx] = l < na_blk ? utot[(size_t)(a0 + l) * U + q] : make_double2(0.0, 0.0);
+      us[idx] = l < na_blk ? utot[(size_t)(a0 + l) * U + S.u_of_h[q]] : make_double2(0.0, 0.0);
     }
     __syncthreads();
     const int64_t atom = a0 + lane;
@@ -720,13 +748,15 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 1) k_snap_yatoms(const __grid_c
       for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
         const int jjz = S.y_jjz[q];
         const ZDev z = S.idxz[jjz];
-        const double2* p1 = us + (size_t)z.u1base * YS_ATOMS + lane;
-        const double2* p2 = us + (size_t)z.u2base * YS_ATOMS + lane;
+        // row/column starts of the two U factors (u1base/u2base decode)
+        const int ub1 = z.u1base - S.idxu_block[z.j1], ub2 = z.u2base - S.idxu_block[z.j2];
+        const int mb1min = ub1 / (z.j1 + 1), ma1min = ub1 - mb1min * (z.j1 + 1);
+        const int mb2max = ub2 / (z.j2 + 1), ma2max = ub2 - mb2max * (z.j2 + 1);
         double2 zz;
         switch (z.na) {  // warp-uniform: every lane walks the same Z entry
-#define IPG_NA(NA) \
-  case NA:         \
-    zz = zitem_lanes<NA>(z, S.cglist + z.cgoff, p1, p2); \
+#define IPG_NA(NA)                                                                                        \
+  case NA:                                                                                                \
+    zz = zitem_lanes<NA>(z, S.cglist + z.cgoff, us + lane, S.half_block, mb1min, ma1min, mb2max, ma2max); \
     break;
           IPG_NA(1) IPG_NA(2) IPG_NA(3) IPG_NA(4) IPG_NA(5) IPG_NA(6) IPG_NA(7) IPG_NA(8) IPG_NA(9) IPG_NA(10)
 #undef IPG_NA
@@ -746,7 +776,7 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 1) k_snap_yatoms(const __grid_c
       yr *= w;
       yi *= w;
       if (valid) yout[(size_t)h * n + atom] = make_double2(yr, yi);
-      const double2 u = us[(size_t)S.u_of_h[h] * YS_ATOMS + lane];
+      const double2 u = us[(size_t)h * YS_ATOMS + lane];
       e += u.x * yr + u.y * yi;
     }
     esum[warp][lane] = e;
@@ -1252,7 +1282,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     io.yout = yout;
     if (n) {
       IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
-      const size_t ysm = (size_t)dev.idxu_max * YS_ATOMS * sizeof(double2);
+      const size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
         CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yatoms, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
