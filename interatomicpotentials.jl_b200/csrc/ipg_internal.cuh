@@ -178,8 +178,11 @@ struct PairList {
 
 // mode: IPG_NLIST_HALF (cut[0] = rcut) or IPG_NLIST_FULL (cut = nsp*nsp cutsq), with
 // IPG_NLIST_LITERAL_SQRT optionally or-ed in.  want_transpose builds d_in_off/d_in_pair.
+// sorted: each atom's neighbors ascending (the reference's order); otherwise the
+// emission order (stencil cells in fixed order, ascending inside a cell), which is
+// equally deterministic.
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
-                    const double* h_cut, int mode, bool want_transpose, PairList& pl);
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true);
 
 // Device helper: the distinct neighbor-cell coordinates along one axis (<= 3).
 __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {

@@ -126,6 +126,7 @@ struct PairTest {
   int literal;       // utl.jl:81 literal search radius
   int nsp;
   double rcut;       // HALF: cutoff; FULL: candidate radius (cutmax or sqrt(cutmax))
+  double rcut2_lo, rcut2_hi;  // rcut^2 (1 -/+ 1e-12)
   double cutsq[64];  // FULL: [nsp][nsp], nsp <= 8
 };
 
@@ -140,7 +141,11 @@ __device__ __forceinline__ bool pair_ok(const PairTest& t, const double* L, int3
   double s0 = pe_axis_dev(L[0], xi.x, xj.x);
   double s1 = pe_axis_dev(L[1], xi.y, xj.y);
   double s2 = pe_axis_dev(L[2], xi.z, xj.z);
-  if (sqrt(sumsq3_dev(s0, s1, s2)) > t.rcut) return false;
+  // sqrt(d2) <= rcut decided exactly; the squared bounds (1e-12 relative margin, far
+  // above the rounding of sqrt and of rcut^2) settle all but the boundary cases
+  const double d2 = sumsq3_dev(s0, s1, s2);
+  if (d2 > t.rcut2_hi) return false;
+  if (d2 >= t.rcut2_lo && sqrt(d2) > t.rcut) return false;
   r[0] = disp_axis_dev(L[0], xi.x, xj.x);
   r[1] = disp_axis_dev(L[1], xi.y, xj.y);
   r[2] = disp_axis_dev(L[2], xi.z, xj.z);
@@ -339,7 +344,7 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
 }
 
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
-                    const double* h_cut, int mode, bool want_transpose, PairList& pl) {
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted) {
   (void)d_species;
   std::string pre(prefix);
   PairTest t;
@@ -359,6 +364,8 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
     double cutmax = std::sqrt(cutmax2);
     t.rcut = t.literal ? std::sqrt(cutmax) : cutmax;
   }
+  t.rcut2_lo = t.rcut * t.rcut * (1.0 - 1e-12);
+  t.rcut2_hi = t.rcut * t.rcut * (1.0 + 1e-12);
   int64_t n = cl.n;
   pl.n = n;
   int64_t* cnt;
@@ -377,7 +384,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   if (n > 0) {
     IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
-    IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
+    if (sorted) IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
   }
   if (want_transpose) {
     int64_t* fill;

@@ -26,6 +26,7 @@ struct PairTermDev {
 struct PairTerms {
   int nterms;
   double rcut_max;
+  double rmax2_hi;  // rcut_max^2 (1 + 1e-12): candidates beyond it are out for sure
   PairTermDev t[IPG_MAX_PAIR_TERMS];
 };
 
@@ -129,7 +130,9 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid*
             double p0 = pe_axis_dev(g.L[0], xi.x, xj.x);
             double p1 = pe_axis_dev(g.L[1], xi.y, xj.y);
             double p2 = pe_axis_dev(g.L[2], xi.z, xj.z);
-            double dist = sqrt(sumsq3_dev(p0, p1, p2));
+            const double d2 = sumsq3_dev(p0, p1, p2);
+            if (d2 > c_terms.rmax2_hi) continue;  // beyond every term's cutoff
+            double dist = sqrt(d2);
             if (dist > rmax) continue;
             int sj = (int)xj.w;
             double r0, r1, r2;
@@ -211,6 +214,7 @@ int prepare_terms(ipg_ctx* ctx, const ipg_pair_term* terms, int nterms, PairTerm
     return ipg_fail(ctx, IPG_ERR_ARG, "nterms must be in 0..%d", IPG_MAX_PAIR_TERMS);
   pt.nterms = nterms;
   pt.rcut_max = 0.0;
+  pt.rmax2_hi = 0.0;
   for (int k = 0; k < nterms; k++) {
     const ipg_pair_term& s = terms[k];
     PairTermDev& d = pt.t[k];
@@ -246,6 +250,7 @@ int prepare_terms(ipg_ctx* ctx, const ipg_pair_term* terms, int nterms, PairTerm
         return ipg_fail(ctx, IPG_ERR_ARG, "term %d: unknown kind %d", k, s.kind);
     }
   }
+  pt.rmax2_hi = pt.rcut_max * pt.rcut_max * (1.0 + 1e-12);
   return IPG_OK;
 }
 

@@ -935,15 +935,16 @@ __global__ void k_snap_gather(int64_t n, const int64_t* __restrict__ off, const 
     for (int c = 0; c < 6; c++) w6[6 * k + c] = w[c];
 }
 
-// Per-configuration sums (fixed order): E[c] = beta0 + sum Ei, W6[c] = sum w6.
-__global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ atom_off, const double* __restrict__ Ei,
-                              const double* __restrict__ w6, double beta0, double* __restrict__ E,
-                              double* __restrict__ W6) {
+// Per-configuration sums in fixed order: chunks of atoms (chunk table on the host:
+// config, first atom, end) are reduced by one block each, then the chunks of each
+// configuration are added in order: E[c] = beta0 + sum Ei, W6[c] = sum w6.
+constexpr int RED_CHUNK = 4096;
+__global__ void k_chunk_reduce(const int64_t* __restrict__ chunks, const double* __restrict__ Ei,
+                               const double* __restrict__ w6, double* __restrict__ part) {
   __shared__ double sm[7][128];
-  int c = blockIdx.x;
-  if (c >= nconf) return;
+  const int64_t a0 = chunks[3 * blockIdx.x + 1], a1 = chunks[3 * blockIdx.x + 2];
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int64_t i = atom_off[c] + threadIdx.x; i < atom_off[c + 1]; i += blockDim.x) {
+  for (int64_t i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
     acc[0] += Ei ? Ei[i] : 0.0;
     if (w6)
       for (int q = 0; q < 6; q++) acc[1 + q] += w6[6 * i + q];
@@ -955,11 +956,19 @@ __global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ atom_off, c
       for (int q = 0; q < 7; q++) sm[q][threadIdx.x] += sm[q][threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    if (E) E[c] = beta0 + sm[0][0];
-    if (W6)
-      for (int q = 0; q < 6; q++) W6[6 * c + q] = sm[1 + q][0];
-  }
+  if (threadIdx.x < 7) part[7 * blockIdx.x + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+__global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ conf_chunk, const double* __restrict__ part,
+                              double beta0, double* __restrict__ E, double* __restrict__ W6) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nconf) return;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t k = conf_chunk[c]; k < conf_chunk[c + 1]; k++)
+    for (int q = 0; q < 7; q++) acc[q] += part[7 * k + q];
+  if (E) E[c] = beta0 + acc[0];
+  if (W6)
+    for (int q = 0; q < 6; q++) W6[6 * c + q] = acc[1 + q];
 }
 
 // Per-atom force descriptors: dB_k[block s][b][c] = sum_{p in out(k), s_k = s} dbl_p -
@@ -1080,6 +1089,7 @@ struct ipg_snap {
   int threads = 128;
   int blocks_per_sm = 0;  // 0 = occupancy-derived
   bool generic_adjoint = false;  // force the in-block per-neighbor adjoint (testing)
+  std::vector<int64_t> chunk_tab;  // per-configuration reduction chunks (host staging)
   std::vector<double> beta_host;  // last uploaded beta
 };
 
@@ -1225,7 +1235,7 @@ int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int3
   IPG_RET(ipg_build_cells(s->ctx, "snap_", n, d_pos, d_species, s->p.nspecies, nconf, h_atom_off, h_L, s->radius,
                           cl));
   int mode = IPG_NLIST_FULL | (s->p.literal_sqrt_radius ? IPG_NLIST_LITERAL_SQRT : 0);
-  IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl));
+  IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl, false));
   return IPG_OK;
 }
 
@@ -1317,12 +1327,31 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_TIMED_LAUNCH(ctx, "snap_gather", k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off,
                      pl.d_in_pair, fvec, nch, d_pos, out.F, w6);
   if (out.E || out.W6) {
-    int64_t* d_aoff;
-    IPG_RET(scratch(ctx, "snap_aoff", (size_t)nconf + 1, &d_aoff));
-    int64_t* h = host_scratch<int64_t>(ctx, "snap_aoff_h", nconf + 1);
-    memcpy(h, h_atom_off, sizeof(int64_t) * (nconf + 1));
-    CUDA_RET(ctx, cudaMemcpyAsync(d_aoff, h, sizeof(int64_t) * (nconf + 1), cudaMemcpyHostToDevice, ctx->stream));
-    IPG_LAUNCH(ctx, k_conf_reduce, nconf, 128, 0, nconf, d_aoff, Ei, w6, beta0, out.E, out.W6);
+    // chunk table: [config, first atom, end] per chunk, then each config's chunk range
+    std::vector<int64_t>& ch = s->chunk_tab;
+    ch.clear();
+    std::vector<int64_t> cc(nconf + 1, 0);
+    for (int c = 0; c < nconf; c++) {
+      int64_t a = h_atom_off[c], b = h_atom_off[c + 1];
+      if (a == b) {
+        ch.insert(ch.end(), {c, a, a});
+      }
+      for (int64_t x = a; x < b; x += RED_CHUNK) ch.insert(ch.end(), {c, x, std::min(b, x + RED_CHUNK)});
+      cc[c + 1] = (int64_t)ch.size() / 3;
+    }
+    const int64_t nchunk = (int64_t)ch.size() / 3;
+    int64_t *d_ch, *d_cc;
+    double* part;
+    IPG_RET(scratch(ctx, "snap_chunks", ch.size() + cc.size(), &d_ch));
+    IPG_RET(scratch(ctx, "snap_chunk_part", 7 * (size_t)nchunk, &part));
+    int64_t* hb = host_scratch<int64_t>(ctx, "snap_chunks_h", ch.size() + cc.size());
+    memcpy(hb, ch.data(), sizeof(int64_t) * ch.size());
+    memcpy(hb + ch.size(), cc.data(), sizeof(int64_t) * cc.size());
+    CUDA_RET(ctx, cudaMemcpyAsync(d_ch, hb, sizeof(int64_t) * (ch.size() + cc.size()), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    d_cc = d_ch + ch.size();
+    IPG_LAUNCH(ctx, k_chunk_reduce, (unsigned)nchunk, 128, 0, d_ch, Ei, w6, part);
+    IPG_LAUNCH(ctx, k_conf_reduce, nblk(nconf, 128), 128, 0, nconf, d_cc, part, beta0, out.E, out.W6);
   }
   if (out.dB && n) {
     int32_t* owner;
