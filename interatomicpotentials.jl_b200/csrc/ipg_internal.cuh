@@ -200,6 +200,42 @@ __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {
   }
   return cnt;
 }
+// The 27-cell stencil of cell c as contiguous ranges of the cell-sorted slot array:
+// x-adjacent cells of one (z, y) row are consecutive unless the row wraps, so there are
+// at most 9 rows of at most 3 ranges (usually 9 ranges in all).
+struct StencilRanges {
+  int n;
+  int64_t beg[27], end[27];
+};
+__device__ __forceinline__ void stencil_ranges(const ConfGrid& g, const int* c, const int64_t* __restrict__ cell_start,
+                                               StencilRanges& R) {
+  int sx[3], sy[3], sz[3];
+  const int nx = stencil_axis(c[0], g.nc[0], !isinf(g.L[0]), sx);
+  const int ny = stencil_axis(c[1], g.nc[1], !isinf(g.L[1]), sy);
+  const int nz = stencil_axis(c[2], g.nc[2], !isinf(g.L[2]), sz);
+  // x cells ascending, then runs of consecutive cells merge into one range
+  for (int a = 1; a < nx; a++)
+    for (int b = a; b > 0 && sx[b - 1] > sx[b]; b--) {
+      int t = sx[b];
+      sx[b] = sx[b - 1];
+      sx[b - 1] = t;
+    }
+  R.n = 0;
+  for (int a = 0; a < nz; a++)
+    for (int b = 0; b < ny; b++) {
+      const int64_t row = g.cell_off + ((int64_t)sz[a] * g.nc[1] + sy[b]) * g.nc[0];
+      int d = 0;
+      while (d < nx) {
+        int e = d;
+        while (e + 1 < nx && sx[e + 1] == sx[e] + 1) e++;
+        R.beg[R.n] = cell_start[row + sx[d]];
+        R.end[R.n] = cell_start[row + sx[e] + 1];
+        R.n++;
+        d = e + 1;
+      }
+    }
+}
+
 __device__ __forceinline__ void cell_coords(const ConfGrid& g, double x, double y, double z, int* c) {
   double p[3] = {x, y, z};
 #pragma unroll

@@ -157,43 +157,47 @@ __device__ __forceinline__ bool pair_ok(const PairTest& t, const double* L, int3
   return rsq <= t.cutsq[(int)xi.w * t.nsp + (int)xj.w];
 }
 
+// One warp per atom (cell-sorted order): lanes take consecutive candidates of each
+// stencil range (coalesced), ballots count the members, and the emit pass writes them
+// in candidate order (ballot prefix), so the list is deterministic.
 template <bool EMIT>
-__global__ void k_pair_walk(int64_t n, PairTest t, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ conf,
-                            const int64_t* __restrict__ cell_start, const int32_t* __restrict__ cell_atoms,
-                            const double4* __restrict__ spos, int64_t* __restrict__ cnt,
-                            const int64_t* __restrict__ off, int32_t* __restrict__ outj, double* __restrict__ outr) {
-  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  int32_t i = cell_atoms[s];
-  double4 xi = spos[s];
+__global__ void __launch_bounds__(128) k_pair_walk(int64_t n, PairTest t, const ConfGrid* __restrict__ grid,
+                                                   const int32_t* __restrict__ conf,
+                                                   const int64_t* __restrict__ cell_start,
+                                                   const int32_t* __restrict__ cell_atoms,
+                                                   const double4* __restrict__ spos, int64_t* __restrict__ cnt,
+                                                   const int64_t* __restrict__ off, int32_t* __restrict__ outj,
+                                                   double* __restrict__ outr) {
+  const int lane = threadIdx.x & 31;
+  const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (s >= n) return;  // warp-uniform
+  const int32_t i = cell_atoms[s];
+  const double4 xi = spos[s];
   const ConfGrid g = grid[conf[i]];
   int c[3];
   cell_coords(g, xi.x, xi.y, xi.z, c);
-  int sx[3], sy[3], sz[3];
-  int nx = stencil_axis(c[0], g.nc[0], !isinf(g.L[0]), sx);
-  int ny = stencil_axis(c[1], g.nc[1], !isinf(g.L[1]), sy);
-  int nz = stencil_axis(c[2], g.nc[2], !isinf(g.L[2]), sz);
-  int64_t k = 0, base = EMIT ? off[i] : 0;
-  for (int a = 0; a < nz; a++)
-    for (int b = 0; b < ny; b++)
-      for (int d = 0; d < nx; d++) {
-        int64_t cell = g.cell_off + ((int64_t)sz[a] * g.nc[1] + sy[b]) * g.nc[0] + sx[d];
-        int64_t e = cell_start[cell + 1];
-        for (int64_t q = cell_start[cell]; q < e; q++) {
-          int32_t j = cell_atoms[q];
-          double r[3];
-          if (pair_ok(t, g.L, i, xi, j, spos[q], r)) {
-            if (EMIT) {
-              outj[base + k] = j;
-              outr[3 * (base + k)] = r[0];
-              outr[3 * (base + k) + 1] = r[1];
-              outr[3 * (base + k) + 2] = r[2];
-            }
-            k++;
-          }
-        }
+  StencilRanges R;
+  stencil_ranges(g, c, cell_start, R);
+  int64_t k = 0;
+  const int64_t base = EMIT ? off[i] : 0;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int r = 0; r < R.n; r++)
+    for (int64_t q0 = R.beg[r]; q0 < R.end[r]; q0 += 32) {
+      const int64_t q = q0 + lane;
+      double rr[3];
+      bool ok = false;
+      if (q < R.end[r]) ok = pair_ok(t, g.L, i, xi, cell_atoms[q], spos[q], rr);
+      const unsigned bal = __ballot_sync(0xffffffffu, ok);
+      if (EMIT && ok) {
+        const int64_t o = base + k + __popc(bal & lt);
+        outj[o] = cell_atoms[q];
+        outr[3 * o] = rr[0];
+        outr[3 * o + 1] = rr[1];
+        outr[3 * o + 2] = rr[2];
       }
-  if (!EMIT) cnt[i] = k;
+      k += __popc(bal);
+    }
+  if (!EMIT && lane == 0) cnt[i] = k;
 }
 
 // Sorts each atom's list by neighbor index (insertion sort; lists are short).
@@ -373,7 +377,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   cnt = pl.d_off;
   CUDA_RET(ctx, cudaMemsetAsync(cnt, 0, sizeof(int64_t) * (n + 1), ctx->stream));
   if (n > 0)
-    IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+    IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
   IPG_RET(ipg_scan_i64(ctx, cnt, pl.d_off, n + 1));
   CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -382,7 +386,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0) {
-    IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+    IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
     if (sorted) IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
   }

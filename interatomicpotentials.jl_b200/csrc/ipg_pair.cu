@@ -95,88 +95,124 @@ __device__ __forceinline__ void term_eval(const PairTermDev& t, double R, double
 }
 
 constexpr int PAIR_T = 128;
+constexpr int PAIR_WARPS = PAIR_T / 32;
+
+// One warp per atom (cell-sorted order).  Lanes test consecutive candidates of each
+// stencil range; the pairs within the largest cutoff are compacted into a per-warp
+// shared buffer (ballot prefix, candidate order), and every 32 of them are evaluated by
+// the whole warp, so the term arithmetic (exp, pow) runs on full warps.
+struct Hit {
+  double r0, r1, r2, dist;
+  int sj, pad;
+};
+
+__device__ __forceinline__ void eval_hits(const Hit* __restrict__ hb, int nh, int lane, int si, double* acc,
+                                          double& f0, double& f1, double& f2) {
+  if (lane >= nh) return;
+  const Hit h = hb[lane];
+  const double R = sqrt(h.r0 * h.r0 + h.r1 * h.r1 + h.r2 * h.r2);
+  double V = 0.0, gsum = 0.0;
+  for (int t = 0; t < c_terms.nterms; t++) {
+    const PairTermDev& T = c_terms.t[t];
+    if (h.dist > T.rcut) continue;
+    if (!((T.mask >> si) & 1ull) || !((T.mask >> h.sj) & 1ull)) continue;
+    double v, gg;
+    term_eval(T, R, v, gg);
+    V += T.coeff * v;
+    gsum += T.coeff * gg;
+  }
+  const double fx = gsum * h.r0, fy = gsum * h.r1, fz = gsum * h.r2;
+  f0 += fx;
+  f1 += fy;
+  f2 += fz;
+  acc[0] += 0.5 * V;
+  // empirical_potential.jl:63-64: r * f' -> [xx, yy, zz, zy, zx, yx]
+  acc[1] += 0.5 * h.r0 * fx;
+  acc[2] += 0.5 * h.r1 * fy;
+  acc[3] += 0.5 * h.r2 * fz;
+  acc[4] += 0.5 * h.r2 * fy;
+  acc[5] += 0.5 * h.r2 * fx;
+  acc[6] += 0.5 * h.r1 * fx;
+}
 
 __global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid* __restrict__ grid,
                                                       const int64_t* __restrict__ cell_start,
                                                       const int32_t* __restrict__ cell_atoms,
                                                       const double4* __restrict__ spos, double* __restrict__ F,
                                                       double* __restrict__ partial, int* status) {
-  __shared__ double red[PAIR_T / 32][7];
-  int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ Hit hits[PAIR_WARPS][64];
+  __shared__ double red[PAIR_WARPS][7];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t s = (int64_t)blockIdx.x * PAIR_WARPS + w;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // E, W[6]
-  if (s < n) {
-    int32_t i = cell_atoms[s];
-    double4 xi = spos[s];
-    int si = (int)xi.w;
+  if (s < n) {  // warp-uniform
+    const int32_t i = cell_atoms[s];
+    const double4 xi = spos[s];
+    const int si = (int)xi.w;
     const ConfGrid g = grid[0];
     int c[3];
     cell_coords(g, xi.x, xi.y, xi.z, c);
-    int sx[3], sy[3], sz[3];
-    int nx = stencil_axis(c[0], g.nc[0], !isinf(g.L[0]), sx);
-    int ny = stencil_axis(c[1], g.nc[1], !isinf(g.L[1]), sy);
-    int nz = stencil_axis(c[2], g.nc[2], !isinf(g.L[2]), sz);
+    StencilRanges Rg;
+    stencil_ranges(g, c, cell_start, Rg);
     double f0 = 0.0, f1 = 0.0, f2 = 0.0;
-    const int nt = c_terms.nterms;
     const double rmax = c_terms.rcut_max;
-    for (int a = 0; a < nz; a++)
-      for (int b = 0; b < ny; b++)
-        for (int d = 0; d < nx; d++) {
-          int64_t cell = ((int64_t)sz[a] * g.nc[1] + sy[b]) * g.nc[0] + sx[d];
-          int64_t e = cell_start[cell + 1];
-          for (int64_t q = cell_start[cell]; q < e; q++) {
-            int32_t j = cell_atoms[q];
-            if (j == i) continue;
-            double4 xj = spos[q];
-            double p0 = pe_axis_dev(g.L[0], xi.x, xj.x);
-            double p1 = pe_axis_dev(g.L[1], xi.y, xj.y);
-            double p2 = pe_axis_dev(g.L[2], xi.z, xj.z);
+    Hit* hb = hits[w];
+    int nh = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int r = 0; r < Rg.n; r++)
+      for (int64_t q0 = Rg.beg[r]; q0 < Rg.end[r]; q0 += 32) {
+        const int64_t q = q0 + lane;
+        bool ok = false;
+        Hit h;
+        if (q < Rg.end[r]) {
+          const int32_t j = cell_atoms[q];
+          const double4 xj = spos[q];
+          if (j != i) {
+            const double p0 = pe_axis_dev(g.L[0], xi.x, xj.x);
+            const double p1 = pe_axis_dev(g.L[1], xi.y, xj.y);
+            const double p2 = pe_axis_dev(g.L[2], xi.z, xj.z);
             const double d2 = sumsq3_dev(p0, p1, p2);
-            if (d2 > c_terms.rmax2_hi) continue;  // beyond every term's cutoff
-            double dist = sqrt(d2);
-            if (dist > rmax) continue;
-            int sj = (int)xj.w;
-            double r0, r1, r2;
-            if (j > i) {
-              r0 = disp_axis_dev(g.L[0], xi.x, xj.x);
-              r1 = disp_axis_dev(g.L[1], xi.y, xj.y);
-              r2 = disp_axis_dev(g.L[2], xi.z, xj.z);
-            } else {
-              r0 = -disp_axis_dev(g.L[0], xj.x, xi.x);
-              r1 = -disp_axis_dev(g.L[1], xj.y, xi.y);
-              r2 = -disp_axis_dev(g.L[2], xj.z, xi.z);
+            if (d2 <= c_terms.rmax2_hi) {
+              const double dist = sqrt(d2);
+              if (dist <= rmax) {
+                ok = true;
+                h.dist = dist;
+                h.sj = (int)xj.w;
+                if (j > i) {
+                  h.r0 = disp_axis_dev(g.L[0], xi.x, xj.x);
+                  h.r1 = disp_axis_dev(g.L[1], xi.y, xj.y);
+                  h.r2 = disp_axis_dev(g.L[2], xi.z, xj.z);
+                } else {  // -get_displacement(x_j, x_i): the reference's stored half pair
+                  h.r0 = -disp_axis_dev(g.L[0], xj.x, xi.x);
+                  h.r1 = -disp_axis_dev(g.L[1], xj.y, xi.y);
+                  h.r2 = -disp_axis_dev(g.L[2], xj.z, xi.z);
+                }
+              }
             }
-            double R = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-            double V = 0.0, gsum = 0.0;
-            for (int t = 0; t < nt; t++) {
-              const PairTermDev& T = c_terms.t[t];
-              if (dist > T.rcut) continue;
-              if (!((T.mask >> si) & 1ull) || !((T.mask >> sj) & 1ull)) continue;
-              double v, gg;
-              term_eval(T, R, v, gg);
-              V += T.coeff * v;
-              gsum += T.coeff * gg;
-            }
-            double fx = gsum * r0, fy = gsum * r1, fz = gsum * r2;
-            f0 += fx;
-            f1 += fy;
-            f2 += fz;
-            acc[0] += 0.5 * V;
-            // empirical_potential.jl:63-64: r * f' -> [xx, yy, zz, zy, zx, yx]
-            acc[1] += 0.5 * r0 * fx;
-            acc[2] += 0.5 * r1 * fy;
-            acc[3] += 0.5 * r2 * fz;
-            acc[4] += 0.5 * r2 * fy;
-            acc[5] += 0.5 * r2 * fx;
-            acc[6] += 0.5 * r1 * fx;
           }
         }
-    if (F) {
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) hb[nh + __popc(bal & lt)] = h;
+        nh += __popc(bal);
+        __syncwarp();
+        if (nh >= 32) {
+          eval_hits(hb, 32, lane, si, acc, f0, f1, f2);
+          __syncwarp();
+          if (lane < nh - 32) hb[lane] = hb[32 + lane];
+          nh -= 32;
+          __syncwarp();
+        }
+      }
+    eval_hits(hb, nh, lane, si, acc, f0, f1, f2);
+    f0 = warp_sum(f0);
+    f1 = warp_sum(f1);
+    f2 = warp_sum(f2);
+    if (F && lane == 0) {
       F[3 * (int64_t)i] = f0;
       F[3 * (int64_t)i + 1] = f1;
       F[3 * (int64_t)i + 2] = f2;
     }
   }
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     double v = warp_sum(acc[k]);
@@ -185,7 +221,7 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid*
   __syncthreads();
   if (threadIdx.x < 7) {
     double v = 0.0;
-    for (int q = 0; q < PAIR_T / 32; q++) v += red[q][threadIdx.x];
+    for (int q = 0; q < PAIR_WARPS; q++) v += red[q][threadIdx.x];
     partial[(int64_t)blockIdx.x * 7 + threadIdx.x] = v;
   }
 }
@@ -264,7 +300,7 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
   int64_t aoff[2] = {0, n};
   CellList cl;
   IPG_RET(ipg_build_cells(ctx, "pair_", n, d_pos, d_species, 64, 1, aoff, L, pt.rcut_max, cl));
-  int64_t nb = std::max<int64_t>(1, (n + PAIR_T - 1) / PAIR_T);
+  int64_t nb = std::max<int64_t>(1, (n + PAIR_WARPS - 1) / PAIR_WARPS);
   double *partial, *red;
   IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
   IPG_RET(scratch(ctx, "pair_red", 8, &red));
