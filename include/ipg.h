@@ -141,6 +141,20 @@ IPG_API int ipg_pair_eval(ipg_ctx* ctx, int64_t n, const double* pos, const int3
 IPG_API int ipg_pair_eval_dev(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
                       const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
                       uint32_t flags);
+/* ipg_pair_eval_dev for callers that cannot allocate device memory (no counterpart in
+ * the reference): an MD engine that owns all device memory up front, or a host that
+ * holds only a stream and device buffers and must not create a context (creating one
+ * allocates).  Same inputs, outputs and results; no context, no allocation.  Its scratch
+ * is a fixed device array of about 4.3 MB that every GPU loading the library keeps until
+ * exit; at most 65,536 atoms (larger n returns IPG_ERR_CAPACITY before any launch).
+ * Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream) on the
+ * current device and not synchronised.  Calls share the scratch array: calls that overlap
+ * on the GPU race, so serialise them (one stream).  The first call on a device resolves
+ * the scratch address; make it before any stream capture.  Device-side input errors
+ * (non-finite positions) are not reported. */
+IPG_API int ipg_pair_eval_noalloc(void* stream, int64_t n, const double* d_pos, const int32_t* d_species,
+                                  const double L[3], const ipg_pair_term* terms, int32_t nterms, double* d_E,
+                                  double* d_F, double* d_W6, uint32_t flags);
 
 /* ---- SNAP -------------------------------------------------------------------------------
  * ipg_snap_params mirrors SNAP{S,T} (src/BasisSystems/SNAP/types/types.jl:8-25).

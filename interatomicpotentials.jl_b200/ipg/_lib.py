@@ -30,7 +30,7 @@ MAX_PAIR_TERMS = 16
 API_SYMBOLS = (
     "ipg_create", "ipg_destroy", "ipg_last_error", "ipg_set_timeout_ms", "ipg_set_stream", "ipg_version",
     "ipg_launch_count", "ipg_timing_enable", "ipg_timing_read", "ipg_neighbor_build", "ipg_nlist_size", "ipg_nlist_export", "ipg_nlist_free",
-    "ipg_pair_eval", "ipg_pair_eval_dev", "ipg_snap_create", "ipg_snap_destroy", "ipg_snap_ncoeff",
+    "ipg_pair_eval", "ipg_pair_eval_dev", "ipg_pair_eval_noalloc", "ipg_snap_create", "ipg_snap_destroy", "ipg_snap_ncoeff",
     "ipg_snap_descriptors", "ipg_snap_energy_forces", "ipg_snap_energy_forces_dev", "ipg_snap_vjp_beta",
     "ipg_snap_batch_energy_forces", "ipg_snap_batch_energy_forces_dev", "ipg_snap_batch_loss_grad",
 )
@@ -83,6 +83,7 @@ def lib():
         "ipg_nlist_free": (C.c_int, [vp]),
         "ipg_pair_eval": (C.c_int, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, u32]),
         "ipg_pair_eval_dev": (C.c_int, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, u32]),
+        "ipg_pair_eval_noalloc": (C.c_int, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, u32]),
         "ipg_snap_create": (C.c_int, [vp, vp, C.POINTER(vp)]),
         "ipg_snap_destroy": (C.c_int, [vp]),
         "ipg_snap_ncoeff": (C.c_int, [vp, C.POINTER(i32)]),
