@@ -824,6 +824,68 @@ __global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ S
   for (int k = 0; k < 3; k++) out[k] = 2.0 * (G.dsu[k] * S0 + G.sfac * Sk[k]);
 }
 
+// Adjoint per-neighbor kernel, all chains of a pair in one thread (saved start rows in
+// shared memory): part[p][0][3] = dE_i/dr_ij.
+constexpr int PAIR_ALL_T = 128;
+template <int J>
+__global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_constant__ SnapDev S, int64_t np,
+                                                                  int64_t natoms, const int32_t* __restrict__ owner,
+                                                                  const int32_t* __restrict__ nbr,
+                                                                  const double* __restrict__ rij,
+                                                                  const int32_t* __restrict__ species,
+                                                                  const double2* __restrict__ Yw,
+                                                                  double* __restrict__ part) {
+  extern __shared__ double2 save[];  // [4 (J+1)][PAIR_ALL_T]
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const int i = owner[p];
+  const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
+  const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+  PairGeom PG;
+  geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+  snapchain::Geom G;
+  G.a = PG.a;
+  G.b = PG.b;
+  G.sfac = PG.sfac;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    G.da[k] = PG.da[k];
+    G.db[k] = PG.db[k];
+    G.dsu[k] = PG.dsfac * PG.u[k];
+  }
+  double S0, Sk[3];
+  snapchain::all_chains_adjoint<J>(G, Yw + i, natoms, S0, Sk, save, PAIR_ALL_T, threadIdx.x);
+  double* out = part + (size_t)p * 3;
+#pragma unroll
+  for (int k = 0; k < 3; k++) out[k] = 2.0 * (G.dsu[k] * S0 + G.sfac * Sk[k]);
+}
+
+template <int J>
+int launch_pair_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+                    const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
+  const size_t sm = (size_t)4 * (J + 1) * PAIR_ALL_T * sizeof(double2);
+  if (sm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_pair_adj_all<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  IPG_TIMED_LAUNCH(ctx, "snap_pair", k_snap_pair_adj_all<J>, nblk(np, PAIR_ALL_T), PAIR_ALL_T, sm, S, np, natoms,
+                   owner, nbr, rij, species, Yw, part);
+  return IPG_OK;
+}
+
+int launch_pair_adj_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+                        const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw,
+                        double* part) {
+  if (np == 0) return IPG_OK;
+  switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_pair_all<JJ>(ctx, S, np, natoms, owner, nbr, rij, species, Yw, part);
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
+  }
+}
+
 constexpr int PAIR_CHAIN_MAX_J = 10;  // twojmax handled by the register-chain kernel
 
 template <int J, int MB>
@@ -1090,6 +1152,7 @@ struct ipg_snap {
   int blocks_per_sm = 0;  // 0 = occupancy-derived
   bool generic_adjoint = false;  // force the in-block per-neighbor adjoint (testing)
   std::vector<int64_t> chunk_tab;  // per-configuration reduction chunks (host staging)
+  bool pair_split = false;  // adjoint pair kernel: one thread per (pair, chain) instead of per pair
   std::vector<double> beta_host;  // last uploaded beta
 };
 
@@ -1283,7 +1346,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   int nch = 1;
   if (mode == MODE_ADJ && chains) {
     // per-atom kernel writes the weighted Y; the register-chain kernel does the neighbors
-    nch = dev.J / 2 + 1;
+    nch = s->pair_split ? dev.J / 2 + 1 : 1;
     double2* yout;
     int32_t* owner;
     IPG_RET(scratch(ctx, "snap_yout", (size_t)n * dev.u_half + 1, &yout));
@@ -1304,7 +1367,10 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       } else {
         IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
       }
-      IPG_RET(launch_pair_adj(ctx, dev, np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+      if (s->pair_split)
+        IPG_RET(launch_pair_adj(ctx, dev, np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+      else
+        IPG_RET(launch_pair_adj_all(ctx, dev, np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
     }
   } else if (mode == MODE_ADJ) {
     IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
@@ -1447,6 +1513,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
     }
   }
   if (const char* g = getenv("IPG_GENERIC_ADJOINT")) s->generic_adjoint = g[0] == '1';
+  if (const char* g = getenv("IPG_PAIR_SPLIT")) s->pair_split = g[0] == '1';
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);

@@ -329,3 +329,82 @@ __device__ __forceinline__ void chain_utot_emit(double2 a, double2 b, double sw,
 }
 
 }  // namespace snapchain
+
+namespace snapchain {
+
+// ---- all chains of one neighbor in one thread ------------------------------------------
+// Chain mb's start row (row mb+1 of level 2mb+1, the mirror of chain mb's row there) is
+// saved when chain mb passes that level and restored for chain mb+1: every half-plane
+// entry is computed once, no staircase.  The saved row lives in shared memory as
+// save[(comp * (J+1) + c) * nthreads + tid] (thread index fastest: conflict-free).
+template <int J, int j>
+__device__ __forceinline__ void save_mirror(const Chain<J>& s, double2* __restrict__ save, int nt, int tid) {
+  constexpr int R = (j + 1) / 2;
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+    const double2 u = s.u[j - c];
+    save[(0 * (J + 1) + c) * nt + tid] = make_double2(sg * u.x, -sg * u.y);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double2 d = s.d[k][j - c];
+      save[((1 + k) * (J + 1) + c) * nt + tid] = make_double2(sg * d.x, -sg * d.y);
+    }
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void load_row(Chain<J>& s, const double2* __restrict__ save, int nt, int tid) {
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    s.u[c] = save[(0 * (J + 1) + c) * nt + tid];
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][c] = save[((1 + k) * (J + 1) + c) * nt + tid];
+  }
+}
+
+template <int J, int j, int MB>
+__device__ __forceinline__ void levels_save(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, int64_t ys,
+                                            double& S0, double* S, double2* save, int nt, int tid) {
+  if constexpr (j <= J) {
+    advance<J, j, MB>(s, G);
+    contract<J, j, MB>(s, Yw, ys, S0, S);
+    if constexpr (j == 2 * MB + 1 && MB + 1 <= J / 2) save_mirror<J, j>(s, save, nt, tid);
+    levels_save<J, j + 1, MB>(s, G, Yw, ys, S0, S, save, nt, tid);
+  }
+}
+
+template <int J, int MB>
+__device__ __forceinline__ void chains_from(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, int64_t ys,
+                                            double& S0, double* S, double2* save, int nt, int tid) {
+  if constexpr (MB <= J / 2) {
+    if constexpr (MB > 0) {
+      // keep the compiler from hoisting this chain's loads into the previous chain
+      asm volatile("" ::: "memory");
+      load_row<J, 2 * MB - 1>(s, save, nt, tid);  // row MB of level 2MB-1
+      advance<J, 2 * MB, MB>(s, G);
+      contract<J, 2 * MB, MB>(s, Yw, ys, S0, S);
+    }
+    levels_save<J, 2 * MB + 1, MB>(s, G, Yw, ys, S0, S, save, nt, tid);
+    chains_from<J, MB + 1>(s, G, Yw, ys, S0, S, save, nt, tid);
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void all_chains_adjoint(const Geom& G, const double2* __restrict__ Yw, int64_t ys,
+                                                   double& S0, double* S, double2* save, int nt, int tid) {
+  Chain<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);
+  S0 = 0.0;
+  S[0] = S[1] = S[2] = 0.0;
+  contract<J, 0, 0>(s, Yw, ys, S0, S);
+  chains_from<J, 0>(s, G, Yw, ys, S0, S, save, nt, tid);
+}
+
+}  // namespace snapchain
