@@ -43,6 +43,14 @@ WORKLOAD = ("snap_j8: SNAP twojmax=8 (55 components), 2 species (weights 1.0/0.5
             "adjoint-Y energy+forces (neighbor build included)")
 
 
+# timing name -> kernel
+KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot<8,MB>",
+                "snap_pair": "k_snap_pair_adj_all<8>"}
+# DRAM bytes per atom of one launch, from the ncu capture summarised in
+# profiles/k_snap_yatoms_snap_j8.md (16,000 atoms; traffic grows with the atom count).
+NCU_DRAM_BYTES_PER_ATOM = {}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -281,19 +289,36 @@ def main():
     e2e = {"value": world * n * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": int(24 * n + 4 * n + 8 * nsp * K), "d2h_bytes_per_step": int(24 * n + 8 * 8)}
 
-    # roofline of the dominant kernel (the fused per-atom SNAP kernel, FP64 pipe)
+    # roofline: every timed SNAP kernel against the measured FP64 peak; the dominant one (largest
+    # share of the step) is the headline.  Flops are algorithmic (ipg/flops.py), per launch.
     probe = C.CDLL(os.path.join(ROOT, "interatomicpotentials.jl_b200", "ipg", "libipg_probe.so"))
     probe.ipg_probe_fp64_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     tf = C.c_double()
     probe.ipg_probe_fp64_peak(local, 5, C.byref(tf), None)
     fp64_peak = tf.value
-    ka_ms, ka_n = kt.get("snap_atom", (0.0, 0))
-    flops_launch = FL.snap_atom_kernel(prm["twojmax"], n, npairs, "adjoint")
-    achieved = flops_launch / (ka_ms / max(ka_n, 1) * 1e-3) / 1e12 if ka_n else None
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": (achieved / fp64_peak) if achieved else None, "traffic": None,
-                "kernel": "k_snap_atom<adjoint>", "peak_source": "measured DFMA probe (libipg_probe.so), this run",
-                "flops_per_launch": flops_launch, "avg_launch_ms": ka_ms / max(ka_n, 1)}
+    kflops = FL.adjoint_kernels(prm["twojmax"], n, npairs)
+    per_kernel = {}
+    for k, fl in kflops.items():
+        k_ms, k_n = kt.get(k, (0.0, 0))
+        if not k_n:
+            continue
+        avg = k_ms / k_n
+        ach = fl / (avg * 1e-3) / 1e12
+        per_kernel[k] = {"kernel": KERNEL_NAMES[k], "flops_per_launch": fl, "avg_launch_ms": avg,
+                         "achieved_tflops": ach, "frac": ach / fp64_peak, "share_of_step": k_ms / ms_adj}
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["share_of_step"]) if per_kernel else None
+    traffic = None
+    if dom in NCU_DRAM_BYTES_PER_ATOM:
+        traffic = NCU_DRAM_BYTES_PER_ATOM[dom] * n
+    roofline = {"bound": "fp64", "achieved": per_kernel[dom]["achieved_tflops"] if dom else None,
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": per_kernel[dom]["frac"] if dom else None,
+                "traffic": traffic, "kernel": KERNEL_NAMES.get(dom), "flops_per_launch": kflops.get(dom),
+                "avg_launch_ms": per_kernel[dom]["avg_launch_ms"] if dom else None,
+                "peak_source": "measured DFMA probe (libipg_probe.so) in this run; the HBM peak of "
+                               "MEASURED_PEAKS.json does not bound these FP64-pipe kernels",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the "
+                                  "16,000-atom case, scaled by atoms" if traffic else None,
+                "kernels": per_kernel}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_adj / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -748,10 +748,7 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yatoms(const __grid_c
       for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
         const int jjz = S.y_jjz[q];
         const ZDev z = S.idxz[jjz];
-        // row/column starts of the two U factors (u1base/u2base decode)
-        const int ub1 = z.u1base - S.idxu_block[z.j1], ub2 = z.u2base - S.idxu_block[z.j2];
-        const int mb1min = ub1 / (z.j1 + 1), ma1min = ub1 - mb1min * (z.j1 + 1);
-        const int mb2max = ub2 / (z.j2 + 1), ma2max = ub2 - mb2max * (z.j2 + 1);
+        const int mb1min = z.mb1min, ma1min = z.ma1min, mb2max = z.mb2max, ma2max = z.ma2max;
         double2 zz;
         switch (z.na) {  // warp-uniform: every lane walks the same Z entry
 #define IPG_NA(NA)                                                                                        \
@@ -778,6 +775,207 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yatoms(const __grid_c
       if (valid) yout[(size_t)h * n + atom] = make_double2(yr, yi);
       const double2 u = us[(size_t)h * YS_ATOMS + lane];
       e += u.x * yr + u.y * yi;
+    }
+    esum[warp][lane] = e;
+    __syncthreads();
+    if (warp == 0 && valid) {
+      double t = 0.0;
+      for (int w = 0; w < YS_WARPS; w++) t += esum[w][lane];
+      Ei[atom] = (2.0 / 3.0) * t + S.ebias[si];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Row-blocked Y kernel.  Same block shape as k_snap_yatoms (32 atoms in the lanes, the
+// half plane of their Utot in shared memory as [h][atom]), but a warp owns whole target
+// rows (j, mb) of Y and, for each triple (j1, j2, j) feeding the row and each of its nb
+// row pairs (mb1, mb2), evaluates the Z entries of every ma of the row at once:
+//   Y(j, mb, ma) += c cg[mb1][mb2] sum_ma2 ca[ma][ma2] U(j1, mb1, ma + d - ma2) U(j2, mb2, ma2),
+// d = (j1 + j2 - j)/2, c = the triple's Y coefficient (compute_yi.jl:86-118).  The j2 row
+// is walked two columns at a time; each element of the j1 row met by those two columns is
+// loaded once and used for both, so a Utot element is read from shared memory about
+// (NMA + 3) / (2 NMA) times per product instead of twice.  Only the target level j is a
+// template parameter: the code of one instantiation stays small enough for the
+// instruction cache although the warps of a block work on different rows.
+
+constexpr unsigned long long SIGNBIT = 0x8000000000000000ull;
+
+__device__ __forceinline__ double flip(double v, unsigned long long m) {
+  return __longlong_as_double(__double_as_longlong(v) ^ m);
+}
+
+// Guard entries (zeros) before and after the half plane in shared memory: the column
+// walks below read up to YR_GUARD entries past either end of a row.  Those reads meet a
+// CG factor of exactly zero (the factor tables are zero wherever ma1 or ma2 is out of
+// range), so they only have to stay inside the array and be finite.
+__host__ __device__ constexpr int yr_guard(int J) { return J + 2; }
+
+// The j2 row of a row pair: two columns per step, the mirror (a row beyond the half plane,
+// U[j][mb][ma] = (-1)^(ma+mb) conj(U[j][j-mb][j-ma])) handled with runtime strides and
+// sign masks.
+struct YrRow2 {
+  const double2* p;  // logical column 0
+  int st;            // +-YS_ATOMS
+  unsigned long long sx0, cj;  // sign mask of column 0; conjugation mask
+  __device__ __forceinline__ void init(const double2* __restrict__ usl, const int* __restrict__ hblk, int j, int mb) {
+    const bool m = 2 * mb > j;
+    p = usl + (size_t)(hblk[j] + (m ? j - mb : mb) * (j + 1) + (m ? j : 0)) * YS_ATOMS;
+    st = m ? -YS_ATOMS : YS_ATOMS;
+    sx0 = (m && (mb & 1)) ? SIGNBIT : 0ull;
+    cj = m ? SIGNBIT : 0ull;
+  }
+  __device__ __forceinline__ double2 get(int ma) const {  // ma in -1 .. j+1
+    const double2 v = p[ma * st];
+    const unsigned long long sx = ((ma & 1) && cj) ? (sx0 ^ SIGNBIT) : sx0;
+    return make_double2(flip(v.x, sx), flip(v.y, sx ^ cj));
+  }
+};
+
+// One row pair (mb1, mb2) of a triple for the target-row tile ma = ma0 .. ma0+NT-1.  The
+// j1 row is walked as a window: element t of column pair m0 is ma1 = d - m0 - 1 + ma0 + t,
+// met by (ma = ma0 + t - 1, ma2 = m0) and (ma = ma0 + t, ma2 = m0 + 1).  M1: the j1 row is
+// mirrored.  cp: the triple's factors as [m0/2][ma = 0..j][2], rs = j + 1.
+template <int NT, bool M1>
+__device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const int* __restrict__ hblk,
+                                        const double2* __restrict__ cp, int rs, int ma0, int j1, int j2, int d,
+                                        int mb1, int mb2, double cb, double2 (&acc)[NT]) {
+  const double2* p1 = usl + (size_t)(hblk[j1] + (M1 ? j1 - mb1 : mb1) * (j1 + 1) + (M1 ? j1 : 0)) * YS_ATOMS;
+  // mirror sign (-1)^(ma1 + mb1) of the even elements t; the parity of d - m0 - 1 + ma0 is fixed
+  const unsigned long long sxe = (M1 && ((d - 1 + ma0 + mb1) & 1)) ? SIGNBIT : 0ull;
+  YrRow2 r2;
+  r2.init(usl, hblk, j2, mb2);
+  cp += ma0;
+  for (int m0 = 0; m0 <= j2; m0 += 2, cp += rs) {
+    double2 r[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const double2 v = r2.get(m0 + q);
+      r[q] = make_double2(cb * v.x, cb * v.y);
+    }
+    double2 a[NT];
+#pragma unroll
+    for (int i = 0; i < NT; i++) a[i] = __ldg(cp + i);
+    const int base = d - m0 - 1 + ma0;
+    const double2* pb = p1 + (M1 ? -base : base) * YS_ATOMS;
+#pragma unroll
+    for (int t = 0; t <= NT; t++) {
+      double2 u = pb[(M1 ? -t : t) * YS_ATOMS];
+      if (M1) {
+        const unsigned long long sx = (t & 1) ? (sxe ^ SIGNBIT) : sxe;
+        u = make_double2(flip(u.x, sx), flip(u.y, sx ^ SIGNBIT));
+      }
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int i = t - 1 + q;
+        if (i < 0 || i >= NT) continue;
+        const double c = q ? a[i].y : a[i].x;
+        const double tx = c * u.x, ty = c * u.y;
+        acc[i].x = fma(tx, r[q].x, fma(-ty, r[q].y, acc[i].x));
+        acc[i].y = fma(tx, r[q].y, fma(ty, r[q].x, acc[i].y));
+      }
+    }
+  }
+}
+
+// Tile ma0 .. ma0+NT-1 of target row (j, mb): every triple and row pair of the row.
+// Writes Y' = w Y of the tile's entries below nma and returns their Re(conj(U) Y').
+template <int NT>
+__device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, int ma0, int nma,
+                                          const double2* __restrict__ usl, const double* __restrict__ yc, int64_t n,
+                                          int64_t atom, bool valid, double2* __restrict__ yout) {
+  double2 acc[NT];
+#pragma unroll
+  for (int i = 0; i < NT; i++) acc[i] = make_double2(0.0, 0.0);
+  const int j = row.j, rs = j + 1;
+  const double bn = S.bnorm_flag ? 1.0 / (j + 1) : 1.0;
+  for (int t = row.t0; t < row.t1; t++) {
+    const YItemDev it = S.yitems[t];
+    const double c = yc[it.jjz] * bn;
+    const double* __restrict__ cg = S.cglist + it.cg;
+    const double2* __restrict__ cp = reinterpret_cast<const double2*>(S.yca + it.ca);
+    const int j1 = it.j1, j2 = it.j2, d = it.d, s2 = j2 + 1;
+    for (int ib = 0; ib < it.nb; ib++) {
+      const int mb1 = it.mb1min + ib, mb2 = it.mb2max - ib;
+      const double cb = c * __ldg(cg + mb1 * s2 + mb2);
+      if (2 * mb1 > j1)
+        yr_pair<NT, true>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, acc);
+      else
+        yr_pair<NT, false>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, acc);
+    }
+  }
+  double e = 0.0;
+#pragma unroll
+  for (int i = 0; i < NT; i++) {
+    const int ma = ma0 + i;
+    if (ma >= nma) break;
+    const double w = (row.mid && ma == nma - 1) ? 0.5 : 1.0;
+    const double2 y = make_double2(w * acc[i].x, w * acc[i].y);
+    const int h = row.h0 + ma;
+    if (valid) yout[(size_t)h * n + atom] = y;
+    const double2 u = usl[(size_t)h * YS_ATOMS];
+    e += u.x * y.x + u.y * y.y;
+  }
+  return e;
+}
+
+// Tiles of a row of nma entries: at most YR_TILE wide, as even as possible.
+constexpr int YR_TILE = 6;
+
+__device__ __forceinline__ double yr_row(const SnapDev& S, const YRowDev& row, const double2* __restrict__ usl,
+                                         const double* __restrict__ yc, int64_t n, int64_t atom, bool valid,
+                                         double2* __restrict__ yout) {
+  const int nma = row.mid ? row.mb + 1 : row.j + 1;
+  const int ntile = (nma + YR_TILE - 1) / YR_TILE;
+  double e = 0.0;
+  int ma0 = 0;
+  for (int k = 0; k < ntile; k++) {
+    const int w = (nma - ma0 + (ntile - k) - 1) / (ntile - k);  // remaining entries over remaining tiles
+    switch (w) {
+#define IPG_NT(NT) \
+  case NT:         \
+    e += yr_tile<NT>(S, row, ma0, nma, usl, yc, n, atom, valid, yout); \
+    break;
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
+#undef IPG_NT
+      default:
+        break;
+    }
+    ma0 += w;
+  }
+  return e;
+}
+
+__global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_constant__ SnapDev S, int64_t n,
+                                                                 const int32_t* __restrict__ species,
+                                                                 const double2* __restrict__ utot,
+                                                                 double2* __restrict__ yout, double* __restrict__ Ei) {
+  extern __shared__ double2 ush[];  // guard | half plane of Utot [u_half][YS_ATOMS] | guard
+  __shared__ double esum[YS_WARPS][YS_ATOMS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int U = S.idxu_max, UH = S.u_half, G = yr_guard(S.J);
+  double2* us = ush + G * YS_ATOMS;
+  for (int idx = threadIdx.x; idx < G * YS_ATOMS; idx += blockDim.x) {
+    ush[idx] = make_double2(0.0, 0.0);
+    us[UH * YS_ATOMS + idx] = make_double2(0.0, 0.0);
+  }
+  for (int64_t a0 = (int64_t)blockIdx.x * YS_ATOMS; a0 < n; a0 += (int64_t)gridDim.x * YS_ATOMS) {
+    const int na_blk = (int)((n - a0) < YS_ATOMS ? (n - a0) : YS_ATOMS);
+    for (int idx = threadIdx.x; idx < UH * YS_ATOMS; idx += blockDim.x) {
+      const int q = idx / YS_ATOMS, l = idx - q * YS_ATOMS;
+      us[idx] = l < na_blk ? utot[(size_t)(a0 + l) * U + S.u_of_h[q]] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int64_t atom = a0 + lane;
+    const bool valid = lane < na_blk;
+    const int si = valid ? clamp_sp(species[atom], S.nsp) : 0;
+    const double* yc = S.ycoef + (size_t)si * S.idxz_max;
+    const double2* usl = us + lane;
+    double e = 0.0;
+    for (int r = S.yrsched_off[warp]; r < S.yrsched_off[warp + 1]; r++) {
+      const YRowDev row = S.yrows[r];
+      e += yr_row(S, row, usl, yc, n, atom, valid, yout);
     }
     esum[warp][lane] = e;
     __syncthreads();
@@ -1153,6 +1351,7 @@ struct ipg_snap {
   bool generic_adjoint = false;  // force the in-block per-neighbor adjoint (testing)
   std::vector<int64_t> chunk_tab;  // per-configuration reduction chunks (host staging)
   bool pair_split = false;  // adjoint pair kernel: one thread per (pair, chain) instead of per pair
+  bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
   std::vector<double> beta_host;  // last uploaded beta
 };
 
@@ -1176,7 +1375,11 @@ int upload_tables(ipg_snap* s) {
   size_t o_ysh = o_yso + pad(h.ysched_off.size() * 4);
   size_t o_ysw = o_ysh + pad(h.ysched_h.size() * 4);
   size_t o_uoh = o_ysw + pad(h.ysched_w.size() * 8);
-  size_t total = o_uoh + pad(h.u_of_h.size() * 4);
+  size_t o_yrso = o_uoh + pad(h.u_of_h.size() * 4);
+  size_t o_yrows = o_yrso + pad(h.yrsched_off.size() * 4);
+  size_t o_yit = o_yrows + pad(h.yrows.size() * sizeof(YRowDev));
+  size_t o_yca = o_yit + pad(h.yitems.size() * sizeof(YItemDev));
+  size_t total = o_yca + pad(h.yca.size() * 8);
   CUDA_RET(ctx, cudaMalloc(&s->d_tables, total));
   char* b = static_cast<char*>(s->d_tables);
   std::vector<char> hostbuf(total, 0);
@@ -1193,6 +1396,10 @@ int upload_tables(ipg_snap* s) {
   memcpy(hostbuf.data() + o_ysh, h.ysched_h.data(), h.ysched_h.size() * 4);
   memcpy(hostbuf.data() + o_ysw, h.ysched_w.data(), h.ysched_w.size() * 8);
   memcpy(hostbuf.data() + o_uoh, h.u_of_h.data(), h.u_of_h.size() * 4);
+  memcpy(hostbuf.data() + o_yrso, h.yrsched_off.data(), h.yrsched_off.size() * 4);
+  memcpy(hostbuf.data() + o_yrows, h.yrows.data(), h.yrows.size() * sizeof(YRowDev));
+  memcpy(hostbuf.data() + o_yit, h.yitems.data(), h.yitems.size() * sizeof(YItemDev));
+  memcpy(hostbuf.data() + o_yca, h.yca.data(), h.yca.size() * 8);
   CUDA_RET(ctx, cudaMemcpy(b, hostbuf.data(), total, cudaMemcpyHostToDevice));
   SnapDev& d = s->dev;
   memset(&d, 0, sizeof(d));
@@ -1231,6 +1438,10 @@ int upload_tables(ipg_snap* s) {
   d.ysched_h = reinterpret_cast<const int32_t*>(b + o_ysh);
   d.ysched_w = reinterpret_cast<const double*>(b + o_ysw);
   d.u_of_h = reinterpret_cast<const int32_t*>(b + o_uoh);
+  d.yrsched_off = reinterpret_cast<const int32_t*>(b + o_yrso);
+  d.yrows = reinterpret_cast<const YRowDev*>(b + o_yrows);
+  d.yitems = reinterpret_cast<const YItemDev*>(b + o_yit);
+  d.yca = reinterpret_cast<const double*>(b + o_yca);
   s->d_ymult = reinterpret_cast<double*>(b + o_ym);
   s->d_yjjb = reinterpret_cast<int32_t*>(b + o_yjjb);
   return IPG_OK;
@@ -1355,15 +1566,22 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     io.yout = yout;
     if (n) {
       IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
-      const size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
+      size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
-        CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yatoms, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
+        const bool rows = dev.J <= YR_MAX_J && !s->y_entries;
+        const void* kfn = rows ? (const void*)k_snap_yrows : (const void*)k_snap_yatoms;
+        if (rows) ysm += (size_t)2 * yr_guard(dev.J) * YS_ATOMS * sizeof(double2);
+        CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
-        CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yatoms, YS_WARPS * 32, ysm));
+        CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, YS_WARPS * 32, ysm));
         const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
         const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
-        IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
-                         io.utot_in, yout, Ei);
+        if (rows)
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
+                           io.utot_in, yout, Ei);
+        else
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
+                           io.utot_in, yout, Ei);
       } else {
         IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
       }
@@ -1514,6 +1732,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   }
   if (const char* g = getenv("IPG_GENERIC_ADJOINT")) s->generic_adjoint = g[0] == '1';
   if (const char* g = getenv("IPG_PAIR_SPLIT")) s->pair_split = g[0] == '1';
+  if (const char* g = getenv("IPG_Y_ENTRIES")) s->y_entries = g[0] == '1';
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);

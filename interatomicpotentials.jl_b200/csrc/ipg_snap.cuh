@@ -6,13 +6,15 @@
 // One Z entry (one (j1, j2, j, ma, mb) of the idxz list, prebuilt_arrays.jl:183-216),
 // with the start offsets of its CG double sum precomputed.
 struct ZDev {
-  int16_t j1, j2, j, na, nb, pad;
+  int8_t j1, j2, j, na, nb, pad0, pad1, pad2;  // twojmax <= 12 bounds every index
+  int8_t ma1min, ma2max, mb1min, mb2max;       // row/column starts of the two U factors
   int32_t u1base;  // idxu_block[j1] + (j1+1)*mb1min + ma1min
   int32_t u2base;  // idxu_block[j2] + (j2+1)*mb2max + ma2max
   int32_t icga0;   // ma1min*(j2+1) + ma2max
   int32_t icgb0;   // mb1min*(j2+1) + mb2max
   int32_t cgoff;   // idxcg_block[j1][j2][j]
 };
+static_assert(sizeof(ZDev) == 32, "ZDev is read as two 16-byte words");
 
 // One bispectrum component (j1, j2, j) and the three half-plane sums of its
 // derivative (compute_b.jl:207-400): level l[t], first Z index z0[t], factor fac[t].
@@ -23,8 +25,25 @@ struct DBDev {
 };
 
 constexpr int SNAP_MAX_J = 12;
-constexpr int YS_WARPS = 8;     // warps of the atoms-in-lanes Y kernel
-constexpr int YS_ATOMS = 32;    // atoms per block of that kernel (one per lane)
+constexpr int YS_WARPS = 8;     // warps of the atoms-in-lanes Y kernels
+constexpr int YS_ATOMS = 32;    // atoms per block of those kernels (one per lane)
+constexpr int YR_MAX_J = 8;     // largest twojmax of the row-blocked Y kernel
+
+// Row-blocked Y kernel: a target row (j, mb) of the half plane of Y and the (j1, j2)
+// triples whose Z entries feed it.
+struct YRowDev {
+  int8_t j, mb, mid, pad;  // mid: middle row of an even level (weights vanish beyond ma = mb)
+  int32_t h0;              // half-plane index of (j, mb, ma = 0)
+  int32_t t0, t1;          // its triples: yitems[t0 .. t1)
+};
+struct YItemDev {
+  int8_t j1, j2, d, nb, mb1min, mb2max, pad0, pad1;  // d = (j1 + j2 - j) / 2
+  int32_t ca;   // offset in yca of the triple's CG factors, [m0/2][ma][2] (zero where out of range)
+  int32_t cg;   // idxcg_block[j1][j2][j]: the row factors cg[mb1 (j2+1) + mb2]
+  int32_t jjz;  // first Z entry of the triple (its Y coefficient)
+  int32_t pad2;
+};
+static_assert(sizeof(YItemDev) == 24, "YItemDev layout");
 
 struct SnapDev {
   int J, nsp, K, idxu_max, idxz_max, u_half, ext_max, idxcg_max;
@@ -49,6 +68,12 @@ struct SnapDev {
   const int32_t* ysched_h;
   const double* ysched_w;
   const int32_t* u_of_h;      // [u_half] index of half-plane entry h in the full Utot
+  // row-blocked Y kernel (twojmax <= YR_MAX_J): warp w owns target rows
+  // yrows[yrsched_off[w] .. yrsched_off[w+1])
+  const int32_t* yrsched_off;  // [YS_WARPS+1]
+  const YRowDev* yrows;
+  const YItemDev* yitems;
+  const double* yca;
   double ebias[IPG_MAX_SNAP_SPECIES];  // -beta[s] . bzero (energy shift of bzero_flag)
 };
 
@@ -66,6 +91,10 @@ struct SnapHost {
   std::vector<int32_t> zperm;     // Z entries sorted by (nb, na): equal trip counts per warp
   std::vector<int32_t> ysched_off, ysched_h, u_of_h;
   std::vector<double> ysched_w;
+  std::vector<int32_t> yrsched_off;
+  std::vector<YRowDev> yrows;
+  std::vector<YItemDev> yitems;
+  std::vector<double> yca;
 };
 
 int snap_build_tables(const ipg_snap_params& p, SnapHost& h);

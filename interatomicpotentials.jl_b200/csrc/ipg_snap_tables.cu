@@ -96,12 +96,16 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
             int mb2max = (2 * mb - j - (2 * mb1min - j1) + j2) / 2;
             int nb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
             ZDev z;
-            z.j1 = (int16_t)j1;
-            z.j2 = (int16_t)j2;
-            z.j = (int16_t)j;
-            z.na = (int16_t)na;
-            z.nb = (int16_t)nb;
-            z.pad = 0;
+            z.j1 = (int8_t)j1;
+            z.j2 = (int8_t)j2;
+            z.j = (int8_t)j;
+            z.na = (int8_t)na;
+            z.nb = (int8_t)nb;
+            z.pad0 = z.pad1 = z.pad2 = 0;
+            z.ma1min = (int8_t)ma1min;
+            z.ma2max = (int8_t)ma2max;
+            z.mb1min = (int8_t)mb1min;
+            z.mb2max = (int8_t)mb2max;
             z.u1base = h.idxu_block[j1] + (j1 + 1) * mb1min + ma1min;
             z.u2base = h.idxu_block[j2] + (j2 + 1) * mb2max + ma2max;
             z.icga0 = ma1min * (j2 + 1) + ma2max;
@@ -239,5 +243,93 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
   h.y_jjz.assign(h.idxz_max, 0);
   std::vector<int32_t> fill(h.y_off.begin(), h.y_off.end() - 1);
   for (int z = 0; z < h.idxz_max; z++) h.y_jjz[fill[h.zjju_half[z]]++] = z;
+
+  // Row-blocked Y schedule.  Target row (j, mb) of the half plane collects, for every
+  // triple (j1 >= j2, j), the Z entries (j1, j2, j, ma, mb) of all ma at once: the nb row
+  // pairs (mb1, mb2) are the same for every ma, and for one row pair
+  //   Z(ma) += cg[mb1][mb2] sum_ma2 cg[ma + d - ma2][ma2] U(j1, mb1, ma + d - ma2) U(j2, mb2, ma2)
+  // with d = (j1 + j2 - j)/2.  The CG factors ca[ma][ma2] of a triple are stored by column
+  // pair as [m0/2][ma][2] (yca; 16-byte pairs), zero where ma2 > j2 or ma1 = ma + d - ma2
+  // falls outside 0..j1.  Rows go to warps longest first.
+  h.yrows.clear();
+  h.yitems.clear();
+  h.yca.clear();
+  h.yrsched_off.assign(YS_WARPS + 1, 0);
+  if (J <= YR_MAX_J) {
+    std::vector<int32_t> ca_of(jd * jd * jd, -1);
+    for (int j1 = 0; j1 <= J; j1++)
+      for (int j2 = 0; j2 <= j1; j2++)
+        for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2) {
+          const int d = (j1 + j2 - j) / 2, cg0 = h.idxcg_block[blk(j1, j2, j)];
+          ca_of[blk(j1, j2, j)] = (int32_t)h.yca.size();
+          for (int m0 = 0; m0 <= j2; m0 += 2)  // column pairs (m0, m0 + 1), as [m0/2][ma][2]
+            for (int ma = 0; ma <= j; ma++)
+              for (int q = 0; q < 2; q++) {
+                const int ma2 = m0 + q, ma1 = ma + d - ma2;
+                const bool ok = ma2 <= j2 && ma1 >= 0 && ma1 <= j1;
+                h.yca.push_back(ok ? h.cglist[cg0 + ma1 * (j2 + 1) + ma2] : 0.0);
+              }
+        }
+    struct Row {
+      YRowDev r;
+      std::vector<YItemDev> items;
+      double cost;
+    };
+    std::vector<Row> rows;
+    for (int j = 0; j <= J; j++)
+      for (int mb = 0; 2 * mb <= j; mb++) {
+        Row row;
+        row.r.j = (int8_t)j;
+        row.r.mb = (int8_t)mb;
+        row.r.mid = (int8_t)(2 * mb == j);
+        row.r.pad = 0;
+        row.r.h0 = h.half_block[j] + mb * (j + 1);
+        row.cost = 0.0;
+        const int nma = row.r.mid ? mb + 1 : j + 1;
+        for (int j1 = 0; j1 <= J; j1++)
+          for (int j2 = 0; j2 <= j1; j2++) {
+            if (j < j1 - j2 || j > std::min(J, j1 + j2) || ((j1 + j2 + j) & 1)) continue;
+            const int mb1min = std::max(0, (2 * mb - j - j2 + j1) / 2);
+            const int mb2max = (2 * mb - j - (2 * mb1min - j1) + j2) / 2;
+            const int nb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
+            if (nb <= 0) continue;
+            YItemDev it;
+            it.j1 = (int8_t)j1;
+            it.j2 = (int8_t)j2;
+            it.d = (int8_t)((j1 + j2 - j) / 2);
+            it.nb = (int8_t)nb;
+            it.mb1min = (int8_t)mb1min;
+            it.mb2max = (int8_t)mb2max;
+            it.pad0 = it.pad1 = 0;
+            it.ca = ca_of[blk(j1, j2, j)];
+            it.cg = h.idxcg_block[blk(j1, j2, j)];
+            it.jjz = h.idxz_block[blk(j1, j2, j)];
+            it.pad2 = 0;
+            row.items.push_back(it);
+            row.cost += nb * (6.0 * nma * (j2 + 1) + (nma + 2 * j2 + 8));
+          }
+        rows.push_back(row);
+      }
+    std::vector<int> order(rows.size());
+    for (size_t q = 0; q < rows.size(); q++) order[q] = (int)q;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rows[a].cost > rows[b].cost; });
+    std::vector<std::vector<int>> bins(YS_WARPS);
+    std::vector<double> load(YS_WARPS, 0.0);
+    for (int q : order) {
+      const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      bins[w].push_back(q);
+      load[w] += rows[q].cost;
+    }
+    for (int w = 0; w < YS_WARPS; w++) {
+      for (int q : bins[w]) {
+        YRowDev r = rows[q].r;
+        r.t0 = (int32_t)h.yitems.size();
+        h.yitems.insert(h.yitems.end(), rows[q].items.begin(), rows[q].items.end());
+        r.t1 = (int32_t)h.yitems.size();
+        h.yrows.push_back(r);
+      }
+      h.yrsched_off[w + 1] = (int32_t)h.yrows.size();
+    }
+  }
   return IPG_OK;
 }

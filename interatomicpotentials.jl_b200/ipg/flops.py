@@ -102,6 +102,39 @@ def y_atom(J):
     return 4 * len(zs)
 
 
+def u_half(J):
+    """Half-plane entries (mb <= j/2) of all levels."""
+    return sum(1 for _ in _levels(J))
+
+
+def _n_contract(J):
+    """Half-plane entries carrying a non-zero weight (the middle row of an even level stops at j/2)."""
+    return sum(1 for j, mb, ma in _levels(J) if not (2 * mb == j and ma > mb))
+
+
+def yatoms_atom(J):
+    """k_snap_yatoms, one atom: every Z entry, its share of Y, the weight and the Euler energy term."""
+    return z_atom(J) + y_atom(J) + 6 * u_half(J)
+
+
+def utot_pair(J):
+    """k_snap_utot, one directed pair: the U recursion of every half-plane row and the sfac-weighted
+    accumulation (the staircase recomputation of the chain kernels is overhead, not counted)."""
+    return u_pair(J)
+
+
+def chain_adjoint_pair(J):
+    """k_snap_pair_adj_all, one directed pair: U and dU/dr of the half plane, the S0/S_k contraction with
+    the weighted Y (4 flops for S0 and 4 for each S_k per weighted entry), and the final 2(dsfac u S0 + sfac S)."""
+    return du_pair(J) + 16 * _n_contract(J) + 12
+
+
+def adjoint_kernels(J, natoms, npairs):
+    """Flops per launch of each kernel of the adjoint step, keyed like the library's timing names."""
+    return {"snap_atom": natoms * yatoms_atom(J), "snap_utot": npairs * utot_pair(J),
+            "snap_pair": npairs * chain_adjoint_pair(J)}
+
+
 def snap_atom_kernel(J, natoms, npairs, mode):
     """Flops of one launch of the fused per-atom SNAP kernel."""
     atom = z_atom(J) + b_atom(J)
