@@ -812,48 +812,34 @@ __device__ __forceinline__ double flip(double v, unsigned long long m) {
 // range), so they only have to stay inside the array and be finite.
 __host__ __device__ constexpr int yr_guard(int J) { return J + 2; }
 
-// The j2 row of a row pair: two columns per step, the mirror (a row beyond the half plane,
-// U[j][mb][ma] = (-1)^(ma+mb) conj(U[j][j-mb][j-ma])) handled with runtime strides and
-// sign masks.
-struct YrRow2 {
-  const double2* p;  // logical column 0
-  int st;            // +-YS_ATOMS
-  unsigned long long sx0, cj;  // sign mask of column 0; conjugation mask
-  __device__ __forceinline__ void init(const double2* __restrict__ usl, const int* __restrict__ hblk, int j, int mb) {
-    const bool m = 2 * mb > j;
-    p = usl + (size_t)(hblk[j] + (m ? j - mb : mb) * (j + 1) + (m ? j : 0)) * YS_ATOMS;
-    st = m ? -YS_ATOMS : YS_ATOMS;
-    sx0 = (m && (mb & 1)) ? SIGNBIT : 0ull;
-    cj = m ? SIGNBIT : 0ull;
-  }
-  __device__ __forceinline__ double2 get(int ma) const {  // ma in -1 .. j+1
-    const double2 v = p[ma * st];
-    const unsigned long long sx = ((ma & 1) && cj) ? (sx0 ^ SIGNBIT) : sx0;
-    return make_double2(flip(v.x, sx), flip(v.y, sx ^ cj));
-  }
-};
-
 // One row pair (mb1, mb2) of a triple for the target-row tile ma = ma0 .. ma0+NT-1.  The
 // j1 row is walked as a window: element t of column pair m0 is ma1 = d - m0 - 1 + ma0 + t,
-// met by (ma = ma0 + t - 1, ma2 = m0) and (ma = ma0 + t, ma2 = m0 + 1).  M1: the j1 row is
-// mirrored.  cp: the triple's factors as [m0/2][ma = 0..j][2], rs = j + 1.
+// met by (ma = ma0 + t - 1, ma2 = m0) and (ma = ma0 + t, ma2 = m0 + 1).  cp: the triple's
+// factors as [m0/2][ma = 0..j][2], rs = j + 1.
+//
+// Mirrored rows cost no extra instructions.  M1 (the j1 row lies beyond the half plane):
+// U(j1, mb1, ma1) = (-1)^(ma1+mb1) conj(v), and with m0 even the sign splits into
+// (-1)^(ma0+d+mb1), folded into cb, times (-1)^(i+q) with i = ma - ma0, a compile-time
+// constant folded into the FMAs along with the conjugate.  A mirrored j2 row gives
+// (-1)^mb2 (into cb) times (-1)^q and a conjugate, folded into the two per-column scales.
 template <int NT, bool M1>
 __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const int* __restrict__ hblk,
                                         const double2* __restrict__ cp, int rs, int ma0, int j1, int j2, int d,
                                         int mb1, int mb2, double cb, double2 (&acc)[NT]) {
   const double2* p1 = usl + (size_t)(hblk[j1] + (M1 ? j1 - mb1 : mb1) * (j1 + 1) + (M1 ? j1 : 0)) * YS_ATOMS;
-  // mirror sign (-1)^(ma1 + mb1) of the even elements t; the parity of d - m0 - 1 + ma0 is fixed
-  const unsigned long long sxe = (M1 && ((d - 1 + ma0 + mb1) & 1)) ? SIGNBIT : 0ull;
-  YrRow2 r2;
-  r2.init(usl, hblk, j2, mb2);
+  const bool m2 = 2 * mb2 > j2;
+  const double2* p2 = usl + (size_t)(hblk[j2] + (m2 ? j2 - mb2 : mb2) * (j2 + 1) + (m2 ? j2 : 0)) * YS_ATOMS;
+  const int st2 = m2 ? -YS_ATOMS : YS_ATOMS;
+  if (M1 && ((ma0 + d + mb1) & 1)) cb = -cb;
+  if (m2 && (mb2 & 1)) cb = -cb;
+  const double sx0 = cb, sy0 = m2 ? -cb : cb, sx1 = m2 ? -cb : cb, sy1 = cb;
   cp += ma0;
   for (int m0 = 0; m0 <= j2; m0 += 2, cp += rs) {
+    const double2 v0 = p2[0], v1 = p2[st2];
+    p2 += 2 * st2;
     double2 r[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      const double2 v = r2.get(m0 + q);
-      r[q] = make_double2(cb * v.x, cb * v.y);
-    }
+    r[0] = make_double2(sx0 * v0.x, sy0 * v0.y);
+    r[1] = make_double2(sx1 * v1.x, sy1 * v1.y);
     double2 a[NT];
 #pragma unroll
     for (int i = 0; i < NT; i++) a[i] = __ldg(cp + i);
@@ -861,19 +847,21 @@ __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const i
     const double2* pb = p1 + (M1 ? -base : base) * YS_ATOMS;
 #pragma unroll
     for (int t = 0; t <= NT; t++) {
-      double2 u = pb[(M1 ? -t : t) * YS_ATOMS];
-      if (M1) {
-        const unsigned long long sx = (t & 1) ? (sxe ^ SIGNBIT) : sxe;
-        u = make_double2(flip(u.x, sx), flip(u.y, sx ^ SIGNBIT));
-      }
+      const double2 u = pb[(M1 ? -t : t) * YS_ATOMS];
 #pragma unroll
       for (int q = 0; q < 2; q++) {
         const int i = t - 1 + q;
         if (i < 0 || i >= NT) continue;
-        const double c = q ? a[i].y : a[i].x;
+        const double c0 = q ? a[i].y : a[i].x;
+        const double c = (M1 && ((i + q) & 1)) ? -c0 : c0;
         const double tx = c * u.x, ty = c * u.y;
-        acc[i].x = fma(tx, r[q].x, fma(-ty, r[q].y, acc[i].x));
-        acc[i].y = fma(tx, r[q].y, fma(ty, r[q].x, acc[i].y));
+        if (M1) {  // conj(u) r
+          acc[i].x = fma(tx, r[q].x, fma(ty, r[q].y, acc[i].x));
+          acc[i].y = fma(tx, r[q].y, fma(-ty, r[q].x, acc[i].y));
+        } else {
+          acc[i].x = fma(tx, r[q].x, fma(-ty, r[q].y, acc[i].x));
+          acc[i].y = fma(tx, r[q].y, fma(ty, r[q].x, acc[i].y));
+        }
       }
     }
   }
@@ -952,7 +940,8 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
                                                                  const double2* __restrict__ utot,
                                                                  double2* __restrict__ yout, double* __restrict__ Ei) {
   extern __shared__ double2 ush[];  // guard | half plane of Utot [u_half][YS_ATOMS] | guard
-  __shared__ double esum[YS_WARPS][YS_ATOMS];
+  __shared__ double erow[yr_rows(YR_MAX_J)][YS_ATOMS];  // energy term of each target row
+  __shared__ int next_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int U = S.idxu_max, UH = S.u_half, G = yr_guard(S.J);
   double2* us = ush + G * YS_ATOMS;
@@ -966,22 +955,27 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
       const int q = idx / YS_ATOMS, l = idx - q * YS_ATOMS;
       us[idx] = l < na_blk ? utot[(size_t)(a0 + l) * U + S.u_of_h[q]] : make_double2(0.0, 0.0);
     }
+    if (threadIdx.x == 0) next_row = 0;
     __syncthreads();
     const int64_t atom = a0 + lane;
     const bool valid = lane < na_blk;
     const int si = valid ? clamp_sp(species[atom], S.nsp) : 0;
     const double* yc = S.ycoef + (size_t)si * S.idxz_max;
     const double2* usl = us + lane;
-    double e = 0.0;
-    for (int r = S.yrsched_off[warp]; r < S.yrsched_off[warp + 1]; r++) {
+    // rows are handed out longest first to whichever warp is free; a row's result does
+    // not depend on the warp that computes it, and the energy is summed in row order
+    for (;;) {
+      int r = 0;
+      if (lane == 0) r = atomicAdd(&next_row, 1);
+      r = __shfl_sync(0xffffffffu, r, 0);
+      if (r >= S.n_yrows) break;
       const YRowDev row = S.yrows[r];
-      e += yr_row(S, row, usl, yc, n, atom, valid, yout);
+      erow[r][lane] = yr_row(S, row, usl, yc, n, atom, valid, yout);
     }
-    esum[warp][lane] = e;
     __syncthreads();
     if (warp == 0 && valid) {
       double t = 0.0;
-      for (int w = 0; w < YS_WARPS; w++) t += esum[w][lane];
+      for (int r = 0; r < S.n_yrows; r++) t += erow[r][lane];
       Ei[atom] = (2.0 / 3.0) * t + S.ebias[si];
     }
     __syncthreads();
@@ -1375,8 +1369,7 @@ int upload_tables(ipg_snap* s) {
   size_t o_ysh = o_yso + pad(h.ysched_off.size() * 4);
   size_t o_ysw = o_ysh + pad(h.ysched_h.size() * 4);
   size_t o_uoh = o_ysw + pad(h.ysched_w.size() * 8);
-  size_t o_yrso = o_uoh + pad(h.u_of_h.size() * 4);
-  size_t o_yrows = o_yrso + pad(h.yrsched_off.size() * 4);
+  size_t o_yrows = o_uoh + pad(h.u_of_h.size() * 4);
   size_t o_yit = o_yrows + pad(h.yrows.size() * sizeof(YRowDev));
   size_t o_yca = o_yit + pad(h.yitems.size() * sizeof(YItemDev));
   size_t total = o_yca + pad(h.yca.size() * 8);
@@ -1396,7 +1389,6 @@ int upload_tables(ipg_snap* s) {
   memcpy(hostbuf.data() + o_ysh, h.ysched_h.data(), h.ysched_h.size() * 4);
   memcpy(hostbuf.data() + o_ysw, h.ysched_w.data(), h.ysched_w.size() * 8);
   memcpy(hostbuf.data() + o_uoh, h.u_of_h.data(), h.u_of_h.size() * 4);
-  memcpy(hostbuf.data() + o_yrso, h.yrsched_off.data(), h.yrsched_off.size() * 4);
   memcpy(hostbuf.data() + o_yrows, h.yrows.data(), h.yrows.size() * sizeof(YRowDev));
   memcpy(hostbuf.data() + o_yit, h.yitems.data(), h.yitems.size() * sizeof(YItemDev));
   memcpy(hostbuf.data() + o_yca, h.yca.data(), h.yca.size() * 8);
@@ -1438,7 +1430,7 @@ int upload_tables(ipg_snap* s) {
   d.ysched_h = reinterpret_cast<const int32_t*>(b + o_ysh);
   d.ysched_w = reinterpret_cast<const double*>(b + o_ysw);
   d.u_of_h = reinterpret_cast<const int32_t*>(b + o_uoh);
-  d.yrsched_off = reinterpret_cast<const int32_t*>(b + o_yrso);
+  d.n_yrows = (int)h.yrows.size();
   d.yrows = reinterpret_cast<const YRowDev*>(b + o_yrows);
   d.yitems = reinterpret_cast<const YItemDev*>(b + o_yit);
   d.yca = reinterpret_cast<const double*>(b + o_yca);

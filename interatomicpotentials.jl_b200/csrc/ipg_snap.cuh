@@ -28,6 +28,7 @@ constexpr int SNAP_MAX_J = 12;
 constexpr int YS_WARPS = 8;     // warps of the atoms-in-lanes Y kernels
 constexpr int YS_ATOMS = 32;    // atoms per block of those kernels (one per lane)
 constexpr int YR_MAX_J = 8;     // largest twojmax of the row-blocked Y kernel
+constexpr int yr_rows(int J) { return J < 0 ? 0 : yr_rows(J - 1) + J / 2 + 1; }  // target rows (j, mb <= j/2)
 
 // Row-blocked Y kernel: a target row (j, mb) of the half plane of Y and the (j1, j2)
 // triples whose Z entries feed it.
@@ -47,7 +48,7 @@ static_assert(sizeof(YItemDev) == 24, "YItemDev layout");
 
 struct SnapDev {
   int J, nsp, K, idxu_max, idxz_max, u_half, ext_max, idxcg_max;
-  int switch_flag, bzero_flag, bnorm_flag, pad;
+  int switch_flag, bzero_flag, bnorm_flag, n_yrows;
   double rcutfac, rmin0, rfac0, wself;
   double radii[IPG_MAX_SNAP_SPECIES], weight[IPG_MAX_SNAP_SPECIES];
   int idxu_block[SNAP_MAX_J + 2];
@@ -68,9 +69,7 @@ struct SnapDev {
   const int32_t* ysched_h;
   const double* ysched_w;
   const int32_t* u_of_h;      // [u_half] index of half-plane entry h in the full Utot
-  // row-blocked Y kernel (twojmax <= YR_MAX_J): warp w owns target rows
-  // yrows[yrsched_off[w] .. yrsched_off[w+1])
-  const int32_t* yrsched_off;  // [YS_WARPS+1]
+  // row-blocked Y kernel (twojmax <= YR_MAX_J): n_yrows target rows, longest first
   const YRowDev* yrows;
   const YItemDev* yitems;
   const double* yca;
@@ -91,7 +90,6 @@ struct SnapHost {
   std::vector<int32_t> zperm;     // Z entries sorted by (nb, na): equal trip counts per warp
   std::vector<int32_t> ysched_off, ysched_h, u_of_h;
   std::vector<double> ysched_w;
-  std::vector<int32_t> yrsched_off;
   std::vector<YRowDev> yrows;
   std::vector<YItemDev> yitems;
   std::vector<double> yca;

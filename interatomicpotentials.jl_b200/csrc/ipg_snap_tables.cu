@@ -250,11 +250,11 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
   //   Z(ma) += cg[mb1][mb2] sum_ma2 cg[ma + d - ma2][ma2] U(j1, mb1, ma + d - ma2) U(j2, mb2, ma2)
   // with d = (j1 + j2 - j)/2.  The CG factors ca[ma][ma2] of a triple are stored by column
   // pair as [m0/2][ma][2] (yca; 16-byte pairs), zero where ma2 > j2 or ma1 = ma + d - ma2
-  // falls outside 0..j1.  Rows go to warps longest first.
+  // falls outside 0..j1.  Rows are listed longest first (the kernel hands them out in
+  // that order to whichever warp is free).
   h.yrows.clear();
   h.yitems.clear();
   h.yca.clear();
-  h.yrsched_off.assign(YS_WARPS + 1, 0);
   if (J <= YR_MAX_J) {
     std::vector<int32_t> ca_of(jd * jd * jd, -1);
     for (int j1 = 0; j1 <= J; j1++)
@@ -313,22 +313,12 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
     std::vector<int> order(rows.size());
     for (size_t q = 0; q < rows.size(); q++) order[q] = (int)q;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rows[a].cost > rows[b].cost; });
-    std::vector<std::vector<int>> bins(YS_WARPS);
-    std::vector<double> load(YS_WARPS, 0.0);
     for (int q : order) {
-      const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-      bins[w].push_back(q);
-      load[w] += rows[q].cost;
-    }
-    for (int w = 0; w < YS_WARPS; w++) {
-      for (int q : bins[w]) {
-        YRowDev r = rows[q].r;
-        r.t0 = (int32_t)h.yitems.size();
-        h.yitems.insert(h.yitems.end(), rows[q].items.begin(), rows[q].items.end());
-        r.t1 = (int32_t)h.yitems.size();
-        h.yrows.push_back(r);
-      }
-      h.yrsched_off[w + 1] = (int32_t)h.yrows.size();
+      YRowDev r = rows[q].r;
+      r.t0 = (int32_t)h.yitems.size();
+      h.yitems.insert(h.yitems.end(), rows[q].items.begin(), rows[q].items.end());
+      r.t1 = (int32_t)h.yitems.size();
+      h.yrows.push_back(r);
     }
   }
   return IPG_OK;
