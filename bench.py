@@ -46,9 +46,11 @@ WORKLOAD = ("snap_j8: SNAP twojmax=8 (55 components), 2 species (weights 1.0/0.5
 # timing name -> kernel
 KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot<8,MB>",
                 "snap_pair": "k_snap_pair_adj_all<8>"}
-# DRAM bytes per atom of one launch, from the ncu capture summarised in
-# profiles/k_snap_yatoms_snap_j8.md (16,000 atoms; traffic grows with the atom count).
-NCU_DRAM_BYTES_PER_ATOM = {}
+# DRAM bytes (read + write) per atom of one launch, from the ncu --set full capture on the
+# 16,000-atom case summarised in profiles/k_snap_yrows_snap_j8.md and
+# profiles/k_snap_pair_adj_all_snap_j8.md; scaled by atoms (pairs per atom are the same).
+NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.927552e6 + 4.160512e6) / 16000,
+                           "snap_pair": (50.504448e6 + 0.944640e6) / 16000}
 
 
 def peaks():
@@ -60,7 +62,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms during a region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -74,7 +76,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -171,7 +173,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="size of the CPU-baseline sample")
@@ -317,7 +319,7 @@ def main():
                 "peak_source": "measured DFMA probe (libipg_probe.so) in this run; the HBM peak of "
                                "MEASURED_PEAKS.json does not bound these FP64-pipe kernels",
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the "
-                                  "16,000-atom case, scaled by atoms" if traffic else None,
+                                  "16,000-atom case, scaled by atoms (profiles/)" if traffic else None,
                 "kernels": per_kernel}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
