@@ -224,8 +224,12 @@ IPG_API int ipg_snap_vjp_beta(ipg_snap* snap, int64_t n, const double* pos, cons
  * Many configurations at once: atoms of configuration c are atom_offsets[c] ..
  * atom_offsets[c+1]-1 of the flattened arrays; L is [nconfig][3].  Per-configuration
  * energies E [nconfig] (each with beta0) and virials W6 [nconfig][6]; forces [3 n_total].
- * With graph != 0 the whole evaluation is captured once into a CUDA graph per shape and
- * replayed on later calls with the same atom counts.                                    */
+ * _dev with graph != 0: the first call runs eagerly and then captures the evaluation
+ * (neighbor build included) into a CUDA graph; later calls with the same atom_offsets,
+ * boxes, mode and device buffers replay it with one graph launch (new positions, species
+ * and beta are read from the buffers).  The captured pair buffers have 25% headroom over
+ * the pair count seen at capture; a replay that needs more re-runs eagerly and
+ * recaptures.  Configurations with an open axis (L = INFINITY) always run eagerly.      */
 IPG_API int ipg_snap_batch_energy_forces(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
                                  const int32_t* species, const double* L, const double* beta, double beta0,
                                  int32_t mode, double* E, double* F, double* W6);

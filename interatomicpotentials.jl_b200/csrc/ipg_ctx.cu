@@ -27,6 +27,9 @@ int ipg_cuda_check(ipg_ctx* ctx, cudaError_t e, const char* what) {
 int ipg_scratch(ipg_ctx* ctx, const char* name, size_t bytes, void** out) {
   DevBuf& b = ctx->bufs[name];
   if (b.cap < bytes) {
+    if (ctx->capturing)
+      return ipg_fail(ctx, IPG_ERR_CAPACITY, "scratch '%s' would grow during graph capture", name);
+    ctx->scratch_gen++;
     if (b.p) {
       // The stream may still use the old buffer.
       CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));

@@ -42,6 +42,12 @@ struct ipg_ctx {
   };
   std::map<std::string, Timed> timed;
   std::vector<cudaEvent_t> event_pool;
+  // CUDA-graph capture: while capturing, scratch buffers must not move (an allocation
+  // fails the capture) and host tables are not re-uploaded (the replay path uploads them
+  // before each launch).  scratch_gen counts (re)allocations: a graph whose generation
+  // differs refers to freed buffers and is discarded.
+  bool capturing = false;
+  uint64_t scratch_gen = 0;
 };
 
 // Records a start/stop event pair around a launch when timing is enabled.
@@ -168,7 +174,8 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
 // Materialised pair list in CSR form over atoms (original order), neighbors ascending.
 struct PairList {
   int64_t n = 0;
-  int64_t npairs = 0;
+  int64_t npairs = 0;        // exact count, or the capacity in capacity mode (buffer sizes, grids)
+  const int64_t* d_np = nullptr;  // device copy of the count (d_off + n): what pair kernels read
   int64_t* d_off = nullptr;  // [n+1]
   int32_t* d_j = nullptr;    // [npairs]
   double* d_r = nullptr;     // [npairs][3]
@@ -181,8 +188,12 @@ struct PairList {
 // sorted: each atom's neighbors ascending (the reference's order); otherwise the
 // emission order (stencil cells in fixed order, ascending inside a cell), which is
 // equally deterministic.
+// cap > 0 selects capacity mode (no host read-back, so the build can be captured in a CUDA
+// graph): buffers hold cap pairs; a larger count sets IPG_ERR_CAPACITY in the status word
+// and every atom's list is cut at cap, so later kernels stay in bounds.
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
-                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true);
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true,
+                    int64_t cap = 0);
 
 // Device helper: the distinct neighbor-cell coordinates along one axis (<= 3).
 __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {

@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(128) k_pair_walk(int64_t n, PairTest t, const 
   stencil_ranges(g, c, cell_start, R);
   int64_t k = 0;
   const int64_t base = EMIT ? off[i] : 0;
+  const int64_t end = EMIT ? off[i + 1] : 0;
   const unsigned lt = (1u << lane) - 1u;
   for (int r = 0; r < R.n; r++)
     for (int64_t q0 = R.beg[r]; q0 < R.end[r]; q0 += 32) {
@@ -190,14 +191,29 @@ __global__ void __launch_bounds__(128) k_pair_walk(int64_t n, PairTest t, const 
       const unsigned bal = __ballot_sync(0xffffffffu, ok);
       if (EMIT && ok) {
         const int64_t o = base + k + __popc(bal & lt);
-        outj[o] = cell_atoms[q];
-        outr[3 * o] = rr[0];
-        outr[3 * o + 1] = rr[1];
-        outr[3 * o + 2] = rr[2];
+        if (o < end) {  // a list cut at the capacity (capacity mode) drops its tail
+          outj[o] = cell_atoms[q];
+          outr[3 * o] = rr[0];
+          outr[3 * o + 1] = rr[1];
+          outr[3 * o + 2] = rr[2];
+        }
       }
       k += __popc(bal);
     }
   if (!EMIT && lane == 0) cnt[i] = k;
+}
+
+// Capacity mode: a total above cap is an error (status), and every offset is cut at cap
+// so that all later kernels stay inside the buffers.
+// (Offsets are non-decreasing, so cutting each one at cap on its own is the same as
+// cutting the lists; no thread reads another's offset.)
+__global__ void k_clamp_offsets(int64_t n, int64_t* __restrict__ off, int64_t cap, int* __restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  if (off[i] > cap) {
+    if (i == n) atomicExch(status, IPG_ERR_CAPACITY);
+    off[i] = cap;
+  }
 }
 
 // Sorts each atom's list by neighbor index (insertion sort; lists are short).
@@ -225,15 +241,17 @@ __global__ void k_pair_sort(int64_t n, const int64_t* __restrict__ off, int32_t*
 }
 
 // Transpose: for every atom k, the pairs p whose neighbor is k, in ascending p.
-__global__ void k_in_count(int64_t np, const int32_t* __restrict__ j, int64_t* __restrict__ cnt) {
+__global__ void k_in_count(const int64_t* __restrict__ d_np, const int32_t* __restrict__ j,
+                           int64_t* __restrict__ cnt) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
+  if (p >= *d_np) return;
   atomicAdd((unsigned long long*)&cnt[j[p]], 1ull);
 }
-__global__ void k_in_fill(int64_t np, const int32_t* __restrict__ j, const int64_t* __restrict__ in_off,
-                          int64_t* __restrict__ fill, int64_t* __restrict__ in_pair) {
+__global__ void k_in_fill(const int64_t* __restrict__ d_np, const int32_t* __restrict__ j,
+                          const int64_t* __restrict__ in_off, int64_t* __restrict__ fill,
+                          int64_t* __restrict__ in_pair) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
+  if (p >= *d_np) return;
   int32_t k = j[p];
   unsigned long long q = atomicAdd((unsigned long long*)&fill[k], 1ull);
   in_pair[in_off[k] + (int64_t)q] = p;
@@ -278,6 +296,8 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
   }
   IPG_RET(scratch(ctx, (pre + "grid").c_str(), nconf, &cl.d_grid));
   std::vector<double> ext(6 * (size_t)nconf, 0.0);
+  if (any_open && n > 0 && ctx->capturing)
+    return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "open boundaries cannot be captured in a graph");
   if (any_open && n > 0) {
     CUDA_RET(ctx, cudaMemcpyAsync(cl.d_grid, cl.h_grid.data(), sizeof(ConfGrid) * nconf, cudaMemcpyHostToDevice,
                                   ctx->stream));
@@ -322,8 +342,9 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
   }
   if (cell_total >= (int64_t)INT32_MAX) return ipg_fail(ctx, IPG_ERR_CAPACITY, "too many cells");
   cl.ncells = cell_total;
-  CUDA_RET(ctx, cudaMemcpyAsync(cl.d_grid, cl.h_grid.data(), sizeof(ConfGrid) * nconf, cudaMemcpyHostToDevice,
-                                ctx->stream));
+  if (!ctx->capturing)  // a captured graph's grid table is uploaded before each replay
+    CUDA_RET(ctx, cudaMemcpyAsync(cl.d_grid, cl.h_grid.data(), sizeof(ConfGrid) * nconf, cudaMemcpyHostToDevice,
+                                  ctx->stream));
   int64_t *count, *fill;
   int32_t* cell_of;
   IPG_RET(scratch(ctx, (pre + "conf").c_str(), n, &cl.d_conf));
@@ -348,7 +369,7 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
 }
 
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
-                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted) {
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted, int64_t cap) {
   (void)d_species;
   std::string pre(prefix);
   PairTest t;
@@ -380,8 +401,14 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
     IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
   IPG_RET(ipg_scan_i64(ctx, cnt, pl.d_off, n + 1));
-  CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  pl.d_np = pl.d_off + n;
+  if (cap > 0) {  // capacity mode: no read-back
+    pl.npairs = cap;
+    IPG_LAUNCH(ctx, k_clamp_offsets, nblk(n + 1, 256), 256, 0, n, pl.d_off, cap, ctx->d_status);
+  } else {
+    CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   if (pl.npairs >= (int64_t)1 << 40) return ipg_fail(ctx, IPG_ERR_CAPACITY, "pair count overflow");
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
@@ -397,10 +424,10 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
     IPG_RET(scratch(ctx, (pre + "in_pair").c_str(), pl.npairs + 1, &pl.d_in_pair));
     CUDA_RET(ctx, cudaMemsetAsync(pl.d_in_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
     CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (n + 1), ctx->stream));
-    if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.npairs, pl.d_j, pl.d_in_off);
+    if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off);
     IPG_RET(ipg_scan_i64(ctx, pl.d_in_off, pl.d_in_off, n + 1));
     if (pl.npairs > 0) {
-      IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.npairs, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
+      IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
       IPG_LAUNCH(ctx, k_in_sort, nblk(n, 128), 128, 0, n, pl.d_in_off, pl.d_in_pair);
     }
   }

@@ -986,13 +986,13 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
 // ipg_snap_chain.cuh.  Yw is the weighted Y as [h][natoms]; part[p][MB][3] = chain MB's
 // share of dE_i/dr_ij.
 template <int J, int MB>
-__global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ SnapDev S, int64_t np, int64_t natoms,
+__global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ SnapDev S, const int64_t* __restrict__ d_np, int64_t natoms,
                                                        const int32_t* __restrict__ owner,
                                                        const int32_t* __restrict__ nbr, const double* __restrict__ rij,
                                                        const int32_t* __restrict__ species,
                                                        const double2* __restrict__ Yw, double* __restrict__ part) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
+  if (p >= *d_np) return;  // np: the live count (capacity mode sizes the grid larger)
   const int i = owner[p];
   const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
   const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
@@ -1020,7 +1020,8 @@ __global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ S
 // shared memory): part[p][0][3] = dE_i/dr_ij.
 constexpr int PAIR_ALL_T = 128;
 template <int J>
-__global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_constant__ SnapDev S, int64_t np,
+__global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_constant__ SnapDev S,
+                                                                  const int64_t* __restrict__ d_np,
                                                                   int64_t natoms, const int32_t* __restrict__ owner,
                                                                   const int32_t* __restrict__ nbr,
                                                                   const double* __restrict__ rij,
@@ -1029,7 +1030,7 @@ __global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_c
                                                                   double* __restrict__ part) {
   extern __shared__ double2 save[];  // [4 (J+1)][PAIR_ALL_T]
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
+  if (p >= *d_np) return;  // np: the live count (capacity mode sizes the grid larger)
   const int i = owner[p];
   const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
   const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
@@ -1053,24 +1054,24 @@ __global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_c
 }
 
 template <int J>
-int launch_pair_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+int launch_pair_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms, const int32_t* owner,
                     const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
   const size_t sm = (size_t)4 * (J + 1) * PAIR_ALL_T * sizeof(double2);
   if (sm > 48 * 1024)
     CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_pair_adj_all<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  IPG_TIMED_LAUNCH(ctx, "snap_pair", k_snap_pair_adj_all<J>, nblk(np, PAIR_ALL_T), PAIR_ALL_T, sm, S, np, natoms,
+  IPG_TIMED_LAUNCH(ctx, "snap_pair", k_snap_pair_adj_all<J>, nblk(np, PAIR_ALL_T), PAIR_ALL_T, sm, S, d_np, natoms,
                    owner, nbr, rij, species, Yw, part);
   return IPG_OK;
 }
 
-int launch_pair_adj_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+int launch_pair_adj_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms, const int32_t* owner,
                         const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw,
                         double* part) {
   if (np == 0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return launch_pair_all<JJ>(ctx, S, np, natoms, owner, nbr, rij, species, Yw, part);
+    return launch_pair_all<JJ>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, Yw, part);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
 #undef IPG_J
     default:
@@ -1081,24 +1082,24 @@ int launch_pair_adj_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t nato
 constexpr int PAIR_CHAIN_MAX_J = 10;  // twojmax handled by the register-chain kernel
 
 template <int J, int MB>
-int launch_chain(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+int launch_chain(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms, const int32_t* owner,
                  const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
   if constexpr (MB <= J / 2) {
     const int T = 128;
-    IPG_TIMED_LAUNCH(ctx, "snap_pair", (k_snap_pair_adj<J, MB>), nblk(np, T), T, 0, S, np, natoms, owner, nbr, rij,
+    IPG_TIMED_LAUNCH(ctx, "snap_pair", (k_snap_pair_adj<J, MB>), nblk(np, T), T, 0, S, d_np, natoms, owner, nbr, rij,
                      species, Yw, part);
-    return launch_chain<J, MB + 1>(ctx, S, np, natoms, owner, nbr, rij, species, Yw, part);
+    return launch_chain<J, MB + 1>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, Yw, part);
   }
   return IPG_OK;
 }
 
-int launch_pair_adj(ipg_ctx* ctx, const SnapDev& S, int64_t np, int64_t natoms, const int32_t* owner,
+int launch_pair_adj(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms, const int32_t* owner,
                     const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
   if (np == 0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return launch_chain<JJ, 0>(ctx, S, np, natoms, owner, nbr, rij, species, Yw, part);
+    return launch_chain<JJ, 0>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, Yw, part);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
 #undef IPG_J
     default:
@@ -1214,7 +1215,8 @@ __global__ void k_chunk_reduce(const int64_t* __restrict__ chunks, const double*
 }
 
 __global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ conf_chunk, const double* __restrict__ part,
-                              double beta0, double* __restrict__ E, double* __restrict__ W6) {
+                              const double* __restrict__ beta0p, double* __restrict__ E, double* __restrict__ W6) {
+  const double beta0 = *beta0p;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nconf) return;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -1347,6 +1349,28 @@ struct ipg_snap {
   bool pair_split = false;  // adjoint pair kernel: one thread per (pair, chain) instead of per pair
   bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
   std::vector<double> beta_host;  // last uploaded beta
+  // last evaluation's pair count, cell grids and chunk table (host), for graph capture
+  int64_t last_np = 0;
+  std::vector<ConfGrid> last_grid;
+  std::vector<int64_t> last_chunks;
+  // Captured batched evaluations (ipg_snap_batch_energy_forces_dev with graph != 0): the
+  // key is everything the captured launches bake in (shape, boxes, mode, buffers).
+  struct Graph {
+    int32_t nconfig = 0;
+    int mode = 0;
+    std::vector<int64_t> off;
+    std::vector<double> L;
+    const void *pos = nullptr, *sp = nullptr;
+    void *E = nullptr, *F = nullptr, *W6 = nullptr;
+    bool pair_split = false, y_entries = false;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t gen = 0;  // ctx->scratch_gen at capture
+    int64_t cap = 0;   // pair capacity
+    std::vector<ConfGrid> grid;
+    std::vector<int64_t> chunks;
+  };
+  std::vector<Graph> graphs;
+  int64_t graph_replays = 0;
 };
 
 namespace {
@@ -1460,48 +1484,57 @@ int launch_atoms(ipg_snap* s, const SnapDev& dev, const SnapIO& io, int64_t nato
   return IPG_OK;
 }
 
-int set_beta(ipg_snap* s, const double* beta, SnapDev& dev) {
+// Uploads beta [nsp][K], the energy shifts and beta0 (device: beta | ebias[8] | beta0) and
+// the per-Z-entry Y coefficients; while a graph is being captured only the pointers are
+// set (the replay path uploads before each launch).
+int set_beta(ipg_snap* s, const double* beta, double beta0, SnapDev& dev) {
   ipg_ctx* ctx = s->ctx;
   const int K = s->h.idxb_max, nsp = s->p.nspecies;
   double *d_beta, *d_ycoef;
-  IPG_RET(scratch(ctx, "snap_beta", (size_t)nsp * K, &d_beta));
+  const size_t nb = (size_t)nsp * K;
+  IPG_RET(scratch(ctx, "snap_beta", nb + IPG_MAX_SNAP_SPECIES + 1, &d_beta));
   IPG_RET(scratch(ctx, "snap_ycoef", (size_t)nsp * s->h.idxz_max, &d_ycoef));
-  std::vector<double> b(beta ? beta : nullptr, beta ? beta + (size_t)nsp * K : nullptr);
-  if (!beta) b.assign((size_t)nsp * K, 0.0);
-  double* hb = host_scratch<double>(ctx, "snap_beta_h", b.size());
-  memcpy(hb, b.data(), b.size() * 8);
-  CUDA_RET(ctx, cudaMemcpyAsync(d_beta, hb, b.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-  IPG_LAUNCH(ctx, k_ycoef, nblk((int64_t)nsp * s->h.idxz_max, 256), 256, 0, nsp, s->h.idxz_max, K, s->d_ymult,
-             s->d_yjjb, d_beta, d_ycoef);
   dev.beta = d_beta;
   dev.ycoef = d_ycoef;
-  for (int q = 0; q < nsp; q++) {  // -beta[s] . bzero[j(k)] (compute_b.jl:134-155)
+  dev.ebias = d_beta + nb;
+  dev.beta0 = d_beta + nb + IPG_MAX_SNAP_SPECIES;
+  if (ctx->capturing) return IPG_OK;
+  double* hb = host_scratch<double>(ctx, "snap_beta_h", nb + IPG_MAX_SNAP_SPECIES + 1);
+  for (size_t k = 0; k < nb; k++) hb[k] = beta ? beta[k] : 0.0;
+  for (int q = 0; q < IPG_MAX_SNAP_SPECIES; q++) {  // -beta[s] . bzero[j(k)] (compute_b.jl:134-155)
     double t = 0.0;
-    for (int k = 0; k < K; k++) t += b[(size_t)q * K + k] * s->h.bzero[s->h.idxb[3 * k + 2]];
-    dev.ebias[q] = -t;
+    if (q < nsp)
+      for (int k = 0; k < K; k++) t += hb[(size_t)q * K + k] * s->h.bzero[s->h.idxb[3 * k + 2]];
+    hb[nb + q] = -t;
   }
+  hb[nb + IPG_MAX_SNAP_SPECIES] = beta0;
+  CUDA_RET(ctx, cudaMemcpyAsync(d_beta, hb, (nb + IPG_MAX_SNAP_SPECIES + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+  IPG_LAUNCH(ctx, k_ycoef, nblk((int64_t)nsp * s->h.idxz_max, 256), 256, 0, nsp, s->h.idxz_max, K, s->d_ymult,
+             s->d_yjjb, d_beta, d_ycoef);
   return IPG_OK;
 }
 
 int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
-                         const int64_t* h_atom_off, const double* h_L, PairList& pl);
+                         const int64_t* h_atom_off, const double* h_L, PairList& pl, int64_t cap);
 
-// Neighbor build for a set of configurations (device positions).
+// Neighbor build for a set of configurations (device positions); cap > 0: capacity mode.
 int snap_neighbors(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
-                   const int64_t* h_atom_off, const double* h_L, PairList& pl) {
+                   const int64_t* h_atom_off, const double* h_L, PairList& pl, int64_t cap = 0) {
   IPG_RET(ipg_timing_mark(s->ctx, "neighbor", true));
-  int st = snap_neighbors_inner(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl);
+  int st = snap_neighbors_inner(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl, cap);
   if (st) return st;
   return ipg_timing_mark(s->ctx, "neighbor", false);
 }
 
 int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
-                         const int64_t* h_atom_off, const double* h_L, PairList& pl) {
+                         const int64_t* h_atom_off, const double* h_L, PairList& pl, int64_t cap) {
   CellList cl;
   IPG_RET(ipg_build_cells(s->ctx, "snap_", n, d_pos, d_species, s->p.nspecies, nconf, h_atom_off, h_L, s->radius,
                           cl));
+  s->last_grid = cl.h_grid;
   int mode = IPG_NLIST_FULL | (s->p.literal_sqrt_radius ? IPG_NLIST_LITERAL_SQRT : 0);
-  IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl, false));
+  IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl, false,
+                          cap));
   return IPG_OK;
 }
 
@@ -1518,14 +1551,15 @@ struct EvalOut {
 // MODE_PLAIN.  Writes device outputs; does not synchronise.
 int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
               const int64_t* h_atom_off, const double* h_L, const double* beta, double beta0, int mode,
-              const EvalOut& out) {
+              const EvalOut& out, int64_t cap = 0) {
   ipg_ctx* ctx = s->ctx;
   SnapDev dev = s->dev;
-  IPG_RET(set_beta(s, beta, dev));
+  IPG_RET(set_beta(s, beta, beta0, dev));
   PairList pl;
-  IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl));
+  IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl, cap));
   const int K = dev.K, nsp = dev.nsp;
   const int64_t np = pl.npairs;
+  if (cap == 0) s->last_np = np;
   double *Ei, *fvec = nullptr, *dbl = nullptr, *w6 = nullptr;
   IPG_RET(scratch(ctx, "snap_Ei", (size_t)n + 1, &Ei));
   SnapIO io;
@@ -1578,9 +1612,9 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
         IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
       }
       if (s->pair_split)
-        IPG_RET(launch_pair_adj(ctx, dev, np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+        IPG_RET(launch_pair_adj(ctx, dev, np, pl.d_np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
       else
-        IPG_RET(launch_pair_adj_all(ctx, dev, np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+        IPG_RET(launch_pair_adj_all(ctx, dev, np, pl.d_np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
     }
   } else if (mode == MODE_ADJ) {
     IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
@@ -1623,11 +1657,13 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     int64_t* hb = host_scratch<int64_t>(ctx, "snap_chunks_h", ch.size() + cc.size());
     memcpy(hb, ch.data(), sizeof(int64_t) * ch.size());
     memcpy(hb + ch.size(), cc.data(), sizeof(int64_t) * cc.size());
-    CUDA_RET(ctx, cudaMemcpyAsync(d_ch, hb, sizeof(int64_t) * (ch.size() + cc.size()), cudaMemcpyHostToDevice,
-                                  ctx->stream));
+    s->last_chunks.assign(hb, hb + ch.size() + cc.size());
+    if (!ctx->capturing)  // a captured graph's chunk table is uploaded before each replay
+      CUDA_RET(ctx, cudaMemcpyAsync(d_ch, hb, sizeof(int64_t) * (ch.size() + cc.size()), cudaMemcpyHostToDevice,
+                                    ctx->stream));
     d_cc = d_ch + ch.size();
     IPG_LAUNCH(ctx, k_chunk_reduce, (unsigned)nchunk, 128, 0, d_ch, Ei, w6, part);
-    IPG_LAUNCH(ctx, k_conf_reduce, nblk(nconf, 128), 128, 0, nconf, d_cc, part, beta0, out.E, out.W6);
+    IPG_LAUNCH(ctx, k_conf_reduce, nblk(nconf, 128), 128, 0, nconf, d_cc, part, dev.beta0, out.E, out.W6);
   }
   if (out.dB && n) {
     int32_t* owner;
@@ -1648,6 +1684,112 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_LAUNCH(ctx, k_sum_partials, nblk(width, 128), 128, 0, grid, width, part, out.Wd, 0.0);
   }
   return IPG_OK;
+}
+
+// ---- CUDA-graph replay of batched evaluations -------------------------------------------
+constexpr int IPG_ERR_NOT_CAPTURED = 1;  // internal: no graph for this key (not an API code)
+
+ipg_snap::Graph* find_graph(ipg_snap* s, int32_t nconfig, const int64_t* off, const double* L, int mode,
+                            const void* pos, const void* sp, const EvalOut& o) {
+  for (auto& g : s->graphs) {
+    if (g.nconfig != nconfig || g.mode != mode || g.pos != pos || g.sp != sp || g.E != o.E || g.F != o.F ||
+        g.W6 != o.W6 || g.pair_split != s->pair_split || g.y_entries != s->y_entries)
+      continue;
+    if (memcmp(g.off.data(), off, sizeof(int64_t) * (nconfig + 1)) != 0) continue;
+    if (memcmp(g.L.data(), L, sizeof(double) * 3 * nconfig) != 0) continue;
+    return &g;
+  }
+  return nullptr;
+}
+
+void drop_graph(ipg_snap* s, ipg_snap::Graph* g) {
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  s->graphs.erase(s->graphs.begin() + (g - s->graphs.data()));
+}
+
+// Replays the graph captured for this key: beta, the cell grids and the chunk table are
+// uploaded first (the graph reads them from the same buffers), then one graph launch.
+// Returns IPG_ERR_NOT_CAPTURED when there is no usable graph, IPG_ERR_CAPACITY when the
+// pair count outgrew the captured capacity (the graph is dropped; the caller re-runs).
+int batch_graph_replay(ipg_snap* s, int32_t nconfig, const int64_t* off, const double* d_pos, const int32_t* d_sp,
+                       const double* L, const double* beta, double beta0, int mode, const EvalOut& o) {
+  ipg_ctx* ctx = s->ctx;
+  ipg_snap::Graph* g = find_graph(s, nconfig, off, L, mode, d_pos, d_sp, o);
+  if (!g) return IPG_ERR_NOT_CAPTURED;
+  if (g->gen != ctx->scratch_gen) {  // a scratch buffer moved since the capture
+    drop_graph(s, g);
+    return IPG_ERR_NOT_CAPTURED;
+  }
+  SnapDev dev = s->dev;
+  IPG_RET(set_beta(s, beta, beta0, dev));
+  ConfGrid* d_grid;
+  int64_t* d_ch;
+  IPG_RET(scratch(ctx, "snap_grid", g->grid.size(), &d_grid));
+  IPG_RET(scratch(ctx, "snap_chunks", g->chunks.size(), &d_ch));
+  if (g->gen != ctx->scratch_gen) {  // set_beta or the lookups above had to allocate
+    drop_graph(s, g);
+    return IPG_ERR_NOT_CAPTURED;
+  }
+  CUDA_RET(ctx, cudaMemcpyAsync(d_grid, g->grid.data(), sizeof(ConfGrid) * g->grid.size(), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  CUDA_RET(ctx, cudaMemcpyAsync(d_ch, g->chunks.data(), sizeof(int64_t) * g->chunks.size(), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  IPG_RET(ipg_status_reset(ctx));
+  CUDA_RET(ctx, cudaGraphLaunch(g->exec, ctx->stream));
+  s->graph_replays++;
+  int st = ipg_status_check(ctx, "ipg_snap_batch_energy_forces_dev (graph)");
+  if (st == IPG_ERR_CAPACITY) drop_graph(s, g);
+  return st;
+}
+
+// Captures the evaluation just run eagerly (same inputs) for later replays.  The pair
+// buffers get 25% headroom over the count just seen; a warm run in capacity mode sizes
+// every scratch buffer first, so nothing allocates while capturing.  Failures only mean
+// that later calls run eagerly.
+void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const double* d_pos, const int32_t* d_sp,
+                         const double* L, const double* beta, double beta0, int mode, const EvalOut& o) {
+  ipg_ctx* ctx = s->ctx;
+  const int64_t n = off[nconfig];
+  const int64_t cap = s->last_np + s->last_np / 4 + 1024;
+  if (ipg_status_reset(ctx) || snap_eval(s, n, d_pos, d_sp, nconfig, off, L, beta, beta0, mode, o, cap) ||
+      ipg_status_check(ctx, "graph warm-up"))
+    return;
+  if (s->graphs.size() >= 8) drop_graph(s, &s->graphs.front());
+  ipg_snap::Graph g;
+  g.nconfig = nconfig;
+  g.mode = mode;
+  g.off.assign(off, off + nconfig + 1);
+  g.L.assign(L, L + 3 * nconfig);
+  g.pos = d_pos;
+  g.sp = d_sp;
+  g.E = o.E;
+  g.F = o.F;
+  g.W6 = o.W6;
+  g.pair_split = s->pair_split;
+  g.y_entries = s->y_entries;
+  g.cap = cap;
+  g.grid = s->last_grid;
+  g.chunks = s->last_chunks;
+  const bool timing = ctx->timing;
+  ctx->timing = false;
+  ctx->capturing = true;
+  cudaGraph_t graph = nullptr;
+  int st = IPG_OK;
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    st = IPG_ERR_CUDA;
+  } else {
+    st = snap_eval(s, n, d_pos, d_sp, nconfig, off, L, beta, beta0, mode, o, cap);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st == IPG_OK && e != cudaSuccess) st = IPG_ERR_CUDA;
+  }
+  ctx->capturing = false;
+  ctx->timing = timing;
+  if (st == IPG_OK && graph && cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess) {
+    g.gen = ctx->scratch_gen;
+    s->graphs.push_back(std::move(g));
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // a failed capture leaves no sticky error behind
 }
 
 int check_common(ipg_snap* s, int64_t n, const void* pos, const void* species, const double* L) {
@@ -1748,6 +1890,8 @@ int ipg_snap_destroy(ipg_snap* s) {
   if (!s) return IPG_ERR_ARG;
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
+  for (auto& g : s->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   if (s->d_tables) cudaFree(s->d_tables);
   delete s;
   return IPG_OK;
@@ -1853,7 +1997,7 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
                     double* d_gbeta) {
   ipg_ctx* ctx = s->ctx;
   SnapDev dev = s->dev;
-  IPG_RET(set_beta(s, beta, dev));
+  IPG_RET(set_beta(s, beta, 0.0, dev));
   PairList pl;
   IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl));
   const int K = dev.K, nsp = dev.nsp;
@@ -1935,17 +2079,25 @@ int ipg_snap_batch_energy_forces_dev(ipg_snap* s, int32_t nconfig, const int64_t
   if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
   for (int c = 0; c < nconfig; c++)
     if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
-  (void)graph;
   int64_t n = atom_offsets[nconfig];
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
-  IPG_RET(ipg_status_reset(ctx));
   EvalOut o;
   o.E = d_E;
   o.F = d_F;
   o.W6 = d_W6;
-  IPG_RET(snap_eval(s, n, d_pos, d_species, nconfig, atom_offsets, L, beta, beta0,
-                    mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN, o));
-  return ipg_status_check(ctx, "ipg_snap_batch_energy_forces_dev");
+  const int emode = mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN;
+  bool periodic = true;
+  for (int k = 0; k < 3 * nconfig; k++) periodic &= std::isfinite(L[k]);
+  const bool use_graph = graph != 0 && periodic && n > 0;
+  if (use_graph) {
+    int st = batch_graph_replay(s, nconfig, atom_offsets, d_pos, d_species, L, beta, beta0, emode, o);
+    if (st != IPG_ERR_CAPACITY && st != IPG_ERR_NOT_CAPTURED) return st;
+  }
+  IPG_RET(ipg_status_reset(ctx));
+  IPG_RET(snap_eval(s, n, d_pos, d_species, nconfig, atom_offsets, L, beta, beta0, emode, o));
+  IPG_RET(ipg_status_check(ctx, "ipg_snap_batch_energy_forces_dev"));
+  if (use_graph) batch_graph_capture(s, nconfig, atom_offsets, d_pos, d_species, L, beta, beta0, emode, o);
+  return IPG_OK;
 }
 
 int ipg_snap_batch_energy_forces(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* pos,

@@ -73,7 +73,9 @@ struct SnapDev {
   const YRowDev* yrows;
   const YItemDev* yitems;
   const double* yca;
-  double ebias[IPG_MAX_SNAP_SPECIES];  // -beta[s] . bzero (energy shift of bzero_flag)
+  const double* beta0;  // [1] energy offset of LBasisPotential (device, like ebias)
+  const double* ebias;  // [nsp] -beta[s] . bzero (energy shift of bzero_flag), device memory so that
+                        // a captured graph sees the beta of each replay
 };
 
 struct SnapHost {

@@ -11,7 +11,7 @@ from .api import (NeighborList, energy_and_force, force, neighborlist, neighborl
 from .context import Context, default_context
 from .empirical import (ZBL, AbstractPotential, BornMayer, Coulomb, EmpiricalPotential, LennardJones,
                         LinearCombinationPotential, MockR2, Morse)
-from .snap import (SNAP, LBasisPotential, compute_all_descriptors, compute_force_descriptors,
+from .snap import (SNAP, DeviceBatch, LBasisPotential, compute_all_descriptors, compute_force_descriptors,
                    compute_local_descriptors, compute_virial_descriptors, get_num_snap_coeffs)
 from .system import System, periodic_system
 from . import units
@@ -19,7 +19,7 @@ from . import units
 __all__ = [
     "IPGError", "Context", "default_context", "System", "periodic_system", "units",
     "AbstractPotential", "EmpiricalPotential", "LennardJones", "BornMayer", "Coulomb", "Morse", "ZBL", "MockR2",
-    "LinearCombinationPotential", "SNAP", "LBasisPotential", "get_num_snap_coeffs",
+    "LinearCombinationPotential", "SNAP", "DeviceBatch", "LBasisPotential", "get_num_snap_coeffs",
     "compute_local_descriptors", "compute_force_descriptors", "compute_virial_descriptors",
     "compute_all_descriptors", "energy_and_force", "potential_energy", "force", "virial", "virial_stress",
     "neighborlist", "neighborlist_snap", "NeighborList",

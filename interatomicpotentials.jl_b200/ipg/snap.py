@@ -190,6 +190,41 @@ class SNAP:
         return loss[0], gb
 
 
+class DeviceBatch:
+    """A fixed set of configurations resident on the GPU as torch tensors, evaluated with
+    ``ipg_snap_batch_energy_forces_dev``.  With ``graph=True`` the first evaluation is captured
+    into a CUDA graph (neighbor build included) and later ones replay it with one launch;
+    positions change in place through :meth:`set_positions`, beta per call.  The library runs on
+    torch's current stream of the snap's device."""
+
+    def __init__(self, snap, systems):
+        import torch
+        off, pos, sp, L = snap._flatten(systems)
+        self.snap, self.off, self.L = snap, off, L
+        self.nconfig = len(systems)
+        dev = torch.device("cuda", snap.ctx.device)
+        self.pos = torch.tensor(pos, dtype=torch.float64, device=dev)
+        self.species = torch.tensor(sp, dtype=torch.int32, device=dev)
+        self.E = torch.zeros(self.nconfig, dtype=torch.float64, device=dev)
+        self.F = torch.zeros((int(off[-1]), 3), dtype=torch.float64, device=dev)
+        self.W = torch.zeros((self.nconfig, 6), dtype=torch.float64, device=dev)
+        snap.ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+
+    def set_positions(self, pos):
+        import torch
+        self.pos.copy_(torch.as_tensor(pos, dtype=torch.float64).reshape(-1, 3))
+
+    def evaluate(self, beta, beta0=0.0, mode="adjoint", graph=True):
+        """Fills (and returns) the device tensors E (nconf,), F (n_total, 3), W (nconf, 6)."""
+        beta = self.snap.beta_blocks(beta)
+        m = SNAP_ADJOINT if mode == "adjoint" else SNAP_PLAIN
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        self.snap.ctx.check(lib().ipg_snap_batch_energy_forces_dev(
+            self.snap._h, self.nconfig, _vp(self.off), ptr(self.pos), ptr(self.species), _vp(self.L), _vp(beta),
+            float(beta0), m, int(bool(graph)), ptr(self.E), ptr(self.F), ptr(self.W)))
+        return self.E, self.F, self.W
+
+
 def compute_local_descriptors(system, snap):
     """snap.jl:103-124 -> B (n, K)."""
     return snap._descriptors(system, DESC_B)[0]

@@ -63,3 +63,86 @@ def test_loss_gradient(batch):
         lp = snap.batch_loss_grad(systems, bp, Fref)[0]
         lm = snap.batch_loss_grad(systems, bm, Fref)[0]
         assert abs((lp - lm) / (2 * h) - g[s_, k]) <= 1e-6 * np.abs(g).max()
+
+
+def _moved(systems, rng, sigma=0.05):
+    return [ipg.System(s.positions + rng.normal(0, sigma, s.positions.shape), s.symbols, s.box, s.periodic)
+            for s in systems]
+
+
+def test_graph_replay(batch):
+    """ipg_snap_batch_energy_forces_dev with graph=1: capture on the first call, one graph launch
+    on later calls (new positions and beta read from the buffers), bitwise equal to eager runs."""
+    import torch
+    systems, snap, orc, beta = batch
+    db = ipg.DeviceBatch(snap, systems)
+    E0, F0, W0 = snap.batch_energy_forces(systems, beta, 0.1)
+    for call in range(3):
+        l0 = snap.ctx.launch_count()
+        E, F, W = db.evaluate(beta, 0.1, graph=True)
+        torch.cuda.synchronize()
+        if call > 0:  # a replay launches only k_ycoef through the library, the rest is the graph
+            assert snap.ctx.launch_count() - l0 <= 2
+        assert np.array_equal(E.cpu().numpy(), E0)
+        assert np.array_equal(F.cpu().numpy(), F0)
+        assert np.array_equal(W.cpu().numpy(), W0)
+    # new positions and beta through the same graph
+    rng = np.random.default_rng(7)
+    moved = _moved(systems, rng)
+    db.set_positions(np.concatenate([s.positions for s in moved]))
+    beta2 = 1.3 * beta
+    l0 = snap.ctx.launch_count()
+    E, F, W = db.evaluate(beta2, -0.2, graph=True)
+    torch.cuda.synchronize()
+    assert snap.ctx.launch_count() - l0 <= 2
+    E1, F1, W1 = snap.batch_energy_forces(moved, beta2, -0.2)
+    assert np.array_equal(E.cpu().numpy(), E1)
+    assert np.array_equal(F.cpu().numpy(), F1)
+    assert np.array_equal(W.cpu().numpy(), W1)
+    # plain mode gets its own graph
+    Ep, Fp, _ = db.evaluate(beta2, -0.2, mode="plain", graph=True)
+    Ep, Fp, _ = db.evaluate(beta2, -0.2, mode="plain", graph=True)
+    assert rel_err(Fp.cpu().numpy(), F1) <= TOL
+
+
+def test_graph_capacity_overflow_reruns(batch):
+    """A replay whose pair count outgrows the captured capacity re-runs eagerly (correct
+    results) and recaptures."""
+    import torch
+    systems, snap, orc, beta = batch
+    db = ipg.DeviceBatch(snap, systems)
+    db.evaluate(beta, 0.0, graph=True)
+    db.evaluate(beta, 0.0, graph=True)
+    # squeeze the largest configuration: many more neighbors than the 25% headroom
+    big = int(np.argmax([len(s) for s in systems]))
+    dense = list(systems)
+    s = systems[big]
+    c = s.positions.mean(axis=0)
+    dense[big] = ipg.System(c + 0.45 * (s.positions - c), s.symbols, s.box, s.periodic)
+    db.set_positions(np.concatenate([x.positions for x in dense]))
+    E, F, W = db.evaluate(beta, 0.0, graph=True)
+    torch.cuda.synchronize()
+    E1, F1, W1 = snap.batch_energy_forces(dense, beta, 0.0)
+    assert np.array_equal(E.cpu().numpy(), E1)
+    assert np.array_equal(F.cpu().numpy(), F1)
+    l0 = snap.ctx.launch_count()
+    E, F, W = db.evaluate(beta, 0.0, graph=True)  # the recaptured graph
+    torch.cuda.synchronize()
+    assert snap.ctx.launch_count() - l0 <= 2
+    assert np.array_equal(F.cpu().numpy(), F1)
+
+
+def test_graph_open_boundaries_run_eagerly():
+    import torch
+    prm = W.snap_j8_params()
+    snap = ipg.SNAP(1, prm["twojmax"], prm["species"], prm["rcutfac"], prm["rmin0"], prm["rfac0"], prm["radii"],
+                    prm["weight"], switch_flag=True)
+    systems = W.batch512(nconf=4, nmin=32, nmax=120)
+    systems = [ipg.System(s.positions, s.symbols, s.box, (True, False, True)) for s in systems]
+    beta = np.random.default_rng(8).normal(0, 1e-2, (2, len(snap)))
+    db = ipg.DeviceBatch(snap, systems)
+    E0, F0, _ = snap.batch_energy_forces(systems, beta, 0.0)
+    for _ in range(2):
+        E, F, _ = db.evaluate(beta, 0.0, graph=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(F.cpu().numpy(), F0)
