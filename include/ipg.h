@@ -220,6 +220,19 @@ IPG_API int ipg_snap_energy_forces_dev(ipg_snap* snap, int64_t n, const double* 
 IPG_API int ipg_snap_vjp_beta(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
                       double gE, const double* gF, double* gbeta, double* gbeta0);
 
+/* Full pullback of (E, F) (the ChainRulesCore.rrule of energy_and_force / potential_energy
+ * for LBasisPotential over SNAP): cotangents gE of E and gF [3n] of F (NULL = 0) give
+ *   gbeta [nspecies][K] and gbeta0 as ipg_snap_vjp_beta, and
+ *   gpos [3n] = d(gE E + gF . F)/dpos = -gE F - H gF    (H: Hessian of E).
+ * -gE F is exact (one adjoint evaluation).  H gF is the derivative of the forces along gF,
+ * taken by central differences with Richardson extrapolation (steps 2e-4 and 1e-4 of the
+ * largest cutoff along gF / max|gF|; four adjoint evaluations, error O(h^4)).  Any of
+ * gbeta, gbeta0, gpos may be NULL; beta [nspecies][K] is needed for gpos.  The reference
+ * defines no rrule; this is the pullback that Zygote / ChainRules callers of
+ * energy_and_force(s, lbp) need.                                                          */
+IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                 const double* beta, double gE, const double* gF, double* gbeta, double* gbeta0, double* gpos);
+
 /* ---- batched SNAP ------------------------------------------------------------------------
  * Many configurations at once: atoms of configuration c are atom_offsets[c] ..
  * atom_offsets[c+1]-1 of the flattened arrays; L is [nconfig][3].  Per-configuration

@@ -1315,6 +1315,28 @@ __global__ void k_ycoef(int nsp, int nz, int K, const double* __restrict__ ymult
   ycoef[t] = ymult[z] * beta[(size_t)s * K + yjjb[z]];
 }
 
+// out = x + t u (3n coordinates).
+__global__ void k_shift(int64_t m, const double* __restrict__ x, const double* __restrict__ u, double t,
+                        double* __restrict__ out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) out[k] = x[k] + t * u[k];
+}
+
+// Position pullback: gpos = -gE F0 + s R, R the Richardson-extrapolated central difference
+// of the forces along the unit direction (steps h and h/2).  Fh = {F(+h), F(-h), F(+h/2), F(-h/2)}.
+__global__ void k_vjp_pos(int64_t m, const double* __restrict__ F0, double gE, const double* __restrict__ Fp,
+                          const double* __restrict__ Fm, const double* __restrict__ Fp2, const double* __restrict__ Fm2,
+                          double h, double s, double* __restrict__ gpos) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  double g = -gE * F0[k];
+  if (Fp) {
+    const double d1 = (Fp[k] - Fm[k]) / (2.0 * h), d2 = (Fp2[k] - Fm2[k]) / h;
+    g += s * (4.0 * d2 - d1) / 3.0;
+  }
+  gpos[k] = g;
+}
+
 // Elementwise loss pieces: g = 2 (F - F_ref), per-atom |F - F_ref|^2.
 __global__ void k_loss_grad(int64_t n, const double* __restrict__ F, const double* __restrict__ Fref,
                             double* __restrict__ g, double* __restrict__ li) {
@@ -2068,6 +2090,61 @@ int ipg_snap_vjp_beta(ipg_snap* s, int64_t n, const double* pos, const int32_t* 
   IPG_RET(ipg_status_check(ctx, "ipg_snap_vjp_beta"));
   if (gbeta0) *gbeta0 = gE;
   return IPG_OK;
+}
+
+int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                 const double* beta, double gE, const double* gF, double* gbeta, double* gbeta0, double* gpos) {
+  IPG_RET(check_common(s, n, pos, species, L));
+  ipg_ctx* ctx = s->ctx;
+  if (gpos && !beta) return ipg_fail(ctx, IPG_ERR_ARG, "the position pullback needs beta");
+  if (gbeta) IPG_RET(ipg_snap_vjp_beta(s, n, pos, species, L, gE, gF, gbeta, nullptr));
+  if (gbeta0) *gbeta0 = gE;
+  if (!gpos || n == 0) return IPG_OK;
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double scale = 0.0;  // max |gF|: the difference step is taken along gF / scale
+  if (gF)
+    for (int64_t k = 0; k < 3 * n; k++) {
+      if (!std::isfinite(gF[k])) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite force cotangent");
+      scale = std::max(scale, std::fabs(gF[k]));
+    }
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  const size_t m = 3 * (size_t)n;
+  double *F0, *Fs, *x, *dir, *gp;
+  IPG_RET(scratch(ctx, "vjp_F0", m, &F0));
+  IPG_RET(scratch(ctx, "vjp_Fs", 4 * m, &Fs));
+  IPG_RET(scratch(ctx, "vjp_x", m, &x));
+  IPG_RET(scratch(ctx, "vjp_dir", m, &dir));
+  IPG_RET(scratch(ctx, "vjp_gpos", m, &gp));
+  IPG_RET(ipg_status_reset(ctx));
+  int64_t aoff[2] = {0, n};
+  EvalOut o;
+  o.F = F0;
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, o));
+  // step: 2e-4 of the largest cutoff (1e-3 for a 5 A cutoff), in the caller's length unit
+  double rmax = 0.0;
+  for (int q = 0; q < s->p.nspecies; q++) rmax = std::max(rmax, 2.0 * s->p.radii[q] * s->p.rcutfac);
+  const double h = 2e-4 * rmax;
+  if (scale > 0.0) {
+    std::vector<double> u(m);
+    for (size_t k = 0; k < m; k++) u[k] = gF[k] / scale;
+    CUDA_RET(ctx, cudaMemcpyAsync(dir, u.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
+    const double steps[4] = {h, -h, 0.5 * h, -0.5 * h};
+    for (int q = 0; q < 4; q++) {
+      IPG_LAUNCH(ctx, k_shift, nblk((int64_t)m, 256), 256, 0, (int64_t)m, d_pos, dir, steps[q], x);
+      EvalOut oq;
+      oq.F = Fs + q * m;
+      IPG_RET(snap_eval(s, n, x, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, oq));
+    }
+    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));  // u is released on return
+  }
+  const bool fd = scale > 0.0;
+  IPG_LAUNCH(ctx, k_vjp_pos, nblk((int64_t)m, 256), 256, 0, (int64_t)m, F0, gE, fd ? Fs : nullptr,
+             fd ? Fs + m : nullptr, fd ? Fs + 2 * m : nullptr, fd ? Fs + 3 * m : nullptr, h, scale, gp);
+  CUDA_RET(ctx, cudaMemcpyAsync(gpos, gp, sizeof(double) * m, cudaMemcpyDeviceToHost, ctx->stream));
+  return ipg_status_check(ctx, "ipg_snap_vjp");
 }
 
 int ipg_snap_batch_energy_forces_dev(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* d_pos,

@@ -156,6 +156,20 @@ class SNAP:
                                                float(gE), _vp(gF), _vp(gb), _vp(gb0)))
         return gb, gb0[0]
 
+    def vjp(self, system, beta, gE=0.0, gF=None):
+        """Pullback of (E, F) (include/ipg.h: ipg_snap_vjp): returns (gbeta (nsp, K), gbeta0,
+        gpos (n, 3)) with gpos = d(gE E + gF . F)/dpos = -gE F - H gF."""
+        n = len(system)
+        sp = self.species_ids(system)
+        beta = self.beta_blocks(beta)
+        gb = np.zeros((len(self.species), self.K))
+        gb0 = np.zeros(1)
+        gp = np.zeros((n, 3))
+        gF = None if gF is None else np.ascontiguousarray(gF, dtype=np.float64).reshape(n, 3)
+        self.ctx.check(lib().ipg_snap_vjp(self._h, n, _vp(system.positions), _vp(sp), _vp(system.L), _vp(beta),
+                                          float(gE), _vp(gF), _vp(gb), _vp(gb0), _vp(gp)))
+        return gb, gb0[0], gp
+
     # ---- batches ----------------------------------------------------------------------
     def _flatten(self, systems):
         off = np.zeros(len(systems) + 1, np.int64)

@@ -1,0 +1,122 @@
+"""Pullbacks of the SNAP energy and forces (ipg_snap_vjp and the torch autograd binding that
+mirrors the Julia rrule): beta and position gradients, checked against the beta VJP that the
+oracle pins, the exact -gE F energy term, central finite differences (h = 1e-5 A as for the
+energy gradient, 1e-4 A for the force term), Hessian symmetry and an oracle-built estimate."""
+import numpy as np
+import pytest
+
+import oracle
+import ipg
+from ipg import workloads as W
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    # 128 atoms, twojmax 8, two species; the 12.8 A box exceeds twice the 5 A cutoff, so every
+    # neighbor has one image and E is smooth (a smaller box switches images as atoms move)
+    system, prm, beta = W.snap_j8(cells=4)
+    snap = ipg.SNAP(1, prm["twojmax"], prm["species"], prm["rcutfac"], prm["rmin0"], prm["rfac0"], prm["radii"],
+                    prm["weight"], switch_flag=True)
+    orc = oracle.Snap(prm["twojmax"], prm["radii"], prm["weight"], prm["rcutfac"], prm["rmin0"], prm["rfac0"],
+                      switch=True)
+    return system, snap, orc, beta
+
+
+def _moved(s, d):
+    return ipg.System(s.positions + d, s.symbols, s.box, s.periodic)
+
+
+def test_vjp_beta_part_and_energy_term(case):
+    system, snap, orc, beta = case
+    rng = np.random.default_rng(11)
+    gF = rng.normal(size=(len(system), 3))
+    gb, gb0, _ = snap.vjp(system, beta, 0.7, gF)
+    gb_ref, gb0_ref = snap.vjp_beta(system, 0.7, gF)
+    assert rel_err(gb, gb_ref) <= 1e-14 and gb0 == 0.7
+    go, _ = orc.vjp_beta(system.positions, snap.species_ids(system), system.L, 0.7, gF)
+    assert rel_err(gb, go) <= 1e-10
+    _, _, gp = snap.vjp(system, beta, 0.7, None)
+    _, F, _ = snap.energy_forces(system, beta)
+    assert rel_err(gp, -0.7 * F) <= 1e-14
+
+
+def test_vjp_positions_finite_differences(case):
+    """gpos . w == d/de [gE E + gF . F](x + e w) by central differences."""
+    system, snap, orc, beta = case
+    rng = np.random.default_rng(12)
+    n = len(system)
+    gE, gF = 0.3, rng.normal(size=(n, 3))
+    _, _, gp = snap.vjp(system, beta, gE, gF)
+
+    def L(s):
+        E, F, _ = snap.energy_forces(s, beta)
+        return gE * E + np.sum(gF * F)
+
+    for seed in (1, 2):
+        w = np.random.default_rng(seed).normal(size=(n, 3))
+        eps = 1e-4
+        fd = (L(_moved(system, eps * w)) - L(_moved(system, -eps * w))) / (2 * eps)
+        assert abs(np.sum(gp * w) - fd) <= 1e-6 * max(abs(fd), 1e-12)
+
+
+def test_hessian_vector_symmetry(case):
+    """a . (H b) == b . (H a): gpos with gE = 0 is -H gF."""
+    system, snap, orc, beta = case
+    rng = np.random.default_rng(13)
+    a, b = rng.normal(size=(2, len(system), 3))
+    _, _, ha = snap.vjp(system, beta, 0.0, a)
+    _, _, hb = snap.vjp(system, beta, 0.0, b)
+    assert abs(np.sum(a * hb) - np.sum(b * ha)) <= 1e-8 * abs(np.sum(a * hb))
+
+
+def test_position_pullback_matches_oracle_estimate(case):
+    """The same Richardson estimate built from the oracle's forces (differences of 1e-13-close
+    forces divided by h = 1e-3 A stay within 1e-9)."""
+    system, snap, orc, beta = case
+    rng = np.random.default_rng(14)
+    gF = rng.normal(size=(len(system), 3))
+    _, _, gp = snap.vjp(system, beta, 0.5, gF)
+    sp = snap.species_ids(system)
+    scale = np.max(np.abs(gF))
+    u = gF / scale
+    h = 2e-4 * 2 * max(W.snap_j8_params()["radii"]) * W.snap_j8_params()["rcutfac"]
+    F = {t: orc.energy_forces(system.positions + t * u, sp, system.L, beta, 0.0)[1] for t in (0, h, -h, h / 2, -h / 2)}
+    d1 = (F[h] - F[-h]) / (2 * h)
+    d2 = (F[h / 2] - F[-h / 2]) / h
+    ref = -0.5 * F[0] + scale * (4 * d2 - d1) / 3
+    assert rel_err(gp, ref) <= 1e-8
+
+
+def test_torch_autograd(case):
+    torch = pytest.importorskip("torch")
+    from ipg.autograd import snap_energy_forces, snap_loss
+    system, snap, orc, beta = case
+    pos = torch.tensor(system.positions, requires_grad=True)
+    b = torch.tensor(beta, requires_grad=True)
+    E, F = snap_energy_forces(snap, system, pos, b, 0.3)
+    E.backward()
+    assert rel_err(pos.grad.numpy(), -F.detach().numpy()) <= 1e-14
+    gb, _ = snap.vjp_beta(system, 1.0, None)
+    assert rel_err(b.grad.numpy(), gb) <= 1e-14
+    # force-matching loss through the force output: beta gradient is exact (F is linear in beta)
+    pos.grad = None
+    b.grad = None
+    E, F = snap_energy_forces(snap, system, pos, b, 0.3)
+    loss = (F ** 2).sum()
+    loss.backward()
+    gb2, _ = snap.vjp_beta(system, 0.0, 2 * F.detach().numpy())
+    assert rel_err(b.grad.numpy(), gb2) <= 1e-14
+    _, _, gp2 = snap.vjp(system, beta, 0.0, 2 * F.detach().numpy())
+    assert rel_err(pos.grad.numpy(), gp2) <= 1e-14
+    # batch loss binding
+    systems = [system, _moved(system, 0.01)]
+    Fref = np.concatenate([snap.energy_forces(s, 1.1 * beta)[1] for s in systems])
+    bl = torch.tensor(beta, requires_grad=True)
+    lval = snap_loss(snap, systems, bl, Fref)
+    lval.backward()
+    l_ref, g_ref = snap.batch_loss_grad(systems, beta, Fref)
+    assert abs(lval.item() - l_ref) <= 1e-14 * l_ref
+    assert rel_err(bl.grad.numpy(), g_ref) <= 1e-14
