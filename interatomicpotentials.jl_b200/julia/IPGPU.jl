@@ -7,7 +7,7 @@
 # C ABI declared in include/ipg.h one to one.
 module IPGPU
 
-using InteratomicPotentials, AtomsBase, StaticArrays, Unitful, UnitfulAtomic
+using InteratomicPotentials, AtomsBase, StaticArrays, Unitful, UnitfulAtomic, ChainRulesCore
 import InteratomicPotentials: energy_and_force, potential_energy, force, virial_stress, virial,
     compute_local_descriptors, compute_force_descriptors, compute_all_descriptors
 
@@ -162,6 +162,78 @@ function energy_and_force(A::AbstractSystem, g::GPU{<:LBasisPotential})
     end
     ccall((:ipg_snap_destroy, libipg), Cint, (Ptr{Cvoid},), h)
     (; e = E[], f = reinterpret(SVector{3,Float64}, F))
+end
+
+# ---- pullbacks (ipg_snap_vjp, ipg_snap_batch_loss_grad) ----------------------------------
+# Cotangents are taken in the library's units (energy as returned, positions in the system's
+# length unit).  gE: cotangent of E; gF: cotangent of F (flat 3n, or nothing).
+function snap_vjp(A::AbstractSystem, lbp::LBasisPotential, gE::Float64, gF)
+    snap = lbp.basis
+    n, K, nsp = length(A), length(snap), length(snap.species)
+    h = handle(snap)
+    x = flatpos(A, ustrip)
+    L = ustrip.(box(A))
+    sp = Int32[findfirst(==(atomic_symbol(A, i)), snap.species) - 1 for i in 1:n]
+    β = repeat(lbp.β, nsp)
+    gβ, gβ0, gx = zeros(K * nsp), Ref(0.0), zeros(3n)
+    g = gF === nothing ? C_NULL : convert(Vector{Float64}, gF)
+    GC.@preserve x L sp β g gβ gx begin
+        check(ccall((:ipg_snap_vjp, libipg), Cint,
+                    (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Int32}, Ptr{Float64}, Ptr{Float64}, Float64,
+                     Ptr{Float64}, Ptr{Float64}, Ref{Float64}, Ptr{Float64}),
+                    h, n, x, sp, L, β, gE, g, gβ, gβ0, gx))
+    end
+    ccall((:ipg_snap_destroy, libipg), Cint, (Ptr{Cvoid},), h)
+    # the reference's beta is one K-vector shared by every species block
+    sum(reshape(gβ, K, nsp); dims = 2)[:, 1], gβ0[], reinterpret(SVector{3,Float64}, gx)
+end
+
+function ChainRulesCore.rrule(::typeof(potential_energy), A::AbstractSystem, g::GPU{<:LBasisPotential})
+    e = potential_energy(A, g)
+    function pullback(ē)
+        gβ, gβ0, gx = snap_vjp(A, g.p, Float64(ustrip(ē)), nothing)
+        (NoTangent(), Tangent{typeof(A)}(; position = gx),
+         Tangent{typeof(g)}(; p = Tangent{typeof(g.p)}(; β = gβ, β0 = [gβ0])))
+    end
+    e, pullback
+end
+
+function ChainRulesCore.rrule(::typeof(force), A::AbstractSystem, g::GPU{<:LBasisPotential})
+    f = force(A, g)
+    function pullback(f̄)
+        gF = reduce(vcat, [collect(Float64.(ustrip.(v))) for v in unthunk(f̄)])
+        gβ, _, gx = snap_vjp(A, g.p, 0.0, gF)
+        (NoTangent(), Tangent{typeof(A)}(; position = gx), Tangent{typeof(g)}(; p = Tangent{typeof(g.p)}(; β = gβ)))
+    end
+    f, pullback
+end
+
+# Force-matching loss over a batch: L = sum |F - F_ref|^2 and dL/dβ in one call
+# (flattened configurations, one persistent evaluation).
+function force_matching_loss(systems::Vector{<:AbstractSystem}, lbp::LBasisPotential, Fref::Vector{Float64})
+    snap = lbp.basis
+    K, nsp = length(snap), length(snap.species)
+    h = handle(snap)
+    off = Int64[0; cumsum(length.(systems))]
+    x = reduce(vcat, [flatpos(s, ustrip) for s in systems])
+    sp = Int32[findfirst(==(atomic_symbol(s, i)), snap.species) - 1 for s in systems for i in 1:length(s)]
+    L = reduce(vcat, [ustrip.(box(s)) for s in systems])
+    β = repeat(lbp.β, nsp)
+    loss, gβ = Ref(0.0), zeros(K * nsp)
+    GC.@preserve off x sp L β Fref gβ begin
+        check(ccall((:ipg_snap_batch_loss_grad, libipg), Cint,
+                    (Ptr{Cvoid}, Int32, Ptr{Int64}, Ptr{Float64}, Ptr{Int32}, Ptr{Float64}, Ptr{Float64}, Float64,
+                     Ptr{Float64}, Ref{Float64}, Ptr{Float64}),
+                    h, length(systems), off, x, sp, L, β, lbp.β0[1], Fref, loss, gβ))
+    end
+    ccall((:ipg_snap_destroy, libipg), Cint, (Ptr{Cvoid},), h)
+    loss[], sum(reshape(gβ, K, nsp); dims = 2)[:, 1]
+end
+
+function ChainRulesCore.rrule(::typeof(force_matching_loss), systems, lbp::LBasisPotential, Fref)
+    l, gβ = force_matching_loss(systems, lbp, Fref)
+    pullback(l̄) = (NoTangent(), NoTangent(), Tangent{typeof(lbp)}(; β = l̄ .* gβ), NoTangent())
+    l, pullback
 end
 
 end # module
