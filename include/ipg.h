@@ -233,6 +233,17 @@ IPG_API int ipg_snap_vjp_beta(ipg_snap* snap, int64_t n, const double* pos, cons
 IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
                  const double* beta, double gE, const double* gF, double* gbeta, double* gbeta0, double* gpos);
 
+/* Autotuner: times the adjoint evaluation of this configuration under each candidate kernel
+ * configuration and keeps the fastest for the handle.  Coordinate descent over the Y kernel
+ * (row-blocked or one Z entry at a time: the twojmax-dependent shared-memory layout), the
+ * per-neighbor kernel (all chains of a pair per thread, or one chain per thread), and the
+ * atoms (warps) per block of the Utot and neighbor-walk kernels (1, 2, 4).  cache_path
+ * (optional): a JSON-lines file keyed by device, twojmax, nspecies and the atom count
+ * rounded up to a power of two; a hit applies the stored choice without timing, a miss
+ * appends the result.  report (optional) receives the choice as one JSON object.        */
+IPG_API int ipg_snap_autotune(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                      const double* beta, const char* cache_path, char* report, int32_t report_len);
+
 /* ---- batched SNAP ------------------------------------------------------------------------
  * Many configurations at once: atoms of configuration c are atom_offsets[c] ..
  * atom_offsets[c+1]-1 of the flattened arrays; L is [nconfig][3].  Per-configuration

@@ -191,9 +191,10 @@ struct PairList {
 // cap > 0 selects capacity mode (no host read-back, so the build can be captured in a CUDA
 // graph): buffers hold cap pairs; a larger count sets IPG_ERR_CAPACITY in the status word
 // and every atom's list is cut at cap, so later kernels stay in bounds.
+// walk_warps: atoms (warps) per block of the neighbor walk, 1..4.
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
                     const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true,
-                    int64_t cap = 0);
+                    int64_t cap = 0, int walk_warps = 4);
 
 // Device helper: the distinct neighbor-cell coordinates along one axis (<= 3).
 __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {

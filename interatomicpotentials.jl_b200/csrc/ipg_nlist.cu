@@ -369,7 +369,9 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
 }
 
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
-                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted, int64_t cap) {
+                    const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted, int64_t cap,
+                    int walk_warps) {
+  const int wt = 32 * std::max(1, std::min(4, walk_warps));
   (void)d_species;
   std::string pre(prefix);
   PairTest t;
@@ -398,7 +400,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   cnt = pl.d_off;
   CUDA_RET(ctx, cudaMemsetAsync(cnt, 0, sizeof(int64_t) * (n + 1), ctx->stream));
   if (n > 0)
-    IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+    IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
   IPG_RET(ipg_scan_i64(ctx, cnt, pl.d_off, n + 1));
   pl.d_np = pl.d_off + n;
@@ -413,7 +415,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0) {
-    IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+    IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
     if (sorted) IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
   }

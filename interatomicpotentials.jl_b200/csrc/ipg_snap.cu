@@ -18,6 +18,9 @@
 // transpose, so every reduction is in a fixed order (bitwise reproducible).
 #include <algorithm>
 
+#include <cstdio>
+#include <string>
+
 #include "ipg_snap.cuh"
 #include "ipg_snap_chain.cuh"
 
@@ -632,21 +635,24 @@ __global__ void __launch_bounds__(128) k_snap_utot(const __grid_constant__ SnapD
 
 template <int J, int MB>
 int launch_utot_chains(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
-                       const double* rij, const int32_t* species, double2* utot) {
+                       const double* rij, const int32_t* species, double2* utot, int warps) {
   if constexpr (MB <= J / 2) {
-    IPG_TIMED_LAUNCH(ctx, "snap_utot", (k_snap_utot<J, MB>), nblk(n, 4), 128, 0, S, n, off, nbr, rij, species, utot);
-    return launch_utot_chains<J, MB + 1>(ctx, S, n, off, nbr, rij, species, utot);
+    IPG_TIMED_LAUNCH(ctx, "snap_utot", (k_snap_utot<J, MB>), nblk(n, warps), 32 * warps, 0, S, n, off, nbr, rij,
+                     species, utot);
+    return launch_utot_chains<J, MB + 1>(ctx, S, n, off, nbr, rij, species, utot, warps);
   }
   return IPG_OK;
 }
 
+// warps: atoms (warps) per block, 1..4.
 int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
-                const double* rij, const int32_t* species, double2* utot) {
+                const double* rij, const int32_t* species, double2* utot, int warps = 4) {
   if (n == 0) return IPG_OK;
+  warps = std::max(1, std::min(4, warps));
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return launch_utot_chains<JJ, 0>(ctx, S, n, off, nbr, rij, species, utot);
+    return launch_utot_chains<JJ, 0>(ctx, S, n, off, nbr, rij, species, utot, warps);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
 #undef IPG_J
     default:
@@ -1370,6 +1376,8 @@ struct ipg_snap {
   std::vector<int64_t> chunk_tab;  // per-configuration reduction chunks (host staging)
   bool pair_split = false;  // adjoint pair kernel: one thread per (pair, chain) instead of per pair
   bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
+  int utot_warps = 4;       // atoms (warps) per block of the Utot kernels
+  int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
   int64_t last_np = 0;
@@ -1385,6 +1393,7 @@ struct ipg_snap {
     const void *pos = nullptr, *sp = nullptr;
     void *E = nullptr, *F = nullptr, *W6 = nullptr;
     bool pair_split = false, y_entries = false;
+    int utot_warps = 0, walk_warps = 0;
     cudaGraphExec_t exec = nullptr;
     uint64_t gen = 0;  // ctx->scratch_gen at capture
     int64_t cap = 0;   // pair capacity
@@ -1556,7 +1565,7 @@ int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int3
   s->last_grid = cl.h_grid;
   int mode = IPG_NLIST_FULL | (s->p.literal_sqrt_radius ? IPG_NLIST_LITERAL_SQRT : 0);
   IPG_RET(ipg_build_pairs(s->ctx, "snap_", cl, d_species, s->p.nspecies, s->cutsq.data(), mode, true, pl, false,
-                          cap));
+                          cap, s->walk_warps));
   return IPG_OK;
 }
 
@@ -1599,7 +1608,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   if (chains && n) {  // Utot from the register-chain kernel
     double2* utot;
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
-    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot));
+    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps));
     io.utot_in = utot;
   }
   int nch = 1;
@@ -1715,7 +1724,8 @@ ipg_snap::Graph* find_graph(ipg_snap* s, int32_t nconfig, const int64_t* off, co
                             const void* pos, const void* sp, const EvalOut& o) {
   for (auto& g : s->graphs) {
     if (g.nconfig != nconfig || g.mode != mode || g.pos != pos || g.sp != sp || g.E != o.E || g.F != o.F ||
-        g.W6 != o.W6 || g.pair_split != s->pair_split || g.y_entries != s->y_entries)
+        g.W6 != o.W6 || g.pair_split != s->pair_split || g.y_entries != s->y_entries ||
+        g.utot_warps != s->utot_warps || g.walk_warps != s->walk_warps)
       continue;
     if (memcmp(g.off.data(), off, sizeof(int64_t) * (nconfig + 1)) != 0) continue;
     if (memcmp(g.L.data(), L, sizeof(double) * 3 * nconfig) != 0) continue;
@@ -1789,6 +1799,8 @@ void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const
   g.W6 = o.W6;
   g.pair_split = s->pair_split;
   g.y_entries = s->y_entries;
+  g.utot_warps = s->utot_warps;
+  g.walk_warps = s->walk_warps;
   g.cap = cap;
   g.grid = s->last_grid;
   g.chunks = s->last_chunks;
@@ -1812,6 +1824,55 @@ void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const
   }
   if (graph) cudaGraphDestroy(graph);
   cudaGetLastError();  // a failed capture leaves no sticky error behind
+}
+
+// ---- autotuner ------------------------------------------------------------------------
+struct TuneChoice {
+  int y_entries = 0, pair_split = 0, utot_warps = 4, walk_warps = 4;
+  double ms = 0.0;
+};
+
+void tune_apply(ipg_snap* s, const TuneChoice& c) {
+  s->y_entries = c.y_entries != 0;
+  s->pair_split = c.pair_split != 0;
+  s->utot_warps = c.utot_warps;
+  s->walk_warps = c.walk_warps;
+}
+
+int json_int(const std::string& line, const char* field, int dflt) {
+  const std::string f = std::string("\"") + field + "\":";
+  const size_t k = line.find(f);
+  if (k == std::string::npos) return dflt;
+  return atoi(line.c_str() + k + f.size());
+}
+
+// Cache: one JSON object per line; the last line with the key wins.
+bool tune_cache_lookup(const char* path, const std::string& key, TuneChoice& c) {
+  FILE* f = fopen(path, "r");
+  if (!f) return false;
+  bool hit = false;
+  char buf[1024];
+  const std::string want = "\"key\": \"" + key + "\"";
+  while (fgets(buf, sizeof(buf), f)) {
+    const std::string line(buf);
+    if (line.find(want) == std::string::npos) continue;
+    c.y_entries = json_int(line, "y_entries", 0);
+    c.pair_split = json_int(line, "pair_split", 0);
+    c.utot_warps = std::max(1, std::min(4, json_int(line, "utot_warps", 4)));
+    c.walk_warps = std::max(1, std::min(4, json_int(line, "walk_warps", 4)));
+    hit = true;
+  }
+  fclose(f);
+  return hit;
+}
+
+std::string tune_json(const std::string& key, const TuneChoice& c, bool cached, int tried) {
+  char buf[768];
+  snprintf(buf, sizeof(buf),
+           "{\"key\": \"%s\", \"y_entries\": %d, \"pair_split\": %d, \"utot_warps\": %d, \"walk_warps\": %d, "
+           "\"ms\": %.4f, \"cached\": %d, \"tried\": %d}",
+           key.c_str(), c.y_entries, c.pair_split, c.utot_warps, c.walk_warps, c.ms, cached ? 1 : 0, tried);
+  return buf;
 }
 
 int check_common(ipg_snap* s, int64_t n, const void* pos, const void* species, const double* L) {
@@ -2039,7 +2100,7 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
   if (dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && n) {
     double2* utot;
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
-    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot));
+    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps));
     io.utot_in = utot;
   }
   int threads = s->threads;
@@ -2145,6 +2206,102 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
              fd ? Fs + m : nullptr, fd ? Fs + 2 * m : nullptr, fd ? Fs + 3 * m : nullptr, h, scale, gp);
   CUDA_RET(ctx, cudaMemcpyAsync(gpos, gp, sizeof(double) * m, cudaMemcpyDeviceToHost, ctx->stream));
   return ipg_status_check(ctx, "ipg_snap_vjp");
+}
+
+int ipg_snap_autotune(ipg_snap* s, int64_t n, const double* pos, const int32_t* species, const double L[3],
+                      const double* beta, const char* cache_path, char* report, int32_t report_len) {
+  IPG_RET(check_common(s, n, pos, species, L));
+  ipg_ctx* ctx = s->ctx;
+  if (!beta) return ipg_fail(ctx, IPG_ERR_ARG, "null beta");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  cudaDeviceProp prop;
+  CUDA_RET(ctx, cudaGetDeviceProperties(&prop, ctx->device));
+  int64_t cls = 1;
+  while (cls < n) cls <<= 1;
+  char kb[320];
+  snprintf(kb, sizeof(kb), "%s|sm%d|twojmax%d|nsp%d|n%lld", prop.name, prop.multiProcessorCount, s->p.twojmax,
+           s->p.nspecies, (long long)cls);
+  const std::string key(kb);
+  TuneChoice best;
+  best.y_entries = s->y_entries;
+  best.pair_split = s->pair_split;
+  best.utot_warps = s->utot_warps;
+  best.walk_warps = s->walk_warps;
+  bool cached = cache_path && cache_path[0] && tune_cache_lookup(cache_path, key, best);
+  int tried = 0;
+  if (!cached && n > 0) {
+    double* d_pos;
+    int32_t* d_sp;
+    IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+    double *dE, *dF;
+    IPG_RET(scratch(ctx, "tune_E", 1, &dE));
+    IPG_RET(scratch(ctx, "tune_F", 3 * (size_t)n, &dF));
+    cudaEvent_t e0, e1;
+    CUDA_RET(ctx, cudaEventCreate(&e0));
+    CUDA_RET(ctx, cudaEventCreate(&e1));
+    int64_t aoff[2] = {0, n};
+    EvalOut o;
+    o.E = dE;
+    o.F = dF;
+    // best of 3 timed adjoint evaluations after one warm-up
+    auto measure = [&](const TuneChoice& c, double* ms) -> int {
+      tune_apply(s, c);
+      IPG_RET(ipg_status_reset(ctx));
+      IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, o));
+      IPG_RET(ipg_status_check(ctx, "ipg_snap_autotune"));
+      double b = 1e30;
+      for (int r = 0; r < 3; r++) {
+        CUDA_RET(ctx, cudaEventRecord(e0, ctx->stream));
+        IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, o));
+        CUDA_RET(ctx, cudaEventRecord(e1, ctx->stream));
+        CUDA_RET(ctx, cudaEventSynchronize(e1));
+        float t = 0.0f;
+        CUDA_RET(ctx, cudaEventElapsedTime(&t, e0, e1));
+        b = std::min(b, (double)t);
+      }
+      tried++;
+      *ms = b;
+      return IPG_OK;
+    };
+    int st = measure(best, &best.ms);
+    // coordinate descent: each knob in turn, the others at their best so far
+    const bool rows_ok = s->dev.J <= YR_MAX_J, chains_ok = s->dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
+    for (int knob = 0; knob < 4 && st == IPG_OK; knob++) {
+      std::vector<int> vals;
+      if (knob == 0 && rows_ok) vals = {0, 1};
+      if (knob == 1 && chains_ok) vals = {0, 1};
+      if (knob == 2 && chains_ok) vals = {1, 2, 4};
+      if (knob == 3) vals = {1, 2, 4};
+      for (int v : vals) {
+        TuneChoice c = best;
+        int* f = knob == 0 ? &c.y_entries : knob == 1 ? &c.pair_split : knob == 2 ? &c.utot_warps : &c.walk_warps;
+        if (*f == v) continue;
+        *f = v;
+        st = measure(c, &c.ms);
+        if (st) break;
+        if (c.ms < best.ms) best = c;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) {
+      tune_apply(s, TuneChoice());
+      return st;
+    }
+    if (cache_path && cache_path[0]) {
+      if (FILE* f = fopen(cache_path, "a")) {
+        fprintf(f, "%s\n", tune_json(key, best, false, tried).c_str());
+        fclose(f);
+      }
+    }
+  }
+  tune_apply(s, best);
+  if (report && report_len > 0) {
+    const std::string js = tune_json(key, best, cached, tried);
+    snprintf(report, (size_t)report_len, "%s", js.c_str());
+  }
+  return IPG_OK;
 }
 
 int ipg_snap_batch_energy_forces_dev(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* d_pos,

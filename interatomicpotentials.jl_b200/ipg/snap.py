@@ -170,6 +170,18 @@ class SNAP:
                                           float(gE), _vp(gF), _vp(gb), _vp(gb0), _vp(gp)))
         return gb, gb0[0], gp
 
+    def autotune(self, system, beta, cache_path=None):
+        """Picks the fastest kernel configuration for workloads like `system`
+        (include/ipg.h: ipg_snap_autotune); returns the choice as a dict."""
+        import json
+        sp = self.species_ids(system)
+        beta = self.beta_blocks(beta)
+        buf = C.create_string_buffer(1024)
+        path = None if cache_path is None else str(cache_path).encode()
+        self.ctx.check(lib().ipg_snap_autotune(self._h, len(system), _vp(system.positions), _vp(sp), _vp(system.L),
+                                               _vp(beta), path, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     # ---- batches ----------------------------------------------------------------------
     def _flatten(self, systems):
         off = np.zeros(len(systems) + 1, np.int64)

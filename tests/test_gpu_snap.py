@@ -248,3 +248,24 @@ def test_twojmax_beyond_shared_memory_is_unsupported():
     with pytest.raises(ipg.IPGError) as e:
         ipg.compute_local_descriptors(s, snap)
     assert e.value.status == -8
+
+
+def test_autotune_choice_and_cache(tmp_path):
+    """The autotuner times the candidate kernel configurations, keeps the fastest, writes the
+    cache, and applies a cached choice without timing; every choice gives the same forces."""
+    system, prm, beta = W.snap_j8(cells=8)
+    snap, orc = make(prm, switch_flag=True)
+    E0, F0, _ = snap.energy_forces(system, beta)
+    cache = tmp_path / "tune.jsonl"
+    rep = snap.autotune(system, beta, cache)
+    assert rep["cached"] == 0 and rep["tried"] >= 6 and rep["ms"] > 0
+    assert rep["utot_warps"] in (1, 2, 4) and rep["walk_warps"] in (1, 2, 4)
+    E1, F1, _ = snap.energy_forces(system, beta)
+    assert abs(E1 - E0) <= 1e-12 * abs(E0) and rel_err(F1, F0) <= 1e-12
+    snap2, _ = make(prm, switch_flag=True)
+    rep2 = snap2.autotune(system, beta, cache)
+    assert rep2["cached"] == 1 and rep2["tried"] == 0
+    for k in ("y_entries", "pair_split", "utot_warps", "walk_warps"):
+        assert rep2[k] == rep[k]
+    E2, F2, _ = snap2.energy_forces(system, beta)
+    assert abs(E2 - E0) <= 1e-12 * abs(E0) and rel_err(F2, F0) <= 1e-12
