@@ -53,6 +53,16 @@ NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.927552e6 + 4.160512e6) / 16000,
                            "snap_pair": (50.504448e6 + 0.944640e6) / 16000}
 
 
+def _hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0  # earlier measurement on this pool
+
+
+HBM_PEAK = _hbm_peak()
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -340,8 +350,8 @@ def main():
         line["adjoint_over_plain"] = value / plain_value
         line["plain_kernel_ms_per_step"] = {k: v[0] / max(2, args.steps // 2) for k, v in ktp.items() if v[1]}
         pair = {}
-        for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000())):
-            pairs = sum(len(x) for x in ipg.neighborlist(s2, p2.get_rcutoff(), ctx=ctx).j)
+        for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000()), ("lc_scaled", W.lc32000(cells=101))):
+            pairs = ipg.api.neighbor_count(s2, p2.get_rcutoff(), ctx=ctx)
             terms = ipg.empirical.empirical_terms(p2)
             idx = {s: k for k, s in enumerate(s2.unique_symbols())}
             arr = (ipg._lib.PairTerm * len(terms))()
@@ -356,11 +366,22 @@ def main():
                 ctx.check(lib().ipg_pair_eval_dev(ctx.handle, len(s2), vp(p_d.data_ptr()), vp(s_d.data_ptr()),
                                                   L2.ctypes.data_as(vp), C.cast(arr, vp), len(terms),
                                                   vp(E_d.data_ptr()), vp(f_d.data_ptr()), vp(W_d.data_ptr()), 7))
-            ms_p, _, _ = timed(pstep, args.steps)
+            psteps = args.steps if len(s2) < 1_000_000 else max(2, min(args.steps, 5))
+            ms_p, _, kp = timed(pstep, psteps, kernel_timing=True)
             # pairs/s counts every term's half pairs, as the reference evaluates them
             term_pairs = pairs * len(terms)
-            pair[name] = {"pairs_per_s": world * term_pairs * args.steps / (ms_p * 1e-3), "ms_per_step":
-                          ms_p / args.steps, "n_atoms": len(s2), "half_pairs": pairs, "terms": len(terms)}
+            pair[name] = {"pairs_per_s": world * term_pairs * psteps / (ms_p * 1e-3), "ms_per_step":
+                          ms_p / psteps, "n_atoms": len(s2), "half_pairs": pairs, "terms": len(terms)}
+            if name == "lc_scaled":
+                # HBM roofline of the pair path: algorithmic bytes per step = positions (24 B),
+                # species (4 B) and forces (24 B) per atom; no pair list is materialised.  The
+                # kernel is bound by candidate filtering and FP64 term evaluation, not by HBM.
+                k_ms = kp.get("pair_eval", (0.0, 0))[0] / psteps
+                nbytes = 52.0 * len(s2)
+                gbps = nbytes / (k_ms * 1e-3) / 1e9 if k_ms else None
+                pair[name]["hbm"] = {"algorithmic_bytes": nbytes, "kernel_ms": k_ms, "achieved_GBps": gbps,
+                                     "peak_GBps": HBM_PEAK, "frac": gbps / HBM_PEAK if gbps else None,
+                                     "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
         line["lj_pairs_per_s"] = pair
 
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -95,6 +95,10 @@ IPG_API int ipg_timing_read(ipg_ctx* ctx, const char* kernel, double* total_ms, 
 IPG_API int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
                        int32_t nspecies, const double* cut, int32_t mode, ipg_nlist** out);
 IPG_API int ipg_nlist_size(const ipg_nlist* nl, int64_t* npairs);
+/* The pair count of the list ipg_neighbor_build would return, without building or copying
+ * it (cell list and one counting walk on the device). */
+IPG_API int ipg_neighbor_count(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
+                       int32_t nspecies, const double* cut, int32_t mode, int64_t* npairs);
 /* offsets [n+1], j [npairs] (0-based), r [3*npairs]; any may be NULL. */
 IPG_API int ipg_nlist_export(const ipg_nlist* nl, int64_t* offsets, int32_t* j, double* r);
 IPG_API int ipg_nlist_free(ipg_nlist* nl);

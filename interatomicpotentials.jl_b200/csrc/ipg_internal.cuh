@@ -194,7 +194,7 @@ struct PairList {
 // walk_warps: atoms (warps) per block of the neighbor walk, 1..4.
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
                     const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true,
-                    int64_t cap = 0, int walk_warps = 4);
+                    int64_t cap = 0, int walk_warps = 4, bool count_only = false);
 
 // Device helper: the distinct neighbor-cell coordinates along one axis (<= 3).
 __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {

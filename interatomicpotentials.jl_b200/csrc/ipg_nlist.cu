@@ -370,7 +370,7 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
 
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
                     const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted, int64_t cap,
-                    int walk_warps) {
+                    int walk_warps, bool count_only) {
   const int wt = 32 * std::max(1, std::min(4, walk_warps));
   (void)d_species;
   std::string pre(prefix);
@@ -412,6 +412,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
     CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
   }
   if (pl.npairs >= (int64_t)1 << 40) return ipg_fail(ctx, IPG_ERR_CAPACITY, "pair count overflow");
+  if (count_only) return IPG_OK;
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0) {
@@ -444,11 +445,12 @@ struct ipg_nlist {
   std::vector<double> r;
 };
 
-extern "C" {
+namespace {
 
-int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
-                       int32_t nspecies, const double* cut, int32_t mode, ipg_nlist** out) {
-  if (!ctx || !out || n < 0 || (n > 0 && !pos) || !L || !cut) return IPG_ERR_ARG;
+// Validates and uploads the inputs and builds the pair list (or only counts it).
+int neighbor_pairs(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
+                   int32_t nspecies, const double* cut, int32_t mode, bool count_only, PairList& pl) {
+  if (!ctx || n < 0 || (n > 0 && !pos) || !L || !cut) return IPG_ERR_ARG;
   if (n >= INT32_MAX) return ipg_fail(ctx, IPG_ERR_ARG, "n too large");
   int base = mode & 0xff;
   if (base != IPG_NLIST_HALF && base != IPG_NLIST_FULL) return ipg_fail(ctx, IPG_ERR_ARG, "bad mode");
@@ -482,9 +484,29 @@ int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double 
   if (!(radius >= 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "cutoff must be >= 0");
   CellList cl;
   IPG_RET(ipg_build_cells(ctx, "nl_", n, d_pos, d_sp, std::max(1, (int)nspecies), 1, aoff, L, radius, cl));
+  IPG_RET(ipg_build_pairs(ctx, "nl_", cl, d_sp, std::max(1, (int)nspecies), cut, mode, false, pl, true, 0, 4,
+                          count_only));
+  return ipg_status_check(ctx, count_only ? "ipg_neighbor_count" : "ipg_neighbor_build");
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipg_neighbor_count(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
+                       int32_t nspecies, const double* cut, int32_t mode, int64_t* npairs) {
+  if (!npairs) return IPG_ERR_ARG;
   PairList pl;
-  IPG_RET(ipg_build_pairs(ctx, "nl_", cl, d_sp, std::max(1, (int)nspecies), cut, mode, false, pl));
-  IPG_RET(ipg_status_check(ctx, "ipg_neighbor_build"));
+  IPG_RET(neighbor_pairs(ctx, n, pos, L, species, nspecies, cut, mode, true, pl));
+  *npairs = pl.npairs;
+  return IPG_OK;
+}
+
+int ipg_neighbor_build(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3], const int32_t* species,
+                       int32_t nspecies, const double* cut, int32_t mode, ipg_nlist** out) {
+  if (!out) return IPG_ERR_ARG;
+  PairList pl;
+  IPG_RET(neighbor_pairs(ctx, n, pos, L, species, nspecies, cut, mode, false, pl));
   ipg_nlist* nl = new ipg_nlist();
   nl->n = n;
   nl->npairs = pl.npairs;

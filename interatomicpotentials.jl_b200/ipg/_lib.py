@@ -29,7 +29,7 @@ MAX_PAIR_TERMS = 16
 # Every symbol include/ipg.h declares.
 API_SYMBOLS = (
     "ipg_create", "ipg_destroy", "ipg_last_error", "ipg_set_timeout_ms", "ipg_set_stream", "ipg_version",
-    "ipg_launch_count", "ipg_timing_enable", "ipg_timing_read", "ipg_neighbor_build", "ipg_nlist_size", "ipg_nlist_export", "ipg_nlist_free",
+    "ipg_launch_count", "ipg_timing_enable", "ipg_timing_read", "ipg_neighbor_build", "ipg_neighbor_count", "ipg_nlist_size", "ipg_nlist_export", "ipg_nlist_free",
     "ipg_pair_eval", "ipg_pair_eval_dev", "ipg_pair_eval_noalloc", "ipg_snap_create", "ipg_snap_destroy", "ipg_snap_ncoeff",
     "ipg_snap_descriptors", "ipg_snap_energy_forces", "ipg_snap_energy_forces_dev", "ipg_snap_vjp_beta",
     "ipg_snap_vjp", "ipg_snap_autotune", "ipg_snap_batch_energy_forces", "ipg_snap_batch_energy_forces_dev", "ipg_snap_batch_loss_grad",
@@ -79,6 +79,7 @@ def lib():
         "ipg_timing_read": (C.c_int, [vp, C.c_char_p, C.POINTER(d), C.POINTER(i64)]),
         "ipg_neighbor_build": (C.c_int, [vp, i64, vp, vp, vp, i32, vp, i32, C.POINTER(vp)]),
         "ipg_nlist_size": (C.c_int, [vp, C.POINTER(i64)]),
+        "ipg_neighbor_count": (C.c_int, [vp, i64, vp, vp, vp, i32, vp, i32, C.POINTER(i64)]),
         "ipg_nlist_export": (C.c_int, [vp, vp, vp, vp]),
         "ipg_nlist_free": (C.c_int, [vp]),
         "ipg_pair_eval": (C.c_int, [vp, i64, vp, vp, vp, vp, i32, vp, vp, vp, u32]),

@@ -125,6 +125,17 @@ def neighborlist_snap(s, snap, ctx=None):
     return _nlist(s, cutsq.ravel(), snap.species_ids(s), nsp, mode, ctx)
 
 
+def neighbor_count(s, rcut, ctx=None):
+    """Number of half pairs within rcut (the size of neighborlist(s, rcut)) without building it."""
+    ctx = ctx or default_context()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    cut = np.array([float(rcut)])
+    out = C.c_int64()
+    ctx.check(lib().ipg_neighbor_count(ctx.handle, len(s), vp(s.positions), vp(s.L), None, 1, vp(cut), 0,
+                                       C.byref(out)))
+    return out.value
+
+
 def _nlist(s, cut, species, nsp, mode, ctx):
     ctx = ctx or default_context()
     vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)

@@ -81,3 +81,11 @@ def test_nonfinite_positions_rejected():
     with pytest.raises(ipg.IPGError) as e:
         ipg.neighborlist(s, 1.0)
     assert e.value.status == -6
+
+
+def test_neighbor_count_matches_built_list():
+    from ipg import workloads as W
+    s1, p1 = W.lj1000()
+    s2, p2 = W.lc32000(cells=6)
+    for s, rc in ((s1, p1.get_rcutoff()), (s2, p2.get_rcutoff())):
+        assert ipg.api.neighbor_count(s, rc) == len(ipg.neighborlist(s, rc)._j)
