@@ -806,17 +806,34 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yatoms(const __grid_c
 // template parameter: the code of one instantiation stays small enough for the
 // instruction cache although the warps of a block work on different rows.
 
-constexpr unsigned long long SIGNBIT = 0x8000000000000000ull;
-
-__device__ __forceinline__ double flip(double v, unsigned long long m) {
-  return __longlong_as_double(__double_as_longlong(v) ^ m);
-}
-
 // Guard entries (zeros) before and after the half plane in shared memory: the column
 // walks below read up to YR_GUARD entries past either end of a row.  Those reads meet a
 // CG factor of exactly zero (the factor tables are zero wherever ma1 or ma2 is out of
 // range), so they only have to stay inside the array and be finite.
 __host__ __device__ constexpr int yr_guard(int J) { return J + 2; }
+
+// Shared memory of k_snap_yrows, in bytes:
+//   front: the triple coefficients [nsp][ntp] (beta-dependent, filled per launch) and the CG
+//          factors of every triple (yca), at least yr_guard entries of Utot long;
+//   Utot:  the half plane of 32 atoms, [u_half][32] double2;
+//   back:  the energy slot of every target row, [rows][32] doubles, at least yr_guard long.
+// The out-of-range window reads fall into front or back: finite values (the free parts are
+// zeroed) that meet CG factors of exactly zero.
+struct YrSmem {
+  int ntp, front, u, back;
+  __host__ __device__ int total() const { return front + u + back; }
+};
+__host__ __device__ inline YrSmem yr_smem(int J, int nsp, int ntrip, int nyca, int uh, int nrows) {
+  YrSmem m;
+  m.ntp = ntrip + (ntrip & 1);
+  const int guard = yr_guard(J) * YS_ATOMS * 16;
+  const int f = (8 * (nsp * m.ntp + nyca) + 15) & ~15;
+  m.front = f > guard ? f : guard;
+  m.u = uh * YS_ATOMS * 16;
+  const int e = nrows * YS_ATOMS * 8;
+  m.back = e > guard ? e : guard;
+  return m;
+}
 
 // One row pair (mb1, mb2) of a triple for the target-row tile ma = ma0 .. ma0+NT-1.  The
 // j1 row is walked as a window: element t of column pair m0 is ma1 = d - m0 - 1 + ma0 + t,
@@ -848,26 +865,33 @@ __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const i
     r[1] = make_double2(sx1 * v1.x, sy1 * v1.y);
     double2 a[NT];
 #pragma unroll
-    for (int i = 0; i < NT; i++) a[i] = __ldg(cp + i);
+    for (int i = 0; i < NT; i++) a[i] = cp[i];
     const int base = d - m0 - 1 + ma0;
     const double2* pb = p1 + (M1 ? -base : base) * YS_ATOMS;
+    double2 u[NT + 1];
 #pragma unroll
-    for (int t = 0; t <= NT; t++) {
-      const double2 u = pb[(M1 ? -t : t) * YS_ATOMS];
+    for (int t = 0; t <= NT; t++) u[t] = pb[(M1 ? -t : t) * YS_ATOMS];
+    // one sweep per column (q = 1: element i, q = 0: element i + 1), so the two updates of an
+    // accumulator are NT terms apart; each term forms the complex product first and adds it
+    // with one FMA per component
 #pragma unroll
-      for (int q = 0; q < 2; q++) {
-        const int i = t - 1 + q;
-        if (i < 0 || i >= NT) continue;
+    for (int q = 1; q >= 0; q--) {
+#pragma unroll
+      for (int i = 0; i < NT; i++) {
+        const double2 v = u[i + 1 - q];
+        const double2 w = r[q];
+        double px, py;
+        if (M1) {  // conj(v) w
+          px = fma(v.x, w.x, v.y * w.y);
+          py = fma(v.x, w.y, -(v.y * w.x));
+        } else {
+          px = fma(v.x, w.x, -(v.y * w.y));
+          py = fma(v.x, w.y, v.y * w.x);
+        }
         const double c0 = q ? a[i].y : a[i].x;
         const double c = (M1 && ((i + q) & 1)) ? -c0 : c0;
-        const double tx = c * u.x, ty = c * u.y;
-        if (M1) {  // conj(u) r
-          acc[i].x = fma(tx, r[q].x, fma(ty, r[q].y, acc[i].x));
-          acc[i].y = fma(tx, r[q].y, fma(-ty, r[q].x, acc[i].y));
-        } else {
-          acc[i].x = fma(tx, r[q].x, fma(-ty, r[q].y, acc[i].x));
-          acc[i].y = fma(tx, r[q].y, fma(ty, r[q].x, acc[i].y));
-        }
+        acc[i].x = fma(c, px, acc[i].x);
+        acc[i].y = fma(c, py, acc[i].y);
       }
     }
   }
@@ -877,8 +901,9 @@ __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const i
 // Writes Y' = w Y of the tile's entries below nma and returns their Re(conj(U) Y').
 template <int NT>
 __device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, int ma0, int nma,
-                                          const double2* __restrict__ usl, const double* __restrict__ yc, int64_t n,
-                                          int64_t atom, bool valid, double2* __restrict__ yout) {
+                                          const double2* __restrict__ usl, const double* __restrict__ yc,
+                                          const double2* __restrict__ cas, int64_t n, int64_t atom, bool valid,
+                                          double2* __restrict__ yout) {
   double2 acc[NT];
 #pragma unroll
   for (int i = 0; i < NT; i++) acc[i] = make_double2(0.0, 0.0);
@@ -886,9 +911,9 @@ __device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, 
   const double bn = S.bnorm_flag ? 1.0 / (j + 1) : 1.0;
   for (int t = row.t0; t < row.t1; t++) {
     const YItemDev it = S.yitems[t];
-    const double c = yc[it.jjz] * bn;
+    const double c = yc[it.trip] * bn;
     const double* __restrict__ cg = S.cglist + it.cg;
-    const double2* __restrict__ cp = reinterpret_cast<const double2*>(S.yca + it.ca);
+    const double2* __restrict__ cp = cas + it.ca / 2;
     const int j1 = it.j1, j2 = it.j2, d = it.d, s2 = j2 + 1;
     for (int ib = 0; ib < it.nb; ib++) {
       const int mb1 = it.mb1min + ib, mb2 = it.mb2max - ib;
@@ -918,8 +943,8 @@ __device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, 
 constexpr int YR_TILE = 6;
 
 __device__ __forceinline__ double yr_row(const SnapDev& S, const YRowDev& row, const double2* __restrict__ usl,
-                                         const double* __restrict__ yc, int64_t n, int64_t atom, bool valid,
-                                         double2* __restrict__ yout) {
+                                         const double* __restrict__ yc, const double2* __restrict__ cas, int64_t n,
+                                         int64_t atom, bool valid, double2* __restrict__ yout) {
   const int nma = row.mid ? row.mb + 1 : row.j + 1;
   const int ntile = (nma + YR_TILE - 1) / YR_TILE;
   double e = 0.0;
@@ -929,7 +954,7 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YRowDev& row, c
     switch (w) {
 #define IPG_NT(NT) \
   case NT:         \
-    e += yr_tile<NT>(S, row, ma0, nma, usl, yc, n, atom, valid, yout); \
+    e += yr_tile<NT>(S, row, ma0, nma, usl, yc, cas, n, atom, valid, yout); \
     break;
       IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
 #undef IPG_NT
@@ -945,15 +970,26 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
                                                                  const int32_t* __restrict__ species,
                                                                  const double2* __restrict__ utot,
                                                                  double2* __restrict__ yout, double* __restrict__ Ei) {
-  extern __shared__ double2 ush[];  // guard | half plane of Utot [u_half][YS_ATOMS] | guard
-  __shared__ double erow[yr_rows(YR_MAX_J)][YS_ATOMS];  // energy term of each target row
+  extern __shared__ __align__(16) unsigned char ysh[];  // layout: yr_smem
   __shared__ int next_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int U = S.idxu_max, UH = S.u_half, G = yr_guard(S.J);
-  double2* us = ush + G * YS_ATOMS;
-  for (int idx = threadIdx.x; idx < G * YS_ATOMS; idx += blockDim.x) {
-    ush[idx] = make_double2(0.0, 0.0);
-    us[UH * YS_ATOMS + idx] = make_double2(0.0, 0.0);
+  const int U = S.idxu_max, UH = S.u_half;
+  const YrSmem M = yr_smem(S.J, S.nsp, S.n_ytrip, S.n_yca, UH, S.n_yrows);
+  double* ycs = reinterpret_cast<double*>(ysh);  // [nsp][ntp] Y coefficient of each triple
+  double* cad = ycs + S.nsp * M.ntp;             // CG factors of every triple
+  const double2* cas = reinterpret_cast<const double2*>(cad);
+  double2* us = reinterpret_cast<double2*>(ysh + M.front);
+  double* erow = reinterpret_cast<double*>(ysh + M.front + M.u);  // [rows][32]
+  for (int idx = threadIdx.x; idx < S.nsp * M.ntp; idx += blockDim.x) {
+    const int sp = idx / M.ntp, t = idx - sp * M.ntp;
+    ycs[idx] = t < S.n_ytrip ? S.ycoef[(size_t)sp * S.idxz_max + S.ytrip_jjz[t]] : 0.0;
+  }
+  for (int idx = threadIdx.x; idx < S.n_yca; idx += blockDim.x) cad[idx] = S.yca[idx];
+  {
+    double* gap = cad + S.n_yca;
+    const int ngap = (M.front - 8 * (S.nsp * M.ntp + S.n_yca)) / 8;
+    for (int idx = threadIdx.x; idx < ngap; idx += blockDim.x) gap[idx] = 0.0;
+    for (int idx = threadIdx.x; idx < M.back / 8; idx += blockDim.x) erow[idx] = 0.0;
   }
   for (int64_t a0 = (int64_t)blockIdx.x * YS_ATOMS; a0 < n; a0 += (int64_t)gridDim.x * YS_ATOMS) {
     const int na_blk = (int)((n - a0) < YS_ATOMS ? (n - a0) : YS_ATOMS);
@@ -966,7 +1002,7 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
     const int64_t atom = a0 + lane;
     const bool valid = lane < na_blk;
     const int si = valid ? clamp_sp(species[atom], S.nsp) : 0;
-    const double* yc = S.ycoef + (size_t)si * S.idxz_max;
+    const double* yc = ycs + si * M.ntp;
     const double2* usl = us + lane;
     // rows are handed out longest first to whichever warp is free; a row's result does
     // not depend on the warp that computes it, and the energy is summed in row order
@@ -976,12 +1012,12 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
       r = __shfl_sync(0xffffffffu, r, 0);
       if (r >= S.n_yrows) break;
       const YRowDev row = S.yrows[r];
-      erow[r][lane] = yr_row(S, row, usl, yc, n, atom, valid, yout);
+      erow[r * YS_ATOMS + lane] = yr_row(S, row, usl, yc, cas, n, atom, valid, yout);
     }
     __syncthreads();
     if (warp == 0 && valid) {
       double t = 0.0;
-      for (int r = 0; r < S.n_yrows; r++) t += erow[r][lane];
+      for (int r = 0; r < S.n_yrows; r++) t += erow[r * YS_ATOMS + lane];
       Ei[atom] = (2.0 / 3.0) * t + S.ebias[si];
     }
     __syncthreads();
@@ -1427,7 +1463,8 @@ int upload_tables(ipg_snap* s) {
   size_t o_yrows = o_uoh + pad(h.u_of_h.size() * 4);
   size_t o_yit = o_yrows + pad(h.yrows.size() * sizeof(YRowDev));
   size_t o_yca = o_yit + pad(h.yitems.size() * sizeof(YItemDev));
-  size_t total = o_yca + pad(h.yca.size() * 8);
+  size_t o_ytj = o_yca + pad(h.yca.size() * 8);
+  size_t total = o_ytj + pad(h.ytrip_jjz.size() * 4);
   CUDA_RET(ctx, cudaMalloc(&s->d_tables, total));
   char* b = static_cast<char*>(s->d_tables);
   std::vector<char> hostbuf(total, 0);
@@ -1447,6 +1484,7 @@ int upload_tables(ipg_snap* s) {
   memcpy(hostbuf.data() + o_yrows, h.yrows.data(), h.yrows.size() * sizeof(YRowDev));
   memcpy(hostbuf.data() + o_yit, h.yitems.data(), h.yitems.size() * sizeof(YItemDev));
   memcpy(hostbuf.data() + o_yca, h.yca.data(), h.yca.size() * 8);
+  memcpy(hostbuf.data() + o_ytj, h.ytrip_jjz.data(), h.ytrip_jjz.size() * 4);
   CUDA_RET(ctx, cudaMemcpy(b, hostbuf.data(), total, cudaMemcpyHostToDevice));
   SnapDev& d = s->dev;
   memset(&d, 0, sizeof(d));
@@ -1489,6 +1527,9 @@ int upload_tables(ipg_snap* s) {
   d.yrows = reinterpret_cast<const YRowDev*>(b + o_yrows);
   d.yitems = reinterpret_cast<const YItemDev*>(b + o_yit);
   d.yca = reinterpret_cast<const double*>(b + o_yca);
+  d.ytrip_jjz = reinterpret_cast<const int32_t*>(b + o_ytj);
+  d.n_ytrip = (int)h.ytrip_jjz.size();
+  d.n_yca = (int)h.yca.size();
   s->d_ymult = reinterpret_cast<double*>(b + o_ym);
   s->d_yjjb = reinterpret_cast<int32_t*>(b + o_yjjb);
   return IPG_OK;
@@ -1627,7 +1668,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
         const bool rows = dev.J <= YR_MAX_J && !s->y_entries;
         const void* kfn = rows ? (const void*)k_snap_yrows : (const void*)k_snap_yatoms;
-        if (rows) ysm += (size_t)2 * yr_guard(dev.J) * YS_ATOMS * sizeof(double2);
+        if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
         CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
         CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, YS_WARPS * 32, ysm));

@@ -42,13 +42,14 @@ struct YItemDev {
   int32_t ca;   // offset in yca of the triple's CG factors, [m0/2][ma][2] (zero where out of range)
   int32_t cg;   // idxcg_block[j1][j2][j]: the row factors cg[mb1 (j2+1) + mb2]
   int32_t jjz;  // first Z entry of the triple (its Y coefficient)
-  int32_t pad2;
+  int32_t trip; // index of the triple (its coefficient slot in the kernel's shared table)
 };
 static_assert(sizeof(YItemDev) == 24, "YItemDev layout");
 
 struct SnapDev {
   int J, nsp, K, idxu_max, idxz_max, u_half, ext_max, idxcg_max;
   int switch_flag, bzero_flag, bnorm_flag, n_yrows;
+  int n_ytrip, n_yca;  // row-blocked Y kernel: triples, doubles in yca
   double rcutfac, rmin0, rfac0, wself;
   double radii[IPG_MAX_SNAP_SPECIES], weight[IPG_MAX_SNAP_SPECIES];
   int idxu_block[SNAP_MAX_J + 2];
@@ -73,6 +74,7 @@ struct SnapDev {
   const YRowDev* yrows;
   const YItemDev* yitems;
   const double* yca;
+  const int32_t* ytrip_jjz;  // [n_ytrip] first Z entry of each triple
   const double* beta0;  // [1] energy offset of LBasisPotential (device, like ebias)
   const double* ebias;  // [nsp] -beta[s] . bzero (energy shift of bzero_flag), device memory so that
                         // a captured graph sees the beta of each replay
@@ -95,6 +97,7 @@ struct SnapHost {
   std::vector<YRowDev> yrows;
   std::vector<YItemDev> yitems;
   std::vector<double> yca;
+  std::vector<int32_t> ytrip_jjz;
 };
 
 int snap_build_tables(const ipg_snap_params& p, SnapHost& h);

@@ -255,13 +255,16 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
   h.yrows.clear();
   h.yitems.clear();
   h.yca.clear();
+  h.ytrip_jjz.clear();
   if (J <= YR_MAX_J) {
-    std::vector<int32_t> ca_of(jd * jd * jd, -1);
+    std::vector<int32_t> ca_of(jd * jd * jd, -1), trip_of(jd * jd * jd, -1);
     for (int j1 = 0; j1 <= J; j1++)
       for (int j2 = 0; j2 <= j1; j2++)
         for (int j = j1 - j2; j <= std::min(J, j1 + j2); j += 2) {
           const int d = (j1 + j2 - j) / 2, cg0 = h.idxcg_block[blk(j1, j2, j)];
           ca_of[blk(j1, j2, j)] = (int32_t)h.yca.size();
+          trip_of[blk(j1, j2, j)] = (int32_t)h.ytrip_jjz.size();
+          h.ytrip_jjz.push_back(h.idxz_block[blk(j1, j2, j)]);
           for (int m0 = 0; m0 <= j2; m0 += 2)  // column pairs (m0, m0 + 1), as [m0/2][ma][2]
             for (int ma = 0; ma <= j; ma++)
               for (int q = 0; q < 2; q++) {
@@ -304,7 +307,7 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
             it.ca = ca_of[blk(j1, j2, j)];
             it.cg = h.idxcg_block[blk(j1, j2, j)];
             it.jjz = h.idxz_block[blk(j1, j2, j)];
-            it.pad2 = 0;
+            it.trip = trip_of[blk(j1, j2, j)];
             row.items.push_back(it);
             row.cost += nb * (6.0 * nma * (j2 + 1) + (nma + 2 * j2 + 8));
           }
