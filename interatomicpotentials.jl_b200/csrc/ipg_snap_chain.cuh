@@ -353,46 +353,96 @@ __device__ __forceinline__ void save_mirror(const Chain<J>& s, double2* __restri
   }
 }
 
+// The row mb is a runtime value: the level code exists once and each chain enters it at its start level (a switch
+// that falls through the levels): the body of the kernel shrinks about (J/2+1)-fold, which
+// the instruction cache needs at twojmax 8.  The rootpq factors come from constant memory
+// by a uniform index; the recursion is written as FMA chains (rootpq scales a and its
+// derivatives once per term, so each term costs 36 FP64 instructions instead of 42).
 template <int J, int j>
-__device__ __forceinline__ void load_row(Chain<J>& s, const double2* __restrict__ save, int nt, int tid) {
+__device__ __forceinline__ void advance_rt(Chain<J>& s, const Geom& G, int mb) {
+  const int col = j - mb;
 #pragma unroll
-  for (int c = 0; c <= j; c++) {
+  for (int ma = j; ma >= 0; --ma) {
+    double2 nu = make_double2(0.0, 0.0);
+    double2 nd[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) nd[k] = make_double2(0.0, 0.0);
+    if (ma > 0) {  // - rootpq[ma][j-mb] conj(b) u[ma-1]
+      const double rp = -c_rpq[ma * RPQ_STRIDE + col];
+      const double2 bb = make_double2(rp * G.b.x, rp * G.b.y);
+      const double2 v = s.u[ma - 1];
+      nu.x = fma(bb.x, v.x, bb.y * v.y);
+      nu.y = fma(bb.x, v.y, -(bb.y * v.x));
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const double2 db = make_double2(rp * G.db[k].x, rp * G.db[k].y);
+        const double2 dv = s.d[k][ma - 1];
+        nd[k].x = fma(db.x, v.x, fma(db.y, v.y, fma(bb.x, dv.x, bb.y * dv.y)));
+        nd[k].y = fma(db.x, v.y, fma(-db.y, v.x, fma(bb.x, dv.y, -(bb.y * dv.x))));
+      }
+    }
+    if (ma < j) {  // + rootpq[j-ma][j-mb] conj(a) u[ma]
+      const double rp = c_rpq[(j - ma) * RPQ_STRIDE + col];
+      const double2 aa = make_double2(rp * G.a.x, rp * G.a.y);
+      const double2 v = s.u[ma];
+      nu.x = fma(aa.x, v.x, fma(aa.y, v.y, nu.x));
+      nu.y = fma(aa.x, v.y, fma(-aa.y, v.x, nu.y));
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const double2 da = make_double2(rp * G.da[k].x, rp * G.da[k].y);
+        const double2 dv = s.d[k][ma];
+        nd[k].x = fma(da.x, v.x, fma(da.y, v.y, fma(aa.x, dv.x, fma(aa.y, dv.y, nd[k].x))));
+        nd[k].y = fma(da.x, v.y, fma(-da.y, v.x, fma(aa.x, dv.y, fma(-aa.y, dv.x, nd[k].y))));
+      }
+    }
+    s.u[ma] = nu;
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][ma] = nd[k];
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void contract_rt(const Chain<J>& s, const double2* __restrict__ Yw, int64_t ys, int mb,
+                                            double& S0, double* S) {
+  const int last = (2 * mb == j) ? mb : j;  // middle row of an even level stops at ma = j/2
+  const double2* y0 = Yw + (int64_t)(half_block(j) + mb * (j + 1)) * ys;
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > last) break;
+    const double2 y = y0[ma * ys];
+    S0 = fma(s.u[ma].x, y.x, fma(s.u[ma].y, y.y, S0));
+#pragma unroll
+    for (int k = 0; k < 3; k++) S[k] = fma(s.d[k][ma].x, y.x, fma(s.d[k][ma].y, y.y, S[k]));
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level_rt(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, int64_t ys,
+                                         int mb, double& S0, double* S, double2* save, int nt, int tid) {
+  if constexpr (j <= J) {
+    advance_rt<J, j>(s, G, mb);
+    contract_rt<J, j>(s, Yw, ys, mb, S0, S);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2)
+      if (j == 2 * mb + 1) save_mirror<J, j>(s, save, nt, tid);  // start row of chain mb+1
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void load_row_rt(Chain<J>& s, const double2* __restrict__ save, int nt, int tid,
+                                            int count) {
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    if (c >= count) break;
     s.u[c] = save[(0 * (J + 1) + c) * nt + tid];
 #pragma unroll
     for (int k = 0; k < 3; k++) s.d[k][c] = save[((1 + k) * (J + 1) + c) * nt + tid];
   }
 }
 
-template <int J, int j, int MB>
-__device__ __forceinline__ void levels_save(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, int64_t ys,
-                                            double& S0, double* S, double2* save, int nt, int tid) {
-  if constexpr (j <= J) {
-    advance<J, j, MB>(s, G);
-    contract<J, j, MB>(s, Yw, ys, S0, S);
-    if constexpr (j == 2 * MB + 1 && MB + 1 <= J / 2) save_mirror<J, j>(s, save, nt, tid);
-    levels_save<J, j + 1, MB>(s, G, Yw, ys, S0, S, save, nt, tid);
-  }
-}
-
-template <int J, int MB>
-__device__ __forceinline__ void chains_from(Chain<J>& s, const Geom& G, const double2* __restrict__ Yw, int64_t ys,
-                                            double& S0, double* S, double2* save, int nt, int tid) {
-  if constexpr (MB <= J / 2) {
-    if constexpr (MB > 0) {
-      // keep the compiler from hoisting this chain's loads into the previous chain
-      asm volatile("" ::: "memory");
-      load_row<J, 2 * MB - 1>(s, save, nt, tid);  // row MB of level 2MB-1
-      advance<J, 2 * MB, MB>(s, G);
-      contract<J, 2 * MB, MB>(s, Yw, ys, S0, S);
-    }
-    levels_save<J, 2 * MB + 1, MB>(s, G, Yw, ys, S0, S, save, nt, tid);
-    chains_from<J, MB + 1>(s, G, Yw, ys, S0, S, save, nt, tid);
-  }
-}
-
 template <int J>
 __device__ __forceinline__ void all_chains_adjoint(const Geom& G, const double2* __restrict__ Yw, int64_t ys,
                                                    double& S0, double* S, double2* save, int nt, int tid) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
   Chain<J> s;
 #pragma unroll
   for (int c = 0; c <= J; c++) {
@@ -404,7 +454,23 @@ __device__ __forceinline__ void all_chains_adjoint(const Geom& G, const double2*
   S0 = 0.0;
   S[0] = S[1] = S[2] = 0.0;
   contract<J, 0, 0>(s, Yw, ys, S0, S);
-  chains_from<J, 0>(s, G, Yw, ys, S0, S, save, nt, tid);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+      asm volatile("" ::: "memory");  // this chain's loads stay after the previous chain's saves
+      load_row_rt<J>(s, save, nt, tid, 2 * mb);  // row mb of level 2mb-1
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {  // chain mb runs levels 2mb (1 for chain 0) .. J
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level_rt<J, JJ>(s, G, Yw, ys, mb, S0, S, save, nt, tid);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
 }
 
 }  // namespace snapchain
