@@ -338,7 +338,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "n_atoms": n, "n_pairs": npairs, "twojmax": prm["twojmax"],
                        "path": "adjoint", "l2": "flushed before every step (256 MiB write)",
-                       "autotuned": {k: tuned[k] for k in ("y_entries", "pair_split", "utot_warps", "walk_warps")},
+                       "autotuned": {k: tuned[k] for k in ("y_entries", "pair_split", "utot_split", "utot_warps", "walk_warps")},
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "gpu_launches": int(launches),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items() if v[1]}}

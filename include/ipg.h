@@ -240,8 +240,9 @@ IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int
 /* Autotuner: times the adjoint evaluation of this configuration under each candidate kernel
  * configuration and keeps the fastest for the handle.  Coordinate descent over the Y kernel
  * (row-blocked or one Z entry at a time: the twojmax-dependent shared-memory layout), the
- * per-neighbor kernel (all chains of a pair per thread, or one chain per thread), and the
- * atoms (warps) per block of the Utot and neighbor-walk kernels (1, 2, 4).  cache_path
+ * per-neighbor kernel (all chains of a pair per thread, or one chain per thread), the Utot
+ * kernel (all chains in one launch, or one launch per chain with 1, 2 or 4 atoms per block)
+ * and the atoms (warps) per block of the neighbor walk (1, 2, 4).  cache_path
  * (optional): a JSON-lines file keyed by device, twojmax, nspecies and the atom count
  * rounded up to a power of two; a hit applies the stored choice without timing, a miss
  * appends the result.  report (optional) receives the choice as one JSON object.        */

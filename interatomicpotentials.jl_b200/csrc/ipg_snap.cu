@@ -633,6 +633,60 @@ __global__ void __launch_bounds__(128) k_snap_utot(const __grid_constant__ SnapD
   }
 }
 
+// Utot of every atom in one launch: one warp per atom, lanes over neighbors (32 at a time),
+// every chain of a neighbor in its lane (snapchain::all_chains_utot); the sums over lanes go
+// through a per-warp staging buffer in shared memory, in fixed order.
+constexpr int UTA_WARPS = 4;
+template <int J>
+__global__ void __launch_bounds__(UTA_WARPS * 32) k_snap_utot_all(const __grid_constant__ SnapDev S, int64_t n,
+                                                                  const int64_t* __restrict__ off,
+                                                                  const int32_t* __restrict__ nbr,
+                                                                  const double* __restrict__ rij,
+                                                                  const int32_t* __restrict__ species,
+                                                                  double2* __restrict__ utot) {
+  __shared__ double2 buf[UTA_WARPS][snapchain::UT_SLOTS * 33];
+  __shared__ int dst[UTA_WARPS][snapchain::UT_SLOTS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t i = (int64_t)blockIdx.x * UTA_WARPS + w;
+  if (i >= n) return;  // warp-uniform; the kernel synchronises only within a warp
+  const int si = clamp_sp(species[i], S.nsp);
+  const int64_t beg = off[i], end = off[i + 1];
+  snapchain::UtStage st;
+  st.buf = buf[w];
+  st.dst = dst[w];
+  st.ut = reinterpret_cast<double*>(utot + (size_t)i * S.idxu_max);
+  st.lane = lane;
+  st.nslot = 0;
+  st.wself = S.wself;
+  for (int64_t p0 = beg; p0 < (end > beg ? end : beg + 1); p0 += 32) {
+    const int64_t p = p0 + lane;
+    double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);
+    double sw = 0.0;  // idle lanes contribute zero
+    if (p < end) {
+      const double x = rij[3 * p], y = rij[3 * p + 1], z = rij[3 * p + 2];
+      const int sj = clamp_sp(species[nbr[p]], S.nsp);
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;  // runtime_arrays.jl:50
+      const double r = sqrt(x * x + y * y + z * z);
+      const double theta0 = (r - S.rmin0) * S.rfac0 * M_PI / (rcut - S.rmin0);
+      const double z0 = r / tan(theta0);
+      const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+      a = make_double2(r0inv * z0, -r0inv * z);
+      b = make_double2(r0inv * y, -r0inv * x);
+      sw = sfac_of(S, r, rcut) * S.weight[sj];
+    }
+    st.first = p0 == beg;
+    snapchain::all_chains_utot<J>(a, b, sw, st);
+  }
+}
+
+template <int J>
+int launch_utot_all(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
+                    const double* rij, const int32_t* species, double2* utot) {
+  IPG_TIMED_LAUNCH(ctx, "snap_utot", k_snap_utot_all<J>, nblk(n, UTA_WARPS), UTA_WARPS * 32, 0, S, n, off, nbr, rij,
+                   species, utot);
+  return IPG_OK;
+}
+
 template <int J, int MB>
 int launch_utot_chains(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
                        const double* rij, const int32_t* species, double2* utot, int warps) {
@@ -644,11 +698,23 @@ int launch_utot_chains(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t*
   return IPG_OK;
 }
 
-// warps: atoms (warps) per block, 1..4.
+// warps: atoms (warps) per block, 1..4, of the per-chain kernels; all_chains: one launch of
+// k_snap_utot_all instead.
 int launch_utot(ipg_ctx* ctx, const SnapDev& S, int64_t n, const int64_t* off, const int32_t* nbr,
-                const double* rij, const int32_t* species, double2* utot, int warps = 4) {
+                const double* rij, const int32_t* species, double2* utot, int warps = 4, bool all_chains = true) {
   if (n == 0) return IPG_OK;
   warps = std::max(1, std::min(4, warps));
+  if (all_chains) {
+    switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_utot_all<JJ>(ctx, S, n, off, nbr, rij, species, utot);
+      IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
+#undef IPG_J
+      default:
+        return IPG_ERR_UNSUPPORTED;
+    }
+  }
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
@@ -1412,7 +1478,8 @@ struct ipg_snap {
   std::vector<int64_t> chunk_tab;  // per-configuration reduction chunks (host staging)
   bool pair_split = false;  // adjoint pair kernel: one thread per (pair, chain) instead of per pair
   bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
-  int utot_warps = 4;       // atoms (warps) per block of the Utot kernels
+  int utot_warps = 4;       // atoms (warps) per block of the per-chain Utot kernels
+  bool utot_split = false;  // Utot: one launch per chain (k_snap_utot) instead of k_snap_utot_all
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
@@ -1649,7 +1716,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   if (chains && n) {  // Utot from the register-chain kernel
     double2* utot;
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
-    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps));
+    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps, !s->utot_split));
     io.utot_in = utot;
   }
   int nch = 1;
@@ -1869,13 +1936,14 @@ void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const
 
 // ---- autotuner ------------------------------------------------------------------------
 struct TuneChoice {
-  int y_entries = 0, pair_split = 0, utot_warps = 4, walk_warps = 4;
+  int y_entries = 0, pair_split = 0, utot_split = 0, utot_warps = 4, walk_warps = 4;
   double ms = 0.0;
 };
 
 void tune_apply(ipg_snap* s, const TuneChoice& c) {
   s->y_entries = c.y_entries != 0;
   s->pair_split = c.pair_split != 0;
+  s->utot_split = c.utot_split != 0;
   s->utot_warps = c.utot_warps;
   s->walk_warps = c.walk_warps;
 }
@@ -1899,6 +1967,7 @@ bool tune_cache_lookup(const char* path, const std::string& key, TuneChoice& c) 
     if (line.find(want) == std::string::npos) continue;
     c.y_entries = json_int(line, "y_entries", 0);
     c.pair_split = json_int(line, "pair_split", 0);
+    c.utot_split = json_int(line, "utot_split", 0);
     c.utot_warps = std::max(1, std::min(4, json_int(line, "utot_warps", 4)));
     c.walk_warps = std::max(1, std::min(4, json_int(line, "walk_warps", 4)));
     hit = true;
@@ -1910,9 +1979,10 @@ bool tune_cache_lookup(const char* path, const std::string& key, TuneChoice& c) 
 std::string tune_json(const std::string& key, const TuneChoice& c, bool cached, int tried) {
   char buf[768];
   snprintf(buf, sizeof(buf),
-           "{\"key\": \"%s\", \"y_entries\": %d, \"pair_split\": %d, \"utot_warps\": %d, \"walk_warps\": %d, "
-           "\"ms\": %.4f, \"cached\": %d, \"tried\": %d}",
-           key.c_str(), c.y_entries, c.pair_split, c.utot_warps, c.walk_warps, c.ms, cached ? 1 : 0, tried);
+           "{\"key\": \"%s\", \"y_entries\": %d, \"pair_split\": %d, \"utot_split\": %d, \"utot_warps\": %d, "
+           "\"walk_warps\": %d, \"ms\": %.4f, \"cached\": %d, \"tried\": %d}",
+           key.c_str(), c.y_entries, c.pair_split, c.utot_split, c.utot_warps, c.walk_warps, c.ms, cached ? 1 : 0,
+           tried);
   return buf;
 }
 
@@ -1991,6 +2061,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_GENERIC_ADJOINT")) s->generic_adjoint = g[0] == '1';
   if (const char* g = getenv("IPG_PAIR_SPLIT")) s->pair_split = g[0] == '1';
   if (const char* g = getenv("IPG_Y_ENTRIES")) s->y_entries = g[0] == '1';
+  if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);
@@ -2141,7 +2212,7 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
   if (dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && n) {
     double2* utot;
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
-    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps));
+    IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps, !s->utot_split));
     io.utot_in = utot;
   }
   int threads = s->threads;
@@ -2267,6 +2338,7 @@ int ipg_snap_autotune(ipg_snap* s, int64_t n, const double* pos, const int32_t* 
   TuneChoice best;
   best.y_entries = s->y_entries;
   best.pair_split = s->pair_split;
+  best.utot_split = s->utot_split;
   best.utot_warps = s->utot_warps;
   best.walk_warps = s->walk_warps;
   bool cached = cache_path && cache_path[0] && tune_cache_lookup(cache_path, key, best);
@@ -2308,15 +2380,17 @@ int ipg_snap_autotune(ipg_snap* s, int64_t n, const double* pos, const int32_t* 
     int st = measure(best, &best.ms);
     // coordinate descent: each knob in turn, the others at their best so far
     const bool rows_ok = s->dev.J <= YR_MAX_J, chains_ok = s->dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
-    for (int knob = 0; knob < 4 && st == IPG_OK; knob++) {
+    for (int knob = 0; knob < 5 && st == IPG_OK; knob++) {
       std::vector<int> vals;
       if (knob == 0 && rows_ok) vals = {0, 1};
       if (knob == 1 && chains_ok) vals = {0, 1};
-      if (knob == 2 && chains_ok) vals = {1, 2, 4};
-      if (knob == 3) vals = {1, 2, 4};
+      if (knob == 2 && chains_ok) vals = {0, 1};
+      if (knob == 3 && chains_ok && best.utot_split) vals = {1, 2, 4};  // per-chain Utot kernels only
+      if (knob == 4) vals = {1, 2, 4};
       for (int v : vals) {
         TuneChoice c = best;
-        int* f = knob == 0 ? &c.y_entries : knob == 1 ? &c.pair_split : knob == 2 ? &c.utot_warps : &c.walk_warps;
+        int* f = knob == 0 ? &c.y_entries : knob == 1 ? &c.pair_split : knob == 2 ? &c.utot_split
+               : knob == 3 ? &c.utot_warps : &c.walk_warps;
         if (*f == v) continue;
         *f = v;
         st = measure(c, &c.ms);

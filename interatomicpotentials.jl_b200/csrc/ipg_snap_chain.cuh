@@ -474,3 +474,143 @@ __device__ __forceinline__ void all_chains_adjoint(const Geom& G, const double2*
 }
 
 }  // namespace snapchain
+
+namespace snapchain {
+
+// ---- Utot, all chains of a neighbor per lane, one launch ----------------------------------
+// advance_u with the row mb a runtime value (FMA chains; rootpq scales a and b per term).
+template <int J, int j>
+__device__ __forceinline__ void advance_u_rt(ChainU<J>& s, double2 a, double2 b, int mb) {
+  const int col = j - mb;
+#pragma unroll
+  for (int ma = j; ma >= 0; --ma) {
+    double2 nu = make_double2(0.0, 0.0);
+    if (ma > 0) {  // - rootpq[ma][j-mb] conj(b) u[ma-1]
+      const double rp = -c_rpq[ma * RPQ_STRIDE + col];
+      const double bx = rp * b.x, by = rp * b.y;
+      const double2 v = s.u[ma - 1];
+      nu.x = fma(bx, v.x, by * v.y);
+      nu.y = fma(bx, v.y, -(by * v.x));
+    }
+    if (ma < j) {  // + rootpq[j-ma][j-mb] conj(a) u[ma]
+      const double rp = c_rpq[(j - ma) * RPQ_STRIDE + col];
+      const double ax = rp * a.x, ay = rp * a.y;
+      const double2 v = s.u[ma];
+      nu.x = fma(ax, v.x, fma(ay, v.y, nu.x));
+      nu.y = fma(ax, v.y, fma(-ay, v.x, nu.y));
+    }
+    s.u[ma] = nu;
+  }
+}
+
+// Warp-wide sums of staged elements.  Each lane (one neighbor) stages sw * U of up to
+// UT_SLOTS elements in shared memory as buf[slot][lane] (33 columns: fewer bank conflicts);
+// a flush has lane pair (2q, 2q+1) sum the real and imaginary part of slot q over the 32
+// lanes in fixed order and write the Utot entry and its inversion-symmetric mirror.
+constexpr int UT_SLOTS = 16;
+struct UtStage {
+  double2* buf;  // [UT_SLOTS][33] of this warp
+  int* dst;      // [UT_SLOTS] packed destination of each slot
+  double* ut;    // this atom's Utot, as doubles
+  int lane, nslot;
+  bool first;    // first chunk of neighbors: write (with wself on the diagonal), else add
+  double wself;
+  // packed destination: entry e | mirror e' << 12 | mirror sign << 24 | diagonal << 25 | has mirror << 26
+  __device__ __forceinline__ void push(double2 v, int packed) {
+    buf[nslot * 33 + lane] = v;
+    if (lane == 0) dst[nslot] = packed;
+    if (++nslot == UT_SLOTS) flush();
+  }
+  __device__ __forceinline__ void flush() {
+    __syncwarp();
+    const int q = lane >> 1, c = lane & 1;
+    if (q < nslot) {
+      const double* col = reinterpret_cast<const double*>(buf + q * 33) + c;
+      double t = 0.0;
+#pragma unroll 8
+      for (int k = 0; k < 32; k++) t += col[2 * k];
+      const int pk = dst[q];
+      const int e = pk & 0xfff;
+      double v = first ? ((c == 0 && ((pk >> 25) & 1)) ? wself : 0.0) : ut[2 * e + c];
+      v += t;
+      ut[2 * e + c] = v;
+      if ((pk >> 26) & 1) {
+        const double sg = ((pk >> 24) & 1) ? -1.0 : 1.0;
+        ut[2 * ((pk >> 12) & 0xfff) + c] = c ? -sg * v : sg * v;
+      }
+    }
+    __syncwarp();
+    nslot = 0;
+  }
+};
+
+// Stages row mb of level j (the half-plane part) with its destinations in the full Utot.
+template <int J, int j>
+__device__ __forceinline__ void stage_row(const ChainU<J>& s, double sw, int mb, UtStage& st) {
+  const int last = (2 * mb == j) ? mb : j;  // middle row: entries beyond ma = mb are mirrors
+  const int ub = u_block(j);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > last) break;
+    const int e = ub + mb * (j + 1) + ma;
+    const bool self_mirror = (2 * mb == j) && ma == mb;
+    const int em = ub + (j - mb) * (j + 1) + (j - ma);
+    const int packed = e | (em << 12) | (((ma + mb) & 1) << 24) | ((ma == mb) << 25) | ((!self_mirror) << 26);
+    st.push(make_double2(sw * s.u[ma].x, sw * s.u[ma].y), packed);
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level_u_rt(ChainU<J>& s, double2 a, double2 b, double sw, int mb, UtStage& st,
+                                           double2 (&sv)[J + 1]) {
+  if constexpr (j <= J) {
+    advance_u_rt<J, j>(s, a, b, mb);
+    stage_row<J, j>(s, sw, mb, st);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2) {
+      if (j == 2 * mb + 1) {  // start row of chain mb+1: the mirror of this row
+        constexpr int R = (j + 1) / 2;
+#pragma unroll
+        for (int c = 0; c <= j; c++) {
+          const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+          sv[c] = make_double2(sg * s.u[j - c].x, -sg * s.u[j - c].y);
+        }
+      }
+    }
+  }
+}
+
+// All chains of one neighbor (sw = 0 on idle lanes), every half-plane entry computed once.
+template <int J>
+__device__ __forceinline__ void all_chains_utot(double2 a, double2 b, double sw, UtStage& st) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
+  ChainU<J> s;
+  double2 sv[J + 1];
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+    sv[c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);
+  stage_row<J, 0>(s, sw, 0, st);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+#pragma unroll
+      for (int c = 0; c <= J; c++)
+        if (c < 2 * mb) s.u[c] = sv[c];
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {  // chain mb runs levels 2mb (1 for chain 0) .. J
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level_u_rt<J, JJ>(s, a, b, sw, mb, st, sv);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
+  st.flush();
+}
+
+}  // namespace snapchain

@@ -265,7 +265,7 @@ def test_autotune_choice_and_cache(tmp_path):
     snap2, _ = make(prm, switch_flag=True)
     rep2 = snap2.autotune(system, beta, cache)
     assert rep2["cached"] == 1 and rep2["tried"] == 0
-    for k in ("y_entries", "pair_split", "utot_warps", "walk_warps"):
+    for k in ("y_entries", "pair_split", "utot_split", "utot_warps", "walk_warps"):
         assert rep2[k] == rep[k]
     E2, F2, _ = snap2.energy_forces(system, beta)
     assert abs(E2 - E0) <= 1e-12 * abs(E0) and rel_err(F2, F0) <= 1e-12
