@@ -1127,6 +1127,7 @@ __global__ void __launch_bounds__(128) k_snap_pair_adj(const __grid_constant__ S
 // Adjoint per-neighbor kernel, all chains of a pair in one thread (saved start rows in
 // shared memory): part[p][0][3] = dE_i/dr_ij.
 constexpr int PAIR_ALL_T = 128;
+constexpr int PAIR_Y_ATOMS = 8;  // atoms whose Y a block of the all-chains kernel stages
 template <int J>
 __global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_constant__ SnapDev S,
                                                                   const int64_t* __restrict__ d_np,
@@ -1135,10 +1136,25 @@ __global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_c
                                                                   const double* __restrict__ rij,
                                                                   const int32_t* __restrict__ species,
                                                                   const double2* __restrict__ Yw,
-                                                                  double* __restrict__ part) {
-  extern __shared__ double2 save[];  // [4 (J+1)][PAIR_ALL_T]
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= *d_np) return;  // np: the live count (capacity mode sizes the grid larger)
+                                                                  double* __restrict__ part, int ystage) {
+  extern __shared__ double2 save[];  // [4 (J+1)][PAIR_ALL_T], then the staged Y [u_half][PAIR_Y_ATOMS]
+  const int64_t np = *d_np;  // the live count (capacity mode sizes the grid larger)
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
+  if (p0 >= np) return;  // block-uniform
+  // The block's pairs are sorted by owner: stage the weighted Y of their few atoms in shared
+  // memory (every Y entry is read once per neighbor), unless they span too many atoms.
+  const int first = owner[p0];
+  const int nat = owner[(p0 + blockDim.x - 1 < np ? p0 + blockDim.x : np) - 1] - first + 1;
+  const bool staged = nat <= ystage;  // ystage: 0 (no staging room) or PAIR_Y_ATOMS
+  double2* ysm = save + 4 * (J + 1) * PAIR_ALL_T;
+  if (staged) {
+    for (int idx = threadIdx.x; idx < S.u_half * nat; idx += blockDim.x) {
+      const int h = idx / nat, a = idx - h * nat;
+      ysm[h * PAIR_Y_ATOMS + a] = Yw[(size_t)h * natoms + first + a];
+    }
+  }
+  __syncthreads();
+  if (p >= np) return;
   const int i = owner[p];
   const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
   const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
@@ -1155,7 +1171,10 @@ __global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_c
     G.dsu[k] = PG.dsfac * PG.u[k];
   }
   double S0, Sk[3];
-  snapchain::all_chains_adjoint<J>(G, Yw + i, natoms, S0, Sk, save, PAIR_ALL_T, threadIdx.x);
+  if (staged)
+    snapchain::all_chains_adjoint<J>(G, ysm + (i - first), PAIR_Y_ATOMS, S0, Sk, save, PAIR_ALL_T, threadIdx.x);
+  else
+    snapchain::all_chains_adjoint<J>(G, Yw + i, natoms, S0, Sk, save, PAIR_ALL_T, threadIdx.x);
   double* out = part + (size_t)p * 3;
 #pragma unroll
   for (int k = 0; k < 3; k++) out[k] = 2.0 * (G.dsu[k] * S0 + G.sfac * Sk[k]);
@@ -1164,11 +1183,15 @@ __global__ void __launch_bounds__(PAIR_ALL_T) k_snap_pair_adj_all(const __grid_c
 template <int J>
 int launch_pair_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms, const int32_t* owner,
                     const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
-  const size_t sm = (size_t)4 * (J + 1) * PAIR_ALL_T * sizeof(double2);
+  // stage Y only while two blocks (the register limit) still fit an SM's shared memory
+  const size_t base = (size_t)4 * (J + 1) * PAIR_ALL_T * sizeof(double2);
+  const size_t with_y = base + (size_t)S.u_half * PAIR_Y_ATOMS * sizeof(double2);
+  const int ystage = with_y <= 113 * 1024 ? PAIR_Y_ATOMS : 0;
+  const size_t sm = ystage ? with_y : base;
   if (sm > 48 * 1024)
     CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_pair_adj_all<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   IPG_TIMED_LAUNCH(ctx, "snap_pair", k_snap_pair_adj_all<J>, nblk(np, PAIR_ALL_T), PAIR_ALL_T, sm, S, d_np, natoms,
-                   owner, nbr, rij, species, Yw, part);
+                   owner, nbr, rij, species, Yw, part, ystage);
   return IPG_OK;
 }
 
