@@ -189,6 +189,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="size of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and pair-workload lines")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-tune", action="store_true", help="skip the (untimed) autotuner and use the default kernel "
+                    "configuration, e.g. so that a profiler's launch list holds only the measured steps")
     ap.add_argument("--cells", type=int, default=30, help="BCC cells per axis (30 -> 54,000 atoms); smaller "
                     "values give the small cases used for profiling")
     args = ap.parse_args()
@@ -230,7 +232,9 @@ def main():
     sp_host = snap.species_ids(system)
     beta_b = snap.beta_blocks(beta)
     npairs = len(ipg.neighborlist_snap(system, snap, ctx=ctx)._j)
-    tuned = snap.autotune(system, beta_b)  # untimed: picks the kernel configuration for this workload
+    # untimed: picks the kernel configuration for this workload
+    tuned = {"y_entries": 0, "pair_split": 0, "utot_split": 0, "utot_warps": 4, "walk_warps": 4} if args.no_tune \
+        else snap.autotune(system, beta_b)
 
     pos_d = torch.tensor(system.positions, device=dev)
     sp_d = torch.tensor(sp_host, device=dev)
