@@ -44,13 +44,14 @@ WORKLOAD = ("snap_j8: SNAP twojmax=8 (55 components), 2 species (weights 1.0/0.5
 
 
 # timing name -> kernel
-KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot<8,MB>",
+KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot_all<8>",
                 "snap_pair": "k_snap_pair_adj_all<8>"}
-# DRAM bytes (read + write) per atom of one launch, from the ncu --set full capture on the
-# 16,000-atom case summarised in profiles/k_snap_yrows_snap_j8.md and
-# profiles/k_snap_pair_adj_all_snap_j8.md; scaled by atoms (pairs per atom are the same).
-NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.927552e6 + 4.160512e6) / 16000,
-                           "snap_pair": (50.504448e6 + 0.944640e6) / 16000}
+# DRAM bytes (read + write) per atom of one launch, from the ncu --set full captures on the
+# 16,000-atom case summarised in profiles/k_snap_{yrows,pair_adj_all,utot_all}_snap_j8.md;
+# scaled by atoms (pairs per atom are the same).
+NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.983104e6 + 2.750464e6) / 16000,
+                           "snap_pair": (52.742912e6 + 0.972800e6) / 16000,
+                           "snap_utot": (11.587584e6 + 17.270272e6) / 16000}
 
 
 def _hbm_peak():
