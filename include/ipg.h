@@ -249,6 +249,19 @@ IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int
 IPG_API int ipg_snap_autotune(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
                       const double* beta, const char* cache_path, char* report, int32_t report_len);
 
+/* Fitting matrices of many configurations (the linear system A beta = b that
+ * PotentialLearning solves; the row layout of get_snap, LAMMPS_SNAP/bispectrum.jl:279-387,
+ * with one column per species block and component, col = s*K + k):
+ *   Ae [nconfig][K*nspecies]     energy rows: sum of B_i over the atoms of species s
+ *                                (E_c = Ae[c] . beta + beta0)
+ *   Af [3 n_total][K*nspecies]   force rows: row 3a + x is dB_a[x][:] (F_a,x = Af[3a+x] . beta)
+ *   Aw [nconfig][6][K*nspecies]  virial rows (W of compute_all_descriptors, snap.jl:267-281)
+ * Atoms as in ipg_snap_batch_energy_forces; any of Ae, Af, Aw may be NULL.  The per-pair
+ * dB/dr of the whole batch is materialised on the device (K*3 doubles per directed pair). */
+IPG_API int ipg_snap_batch_descriptors(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets,
+                                       const double* pos, const int32_t* species, const double* L, double* Ae,
+                                       double* Af, double* Aw);
+
 /* ---- batched SNAP ------------------------------------------------------------------------
  * Many configurations at once: atoms of configuration c are atom_offsets[c] ..
  * atom_offsets[c+1]-1 of the flattened arrays; L is [nconfig][3].  Per-configuration

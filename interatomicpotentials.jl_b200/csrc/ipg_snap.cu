@@ -1363,7 +1363,7 @@ __global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ conf_chunk,
 __global__ void k_snap_dB_atoms(int64_t n, int K, int nsp, const int64_t* __restrict__ off,
                                 const int64_t* __restrict__ in_off, const int64_t* __restrict__ in_pair,
                                 const int32_t* __restrict__ owner, const int32_t* __restrict__ species,
-                                const double* __restrict__ dbl, double* __restrict__ dB) {
+                                const double* __restrict__ dbl, double* __restrict__ dB, int rows) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int64_t k = t / (3 * K);
   int bc = (int)(t - k * 3 * K);
@@ -1386,7 +1386,52 @@ __global__ void k_snap_dB_atoms(int64_t n, int K, int nsp, const int64_t* __rest
       if (s == so) acc[s] -= v;
   }
   const int b = bc / 3, c = bc - 3 * b;
-  for (int s = 0; s < nsp; s++) dB[((size_t)k * K * nsp + (size_t)s * K + b) * 3 + c] = acc[s];
+  if (rows)  // fitting layout: row 3k + c, column s*K + b
+    for (int s = 0; s < nsp; s++) dB[((size_t)k * 3 + c) * K * nsp + (size_t)s * K + b] = acc[s];
+  else
+    for (int s = 0; s < nsp; s++) dB[((size_t)k * K * nsp + (size_t)s * K + b) * 3 + c] = acc[s];
+}
+
+// Fitting rows of each configuration (one block per configuration, threads over columns):
+// Ae[c][s*K + k] = sum of B_i[k] over the atoms i of c with species s, and
+// Aw[c][v][s*K + k] = W of the configuration's atoms (the k_snap_W_desc sum, snap.jl:267-281).
+__global__ void k_snap_fit_rows(int nconf, const int64_t* __restrict__ conf_off, int K, int nsp,
+                                const int32_t* __restrict__ species, const double* __restrict__ B,
+                                const int64_t* __restrict__ off, const int32_t* __restrict__ nbr,
+                                const double* __restrict__ pos, const double* __restrict__ dbl,
+                                double* __restrict__ Ae, double* __restrict__ Aw) {
+  const int c = blockIdx.x;
+  if (c >= nconf) return;
+  const int64_t a0 = conf_off[c], a1 = conf_off[c + 1];
+  const int KN = K * nsp;
+  for (int col = threadIdx.x; col < KN; col += blockDim.x) {
+    const int sp = col / K, b = col - sp * K;
+    if (Ae) {
+      double e = 0.0;
+      for (int64_t i = a0; i < a1; i++)
+        if (clamp_sp(species[i], nsp) == sp) e += B[(size_t)i * K + b];
+      Ae[(size_t)c * KN + col] = e;
+    }
+    if (Aw) {
+      double w[6] = {0, 0, 0, 0, 0, 0};
+      for (int64_t i = a0; i < a1; i++) {
+        if (clamp_sp(species[i], nsp) != sp) continue;
+        const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+        for (int64_t p = off[i]; p < off[i + 1]; p++) {
+          const double* d = dbl + ((size_t)p * K + b) * 3;
+          const int64_t jn = nbr[p];
+          const double dx = xi - pos[3 * jn], dy = yi - pos[3 * jn + 1], dz = zi - pos[3 * jn + 2];
+          w[0] += d[0] * dx;
+          w[1] += d[1] * dy;
+          w[2] += d[2] * dz;
+          w[3] += d[1] * dz;
+          w[4] += d[0] * dz;
+          w[5] += d[0] * dy;
+        }
+      }
+      for (int v = 0; v < 6; v++) Aw[((size_t)c * 6 + v) * KN + col] = w[v];
+    }
+  }
 }
 
 __global__ void k_pair_owner(int64_t n, const int64_t* __restrict__ off, int32_t* __restrict__ owner) {
@@ -1705,8 +1750,11 @@ struct EvalOut {
   double* F = nullptr;   // [3n] device
   double* W6 = nullptr;  // [nconf][6] device
   double* B = nullptr;   // [n][K] device
-  double* dB = nullptr;  // [n][K*nsp][3] device
+  double* dB = nullptr;  // [n][K*nsp][3] device ([3n][K*nsp] with dB_rows)
   double* Wd = nullptr;  // [K*nsp][6] device
+  bool dB_rows = false;
+  double* Ae = nullptr;  // [nconf][K*nsp] fitting energy rows (device)
+  double* Aw = nullptr;  // [nconf][6][K*nsp] fitting virial rows (device)
 };
 
 // Energy / forces / descriptors for device inputs.  mode: MODE_DESC (B/E only), MODE_ADJ,
@@ -1734,7 +1782,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   io.Ei = Ei;
   io.B = out.B;
   io.status = ctx->d_status;
-  const bool need_plain = (mode == MODE_PLAIN) || out.dB || out.Wd;
+  const bool need_plain = (mode == MODE_PLAIN) || out.dB || out.Wd || out.Aw;
   const bool chains = dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
   if (chains && n) {  // Utot from the register-chain kernel
     double2* utot;
@@ -1832,7 +1880,15 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
     IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
     IPG_LAUNCH(ctx, k_snap_dB_atoms, nblk(n * 3 * K, 128), 128, 0, n, K, nsp, pl.d_off, pl.d_in_off, pl.d_in_pair,
-               owner, d_species, dbl, out.dB);
+               owner, d_species, dbl, out.dB, out.dB_rows ? 1 : 0);
+  }
+  if ((out.Ae || out.Aw) && n) {
+    int64_t* d_coff;
+    IPG_RET(scratch(ctx, "snap_fit_off", (size_t)nconf + 1, &d_coff));
+    CUDA_RET(ctx, cudaMemcpyAsync(d_coff, h_atom_off, sizeof(int64_t) * (nconf + 1), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    IPG_LAUNCH(ctx, k_snap_fit_rows, (unsigned)nconf, 128, 0, nconf, d_coff, K, nsp, d_species, out.B, pl.d_off,
+               pl.d_j, d_pos, dbl, out.Ae, out.Aw);
   }
   if (out.Wd) {
     const int width = nsp * K * 6;
@@ -2152,6 +2208,47 @@ int ipg_snap_descriptors(ipg_snap* s, int64_t n, const double* pos, const int32_
     else memset(W, 0, sizeof(double) * K * nsp * 6);
   }
   return ipg_status_check(ctx, "ipg_snap_descriptors");
+}
+
+int ipg_snap_batch_descriptors(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
+                               const int32_t* species, const double* L, double* Ae, double* Af, double* Aw) {
+  if (!s || nconfig < 1 || !atom_offsets || !L) return s ? ipg_fail(s->ctx, IPG_ERR_ARG, "bad batch args") : IPG_ERR_ARG;
+  ipg_ctx* ctx = s->ctx;
+  if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
+  for (int c = 0; c < nconfig; c++)
+    if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
+  const int64_t n = atom_offsets[nconfig];
+  IPG_RET(check_common(s, n, pos, species, L));
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  IPG_RET(check_host_inputs(s, n, pos, species));
+  double* d_pos;
+  int32_t* d_sp;
+  IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
+  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  const size_t KN = (size_t)K * nsp;
+  double *B_d, *Ae_d = nullptr, *Af_d = nullptr, *Aw_d = nullptr;
+  IPG_RET(scratch(ctx, "fit_B", (size_t)n * K + 1, &B_d));
+  if (Ae) IPG_RET(scratch(ctx, "fit_Ae", (size_t)nconfig * KN, &Ae_d));
+  if (Af) IPG_RET(scratch(ctx, "fit_Af", 3 * (size_t)n * KN + 1, &Af_d));
+  if (Aw) IPG_RET(scratch(ctx, "fit_Aw", 6 * (size_t)nconfig * KN, &Aw_d));
+  IPG_RET(ipg_status_reset(ctx));
+  EvalOut o;
+  o.B = B_d;
+  o.dB = Af_d;
+  o.dB_rows = true;
+  o.Ae = Ae_d;
+  o.Aw = Aw_d;
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, nconfig, atom_offsets, L, nullptr, 0.0, MODE_DESC, o));
+  if (Ae) {
+    if (n) CUDA_RET(ctx, cudaMemcpyAsync(Ae, Ae_d, sizeof(double) * nconfig * KN, cudaMemcpyDeviceToHost, ctx->stream));
+    else memset(Ae, 0, sizeof(double) * nconfig * KN);
+  }
+  if (Af && n) CUDA_RET(ctx, cudaMemcpyAsync(Af, Af_d, sizeof(double) * 3 * n * KN, cudaMemcpyDeviceToHost, ctx->stream));
+  if (Aw) {
+    if (n) CUDA_RET(ctx, cudaMemcpyAsync(Aw, Aw_d, sizeof(double) * 6 * nconfig * KN, cudaMemcpyDeviceToHost, ctx->stream));
+    else memset(Aw, 0, sizeof(double) * 6 * nconfig * KN);
+  }
+  return ipg_status_check(ctx, "ipg_snap_batch_descriptors");
 }
 
 int ipg_snap_energy_forces_dev(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species,

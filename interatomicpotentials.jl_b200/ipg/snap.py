@@ -204,6 +204,19 @@ class SNAP:
                                                           _vp(beta), float(beta0), m, _vp(E), _vp(F), _vp(W)))
         return E, F, W
 
+    def fitting_matrices(self, systems):
+        """The fitting system of many configurations (include/ipg.h: ipg_snap_batch_descriptors):
+        energy rows Ae (nconf, K*nsp), force rows Af (3 n_total, K*nsp), virial rows Aw
+        (nconf, 6, K*nsp); column s*K + k belongs to species block s."""
+        off, pos, sp, L = self._flatten(systems)
+        nc, KN = len(systems), self.K * len(self.species)
+        Ae = np.zeros((nc, KN))
+        Af = np.zeros((3 * int(off[-1]), KN))
+        Aw = np.zeros((nc, 6, KN))
+        self.ctx.check(lib().ipg_snap_batch_descriptors(self._h, nc, _vp(off), _vp(pos), _vp(sp), _vp(L), _vp(Ae),
+                                                        _vp(Af), _vp(Aw)))
+        return Ae, Af, Aw
+
     def batch_loss_grad(self, systems, beta, F_ref, beta0=0.0):
         """L = sum |F - F_ref|^2 over the batch and dL/dbeta (nsp, K)."""
         off, pos, sp, L = self._flatten(systems)

@@ -146,3 +146,24 @@ def test_graph_open_boundaries_run_eagerly():
         E, F, _ = db.evaluate(beta, 0.0, graph=True)
         torch.cuda.synchronize()
         assert np.array_equal(F.cpu().numpy(), F0)
+
+
+def test_fitting_matrices(batch):
+    """ipg_snap_batch_descriptors: energy, force and virial rows of every configuration equal
+    the single-configuration descriptors and reproduce E, F and W of the batched evaluation."""
+    systems, snap, orc, beta = batch
+    sub = systems[:6]
+    Ae, Af, Aw = snap.fitting_matrices(sub)
+    K, nsp = len(snap), len(snap.species)
+    off = np.concatenate([[0], np.cumsum([len(s) for s in sub])])
+    for c, s in enumerate(sub):
+        B, dB, Wd = ipg.compute_all_descriptors(s, snap)  # B (n, K), dB (n, 3, K*nsp), W (6, K*nsp)
+        sp = snap.species_ids(s)
+        ae = np.concatenate([B[sp == q].sum(axis=0) for q in range(nsp)])
+        assert rel_err(Ae[c], ae) <= 1e-13
+        assert rel_err(Af[3 * off[c]:3 * off[c + 1]], dB.reshape(-1, K * nsp)) <= 1e-13
+        assert rel_err(Aw[c], Wd) <= 1e-13
+    E, F, Wv = snap.batch_energy_forces(sub, beta, 0.25, mode="plain")
+    b = beta.reshape(-1)
+    assert rel_err(Ae @ b + 0.25, E) <= 1e-12
+    assert rel_err(Af @ b, F.reshape(-1)) <= 1e-12
