@@ -349,6 +349,13 @@ def main():
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items() if v[1]}}
 
     if not args.no_extras:
+        # MD loops: the neighbor list reused under a 0.3 A Verlet skin (positions unchanged here,
+        # so every timed step takes the reuse path: re-measure + filter instead of the cell walk)
+        snap.set_skin(0.3)
+        ms_skin, _, kts = timed(lambda: step(SNAP_ADJOINT), args.steps, kernel_timing=True)
+        snap.set_skin(0.0)
+        line["adjoint_value_skin_reuse"] = world * n * args.steps / (ms_skin * 1e-3)
+        line["skin_kernel_ms_per_step"] = {k: v[0] / args.steps for k, v in kts.items() if v[1]}
         ms_plain, _, ktp = timed(lambda: step(SNAP_PLAIN), max(2, args.steps // 2), kernel_timing=True)
         plain_value = world * n * max(2, args.steps // 2) / (ms_plain * 1e-3)
         line["plain_value"] = plain_value

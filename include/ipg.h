@@ -249,6 +249,17 @@ IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int
 IPG_API int ipg_snap_autotune(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
                       const double* beta, const char* cache_path, char* report, int32_t report_len);
 
+/* Neighbor-list reuse across calls, for MD loops (the Verlet skin that nnlist.jl:1 leaves to
+ * a future neighbor package): with skin > 0 the full SNAP list is built with every cutoff
+ * enlarged by `skin` and kept in the handle; later calls with the same atom count,
+ * configuration offsets and boxes take their pairs from it (re-measured at the current
+ * positions with the same inclusion test as a fresh build) until some atom has moved more
+ * than skin/2 since the build, which rebuilds it.  Results equal those of a fresh build up
+ * to the order of summation.  skin = 0 (the default) builds every call; graph replays and
+ * the literal search radius always build.  ipg_snap_skin_stats counts builds and reuses.  */
+IPG_API int ipg_snap_set_skin(ipg_snap* snap, double skin);
+IPG_API int ipg_snap_skin_stats(const ipg_snap* snap, int64_t* builds, int64_t* reuses);
+
 /* Fitting matrices of many configurations (the linear system A beta = b that
  * PotentialLearning solves; the row layout of get_snap, LAMMPS_SNAP/bispectrum.jl:279-387,
  * with one column per species block and component, col = s*K + k):

@@ -191,6 +191,13 @@ struct PairList {
 // cap > 0 selects capacity mode (no host read-back, so the build can be captured in a CUDA
 // graph): buffers hold cap pairs; a larger count sets IPG_ERR_CAPACITY in the status word
 // and every atom's list is cut at cap, so later kernels stay in bounds.
+// Verlet-skin reuse: pl = the pairs of `cached` (a full list built with enlarged cutoffs over
+// the cell list cl) that pass the true full-list test at d_pos, with their transpose.
+int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const PairList& cached,
+                     const double* d_pos, const int32_t* d_species, int nsp, const double* h_cut, int mode,
+                     PairList& pl);
+// Largest squared minimum-image displacement of d_pos from d_ref (host value, synchronises).
+int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const double* d_ref, double* out);
 // walk_warps: atoms (warps) per block of the neighbor walk, 1..4.
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
                     const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true,

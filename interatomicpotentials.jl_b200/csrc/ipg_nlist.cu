@@ -203,6 +203,74 @@ __global__ void __launch_bounds__(128) k_pair_walk(int64_t n, PairTest t, const 
   if (!EMIT && lane == 0) cnt[i] = k;
 }
 
+// Verlet-skin reuse: the pairs of a list built with enlarged cutoffs that satisfy the true
+// test (pair_ok, the same arithmetic as a fresh build) at the current positions.  One warp
+// per atom, lanes over its cached candidates, emission in the cached order.
+template <bool EMIT>
+__global__ void __launch_bounds__(128) k_filter_walk(int64_t n, PairTest t, const ConfGrid* __restrict__ grid,
+                                                     const int32_t* __restrict__ conf,
+                                                     const int64_t* __restrict__ coff,
+                                                     const int32_t* __restrict__ cj, const double* __restrict__ pos,
+                                                     const int32_t* __restrict__ species, int nsp,
+                                                     int64_t* __restrict__ cnt, const int64_t* __restrict__ off,
+                                                     int32_t* __restrict__ outj, double* __restrict__ outr) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n) return;  // warp-uniform
+  const int si = species ? (species[i] < 0 ? 0 : (species[i] >= nsp ? nsp - 1 : species[i])) : 0;
+  const double4 xi = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], (double)si);
+  const double* L = grid[conf[i]].L;
+  int64_t k = 0;
+  const int64_t base = EMIT ? off[i] : 0;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int64_t q0 = coff[i]; q0 < coff[i + 1]; q0 += 32) {
+    const int64_t q = q0 + lane;
+    double rr[3];
+    bool ok = false;
+    int32_t j = 0;
+    if (q < coff[i + 1]) {
+      j = cj[q];
+      const int sj = species ? (species[j] < 0 ? 0 : (species[j] >= nsp ? nsp - 1 : species[j])) : 0;
+      ok = pair_ok(t, L, (int32_t)i, xi, j, make_double4(pos[3 * j], pos[3 * j + 1], pos[3 * j + 2], (double)sj), rr);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (EMIT && ok) {
+      const int64_t o = base + k + __popc(bal & lt);
+      outj[o] = j;
+      outr[3 * o] = rr[0];
+      outr[3 * o + 1] = rr[1];
+      outr[3 * o + 2] = rr[2];
+    }
+    k += __popc(bal);
+  }
+  if (!EMIT && lane == 0) cnt[i] = k;
+}
+
+// Largest squared minimum-image displacement since the reference positions, as the bit
+// pattern of a non-negative double (ordered like the integers).
+__global__ void k_max_disp2(int64_t n, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ conf,
+                            const double* __restrict__ pos, const double* __restrict__ ref,
+                            unsigned long long* __restrict__ out) {
+  __shared__ unsigned long long sm[256];
+  double m = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* L = grid[conf[i]].L;
+    double d2 = 0.0;
+    for (int a = 0; a < 3; a++) {
+      const double s = pe_axis_dev(L[a], pos[3 * i + a], ref[3 * i + a]);
+      d2 += s * s;
+    }
+    m = fmax(m, d2);
+  }
+  sm[threadIdx.x] = (unsigned long long)__double_as_longlong(m);
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sm[threadIdx.x] = sm[threadIdx.x] > sm[threadIdx.x + o] ? sm[threadIdx.x] : sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicMax(out, sm[0]);
+}
+
 // Capacity mode: a total above cap is an error (status), and every offset is cut at cap
 // so that all later kernels stay inside the buffers.
 // (Offsets are non-decreasing, so cutting each one at cap on its own is the same as
@@ -433,6 +501,70 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
       IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
       IPG_LAUNCH(ctx, k_in_sort, nblk(n, 128), 128, 0, n, pl.d_in_off, pl.d_in_pair);
     }
+  }
+  return IPG_OK;
+}
+
+int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const double* d_ref, double* out) {
+  *out = 0.0;
+  if (cl.n == 0) return IPG_OK;
+  unsigned long long* d_m;
+  IPG_RET(scratch(ctx, "skin_maxdisp", 1, &d_m));
+  CUDA_RET(ctx, cudaMemsetAsync(d_m, 0, sizeof(unsigned long long), ctx->stream));
+  const int64_t grid = std::min<int64_t>(nblk(cl.n, 256), 4 * ctx->num_sms);
+  IPG_LAUNCH(ctx, k_max_disp2, (unsigned)grid, 256, 0, cl.n, cl.d_grid, cl.d_conf, d_pos, d_ref, d_m);
+  unsigned long long h = 0;
+  CUDA_RET(ctx, cudaMemcpyAsync(&h, d_m, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  memcpy(out, &h, sizeof(double));
+  return IPG_OK;
+}
+
+int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const PairList& cached,
+                     const double* d_pos, const int32_t* d_species, int nsp, const double* h_cut, int mode,
+                     PairList& pl) {
+  std::string pre(prefix);
+  PairTest t;
+  memset(&t, 0, sizeof(t));
+  t.mode = IPG_NLIST_FULL;
+  t.literal = (mode & IPG_NLIST_LITERAL_SQRT) ? 1 : 0;
+  t.nsp = nsp;
+  double cutmax2 = 0.0;
+  for (int q = 0; q < nsp * nsp; q++) {
+    t.cutsq[q] = h_cut[q];
+    cutmax2 = std::max(cutmax2, h_cut[q]);
+  }
+  const double cutmax = std::sqrt(cutmax2);
+  t.rcut = t.literal ? std::sqrt(cutmax) : cutmax;
+  t.rcut2_lo = t.rcut * t.rcut * (1.0 - 1e-12);
+  t.rcut2_hi = t.rcut * t.rcut * (1.0 + 1e-12);
+  const int64_t n = cl.n;
+  pl.n = n;
+  IPG_RET(scratch(ctx, (pre + "off").c_str(), n + 1, &pl.d_off));
+  CUDA_RET(ctx, cudaMemsetAsync(pl.d_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+  if (n > 0)
+    IPG_LAUNCH(ctx, k_filter_walk<false>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cached.d_off,
+               cached.d_j, d_pos, d_species, nsp, pl.d_off, nullptr, nullptr, nullptr);
+  IPG_RET(ipg_scan_i64(ctx, pl.d_off, pl.d_off, n + 1));
+  pl.d_np = pl.d_off + n;
+  CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
+  IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
+  if (n > 0)
+    IPG_LAUNCH(ctx, k_filter_walk<true>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cached.d_off,
+               cached.d_j, d_pos, d_species, nsp, nullptr, pl.d_off, pl.d_j, pl.d_r);
+  int64_t* fill;
+  IPG_RET(scratch(ctx, (pre + "in_off").c_str(), n + 1, &pl.d_in_off));
+  IPG_RET(scratch(ctx, (pre + "in_fill").c_str(), n + 1, &fill));
+  IPG_RET(scratch(ctx, (pre + "in_pair").c_str(), pl.npairs + 1, &pl.d_in_pair));
+  CUDA_RET(ctx, cudaMemsetAsync(pl.d_in_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+  CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+  if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off);
+  IPG_RET(ipg_scan_i64(ctx, pl.d_in_off, pl.d_in_off, n + 1));
+  if (pl.npairs > 0) {
+    IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
+    IPG_LAUNCH(ctx, k_in_sort, nblk(n, 128), 128, 0, n, pl.d_in_off, pl.d_in_pair);
   }
   return IPG_OK;
 }

@@ -1573,6 +1573,19 @@ struct ipg_snap {
   };
   std::vector<Graph> graphs;
   int64_t graph_replays = 0;
+  // Verlet-skin reuse of the neighbor list (ipg_snap_set_skin)
+  double skin = 0.0;
+  struct SkinCache {
+    bool valid = false;
+    int64_t n = 0;
+    int nconf = 0;
+    std::vector<int64_t> off;
+    std::vector<double> L;
+    CellList cl;      // buffers under the "skin_" prefix
+    PairList pairs;   // the list with enlarged cutoffs
+    double* ref = nullptr;  // positions at the build
+  } sk;
+  int64_t skin_builds = 0, skin_reuses = 0;
 };
 
 namespace {
@@ -1735,6 +1748,46 @@ int snap_neighbors(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d
 
 int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
                          const int64_t* h_atom_off, const double* h_L, PairList& pl, int64_t cap) {
+  const int mode_sk = IPG_NLIST_FULL | (s->p.literal_sqrt_radius ? IPG_NLIST_LITERAL_SQRT : 0);
+  if (s->skin > 0.0 && cap == 0 && !s->ctx->capturing && n > 0 && !s->p.literal_sqrt_radius) {
+    // Verlet skin: reuse the list built with cutoffs + skin while no atom has moved more
+    // than skin/2 since that build (then every pair now within a cutoff is in it)
+    ipg_snap::SkinCache& C = s->sk;
+    bool valid = C.valid && C.n == n && C.nconf == nconf &&
+                 memcmp(C.off.data(), h_atom_off, sizeof(int64_t) * (nconf + 1)) == 0 &&
+                 memcmp(C.L.data(), h_L, sizeof(double) * 3 * nconf) == 0;
+    if (valid) {
+      double d2;
+      IPG_RET(ipg_max_disp2(s->ctx, C.cl, d_pos, C.ref, &d2));
+      valid = d2 <= 0.25 * s->skin * s->skin;
+    }
+    if (!valid) {
+      const int nsp = s->p.nspecies;
+      std::vector<double> cut2(nsp * nsp);
+      for (int q = 0; q < nsp * nsp; q++) {
+        const double r = std::sqrt(s->cutsq[q]) + s->skin;
+        cut2[q] = r * r;
+      }
+      IPG_RET(ipg_build_cells(s->ctx, "skin_", n, d_pos, d_species, nsp, nconf, h_atom_off, h_L,
+                              s->radius + s->skin, C.cl));
+      IPG_RET(ipg_build_pairs(s->ctx, "skin_", C.cl, d_species, nsp, cut2.data(), IPG_NLIST_FULL, false, C.pairs,
+                              false, 0, s->walk_warps));
+      IPG_RET(scratch(s->ctx, "skin_ref", 3 * (size_t)n, &C.ref));
+      CUDA_RET(s->ctx, cudaMemcpyAsync(C.ref, d_pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice,
+                                       s->ctx->stream));
+      C.valid = true;
+      C.n = n;
+      C.nconf = nconf;
+      C.off.assign(h_atom_off, h_atom_off + nconf + 1);
+      C.L.assign(h_L, h_L + 3 * nconf);
+      s->skin_builds++;
+    } else {
+      s->skin_reuses++;
+    }
+    s->last_grid = C.cl.h_grid;
+    return ipg_filter_pairs(s->ctx, "snap_", C.cl, C.pairs, d_pos, d_species, s->p.nspecies, s->cutsq.data(),
+                            mode_sk, pl);
+  }
   CellList cl;
   IPG_RET(ipg_build_cells(s->ctx, "snap_", n, d_pos, d_species, s->p.nspecies, nconf, h_atom_off, h_L, s->radius,
                           cl));
@@ -2208,6 +2261,21 @@ int ipg_snap_descriptors(ipg_snap* s, int64_t n, const double* pos, const int32_
     else memset(W, 0, sizeof(double) * K * nsp * 6);
   }
   return ipg_status_check(ctx, "ipg_snap_descriptors");
+}
+
+int ipg_snap_set_skin(ipg_snap* s, double skin) {
+  if (!s) return IPG_ERR_ARG;
+  if (!(skin >= 0.0) || !std::isfinite(skin)) return ipg_fail(s->ctx, IPG_ERR_ARG, "skin must be finite and >= 0");
+  s->skin = skin;
+  s->sk.valid = false;
+  return IPG_OK;
+}
+
+int ipg_snap_skin_stats(const ipg_snap* s, int64_t* builds, int64_t* reuses) {
+  if (!s) return IPG_ERR_ARG;
+  if (builds) *builds = s->skin_builds;
+  if (reuses) *reuses = s->skin_reuses;
+  return IPG_OK;
 }
 
 int ipg_snap_batch_descriptors(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* pos,

@@ -32,7 +32,8 @@ API_SYMBOLS = (
     "ipg_launch_count", "ipg_timing_enable", "ipg_timing_read", "ipg_neighbor_build", "ipg_neighbor_count", "ipg_nlist_size", "ipg_nlist_export", "ipg_nlist_free",
     "ipg_pair_eval", "ipg_pair_eval_dev", "ipg_pair_eval_noalloc", "ipg_snap_create", "ipg_snap_destroy", "ipg_snap_ncoeff",
     "ipg_snap_descriptors", "ipg_snap_energy_forces", "ipg_snap_energy_forces_dev", "ipg_snap_vjp_beta",
-    "ipg_snap_vjp", "ipg_snap_autotune", "ipg_snap_batch_descriptors", "ipg_snap_batch_energy_forces", "ipg_snap_batch_energy_forces_dev", "ipg_snap_batch_loss_grad",
+    "ipg_snap_vjp", "ipg_snap_autotune", "ipg_snap_batch_descriptors", "ipg_snap_set_skin", "ipg_snap_skin_stats",
+    "ipg_snap_batch_energy_forces", "ipg_snap_batch_energy_forces_dev", "ipg_snap_batch_loss_grad",
 )
 
 
@@ -95,6 +96,8 @@ def lib():
         "ipg_snap_vjp": (C.c_int, [vp, i64, vp, vp, vp, vp, d, vp, vp, vp, vp]),
         "ipg_snap_autotune": (C.c_int, [vp, i64, vp, vp, vp, vp, C.c_char_p, C.c_char_p, i32]),
         "ipg_snap_batch_descriptors": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, vp, vp]),
+        "ipg_snap_set_skin": (C.c_int, [vp, d]),
+        "ipg_snap_skin_stats": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64)]),
         "ipg_snap_batch_energy_forces": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, i32, vp, vp, vp]),
         "ipg_snap_batch_energy_forces_dev": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, i32, i32, vp, vp, vp]),
         "ipg_snap_batch_loss_grad": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, vp, vp, vp]),

@@ -204,6 +204,17 @@ class SNAP:
                                                           _vp(beta), float(beta0), m, _vp(E), _vp(F), _vp(W)))
         return E, F, W
 
+    def set_skin(self, skin):
+        """Reuse the neighbor list across calls while atoms move less than skin/2
+        (include/ipg.h: ipg_snap_set_skin); 0 builds every call."""
+        self.ctx.check(lib().ipg_snap_set_skin(self._h, float(skin)))
+
+    def skin_stats(self):
+        """(list builds, list reuses) since the handle was created."""
+        b, r = C.c_int64(), C.c_int64()
+        self.ctx.check(lib().ipg_snap_skin_stats(self._h, C.byref(b), C.byref(r)))
+        return b.value, r.value
+
     def fitting_matrices(self, systems):
         """The fitting system of many configurations (include/ipg.h: ipg_snap_batch_descriptors):
         energy rows Ae (nconf, K*nsp), force rows Af (3 n_total, K*nsp), virial rows Aw

@@ -269,3 +269,28 @@ def test_autotune_choice_and_cache(tmp_path):
         assert rep2[k] == rep[k]
     E2, F2, _ = snap2.energy_forces(system, beta)
     assert abs(E2 - E0) <= 1e-12 * abs(E0) and rel_err(F2, F0) <= 1e-12
+
+
+def test_verlet_skin_reuse():
+    """An MD-like sequence of small moves: with a skin the list is reused (and rebuilt after
+    a large move), and every step equals a fresh evaluation to rounding."""
+    system, prm, beta = W.snap_j8(cells=6)
+    fresh, orc = make(prm, switch_flag=True)
+    md, _ = make(prm, switch_flag=True)
+    md.set_skin(0.4)
+    rng = np.random.default_rng(21)
+    pos = system.positions.copy()
+    for step in range(6):
+        pos = pos + rng.normal(0, 0.02, pos.shape)  # well inside skin/2 per step at first
+        if step == 4:
+            pos = pos + rng.normal(0, 0.3, pos.shape)  # some atom moves more than skin/2
+        s = ipg.System(pos, system.symbols, system.box, system.periodic)
+        E0, F0, W0 = fresh.energy_forces(s, beta)
+        E1, F1, W1 = md.energy_forces(s, beta)
+        assert abs(E1 - E0) <= 1e-12 * abs(E0)
+        assert rel_err(F1, F0) <= 1e-12 and rel_err(W1, W0) <= 1e-12
+    builds, reuses = md.skin_stats()
+    assert builds >= 2 and reuses >= 3 and builds + reuses == 6
+    # the skin list also serves the plain path and the descriptors
+    E2, F2, _ = md.energy_forces(s, beta, mode="plain")
+    assert rel_err(F2, F0) <= 1e-12
