@@ -516,19 +516,24 @@ struct UtStage {
   bool first;    // first chunk of neighbors: write (with wself on the diagonal), else add
   double wself;
   // packed destination: entry e | mirror e' << 12 | mirror sign << 24 | diagonal << 25 | has mirror << 26
+  // stages one element; the caller makes room first (room(), once per row)
   __device__ __forceinline__ void push(double2 v, int packed) {
     buf[nslot * 33 + lane] = v;
     if (lane == 0) dst[nslot] = packed;
-    if (++nslot == UT_SLOTS) flush();
+    ++nslot;
+  }
+  __device__ __forceinline__ void room(int need) {
+    if (nslot + need > UT_SLOTS) flush();
   }
   __device__ __forceinline__ void flush() {
     __syncwarp();
     const int q = lane >> 1, c = lane & 1;
     if (q < nslot) {
       const double* col = reinterpret_cast<const double*>(buf + q * 33) + c;
-      double t = 0.0;
-#pragma unroll 8
-      for (int k = 0; k < 32; k++) t += col[2 * k];
+      double t4[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a shorter dependency chain
+#pragma unroll
+      for (int k = 0; k < 32; k++) t4[k & 3] += col[2 * k];
+      const double t = (t4[0] + t4[1]) + (t4[2] + t4[3]);
       const int pk = dst[q];
       const int e = pk & 0xfff;
       double v = first ? ((c == 0 && ((pk >> 25) & 1)) ? wself : 0.0) : ut[2 * e + c];
@@ -547,8 +552,10 @@ struct UtStage {
 // Stages row mb of level j (the half-plane part) with its destinations in the full Utot.
 template <int J, int j>
 __device__ __forceinline__ void stage_row(const ChainU<J>& s, double sw, int mb, UtStage& st) {
+  static_assert(j + 1 <= UT_SLOTS, "a row must fit the staging buffer");
   const int last = (2 * mb == j) ? mb : j;  // middle row: entries beyond ma = mb are mirrors
   const int ub = u_block(j);
+  st.room(last + 1);
 #pragma unroll
   for (int ma = 0; ma <= j; ma++) {
     if (ma > last) break;
