@@ -114,7 +114,7 @@ __device__ __forceinline__ void dev_raise(int* status, int code) { atomicCAS(sta
 // Minimum-image arithmetic of the reference, reproduced bit for bit (no FMA contraction).
 // Julia mod(x, y) for y > 0 finite (the sign of the result follows y).
 __device__ __forceinline__ double jl_mod_dev(double x, double L) {
-  double r = (x >= 0.0 && x < L) ? x : fmod(x, L);
+  double r = (fabs(x) < L) ? x : fmod(x, L);  // fmod(x, L) == x exactly when |x| < L
   if (r == 0.0) return 0.0;
   if (r < 0.0) r = __dadd_rn(r, L);
   return r;
@@ -207,9 +207,9 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
 __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {
   int cnt = 0;
   for (int d = -1; d <= 1; d++) {
-    int k = c + d;
+    int k = c + d;  // c is in 0..nc-1, so one wrap suffices
     if (per) {
-      k = (k % nc + nc) % nc;
+      k = k < 0 ? k + nc : (k >= nc ? k - nc : k);
     } else if (k < 0 || k >= nc) {
       continue;
     }
