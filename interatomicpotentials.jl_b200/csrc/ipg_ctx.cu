@@ -1,6 +1,8 @@
 // ipg_ctx.cu — context lifetime, error reporting, device scratch, status word, scan.
 #include <cstdarg>
 
+#include <cstdlib>
+
 #include "ipg_internal.cuh"
 
 int ipg_fail(ipg_ctx* ctx, int code, const char* fmt, ...) {
@@ -205,6 +207,7 @@ int ipg_create(int device, ipg_ctx** out) {
   ipg_ctx* ctx = new ipg_ctx();
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
+  if (const char* e = getenv("IPG_WALK_BY_ATOM")) ctx->walk_by_cell = e[0] != '1';
   int dev0 = 0;
   cudaGetDevice(&dev0);
   if (cudaSetDevice(device) != cudaSuccess ||

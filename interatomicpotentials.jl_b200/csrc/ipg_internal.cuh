@@ -48,6 +48,7 @@ struct ipg_ctx {
   // differs refers to freed buffers and is discarded.
   bool capturing = false;
   uint64_t scratch_gen = 0;
+  bool walk_by_cell = true;  // neighbor walk: one warp per cell (false: one warp per atom)
 };
 
 // Records a start/stop event pair around a launch when timing is enabled.

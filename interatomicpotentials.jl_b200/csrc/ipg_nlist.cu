@@ -284,6 +284,85 @@ __global__ void k_clamp_offsets(int64_t n, int64_t* __restrict__ off, int64_t ca
   }
 }
 
+// The same walk with one warp per cell: every atom of a cell has the same stencil, so each
+// chunk of 32 candidates is loaded once and tested against every atom of the cell (their
+// positions, ids and output cursors staged in shared memory, read as broadcasts).  Each
+// atom's hits come out in the same order as from k_pair_walk.
+constexpr int WALKC_WARPS = 4;
+struct WalkAtom {
+  double4 x;
+  int64_t base, end, k;
+  int32_t i, pad;
+};
+template <bool EMIT>
+__global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
+    int64_t ncells, PairTest t, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ conf,
+    const int64_t* __restrict__ cell_start, const int32_t* __restrict__ cell_atoms, const double4* __restrict__ spos,
+    int64_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ outj,
+    double* __restrict__ outr) {
+  __shared__ WalkAtom sa[WALKC_WARPS][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t c = (int64_t)blockIdx.x * WALKC_WARPS + w;
+  if (c >= ncells) return;  // warp-uniform; the kernel synchronises only within a warp
+  const int64_t s0 = cell_start[c], s1 = cell_start[c + 1];
+  if (s0 == s1) return;
+  const ConfGrid g = grid[conf[cell_atoms[s0]]];
+  int cc[3];
+  {
+    const double4 x0 = spos[s0];
+    cell_coords(g, x0.x, x0.y, x0.z, cc);
+  }
+  StencilRanges R;
+  stencil_ranges(g, cc, cell_start, R);
+  const unsigned lt = (1u << lane) - 1u;
+  WalkAtom* A = sa[w];
+  for (int64_t g0 = s0; g0 < s1; g0 += 32) {
+    const int G = (int)((s1 - g0) < 32 ? (s1 - g0) : 32);
+    __syncwarp();
+    if (lane < G) {
+      const int32_t i = cell_atoms[g0 + lane];
+      A[lane].i = i;
+      A[lane].x = spos[g0 + lane];
+      A[lane].k = 0;
+      if (EMIT) {
+        A[lane].base = off[i];
+        A[lane].end = off[i + 1];
+      }
+    }
+    __syncwarp();
+    for (int r = 0; r < R.n; r++)
+      for (int64_t q0 = R.beg[r]; q0 < R.end[r]; q0 += 32) {
+        const int64_t q = q0 + lane;
+        const bool inq = q < R.end[r];
+        int32_t j = 0;
+        double4 xj = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (inq) {
+          j = cell_atoms[q];
+          xj = spos[q];
+        }
+        for (int ii = 0; ii < G; ii++) {
+          const int32_t i = A[ii].i;
+          double rr[3];
+          const bool ok = inq && pair_ok(t, g.L, i, A[ii].x, j, xj, rr);
+          const unsigned bal = __ballot_sync(0xffffffffu, ok);
+          if (EMIT && ok) {
+            const int64_t o = A[ii].base + A[ii].k + __popc(bal & lt);
+            if (o < A[ii].end) {  // a list cut at the capacity (capacity mode) drops its tail
+              outj[o] = j;
+              outr[3 * o] = rr[0];
+              outr[3 * o + 1] = rr[1];
+              outr[3 * o + 2] = rr[2];
+            }
+          }
+          __syncwarp();
+          if (lane == 0) A[ii].k += __popc(bal);
+          __syncwarp();
+        }
+      }
+    if (!EMIT && lane < G) cnt[A[lane].i] = A[lane].k;
+  }
+}
+
 // Sorts each atom's list by neighbor index (insertion sort; lists are short).
 __global__ void k_pair_sort(int64_t n, const int64_t* __restrict__ off, int32_t* __restrict__ j,
                             double* __restrict__ r) {
@@ -467,9 +546,15 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   IPG_RET(scratch(ctx, (pre + "off").c_str(), n + 1, &pl.d_off));
   cnt = pl.d_off;
   CUDA_RET(ctx, cudaMemsetAsync(cnt, 0, sizeof(int64_t) * (n + 1), ctx->stream));
-  if (n > 0)
-    IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
-               cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
+  const bool by_cell = ctx->walk_by_cell;
+  if (n > 0) {
+    if (by_cell)
+      IPG_LAUNCH(ctx, k_pair_walk_cells<false>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
+                 cl.d_grid, cl.d_conf, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
+    else
+      IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+                 cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
+  }
   IPG_RET(ipg_scan_i64(ctx, cnt, pl.d_off, n + 1));
   pl.d_np = pl.d_off + n;
   if (cap > 0) {  // capacity mode: no read-back
@@ -484,8 +569,13 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0) {
-    IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
-               cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
+    if (by_cell)
+      IPG_LAUNCH(ctx, k_pair_walk_cells<true>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
+                 cl.d_grid, cl.d_conf, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j,
+                 pl.d_r);
+    else
+      IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
+                 cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
     if (sorted) IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
   }
   if (want_transpose) {
