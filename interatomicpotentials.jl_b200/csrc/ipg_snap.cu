@@ -966,7 +966,7 @@ __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const i
 // Tile ma0 .. ma0+NT-1 of target row (j, mb): every triple and row pair of the row.
 // Writes Y' = w Y of the tile's entries below nma and returns their Re(conj(U) Y').
 template <int NT>
-__device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, int ma0, int nma,
+__device__ __forceinline__ double yr_tile(const SnapDev& S, const YConst& T, const YRowDev& row, int ma0, int nma,
                                           const double2* __restrict__ usl, const double* __restrict__ yc,
                                           const double2* __restrict__ cas, int64_t n, int64_t atom, bool valid,
                                           double2* __restrict__ yout) {
@@ -976,14 +976,13 @@ __device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, 
   const int j = row.j, rs = j + 1;
   const double bn = S.bnorm_flag ? 1.0 / (j + 1) : 1.0;
   for (int t = row.t0; t < row.t1; t++) {
-    const YItemDev it = S.yitems[t];
+    const YItemDev it = T.items[t];
     const double c = yc[it.trip] * bn;
-    const double* __restrict__ cg = S.cglist + it.cg;
     const double2* __restrict__ cp = cas + it.ca / 2;
-    const int j1 = it.j1, j2 = it.j2, d = it.d, s2 = j2 + 1;
+    const int j1 = it.j1, j2 = it.j2, d = it.d;
     for (int ib = 0; ib < it.nb; ib++) {
       const int mb1 = it.mb1min + ib, mb2 = it.mb2max - ib;
-      const double cb = c * __ldg(cg + mb1 * s2 + mb2);
+      const double cb = c * T.cb[it.cg + ib];  // cg[mb1][mb2] of this row pair
       if (2 * mb1 > j1)
         yr_pair<NT, true>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, acc);
       else
@@ -1008,9 +1007,10 @@ __device__ __forceinline__ double yr_tile(const SnapDev& S, const YRowDev& row, 
 // Tiles of a row of nma entries: at most YR_TILE wide, as even as possible.
 constexpr int YR_TILE = 6;
 
-__device__ __forceinline__ double yr_row(const SnapDev& S, const YRowDev& row, const double2* __restrict__ usl,
-                                         const double* __restrict__ yc, const double2* __restrict__ cas, int64_t n,
-                                         int64_t atom, bool valid, double2* __restrict__ yout) {
+__device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, const YRowDev& row,
+                                         const double2* __restrict__ usl, const double* __restrict__ yc,
+                                         const double2* __restrict__ cas, int64_t n, int64_t atom, bool valid,
+                                         double2* __restrict__ yout) {
   const int nma = row.mid ? row.mb + 1 : row.j + 1;
   const int ntile = (nma + YR_TILE - 1) / YR_TILE;
   double e = 0.0;
@@ -1020,7 +1020,7 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YRowDev& row, c
     switch (w) {
 #define IPG_NT(NT) \
   case NT:         \
-    e += yr_tile<NT>(S, row, ma0, nma, usl, yc, cas, n, atom, valid, yout); \
+    e += yr_tile<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout); \
     break;
       IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
 #undef IPG_NT
@@ -1032,7 +1032,7 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YRowDev& row, c
   return e;
 }
 
-__global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_constant__ SnapDev S, int64_t n,
+__global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_constant__ SnapDev S, const __grid_constant__ YConst T, int64_t n,
                                                                  const int32_t* __restrict__ species,
                                                                  const double2* __restrict__ utot,
                                                                  double2* __restrict__ yout, double* __restrict__ Ei) {
@@ -1076,14 +1076,14 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
       int r = 0;
       if (lane == 0) r = atomicAdd(&next_row, 1);
       r = __shfl_sync(0xffffffffu, r, 0);
-      if (r >= S.n_yrows) break;
-      const YRowDev row = S.yrows[r];
-      erow[r * YS_ATOMS + lane] = yr_row(S, row, usl, yc, cas, n, atom, valid, yout);
+      if (r >= T.nrows) break;
+      const YRowDev row = T.rows[r];
+      erow[r * YS_ATOMS + lane] = yr_row(S, T, row, usl, yc, cas, n, atom, valid, yout);
     }
     __syncthreads();
     if (warp == 0 && valid) {
       double t = 0.0;
-      for (int r = 0; r < S.n_yrows; r++) t += erow[r * YS_ATOMS + lane];
+      for (int r = 0; r < T.nrows; r++) t += erow[r * YS_ATOMS + lane];
       Ei[atom] = (2.0 / 3.0) * t + S.ebias[si];
     }
     __syncthreads();
@@ -1857,7 +1857,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
       size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
-        const bool rows = dev.J <= YR_MAX_J && !s->y_entries;
+        const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
         const void* kfn = rows ? (const void*)k_snap_yrows : (const void*)k_snap_yatoms;
         if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
         CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
@@ -1866,8 +1866,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
         const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
         const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
         if (rows)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
-                           io.utot_in, yout, Ei);
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
+                           d_species, io.utot_in, yout, Ei);
         else
           IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
                            io.utot_in, yout, Ei);
@@ -2567,7 +2567,7 @@ int ipg_snap_autotune(ipg_snap* s, int64_t n, const double* pos, const int32_t* 
     };
     int st = measure(best, &best.ms);
     // coordinate descent: each knob in turn, the others at their best so far
-    const bool rows_ok = s->dev.J <= YR_MAX_J, chains_ok = s->dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
+    const bool rows_ok = s->dev.J <= YR_MAX_J && s->h.yconst_ok, chains_ok = s->dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
     for (int knob = 0; knob < 5 && st == IPG_OK; knob++) {
       std::vector<int> vals;
       if (knob == 0 && rows_ok) vals = {0, 1};

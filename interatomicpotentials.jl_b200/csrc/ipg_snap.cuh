@@ -46,6 +46,16 @@ struct YItemDev {
 };
 static_assert(sizeof(YItemDev) == 24, "YItemDev layout");
 
+// The row-blocked Y kernel's warp-uniform tables, passed by value as a kernel parameter
+// (constant bank: uniform reads through the constant cache, private to each launch).
+constexpr int YC_ROWS = 28, YC_ITEMS = 400, YC_RP = 1536;
+struct YConst {
+  YRowDev rows[YC_ROWS];    // target rows, longest first
+  YItemDev items[YC_ITEMS]; // their triples (field cg: offset of the first row factor in cb)
+  double cb[YC_RP];         // cg[mb1][mb2] of every row pair of every item
+  int nrows, nitems, nrp, pad;
+};
+
 struct SnapDev {
   int J, nsp, K, idxu_max, idxz_max, u_half, ext_max, idxcg_max;
   int switch_flag, bzero_flag, bnorm_flag, n_yrows;
@@ -98,6 +108,8 @@ struct SnapHost {
   std::vector<YItemDev> yitems;
   std::vector<double> yca;
   std::vector<int32_t> ytrip_jjz;
+  bool yconst_ok = false;  // the tables fit YConst
+  YConst yconst;
 };
 
 int snap_build_tables(const ipg_snap_params& p, SnapHost& h);

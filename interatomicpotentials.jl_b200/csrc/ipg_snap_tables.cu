@@ -8,6 +8,7 @@
 // are new and serve the CUDA kernels.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "ipg_snap.cuh"
 
@@ -322,6 +323,27 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
       h.yitems.insert(h.yitems.end(), rows[q].items.begin(), rows[q].items.end());
       r.t1 = (int32_t)h.yitems.size();
       h.yrows.push_back(r);
+    }
+    // the constant-bank copy: item.cg becomes the offset of its first row factor in cb
+    memset(&h.yconst, 0, sizeof(h.yconst));
+    int nrp = 0;
+    for (const YItemDev& it : h.yitems) nrp += it.nb;
+    h.yconst_ok = (int)h.yrows.size() <= YC_ROWS && (int)h.yitems.size() <= YC_ITEMS && nrp <= YC_RP;
+    if (h.yconst_ok) {
+      YConst& C = h.yconst;
+      C.nrows = (int)h.yrows.size();
+      C.nitems = (int)h.yitems.size();
+      for (int q = 0; q < C.nrows; q++) C.rows[q] = h.yrows[q];
+      int o = 0;
+      for (int t = 0; t < C.nitems; t++) {
+        YItemDev it = h.yitems[t];
+        const int cg0 = it.cg;
+        it.cg = o;
+        for (int ib = 0; ib < it.nb; ib++)
+          C.cb[o++] = h.cglist[cg0 + (it.mb1min + ib) * (it.j2 + 1) + (it.mb2max - ib)];
+        C.items[t] = it;
+      }
+      C.nrp = o;
     }
   }
   return IPG_OK;
