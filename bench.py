@@ -356,6 +356,23 @@ def main():
         snap.set_skin(0.0)
         line["adjoint_value_skin_reuse"] = world * n * args.steps / (ms_skin * 1e-3)
         line["skin_kernel_ms_per_step"] = {k: v[0] / args.steps for k, v in kts.items() if v[1]}
+        # Batched: 512 configurations (32..2000 atoms, crystals and liquids, ~0.54 M atoms) in one
+        # evaluation, eager and as a CUDA-graph replay (ipg_snap_batch_energy_forces_dev), and one
+        # force-matching training step (loss and dL/dbeta, host buffers)
+        systems_b = W.batch512()
+        nb_atoms = sum(len(x) for x in systems_b)
+        db = ipg.DeviceBatch(snap, systems_b)
+        ms_be, _, _ = timed(lambda: db.evaluate(beta_b, 0.0, graph=False), max(2, args.steps // 5))
+        db.evaluate(beta_b, 0.0, graph=True)  # capture (untimed)
+        ms_bg, _, _ = timed(lambda: db.evaluate(beta_b, 0.0, graph=True), max(2, args.steps // 5))
+        Fref_b = np.asarray(db.F.cpu().numpy()) * 1.01
+        ms_bl, _, _ = timed(lambda: snap.batch_loss_grad(systems_b, beta_b, Fref_b), 2)
+        ctx.set_stream(stream.cuda_stream)
+        line["batch512"] = {"n_configs": len(systems_b), "n_atoms": nb_atoms,
+                            "eager_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_be * 1e-3),
+                            "graph_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_bg * 1e-3),
+                            "loss_grad_ms": ms_bl / 2}
+        del db
         ms_plain, _, ktp = timed(lambda: step(SNAP_PLAIN), max(2, args.steps // 2), kernel_timing=True)
         plain_value = world * n * max(2, args.steps // 2) / (ms_plain * 1e-3)
         line["plain_value"] = plain_value
