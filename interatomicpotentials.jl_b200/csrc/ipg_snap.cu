@@ -19,6 +19,7 @@
 #include <algorithm>
 
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 
 #include "ipg_snap.cuh"
@@ -1032,6 +1033,62 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, cons
   return e;
 }
 
+// Z output variant (k_snap_yrows<true>): every item's Z tile goes to zout[jjz][atom]
+// (entries of the half plane; the middle row of an even level up to ma = mb), nothing is
+// summed across items.  Z carries the 1/(j+1) of bnorm_flag (compute_z.jl:49-56).
+template <int NT>
+__device__ __forceinline__ void yr_tile_z(const SnapDev& S, const YConst& T, const YRowDev& row, int ma0, int nma,
+                                          const double2* __restrict__ usl, const double2* __restrict__ cas, int64_t n,
+                                          int64_t atom, bool valid, double2* __restrict__ zout) {
+  const int j = row.j, rs = j + 1;
+  const double bn = S.bnorm_flag ? 1.0 / (j + 1) : 1.0;
+  for (int t = row.t0; t < row.t1; t++) {
+    const YItemDev it = T.items[t];
+    double2 acc[NT];
+#pragma unroll
+    for (int i = 0; i < NT; i++) acc[i] = make_double2(0.0, 0.0);
+    const double2* __restrict__ cp = cas + it.ca / 2;
+    const int j1 = it.j1, j2 = it.j2, d = it.d;
+    for (int ib = 0; ib < it.nb; ib++) {
+      const int mb1 = it.mb1min + ib, mb2 = it.mb2max - ib;
+      const double cb = bn * T.cb[it.cg + ib];
+      if (2 * mb1 > j1)
+        yr_pair<NT, true>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, acc);
+      else
+        yr_pair<NT, false>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, acc);
+    }
+    if (valid) {
+      const int64_t z0 = it.jjz + row.mb * (j + 1) + ma0;
+#pragma unroll
+      for (int i = 0; i < NT; i++)
+        if (ma0 + i < nma) zout[(size_t)(z0 + i) * n + atom] = acc[i];
+    }
+  }
+}
+
+__device__ __forceinline__ void yr_row_z(const SnapDev& S, const YConst& T, const YRowDev& row,
+                                         const double2* __restrict__ usl, const double2* __restrict__ cas, int64_t n,
+                                         int64_t atom, bool valid, double2* __restrict__ zout) {
+  const int nma = row.mid ? row.mb + 1 : row.j + 1;
+  const int ntile = (nma + YR_TILE - 1) / YR_TILE;
+  int ma0 = 0;
+  for (int k = 0; k < ntile; k++) {
+    const int w = (nma - ma0 + (ntile - k) - 1) / (ntile - k);
+    switch (w) {
+#define IPG_NT(NT) \
+  case NT:         \
+    yr_tile_z<NT>(S, T, row, ma0, nma, usl, cas, n, atom, valid, zout); \
+    break;
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
+#undef IPG_NT
+      default:
+        break;
+    }
+    ma0 += w;
+  }
+}
+
+template <bool ZOUT>
 __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_constant__ SnapDev S, const __grid_constant__ YConst T, int64_t n,
                                                                  const int32_t* __restrict__ species,
                                                                  const double2* __restrict__ utot,
@@ -1078,16 +1135,201 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
       r = __shfl_sync(0xffffffffu, r, 0);
       if (r >= T.nrows) break;
       const YRowDev row = T.rows[r];
-      erow[r * YS_ATOMS + lane] = yr_row(S, T, row, usl, yc, cas, n, atom, valid, yout);
+      if (ZOUT)
+        yr_row_z(S, T, row, usl, cas, n, atom, valid, yout);  // yout: Z [idxz_max][n]
+      else
+        erow[r * YS_ATOMS + lane] = yr_row(S, T, row, usl, yc, cas, n, atom, valid, yout);
     }
     __syncthreads();
-    if (warp == 0 && valid) {
+    if (!ZOUT && warp == 0 && valid) {
       double t = 0.0;
       for (int r = 0; r < T.nrows; r++) t += erow[r * YS_ATOMS + lane];
       Ei[atom] = (2.0 / 3.0) * t + S.ebias[si];
     }
     __syncthreads();
   }
+}
+
+// ---- beta pullback from the register chains (twojmax <= YR_MAX_J) -------------------------
+// The cotangent g of the forces pulls back to
+//   gbeta[s][b] = sum over atoms i of species s of
+//                 2 sum_t fac_t sum_half w Re(conj(V_i) Z_i(t)) + gE B_i[b],
+//   V_i = sum over neighbors j of (g_i - g_j) . dU_ij/dr_ij      (half plane of every level),
+// the terms t, levels and factors of each component being those of dB/dr (compute_b.jl:
+// 207-400).  V comes from k_snap_vsum (every chain of a neighbor per lane), Z from
+// k_snap_yrows<true>, and k_snap_gbeta contracts them with the atoms in lanes.
+
+// V of atoms a0 .. a0+nc-1 as V[h][nc]: one warp per atom, lanes over neighbors (32 at a
+// time), v_h = A u_h + sum_k B_k du_k,h with A = dsfac gv.uhat, B_k = sfac gv_k, gv = g_i - g_j;
+// the sums over lanes go through the staging buffer in fixed order.
+constexpr int VS_WARPS = 4;
+template <int J>
+__global__ void __launch_bounds__(VS_WARPS * 32) k_snap_vsum(const __grid_constant__ SnapDev S, int64_t a0, int64_t nc,
+                                                             const int64_t* __restrict__ off,
+                                                             const int32_t* __restrict__ nbr,
+                                                             const double* __restrict__ rij,
+                                                             const int32_t* __restrict__ species,
+                                                             const double* __restrict__ g, double2* __restrict__ V) {
+  extern __shared__ double2 vsh[];  // saved start rows [4 (J+1)][VS_WARPS 32], then [VS_WARPS][UT_SLOTS 33]
+  __shared__ int dst[VS_WARPS][snapchain::UT_SLOTS];
+  constexpr int NT = VS_WARPS * 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t li = (int64_t)blockIdx.x * VS_WARPS + w;
+  if (li >= nc) return;  // warp-uniform; the kernel synchronises only within a warp
+  const int64_t i = a0 + li;
+  const int si = clamp_sp(species[i], S.nsp);
+  const int64_t beg = off[i], end = off[i + 1];
+  const double gi0 = g[3 * i], gi1 = g[3 * i + 1], gi2 = g[3 * i + 2];
+  snapchain::UtStage st;
+  st.buf = vsh + 4 * (J + 1) * NT + w * snapchain::UT_SLOTS * 33;
+  st.dst = dst[w];
+  st.ut = reinterpret_cast<double*>(V + li);
+  st.stride = nc;
+  st.lane = lane;
+  st.nslot = 0;
+  st.wself = 0.0;
+  for (int64_t p0 = beg; p0 < (end > beg ? end : beg + 1); p0 += 32) {
+    const int64_t p = p0 + lane;
+    snapchain::Geom G;  // idle lanes: the identity rotation with zero weights
+    G.a = make_double2(1.0, 0.0);
+    G.b = make_double2(0.0, 0.0);
+    G.sfac = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      G.da[k] = make_double2(0.0, 0.0);
+      G.db[k] = make_double2(0.0, 0.0);
+      G.dsu[k] = 0.0;
+    }
+    double A = 0.0, Bk[3] = {0.0, 0.0, 0.0};
+    if (p < end) {
+      const int32_t jn = nbr[p];
+      const int sj = clamp_sp(species[jn], S.nsp);
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+      PairGeom PG;
+      geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+      G.a = PG.a;
+      G.b = PG.b;
+      G.sfac = PG.sfac;
+      const double gv[3] = {gi0 - g[3 * jn], gi1 - g[3 * jn + 1], gi2 - g[3 * jn + 2]};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        G.da[k] = PG.da[k];
+        G.db[k] = PG.db[k];
+        A += gv[k] * (PG.dsfac * PG.u[k]);
+        Bk[k] = PG.sfac * gv[k];
+      }
+    }
+    st.first = p0 == beg;
+    snapchain::all_chains_v<J>(G, A, Bk, st, vsh, NT, threadIdx.x);
+  }
+}
+
+template <int J>
+int launch_vsum_j(ipg_ctx* ctx, const SnapDev& S, int64_t a0, int64_t nc, const int64_t* off, const int32_t* nbr,
+                  const double* rij, const int32_t* species, const double* g, double2* V) {
+  const size_t sm = ((size_t)4 * (J + 1) * VS_WARPS * 32 + (size_t)VS_WARPS * snapchain::UT_SLOTS * 33) * sizeof(double2);
+  if (sm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_vsum<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  IPG_TIMED_LAUNCH(ctx, "snap_vsum", k_snap_vsum<J>, nblk(nc, VS_WARPS), VS_WARPS * 32, sm, S, a0, nc, off, nbr, rij,
+                   species, g, V);
+  return IPG_OK;
+}
+
+int launch_vsum(ipg_ctx* ctx, const SnapDev& S, int64_t a0, int64_t nc, const int64_t* off, const int32_t* nbr,
+                const double* rij, const int32_t* species, const double* g, double2* V) {
+  if (nc == 0) return IPG_OK;
+  switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_vsum_j<JJ>(ctx, S, a0, nc, off, nbr, rij, species, g, V);
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
+  }
+}
+
+// sum over the half plane of level l, entries z0.. of Z: w Re(conj(X) Z), w = 1 below the
+// middle element of an even level, 1/2 on it (the weights of compute_b.jl:207-400)
+__device__ __forceinline__ double half_dot(const double2* __restrict__ xs, int l, int hb,
+                                           const double2* __restrict__ Z, int64_t z0, int64_t zs) {
+  const int nf = nfull_of(l);
+  const double2* __restrict__ x = xs + (size_t)hb * YS_ATOMS;
+  const double2* __restrict__ z = Z + z0 * zs;
+  double s0 = 0.0, s1 = 0.0;
+  for (int e = 0; e < nf; e++) {
+    const double2 a = x[(size_t)e * YS_ATOMS], c = z[e * zs];
+    s0 = fma(a.x, c.x, s0);
+    s1 = fma(a.y, c.y, s1);
+  }
+  double s = s0 + s1;
+  if (!(l & 1)) {
+    const int e = (l / 2) * (l + 1) + l / 2;
+    const double2 a = x[(size_t)e * YS_ATOMS], c = z[e * zs];
+    s += 0.5 * (a.x * c.x + a.y * c.y);
+  }
+  return s;
+}
+
+// Contraction of V (and, with gE != 0, Utot for B) with Z for atoms a0 .. a0+nc-1: 32 atoms
+// per tile in lanes, V (Utot) of the tile staged in shared memory as [u_half][32], the warps
+// of a block taking components b = warp, warp + GB_WARPS, ...; per species, the lane values
+// are warp sums added in tile order to the block's partial gpart[block][nsp][K].
+constexpr int GB_WARPS = 16;
+__global__ void __launch_bounds__(GB_WARPS * 32) k_snap_gbeta(const __grid_constant__ SnapDev S, int64_t a0,
+                                                              int64_t nc, const int32_t* __restrict__ species,
+                                                              const double2* __restrict__ Z,
+                                                              const double2* __restrict__ V,
+                                                              const double2* __restrict__ utot, double gE,
+                                                              double* __restrict__ gpart) {
+  extern __shared__ __align__(16) unsigned char gsh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int UH = S.u_half, K = S.K, nsp = S.nsp;
+  const bool withB = gE != 0.0;
+  double2* vs = reinterpret_cast<double2*>(gsh);  // [UH][32]
+  double2* us = vs + (size_t)UH * YS_ATOMS;       // [UH][32] when withB
+  double* gacc = reinterpret_cast<double*>(us + (withB ? (size_t)UH * YS_ATOMS : 0));  // [nsp][K]
+  for (int q = threadIdx.x; q < nsp * K; q += blockDim.x) gacc[q] = 0.0;
+  const int64_t ntile = (nc + YS_ATOMS - 1) / YS_ATOMS;
+  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int64_t l0 = t * YS_ATOMS;
+    const int na = (int)((nc - l0) < YS_ATOMS ? (nc - l0) : YS_ATOMS);
+    __syncthreads();  // the previous tile's reads of vs / us are done
+    for (int idx = threadIdx.x; idx < UH * YS_ATOMS; idx += blockDim.x) {
+      const int q = idx / YS_ATOMS, l = idx - q * YS_ATOMS;
+      vs[idx] = l < na ? V[(size_t)q * nc + l0 + l] : make_double2(0.0, 0.0);
+      if (withB)
+        us[idx] = l < na ? utot[(size_t)(a0 + l0 + l) * S.idxu_max + S.u_of_h[q]] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const bool valid = lane < na;
+    const int64_t la = l0 + (valid ? lane : 0);  // idle lanes read atom l0's Z and drop it
+    const int si = valid ? clamp_sp(species[a0 + la], S.nsp) : -1;
+    const double2* vl = vs + lane;
+    const double2* ul = us + lane;
+    const double2* Zl = Z + la;
+    for (int b = warp; b < K; b += GB_WARPS) {
+      const DBDev d = S.db[b];
+      double tot = 0.0;
+#pragma unroll
+      for (int term = 0; term < 3; term++) {
+        const int l = d.l[term];
+        tot += d.fac[term] * half_dot(vl, l, S.half_block[l], Zl, d.z0[term], nc);
+      }
+      double val = 2.0 * tot;
+      if (withB) {
+        const int l = d.l[0];
+        const double B = 2.0 * half_dot(ul, l, S.half_block[l], Zl, d.z0[0], nc) - (S.bzero_flag ? S.bzero[l] : 0.0);
+        val += gE * B;
+      }
+      for (int sp = 0; sp < nsp; sp++) {
+        const double x = warp_sum(si == sp ? val : 0.0);
+        if (lane == 0) gacc[sp * K + b] += x;
+      }
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nsp * K; q += blockDim.x) gpart[(size_t)blockIdx.x * nsp * K + q] = gacc[q];
 }
 
 // Adjoint per-neighbor kernel: one thread per (directed pair, chain MB); see
@@ -1548,6 +1790,7 @@ struct ipg_snap {
   bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
   int utot_warps = 4;       // atoms (warps) per block of the per-chain Utot kernels
   bool utot_split = false;  // Utot: one launch per chain (k_snap_utot) instead of k_snap_utot_all
+  int64_t vjp_chunk = 0;     // atoms per Z chunk of the beta pullback (0: about 4 GiB of Z)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
@@ -1858,7 +2101,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
         const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
-        const void* kfn = rows ? (const void*)k_snap_yrows : (const void*)k_snap_yatoms;
+        const void* kfn = rows ? (const void*)k_snap_yrows<false> : (const void*)k_snap_yatoms;
         if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
         CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
@@ -1866,7 +2109,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
         const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
         const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
         if (rows)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<false>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
                            d_species, io.utot_in, yout, Ei);
         else
           IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
@@ -2194,6 +2437,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_PAIR_SPLIT")) s->pair_split = g[0] == '1';
   if (const char* g = getenv("IPG_Y_ENTRIES")) s->y_entries = g[0] == '1';
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
+  if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);
@@ -2402,6 +2646,44 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
     IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps, !s->utot_split));
     io.utot_in = utot;
+  }
+  if (io.utot_in && dev.J <= YR_MAX_J && s->h.yconst_ok) {
+    // register-chain path: Z (row-blocked kernel) and V per chunk of atoms, then the
+    // contraction; chunks bound the Z buffer (idxz_max entries per atom) to about 4 GiB
+    const int64_t zbytes = (int64_t)dev.idxz_max * (int64_t)sizeof(double2);
+    int64_t C = std::max<int64_t>(YS_ATOMS, (((int64_t)4 << 30) / zbytes) / YS_ATOMS * YS_ATOMS);
+    if (s->vjp_chunk > 0) C = std::max<int64_t>(YS_ATOMS, s->vjp_chunk / YS_ATOMS * YS_ATOMS);
+    C = std::min(C, n);
+    const int64_t nchunk = (n + C - 1) / C;
+    double2 *Z, *V;
+    IPG_RET(scratch(ctx, "snap_vjp_Z", (size_t)C * dev.idxz_max + 1, &Z));
+    IPG_RET(scratch(ctx, "snap_vjp_V", (size_t)C * dev.u_half + 1, &V));
+    const int ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yrows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+    int yper = 1, gper = 1;
+    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&yper, k_snap_yrows<true>, YS_WARPS * 32, ysm));
+    const bool withB = gE != 0.0;
+    const int gsm = (int)((withB ? 2 : 1) * (size_t)dev.u_half * YS_ATOMS * sizeof(double2) + (size_t)nsp * K * 8);
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_gbeta, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
+    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&gper, k_snap_gbeta, GB_WARPS * 32, gsm));
+    const int64_t gmax = (int64_t)ctx->num_sms * std::max(1, gper);
+    double* gpart;
+    IPG_RET(scratch(ctx, "snap_gpart", (size_t)(nchunk * gmax) * nsp * K + 1, &gpart));
+    int64_t rows = 0;  // partial rows written, in chunk order
+    for (int64_t c = 0; c < nchunk; c++) {
+      const int64_t a0 = c * C, nc = std::min(C, n - a0);
+      const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
+      const int64_t yg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, yper));
+      IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<true>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
+                       d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr);
+      IPG_RET(launch_vsum(ctx, dev, a0, nc, pl.d_off, pl.d_j, pl.d_r, d_species, d_g, V));
+      const int64_t gg = std::min(tiles, gmax);
+      IPG_TIMED_LAUNCH(ctx, "snap_gbeta", k_snap_gbeta, (unsigned)gg, GB_WARPS * 32, gsm, dev, a0, nc, d_species, Z,
+                       V, io.utot_in, gE, gpart + (size_t)rows * nsp * K);
+      rows += gg;
+    }
+    IPG_LAUNCH(ctx, k_sum_partials, nblk((int64_t)nsp * K, 128), 128, 0, rows, nsp * K, gpart, d_gbeta, 0.0);
+    return IPG_OK;
   }
   int threads = s->threads;
   SmemLayout L = smem_layout(dev, threads / 32, MODE_VJP, true);

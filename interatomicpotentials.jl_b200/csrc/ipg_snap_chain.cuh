@@ -511,7 +511,8 @@ constexpr int UT_SLOTS = 16;
 struct UtStage {
   double2* buf;  // [UT_SLOTS][33] of this warp
   int* dst;      // [UT_SLOTS] packed destination of each slot
-  double* ut;    // this atom's Utot, as doubles
+  double* ut;    // this atom's entry 0, as doubles; entry e at ut[2 e stride + c]
+  int64_t stride = 1;
   int lane, nslot;
   bool first;    // first chunk of neighbors: write (with wself on the diagonal), else add
   double wself;
@@ -536,12 +537,13 @@ struct UtStage {
       const double t = (t4[0] + t4[1]) + (t4[2] + t4[3]);
       const int pk = dst[q];
       const int e = pk & 0xfff;
-      double v = first ? ((c == 0 && ((pk >> 25) & 1)) ? wself : 0.0) : ut[2 * e + c];
+      double* pe = ut + 2 * (int64_t)e * stride + c;
+      double v = first ? ((c == 0 && ((pk >> 25) & 1)) ? wself : 0.0) : *pe;
       v += t;
-      ut[2 * e + c] = v;
+      *pe = v;
       if ((pk >> 26) & 1) {
         const double sg = ((pk >> 24) & 1) ? -1.0 : 1.0;
-        ut[2 * ((pk >> 12) & 0xfff) + c] = c ? -sg * v : sg * v;
+        ut[2 * (int64_t)((pk >> 12) & 0xfff) * stride + c] = c ? -sg * v : sg * v;
       }
     }
     __syncwarp();
@@ -610,6 +612,78 @@ __device__ __forceinline__ void all_chains_utot(double2 a, double2 b, double sw,
 #define IPG_LEVEL(JJ) \
   case JJ:            \
     level_u_rt<J, JJ>(s, a, b, sw, mb, st, sv);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
+  st.flush();
+}
+
+}  // namespace snapchain
+
+namespace snapchain {
+
+// ---- V = sum over neighbors of g_ij . dU/dr_ij (the beta pullback of the forces) --------
+// Per lane one neighbor, all chains with derivatives (the runtime-row level code of the
+// adjoint kernel); each half-plane entry h contributes
+//   v_h = sum_k gv_k (dsfac uhat_k u_h + sfac du_k,h) = A u_h + sum_k B_k du_k,h
+// (A = dsfac gv.uhat, B_k = sfac gv_k), summed over the warp's lanes through the staging
+// buffer into V[h] of the atom.
+template <int J, int j>
+__device__ __forceinline__ void stage_v(const Chain<J>& s, double A, const double* Bk, int mb, UtStage& st) {
+  const int last = (2 * mb == j) ? mb : j;
+  const int hb = half_block(j) + mb * (j + 1);
+  st.room(last + 1);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > last) break;
+    double vx = A * s.u[ma].x, vy = A * s.u[ma].y;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      vx = fma(Bk[k], s.d[k][ma].x, vx);
+      vy = fma(Bk[k], s.d[k][ma].y, vy);
+    }
+    st.push(make_double2(vx, vy), hb + ma);  // packed: entry only (no mirror, no diagonal)
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level_v(Chain<J>& s, const Geom& G, double A, const double* Bk, int mb, UtStage& st,
+                                        double2* save, int nt, int tid) {
+  if constexpr (j <= J) {
+    advance_rt<J, j>(s, G, mb);
+    stage_v<J, j>(s, A, Bk, mb, st);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2)
+      if (j == 2 * mb + 1) save_mirror<J, j>(s, save, nt, tid);
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void all_chains_v(const Geom& G, double A, const double* Bk, UtStage& st, double2* save,
+                                             int nt, int tid) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
+  Chain<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) s.d[k][c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);
+  stage_v<J, 0>(s, A, Bk, 0, st);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+      asm volatile("" ::: "memory");
+      load_row_rt<J>(s, save, nt, tid, 2 * mb);
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level_v<J, JJ>(s, G, A, Bk, mb, st, save, nt, tid);
       IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
       IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
 #undef IPG_LEVEL

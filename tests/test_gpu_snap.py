@@ -241,6 +241,30 @@ def test_adjoint_paths_agree(J, monkeypatch):
         assert rel_err(w, wo) <= TOL
 
 
+@pytest.mark.parametrize("J", [4, 7, 8, 11])
+def test_vjp_paths_agree(J, monkeypatch):
+    """The beta pullback: twojmax <= 8 runs the register-chain path (Z by the row-blocked kernel,
+    V per neighbor chain, contraction per atom tile), in chunks of atoms when IPG_VJP_CHUNK is
+    set; larger twojmax or IPG_GENERIC_ADJOINT=1 the per-atom block kernel.  All equal the
+    oracle, with and without the energy term gE B."""
+    rng = np.random.default_rng(200 + J)
+    pos = rng.uniform(0, 7, (100, 3))
+    s = ipg.System(pos, list(np.where(rng.random(100) < 0.6, "A", "B")), [7.0] * 3)
+    prm = dict(twojmax=J, species=["A", "B"], rcutfac=2.2, rmin0=0.1, rfac0=0.98, radii=[1.0, 0.8],
+               weight=[1.0, 0.7], switch_flag=True, bzero_flag=J % 2 == 0)
+    gF = rng.normal(size=(100, 3))
+    _, orc = make(prm)
+    for gE in (0.0, 0.7):
+        go, _ = orc.vjp_beta(s.positions, np.array([0 if x == "A" else 1 for x in s.symbols], np.int32), s.L, gE,
+                             gF)
+        for generic, chunk in (("0", "0"), ("0", "40"), ("1", "0")):
+            monkeypatch.setenv("IPG_GENERIC_ADJOINT", generic)
+            monkeypatch.setenv("IPG_VJP_CHUNK", chunk)
+            snap, _ = make(prm)
+            gb, _ = snap.vjp_beta(s, gE, gF)
+            assert rel_err(gb, go) <= TOL, (gE, generic, chunk)
+
+
 def test_twojmax_beyond_shared_memory_is_unsupported():
     """twojmax 12 needs more than 227 KB of shared memory per block: a clean error."""
     s = ipg.System(np.random.default_rng(0).uniform(0, 5, (10, 3)), ["A"] * 10, [5.0] * 3)
