@@ -1332,6 +1332,51 @@ __global__ void __launch_bounds__(GB_WARPS * 32) k_snap_gbeta(const __grid_const
   for (int q = threadIdx.x; q < nsp * K; q += blockDim.x) gpart[(size_t)blockIdx.x * nsp * K + q] = gacc[q];
 }
 
+// Bispectrum components from Z (k_snap_yrows<true>) and Utot for atoms a0 .. a0+nc-1
+// (compute_b.jl:17-94): B_b = 2 sum_half w Re(conj(U_j) Z(j1,j2,j)) - bzero_j, 32 atoms per
+// tile in lanes, the warps over components; Ei = beta[s_i] . B_i (the bzero shift inside B).
+// B [n][K] (optional) and Ei [n] are indexed by the global atom.
+__global__ void __launch_bounds__(GB_WARPS * 32) k_snap_bdesc(const __grid_constant__ SnapDev S, int64_t a0,
+                                                              int64_t nc, const int32_t* __restrict__ species,
+                                                              const double2* __restrict__ Z,
+                                                              const double2* __restrict__ utot, double* __restrict__ B,
+                                                              double* __restrict__ Ei) {
+  extern __shared__ __align__(16) unsigned char bsh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int UH = S.u_half, K = S.K;
+  double2* us = reinterpret_cast<double2*>(bsh);                      // [UH][32]
+  double* bs = reinterpret_cast<double*>(us + (size_t)UH * YS_ATOMS);  // [K][32]
+  const int64_t ntile = (nc + YS_ATOMS - 1) / YS_ATOMS;
+  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int64_t l0 = t * YS_ATOMS;
+    const int na = (int)((nc - l0) < YS_ATOMS ? (nc - l0) : YS_ATOMS);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < UH * YS_ATOMS; idx += blockDim.x) {
+      const int q = idx / YS_ATOMS, l = idx - q * YS_ATOMS;
+      us[idx] = l < na ? utot[(size_t)(a0 + l0 + l) * S.idxu_max + S.u_of_h[q]] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const bool valid = lane < na;
+    const int64_t la = l0 + (valid ? lane : 0);
+    for (int b = warp; b < K; b += GB_WARPS) {
+      const DBDev d = S.db[b];
+      const int l = d.l[0];
+      const double v = 2.0 * half_dot(us + lane, l, S.half_block[l], Z + la, d.z0[0], nc) -
+                       (S.bzero_flag ? S.bzero[l] : 0.0);
+      bs[b * YS_ATOMS + lane] = v;
+      if (B && valid) B[(size_t)(a0 + la) * K + b] = v;
+    }
+    __syncthreads();
+    if (warp == 0 && valid) {
+      const int si = clamp_sp(species[a0 + la], S.nsp);
+      const double* bt = S.beta + (size_t)si * K;
+      double e = 0.0;
+      for (int b = 0; b < K; b++) e = fma(bt[b], bs[b * YS_ATOMS + lane], e);
+      Ei[a0 + la] = e;
+    }
+  }
+}
+
 // Adjoint per-neighbor kernel: one thread per (directed pair, chain MB); see
 // ipg_snap_chain.cuh.  Yw is the weighted Y as [h][natoms]; part[p][MB][3] = chain MB's
 // share of dE_i/dr_ij.
@@ -2051,7 +2096,26 @@ struct EvalOut {
   bool dB_rows = false;
   double* Ae = nullptr;  // [nconf][K*nsp] fitting energy rows (device)
   double* Aw = nullptr;  // [nconf][6][K*nsp] fitting virial rows (device)
+  PairList* pl_out = nullptr;          // receives the pair list (stays valid until the next build)
+  const double2** utot_out = nullptr;  // receives Utot [n][idxu_max] when the chain kernel made it
 };
+
+// Atoms per chunk of the Z buffer (idxz_max entries per atom): about 4 GiB, or IPG_VJP_CHUNK.
+int64_t zrows_chunk(const ipg_snap* s, const SnapDev& dev, int64_t n) {
+  const int64_t zbytes = (int64_t)dev.idxz_max * (int64_t)sizeof(double2);
+  int64_t C = std::max<int64_t>(YS_ATOMS, (((int64_t)4 << 30) / zbytes) / YS_ATOMS * YS_ATOMS);
+  if (s->vjp_chunk > 0) C = std::max<int64_t>(YS_ATOMS, s->vjp_chunk / YS_ATOMS * YS_ATOMS);
+  return std::max<int64_t>(1, std::min(C, n));
+}
+
+// Shared memory and blocks per SM of k_snap_yrows<true>.
+int zrows_config(ipg_ctx* ctx, const SnapDev& dev, int* ysm, int* per_sm) {
+  *ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
+  CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yrows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, *ysm));
+  *per_sm = 1;
+  CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_snap_yrows<true>, YS_WARPS * 32, *ysm));
+  return IPG_OK;
+}
 
 // Energy / forces / descriptors for device inputs.  mode: MODE_DESC (B/E only), MODE_ADJ,
 // MODE_PLAIN.  Writes device outputs; does not synchronise.
@@ -2135,6 +2199,27 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       if (n) IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, nsp, dbl, dev.beta, K,
                                fvec);
     }
+  } else if (chains && n && dev.J <= YR_MAX_J && s->h.yconst_ok && cap == 0) {
+    // Z from the row-blocked kernel per chunk of atoms, then B (and E_i) per atom tile
+    const int64_t C = zrows_chunk(s, dev, n);
+    double2* Z;
+    IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
+    int ysm, yper;
+    IPG_RET(zrows_config(ctx, dev, &ysm, &yper));
+    const int bsm = (int)((size_t)dev.u_half * YS_ATOMS * sizeof(double2) + (size_t)K * YS_ATOMS * 8);
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_bdesc, cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
+    int bper = 1;
+    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bper, k_snap_bdesc, GB_WARPS * 32, bsm));
+    for (int64_t a0 = 0; a0 < n; a0 += C) {
+      const int64_t nc = std::min(C, n - a0);
+      const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
+      const int64_t yg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, yper));
+      IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<true>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
+                       d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr);
+      const int64_t bg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, bper));
+      IPG_TIMED_LAUNCH(ctx, "snap_bdesc", k_snap_bdesc, (unsigned)bg, GB_WARPS * 32, bsm, dev, a0, nc, d_species, Z,
+                       io.utot_in, out.B, Ei);
+    }
   } else {
     if (n) IPG_RET(launch_atoms<MODE_DESC>(s, dev, io, n, nullptr));
   }
@@ -2197,6 +2282,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_LAUNCH(ctx, k_snap_W_desc, (unsigned)grid, 64, sm, n, K, nsp, pl.d_off, pl.d_j, d_species, d_pos, dbl, part);
     IPG_LAUNCH(ctx, k_sum_partials, nblk(width, 128), 128, 0, grid, width, part, out.Wd, 0.0);
   }
+  if (out.pl_out) *out.pl_out = pl;
+  if (out.utot_out) *out.utot_out = io.utot_in;
   return IPG_OK;
 }
 
@@ -2619,14 +2706,19 @@ namespace {
 
 // gbeta = sum over blocks of the VJP partials (device), for device inputs already
 // resident.  g = cotangent of forces [3n] (device), gE scalar.
+// reuse_pl / reuse_utot: the pair list and Utot of an evaluation of the same positions just
+// before (snap_eval's pl_out / utot_out), or null to build them here.
 int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
                     const int64_t* h_atom_off, const double* h_L, const double* beta, double gE, const double* d_g,
-                    double* d_gbeta) {
+                    double* d_gbeta, const PairList* reuse_pl = nullptr, const double2* reuse_utot = nullptr) {
   ipg_ctx* ctx = s->ctx;
   SnapDev dev = s->dev;
   IPG_RET(set_beta(s, beta, 0.0, dev));
   PairList pl;
-  IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl));
+  if (reuse_pl)
+    pl = *reuse_pl;
+  else
+    IPG_RET(snap_neighbors(s, n, d_pos, d_species, nconf, h_atom_off, h_L, pl));
   const int K = dev.K, nsp = dev.nsp;
   double* Ei;
   IPG_RET(scratch(ctx, "snap_Ei", (size_t)n + 1, &Ei));
@@ -2641,7 +2733,9 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
   io.g = d_g;
   io.gE = gE;
   io.status = ctx->d_status;
-  if (dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && n) {
+  if (reuse_pl && reuse_utot) {
+    io.utot_in = reuse_utot;
+  } else if (dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && n) {
     double2* utot;
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
     IPG_RET(launch_utot(ctx, dev, n, pl.d_off, pl.d_j, pl.d_r, d_species, utot, s->utot_warps, !s->utot_split));
@@ -2649,19 +2743,14 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
   }
   if (io.utot_in && dev.J <= YR_MAX_J && s->h.yconst_ok) {
     // register-chain path: Z (row-blocked kernel) and V per chunk of atoms, then the
-    // contraction; chunks bound the Z buffer (idxz_max entries per atom) to about 4 GiB
-    const int64_t zbytes = (int64_t)dev.idxz_max * (int64_t)sizeof(double2);
-    int64_t C = std::max<int64_t>(YS_ATOMS, (((int64_t)4 << 30) / zbytes) / YS_ATOMS * YS_ATOMS);
-    if (s->vjp_chunk > 0) C = std::max<int64_t>(YS_ATOMS, s->vjp_chunk / YS_ATOMS * YS_ATOMS);
-    C = std::min(C, n);
+    // contraction
+    const int64_t C = zrows_chunk(s, dev, n);
     const int64_t nchunk = (n + C - 1) / C;
     double2 *Z, *V;
-    IPG_RET(scratch(ctx, "snap_vjp_Z", (size_t)C * dev.idxz_max + 1, &Z));
+    IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
     IPG_RET(scratch(ctx, "snap_vjp_V", (size_t)C * dev.u_half + 1, &V));
-    const int ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
-    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yrows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
-    int yper = 1, gper = 1;
-    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&yper, k_snap_yrows<true>, YS_WARPS * 32, ysm));
+    int ysm, yper, gper = 1;
+    IPG_RET(zrows_config(ctx, dev, &ysm, &yper));
     const bool withB = gE != 0.0;
     const int gsm = (int)((withB ? 2 : 1) * (size_t)dev.u_half * YS_ATOMS * sizeof(double2) + (size_t)nsp * K * 8);
     CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_gbeta, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
@@ -2977,6 +3066,10 @@ int ipg_snap_batch_loss_grad(ipg_snap* s, int32_t nconfig, const int64_t* atom_o
   IPG_RET(ipg_status_reset(ctx));
   EvalOut o;
   o.F = d_F;
+  PairList pl;
+  const double2* utot = nullptr;
+  o.pl_out = &pl;
+  o.utot_out = &utot;
   IPG_RET(snap_eval(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, beta0, MODE_ADJ, o));
   if (n) {
     IPG_LAUNCH(ctx, k_loss_grad, nblk(n, 256), 256, 0, n, d_F, d_Fref, d_g, d_li);
@@ -2984,7 +3077,8 @@ int ipg_snap_batch_loss_grad(ipg_snap* s, int32_t nconfig, const int64_t* atom_o
   } else {
     CUDA_RET(ctx, cudaMemsetAsync(d_l, 0, sizeof(double), ctx->stream));
   }
-  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, 0.0, d_g, d_gb));
+  // same positions: the pullback reuses the evaluation's pair list and Utot
+  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, 0.0, d_g, d_gb, &pl, utot));
   CUDA_RET(ctx, cudaMemcpyAsync(gbeta, d_gb, sizeof(double) * nsp * K, cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_RET(ctx, cudaMemcpyAsync(loss, d_l, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   (void)beta0;

@@ -265,6 +265,25 @@ def test_vjp_paths_agree(J, monkeypatch):
             assert rel_err(gb, go) <= TOL, (gE, generic, chunk)
 
 
+@pytest.mark.parametrize("J", [5, 8, 11])
+def test_descriptor_paths_agree(J, monkeypatch):
+    """Local descriptors: Z from the row-blocked kernel and B per atom tile for twojmax <= 8
+    (whole, or in chunks of 40 atoms), the per-atom block kernel otherwise."""
+    rng = np.random.default_rng(300 + J)
+    pos = rng.uniform(0, 7, (100, 3))
+    s = ipg.System(pos, list(np.where(rng.random(100) < 0.6, "A", "B")), [7.0] * 3)
+    prm = dict(twojmax=J, species=["A", "B"], rcutfac=2.2, rmin0=0.1, rfac0=0.98, radii=[1.0, 0.8],
+               weight=[1.0, 0.7], switch_flag=True, bzero_flag=J % 2 == 0)
+    _, orc = make(prm)
+    sp = np.array([0 if x == "A" else 1 for x in s.symbols], np.int32)
+    Bo, _, _ = orc.descriptors(s.positions, sp, s.L)
+    for generic, chunk in (("0", "0"), ("0", "40"), ("1", "0")):
+        monkeypatch.setenv("IPG_GENERIC_ADJOINT", generic)
+        monkeypatch.setenv("IPG_VJP_CHUNK", chunk)
+        snap, _ = make(prm)
+        assert rel_err(ipg.compute_local_descriptors(s, snap), Bo) <= TOL, (generic, chunk)
+
+
 def test_twojmax_beyond_shared_memory_is_unsupported():
     """twojmax 12 needs more than 227 KB of shared memory per block: a clean error."""
     s = ipg.System(np.random.default_rng(0).uniform(0, 5, (10, 3)), ["A"] * 10, [5.0] * 3)
