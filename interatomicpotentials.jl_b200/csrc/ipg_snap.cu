@@ -1377,6 +1377,206 @@ __global__ void __launch_bounds__(GB_WARPS * 32) k_snap_bdesc(const __grid_const
   }
 }
 
+// ---- plain dB/dr path from the register chains (twojmax <= YR_MAX_J) ----------------------
+// dB_i/dr_ij [b][k] = 2 sum_t fac_t sum_half w Re(conj(dU_ij,k) Z_i(t)) (compute_dbidrj.jl;
+// compute_b.jl:207-400).  Every Z triple z belongs to one component jjb(z) with one
+// multiplier m(z) (its coincidence count and, unnormalised, (j1+1)/(j+1)), the same pair the
+// Y coefficients use, so dB[b][k] = 2 sum_{z: jjb(z) = b} m(z) sum_half w Re(conj(dU_k) Z_z).
+// k_snap_dupair writes each pair's dU (all chains in one thread) to a pair-major buffer,
+// k_snap_dbcon contracts it with the owner's Z: one thread per pair, the Z triples of a level
+// unrolled at compile time (their tables below are constexpr restatements of the host's
+// idxz / idxb / y_jjb / y_mult loops), one component k per pass.
+namespace plaintab {
+constexpr int zrow_count(int j) { return (j / 2 + 1) * (j + 1); }
+constexpr int imin(int a, int b) { return a < b ? a : b; }
+constexpr int nfull_c(int l) { return ((l + 1) / 2) * (l + 1) + ((l & 1) ? 0 : l / 2); }
+constexpr int idxb_of(int J, int a, int b, int c) {
+  int k = 0;
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= imin(J, j1 + j2); j += 2)
+        if (j >= j1) {
+          if (j1 == a && j2 == b && j == c) return k;
+          k++;
+        }
+  return -1;
+}
+constexpr int nb_of(int J) {
+  int k = 0;
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= imin(J, j1 + j2); j += 2)
+        if (j >= j1) k++;
+  return k;
+}
+constexpr int LMAX = 64;
+struct Level {  // the Z triples (j1, j2, L) of level L
+  int n = 0;
+  int z0[LMAX] = {};   // first Z entry
+  int jjb[LMAX] = {};  // component
+  double m[LMAX] = {}, mn[LMAX] = {};  // multiplier without / with bnorm_flag
+};
+constexpr Level level_of(int J, int L) {
+  Level T;
+  int z = 0;
+  for (int j1 = 0; j1 <= J; j1++)
+    for (int j2 = 0; j2 <= j1; j2++)
+      for (int j = j1 - j2; j <= imin(J, j1 + j2); j += 2) {
+        if (j == L && T.n < LMAX) {
+          int jjb = 0;
+          double mult = 1.0;
+          if (j >= j1) {
+            jjb = idxb_of(J, j1, j2, j);
+            mult = (j1 == j) ? ((j2 == j) ? 3.0 : 2.0) : 1.0;
+          } else if (j >= j2) {
+            jjb = idxb_of(J, j, j2, j1);
+            mult = (j2 == j) ? 2.0 : 1.0;
+          } else {
+            jjb = idxb_of(J, j2, j, j1);
+          }
+          T.z0[T.n] = z;
+          T.jjb[T.n] = jjb;
+          T.mn[T.n] = mult;
+          T.m[T.n] = (j1 > j) ? mult * (j1 + 1.0) / (j + 1.0) : mult;
+          T.n++;
+        }
+        z += zrow_count(j);
+      }
+  return T;
+}
+}  // namespace plaintab
+
+constexpr int DB_T = 128;  // threads (pairs) per block of the plain chain kernels
+
+template <int J>
+__global__ void __launch_bounds__(DB_T) k_snap_dupair(const __grid_constant__ SnapDev S, int64_t q0, int64_t nq,
+                                                      const int32_t* __restrict__ owner,
+                                                      const int32_t* __restrict__ nbr,
+                                                      const double* __restrict__ rij,
+                                                      const int32_t* __restrict__ species,
+                                                      double2* __restrict__ dU) {
+  extern __shared__ double2 dsave[];  // saved start rows [4 (J+1)][DB_T]
+  const int64_t t = (int64_t)blockIdx.x * DB_T + threadIdx.x;
+  if (t >= nq) return;  // no block-level synchronisation below
+  const int64_t p = q0 + t;
+  const int si = clamp_sp(species[owner[p]], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
+  const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+  PairGeom PG;
+  geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+  snapchain::Geom G;
+  G.a = PG.a;
+  G.b = PG.b;
+  G.sfac = PG.sfac;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    G.da[k] = PG.da[k];
+    G.db[k] = PG.db[k];
+    G.dsu[k] = PG.dsfac * PG.u[k];
+  }
+  snapchain::all_chains_store<J>(G, dU + t, S.u_half, nq, dsave, DB_T, threadIdx.x);
+}
+
+// Triples Q.. of level L: c[Q] += Re(conj(d) Z_Q[e]) (zp: this pair's owner column at entry e)
+template <int J, int L, int Q, int NQ>
+__device__ __forceinline__ void dbcon_terms(double (&c)[NQ], double2 d, const double2* __restrict__ zp, int64_t zs) {
+  if constexpr (Q < NQ) {
+    constexpr int z0 = plaintab::level_of(J, L).z0[Q];
+    const double2 z = zp[z0 * zs];
+    c[Q] = fma(d.x, z.x, fma(d.y, z.y, c[Q]));
+    dbcon_terms<J, L, Q + 1, NQ>(c, d, zp, zs);
+  }
+}
+
+template <int J, int L, int Q, int NQ, int NB>
+__device__ __forceinline__ void dbcon_add(double (&acc)[NB], const double (&c)[NQ], bool bnorm) {
+  if constexpr (Q < NQ) {
+    constexpr plaintab::Level T = plaintab::level_of(J, L);
+    constexpr int b = T.jjb[Q];
+    constexpr double m = T.m[Q], mn = T.mn[Q];
+    acc[b] = fma(bnorm ? mn : m, c[Q], acc[b]);
+    dbcon_add<J, L, Q + 1, NQ, NB>(acc, c, bnorm);
+  }
+}
+
+// Levels L.. of one component k: dk = dU_k of this pair at half-plane entry 0 (pair stride ps)
+template <int J, int L, int NB>
+__device__ __forceinline__ void dbcon_levels(double (&acc)[NB], const double2* __restrict__ dk, int64_t ps,
+                                             const double2* __restrict__ zc, int64_t zs, bool bnorm) {
+  if constexpr (L <= J) {
+    constexpr int NQ = plaintab::level_of(J, L).n;
+    constexpr int nf = plaintab::nfull_c(L);
+    constexpr int ne = nf + ((L & 1) ? 0 : 1);  // the middle element of an even level, weight 1/2
+    double c[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) c[q] = 0.0;
+    const double2* d = dk + (int64_t)snapchain::half_block(L) * ps;
+#pragma unroll 1
+    for (int e = 0; e < ne; e++) {
+      double2 v = d[e * ps];
+      if (!(L & 1) && e == nf) {
+        v.x *= 0.5;
+        v.y *= 0.5;
+      }
+      dbcon_terms<J, L, 0, NQ>(c, v, zc + e * zs, zs);
+    }
+    dbcon_add<J, L, 0, NQ, NB>(acc, c, bnorm);
+    dbcon_levels<J, L + 1, NB>(acc, dk, ps, zc, zs, bnorm);
+  }
+}
+
+// dbl[p][b][k] for pairs q0 .. q0+nq-1, whose owners lie in the Z chunk of atoms a0.. (stride zs)
+template <int J>
+__global__ void __launch_bounds__(DB_T) k_snap_dbcon(const __grid_constant__ SnapDev S, int64_t q0, int64_t nq,
+                                                     const int32_t* __restrict__ owner, int64_t a0, int64_t zs,
+                                                     const double2* __restrict__ Z, const double2* __restrict__ dU,
+                                                     double* __restrict__ dbl) {
+  constexpr int NB = plaintab::nb_of(J);
+  const int64_t t = (int64_t)blockIdx.x * DB_T + threadIdx.x;
+  if (t >= nq) return;
+  const int64_t p = q0 + t;
+  const double2* zc = Z + (owner[p] - a0);
+  const bool bnorm = S.bnorm_flag != 0;
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    double acc[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) acc[b] = 0.0;
+    dbcon_levels<J, 0, NB>(acc, dU + (int64_t)k * S.u_half * nq + t, nq, zc, zs, bnorm);
+    double* out = dbl + (size_t)p * NB * 3 + k;
+#pragma unroll
+    for (int b = 0; b < NB; b++) out[3 * b] = 2.0 * acc[b];
+  }
+}
+
+template <int J>
+int plain_chunk_j(ipg_ctx* ctx, const SnapDev& S, int64_t q0, int64_t nq, const int32_t* owner, const int32_t* nbr,
+                  const double* rij, const int32_t* species, int64_t a0, int64_t zs, const double2* Z, double2* dU,
+                  double* dbl) {
+  if (plaintab::nb_of(J) != S.K) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "plain chain tables disagree");
+  const size_t sm = (size_t)4 * (J + 1) * DB_T * sizeof(double2);
+  if (sm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dupair<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  IPG_TIMED_LAUNCH(ctx, "snap_dupair", k_snap_dupair<J>, nblk(nq, DB_T), DB_T, sm, S, q0, nq, owner, nbr, rij, species,
+                   dU);
+  IPG_TIMED_LAUNCH(ctx, "snap_dbcon", k_snap_dbcon<J>, nblk(nq, DB_T), DB_T, 0, S, q0, nq, owner, a0, zs, Z, dU, dbl);
+  return IPG_OK;
+}
+
+int plain_chunk(ipg_ctx* ctx, const SnapDev& S, int64_t q0, int64_t nq, const int32_t* owner, const int32_t* nbr,
+                const double* rij, const int32_t* species, int64_t a0, int64_t zs, const double2* Z, double2* dU,
+                double* dbl) {
+  if (nq == 0) return IPG_OK;
+  switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return plain_chunk_j<JJ>(ctx, S, q0, nq, owner, nbr, rij, species, a0, zs, Z, dU, dbl);
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
+  }
+}
+
 // Adjoint per-neighbor kernel: one thread per (directed pair, chain MB); see
 // ipg_snap_chain.cuh.  Yw is the weighted Y as [h][natoms]; part[p][MB][3] = chain MB's
 // share of dE_i/dr_ij.
@@ -1835,7 +2035,9 @@ struct ipg_snap {
   bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
   int utot_warps = 4;       // atoms (warps) per block of the per-chain Utot kernels
   bool utot_split = false;  // Utot: one launch per chain (k_snap_utot) instead of k_snap_utot_all
-  int64_t vjp_chunk = 0;     // atoms per Z chunk of the beta pullback (0: about 4 GiB of Z)
+  int64_t vjp_chunk = 0;     // atoms per Z chunk (0: about 4 GiB of Z)
+  int64_t du_chunk = 0;      // pairs per dU chunk of the plain path (0: about 4 GiB of dU)
+  bool generic_plain = false;  // plain path: the per-atom block kernel (IPG_GENERIC_PLAIN=1)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
@@ -2117,6 +2319,52 @@ int zrows_config(ipg_ctx* ctx, const SnapDev& dev, int* ysm, int* per_sm) {
   return IPG_OK;
 }
 
+// Plain dB/dr path on the register chains: per chunk of atoms, Z (row-blocked kernel) and B,
+// E_i; per chunk of the pairs those atoms own, dU (k_snap_dupair) and dbl (k_snap_dbcon).
+// With more than one atom chunk the pair offsets are read back to size the pair chunks.
+int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const PairList& pl,
+                 const int32_t* d_species, const double2* utot, double* B, double* Ei, double* dbl) {
+  ipg_ctx* ctx = s->ctx;
+  int32_t* owner;
+  IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
+  if (np) IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
+  const int64_t C = zrows_chunk(s, dev, n);
+  double2 *Z, *dU;
+  IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
+  const int64_t dbytes = 3 * (int64_t)dev.u_half * (int64_t)sizeof(double2);
+  int64_t P = std::max<int64_t>(DB_T, (((int64_t)4 << 30) / dbytes) / DB_T * DB_T);
+  if (s->du_chunk > 0) P = std::max<int64_t>(DB_T, s->du_chunk / DB_T * DB_T);
+  P = std::max<int64_t>(1, std::min(P, np));
+  IPG_RET(scratch(ctx, "snap_dU", (size_t)P * 3 * dev.u_half + 1, &dU));
+  int ysm, yper;
+  IPG_RET(zrows_config(ctx, dev, &ysm, &yper));
+  const int bsm = (int)((size_t)dev.u_half * YS_ATOMS * sizeof(double2) + (size_t)dev.K * YS_ATOMS * 8);
+  CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_bdesc, cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
+  int bper = 1;
+  CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bper, k_snap_bdesc, GB_WARPS * 32, bsm));
+  std::vector<int64_t> hoff;
+  if (C < n) {
+    hoff.resize(n + 1);
+    CUDA_RET(ctx, cudaMemcpyAsync(hoff.data(), pl.d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  for (int64_t a0 = 0; a0 < n; a0 += C) {
+    const int64_t nc = std::min(C, n - a0);
+    const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
+    const int64_t yg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, yper));
+    IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<true>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
+                     d_species + a0, utot + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr);
+    const int64_t bg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, bper));
+    IPG_TIMED_LAUNCH(ctx, "snap_bdesc", k_snap_bdesc, (unsigned)bg, GB_WARPS * 32, bsm, dev, a0, nc, d_species, Z,
+                     utot, B, Ei);
+    const int64_t pb = C < n ? hoff[a0] : 0, pe = C < n ? hoff[a0 + nc] : np;
+    for (int64_t q0 = pb; q0 < pe; q0 += P)
+      IPG_RET(plain_chunk(ctx, dev, q0, std::min(P, pe - q0), owner, pl.d_j, pl.d_r, d_species, a0, nc, Z, dU, dbl));
+  }
+  return IPG_OK;
+}
+
 // Energy / forces / descriptors for device inputs.  mode: MODE_DESC (B/E only), MODE_ADJ,
 // MODE_PLAIN.  Writes device outputs; does not synchronise.
 int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
@@ -2193,7 +2441,10 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   } else if (need_plain) {
     IPG_RET(scratch(ctx, "snap_dbl", (size_t)np * K * 3 + 3, &dbl));
     io.dbl = dbl;
-    if (n) IPG_RET(launch_atoms<MODE_PLAIN>(s, dev, io, n, nullptr));
+    if (n && chains && dev.J <= YR_MAX_J && s->h.yconst_ok && cap == 0 && !s->generic_plain)
+      IPG_RET(plain_chains(s, dev, n, np, pl, d_species, io.utot_in, out.B, Ei, dbl));
+    else if (n)
+      IPG_RET(launch_atoms<MODE_PLAIN>(s, dev, io, n, nullptr));
     if (out.F || out.W6) {
       IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
       if (n) IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, nsp, dbl, dev.beta, K,
@@ -2525,6 +2776,8 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_Y_ENTRIES")) s->y_entries = g[0] == '1';
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
+  if (const char* g = getenv("IPG_DU_CHUNK")) s->du_chunk = std::max<int64_t>(0, atoll(g));
+  if (const char* g = getenv("IPG_GENERIC_PLAIN")) s->generic_plain = g[0] == '1';
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);

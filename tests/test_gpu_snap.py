@@ -284,6 +284,33 @@ def test_descriptor_paths_agree(J, monkeypatch):
         assert rel_err(ipg.compute_local_descriptors(s, snap), Bo) <= TOL, (generic, chunk)
 
 
+@pytest.mark.parametrize("J", [3, 6, 8, 9])
+def test_plain_paths_agree(J, monkeypatch):
+    """The plain dB/dr path: for twojmax <= 8 dU from the register chains and the contraction
+    with Z per pair (whole, or in chunks of 40 atoms and 256 pairs), otherwise (or with
+    IPG_GENERIC_PLAIN=1) the per-atom block kernel; B, dB, W, E and F all equal the oracle."""
+    rng = np.random.default_rng(400 + J)
+    pos = rng.uniform(0, 7, (100, 3))
+    s = ipg.System(pos, list(np.where(rng.random(100) < 0.6, "A", "B")), [7.0] * 3)
+    prm = dict(twojmax=J, species=["A", "B"], rcutfac=2.2, rmin0=0.1, rfac0=0.98, radii=[1.0, 0.8],
+               weight=[1.0, 0.7], switch_flag=True, bzero_flag=J % 2 == 0)
+    _, orc = make(prm)
+    sp = np.array([0 if x == "A" else 1 for x in s.symbols], np.int32)
+    Bo, dBo, Wo = orc.descriptors(s.positions, sp, s.L)
+    beta = rng.normal(0, 1e-2, (2, Bo.shape[1]))
+    eo, fo, wo = orc.energy_forces(s.positions, sp, s.L, beta, 0.0)
+    for generic, zchunk, pchunk in (("0", "0", "0"), ("0", "40", "256"), ("1", "0", "0")):
+        monkeypatch.setenv("IPG_GENERIC_PLAIN", generic)
+        monkeypatch.setenv("IPG_VJP_CHUNK", zchunk)
+        monkeypatch.setenv("IPG_DU_CHUNK", pchunk)
+        snap, _ = make(prm)
+        B, dB, Wd = ipg.compute_all_descriptors(s, snap)
+        assert rel_err(B, Bo) <= TOL, (generic, zchunk)
+        assert rel_err(dB, dBo.transpose(0, 2, 1)) <= TOL and rel_err(Wd, Wo.T) <= TOL, (generic, zchunk)
+        e, f, w = snap.energy_forces(s, beta, 0.0, mode="plain")
+        assert abs(e - eo) <= TOL * abs(eo) and rel_err(f, fo) <= TOL and rel_err(w, wo) <= TOL, (generic, zchunk)
+
+
 def test_twojmax_beyond_shared_memory_is_unsupported():
     """twojmax 12 needs more than 227 KB of shared memory per block: a clean error."""
     s = ipg.System(np.random.default_rng(0).uniform(0, 5, (10, 3)), ["A"] * 10, [5.0] * 3)
