@@ -1416,7 +1416,8 @@ struct Level {  // the Z triples (j1, j2, L) of level L
   int jjb[LMAX] = {};  // component
   double m[LMAX] = {}, mn[LMAX] = {};  // multiplier without / with bnorm_flag
 };
-constexpr Level level_of(int J, int L) {
+// Group g of G: the triples whose component b has b % G == g, with jjb = b / G.
+constexpr Level level_of(int J, int L, int G = 1, int g = 0) {
   Level T;
   int z = 0;
   for (int j1 = 0; j1 <= J; j1++)
@@ -1434,8 +1435,12 @@ constexpr Level level_of(int J, int L) {
           } else {
             jjb = idxb_of(J, j2, j, j1);
           }
+          if (jjb % G != g) {
+            z += zrow_count(j);
+            continue;
+          }
           T.z0[T.n] = z;
-          T.jjb[T.n] = jjb;
+          T.jjb[T.n] = jjb / G;
           T.mn[T.n] = mult;
           T.m[T.n] = (j1 > j) ? mult * (j1 + 1.0) / (j + 1.0) : mult;
           T.n++;
@@ -1476,100 +1481,155 @@ __global__ void __launch_bounds__(DB_T) k_snap_dupair(const __grid_constant__ Sn
   snapchain::all_chains_store<J>(G, dU + t, S.u_half, nq, dsave, DB_T, threadIdx.x);
 }
 
-// Triples Q.. of level L: c[Q] += Re(conj(d) Z_Q[e]) (zp: this pair's owner column at entry e)
-template <int J, int L, int Q, int NQ>
-__device__ __forceinline__ void dbcon_terms(double (&c)[NQ], double2 d, const double2* __restrict__ zp, int64_t zs) {
+// Triples Q.. of level L: c[Q] += Re(conj(d) Z_Q[e]) (zp: this pair's owner column at entry
+// e of the staged Z, ZS entries per Z index: compile-time offsets)
+template <int J, int L, int G, int g, int Q, int NQ, int ZS>
+__device__ __forceinline__ void dbcon_terms(double (&c)[NQ], double2 d, const double2* __restrict__ zp) {
   if constexpr (Q < NQ) {
-    constexpr int z0 = plaintab::level_of(J, L).z0[Q];
-    const double2 z = zp[z0 * zs];
+    constexpr int z0 = plaintab::level_of(J, L, G, g).z0[Q];
+    const double2 z = zp[z0 * ZS];
     c[Q] = fma(d.x, z.x, fma(d.y, z.y, c[Q]));
-    dbcon_terms<J, L, Q + 1, NQ>(c, d, zp, zs);
+    dbcon_terms<J, L, G, g, Q + 1, NQ, ZS>(c, d, zp);
   }
 }
 
-template <int J, int L, int Q, int NQ, int NB>
+template <int J, int L, int G, int g, int Q, int NQ, int NB>
 __device__ __forceinline__ void dbcon_add(double (&acc)[NB], const double (&c)[NQ], bool bnorm) {
   if constexpr (Q < NQ) {
-    constexpr plaintab::Level T = plaintab::level_of(J, L);
+    constexpr plaintab::Level T = plaintab::level_of(J, L, G, g);
     constexpr int b = T.jjb[Q];
     constexpr double m = T.m[Q], mn = T.mn[Q];
     acc[b] = fma(bnorm ? mn : m, c[Q], acc[b]);
-    dbcon_add<J, L, Q + 1, NQ, NB>(acc, c, bnorm);
+    dbcon_add<J, L, G, g, Q + 1, NQ, NB>(acc, c, bnorm);
   }
 }
 
 // Levels L.. of one component k: dk = dU_k of this pair at half-plane entry 0 (pair stride ps)
-template <int J, int L, int NB>
+constexpr int DBC_PF = 4;
+template <int J, int L, int G, int g, int NB, int ZS>
 __device__ __forceinline__ void dbcon_levels(double (&acc)[NB], const double2* __restrict__ dk, int64_t ps,
-                                             const double2* __restrict__ zc, int64_t zs, bool bnorm) {
-  if constexpr (L <= J) {
-    constexpr int NQ = plaintab::level_of(J, L).n;
+                                             const double2* __restrict__ zc, bool bnorm) {
+  if constexpr (L <= J && plaintab::level_of(J, L, G, g).n == 0) {
+    dbcon_levels<J, L + 1, G, g, NB, ZS>(acc, dk, ps, zc, bnorm);
+  } else if constexpr (L <= J) {
+    constexpr int NQ = plaintab::level_of(J, L, G, g).n;
     constexpr int nf = plaintab::nfull_c(L);
     constexpr int ne = nf + ((L & 1) ? 0 : 1);  // the middle element of an even level, weight 1/2
     double c[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) c[q] = 0.0;
     const double2* d = dk + (int64_t)snapchain::half_block(L) * ps;
+    // dU entries stream from device memory: DBC_PF of them are in flight ahead of their use
+    double2 buf[DBC_PF];
+#pragma unroll
+    for (int i = 0; i < DBC_PF; i++) buf[i] = i < ne ? d[i * ps] : make_double2(0.0, 0.0);
 #pragma unroll 1
-    for (int e = 0; e < ne; e++) {
-      double2 v = d[e * ps];
-      if (!(L & 1) && e == nf) {
-        v.x *= 0.5;
-        v.y *= 0.5;
+    for (int e0 = 0; e0 < ne; e0 += DBC_PF) {
+#pragma unroll
+      for (int i = 0; i < DBC_PF; i++) {
+        const int e = e0 + i;
+        if (e < ne) {
+          double2 v = buf[i];
+          if (e + DBC_PF < ne) buf[i] = d[(e + DBC_PF) * ps];
+          if (!(L & 1) && e == nf) {
+            v.x *= 0.5;
+            v.y *= 0.5;
+          }
+          dbcon_terms<J, L, G, g, 0, NQ, ZS>(c, v, zc + e * ZS);
+        }
       }
-      dbcon_terms<J, L, 0, NQ>(c, v, zc + e * zs, zs);
     }
-    dbcon_add<J, L, 0, NQ, NB>(acc, c, bnorm);
-    dbcon_levels<J, L + 1, NB>(acc, dk, ps, zc, zs, bnorm);
+    dbcon_add<J, L, G, g, 0, NQ, NB>(acc, c, bnorm);
+    dbcon_levels<J, L + 1, G, g, NB, ZS>(acc, dk, ps, zc, bnorm);
   }
 }
 
-// dbl[p][b][k] for pairs q0 .. q0+nq-1, whose owners lie in the Z chunk of atoms a0.. (stride zs)
-template <int J>
-__global__ void __launch_bounds__(DB_T) k_snap_dbcon(const __grid_constant__ SnapDev S, int64_t q0, int64_t nq,
-                                                     const int32_t* __restrict__ owner, int64_t a0, int64_t zs,
-                                                     const double2* __restrict__ Z, const double2* __restrict__ dU,
-                                                     double* __restrict__ dbl) {
+// dbl[p][b][k] for the pairs of owners b0 .. b1-1 (pairs q0.. in the dU buffer, stride ps),
+// the owners' Z in the chunk of atoms a0.. (stride zs).  A block takes DBC_OWN owners, stages
+// their Z in shared memory as [idxz][DBC_OWN] and runs one thread per (pair, component k,
+// group g of the components b = g, g + DBC_G, ...).  One group (all 55 accumulators of
+// twojmax 8 in one thread) measured fastest: more groups shorten the accumulators but repeat
+// every dU load per group, and the kernel is bound by the dU bytes in flight.
+constexpr int DBC_OWN = 4, DBC_P = 128, DBC_G = 1;
+
+template <int J, int g>
+__device__ __forceinline__ void dbcon_pair(const double2* __restrict__ dk, int64_t ps, const double2* __restrict__ zc,
+                                           bool bnorm, double* __restrict__ out) {
   constexpr int NB = plaintab::nb_of(J);
-  const int64_t t = (int64_t)blockIdx.x * DB_T + threadIdx.x;
-  if (t >= nq) return;
-  const int64_t p = q0 + t;
-  const double2* zc = Z + (owner[p] - a0);
-  const bool bnorm = S.bnorm_flag != 0;
-#pragma unroll 1
-  for (int k = 0; k < 3; k++) {
-    double acc[NB];
+  constexpr int NBG = (NB + DBC_G - 1) / DBC_G;
+  double acc[NBG];
 #pragma unroll
-    for (int b = 0; b < NB; b++) acc[b] = 0.0;
-    dbcon_levels<J, 0, NB>(acc, dU + (int64_t)k * S.u_half * nq + t, nq, zc, zs, bnorm);
-    double* out = dbl + (size_t)p * NB * 3 + k;
+  for (int b = 0; b < NBG; b++) acc[b] = 0.0;
+  dbcon_levels<J, 0, DBC_G, g, NBG, DBC_OWN>(acc, dk, ps, zc, bnorm);
 #pragma unroll
-    for (int b = 0; b < NB; b++) out[3 * b] = 2.0 * acc[b];
+  for (int b = 0; b < NBG; b++)
+    if (b * DBC_G + g < NB) out[3 * (b * DBC_G + g)] = 2.0 * acc[b];
+}
+
+template <int J, int g>
+__device__ __forceinline__ void dbcon_group(int gr, const double2* __restrict__ dk, int64_t ps,
+                                            const double2* __restrict__ zc, bool bnorm, double* __restrict__ out) {
+  if constexpr (g < DBC_G) {
+    if (gr == g)
+      dbcon_pair<J, g>(dk, ps, zc, bnorm, out);
+    else
+      dbcon_group<J, g + 1>(gr, dk, ps, zc, bnorm, out);
   }
 }
 
 template <int J>
-int plain_chunk_j(ipg_ctx* ctx, const SnapDev& S, int64_t q0, int64_t nq, const int32_t* owner, const int32_t* nbr,
-                  const double* rij, const int32_t* species, int64_t a0, int64_t zs, const double2* Z, double2* dU,
-                  double* dbl) {
+__global__ void __launch_bounds__(3 * DBC_G * DBC_P) k_snap_dbcon(const __grid_constant__ SnapDev S, int64_t b0,
+                                                                  int64_t b1, const int64_t* __restrict__ off,
+                                                                  const int32_t* __restrict__ owner, int64_t q0,
+                                                                  int64_t ps, int64_t a0, int64_t zs,
+                                                                  const double2* __restrict__ Z,
+                                                                  const double2* __restrict__ dU,
+                                                                  double* __restrict__ dbl) {
+  extern __shared__ double2 zsm[];  // [idxz_max][DBC_OWN]
+  constexpr int NB = plaintab::nb_of(J);
+  const int64_t o0 = b0 + (int64_t)blockIdx.x * DBC_OWN;
+  const int no = (int)((b1 - o0) < DBC_OWN ? (b1 - o0) : DBC_OWN);
+  for (int idx = threadIdx.x; idx < S.idxz_max * DBC_OWN; idx += blockDim.x) {
+    const int z = idx / DBC_OWN, o = idx - z * DBC_OWN;
+    zsm[idx] = o < no ? Z[(size_t)z * zs + (o0 + o - a0)] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const int64_t pb = off[o0], pe = off[o0 + no];
+  const int role = threadIdx.x / DBC_P, tl = threadIdx.x - role * DBC_P;  // warp-uniform role
+  const int k = role / DBC_G, gr = role - k * DBC_G;
+  const bool bnorm = S.bnorm_flag != 0;
+  for (int64_t p = pb + tl; p < pe; p += DBC_P)
+    dbcon_group<J, 0>(gr, dU + (int64_t)k * S.u_half * ps + (p - q0), ps, zsm + (owner[p] - o0), bnorm,
+                      dbl + (size_t)p * NB * 3 + k);
+}
+
+template <int J>
+int plain_chunk_j(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const int64_t* off, int64_t q0, int64_t nq,
+                  const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species, int64_t a0,
+                  int64_t zs, const double2* Z, double2* dU, double* dbl) {
   if (plaintab::nb_of(J) != S.K) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "plain chain tables disagree");
   const size_t sm = (size_t)4 * (J + 1) * DB_T * sizeof(double2);
   if (sm > 48 * 1024)
     CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dupair<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  IPG_TIMED_LAUNCH(ctx, "snap_dupair", k_snap_dupair<J>, nblk(nq, DB_T), DB_T, sm, S, q0, nq, owner, nbr, rij, species,
-                   dU);
-  IPG_TIMED_LAUNCH(ctx, "snap_dbcon", k_snap_dbcon<J>, nblk(nq, DB_T), DB_T, 0, S, q0, nq, owner, a0, zs, Z, dU, dbl);
+  if (nq > 0)
+    IPG_TIMED_LAUNCH(ctx, "snap_dupair", k_snap_dupair<J>, nblk(nq, DB_T), DB_T, sm, S, q0, nq, owner, nbr, rij,
+                     species, dU);
+  const size_t zsm = (size_t)S.idxz_max * DBC_OWN * sizeof(double2);
+  if (zsm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dbcon<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm));
+  IPG_TIMED_LAUNCH(ctx, "snap_dbcon", k_snap_dbcon<J>, nblk(b1 - b0, DBC_OWN), 3 * DBC_G * DBC_P, zsm, S, b0, b1, off, owner,
+                   q0, nq, a0, zs, Z, dU, dbl);
   return IPG_OK;
 }
 
-int plain_chunk(ipg_ctx* ctx, const SnapDev& S, int64_t q0, int64_t nq, const int32_t* owner, const int32_t* nbr,
-                const double* rij, const int32_t* species, int64_t a0, int64_t zs, const double2* Z, double2* dU,
-                double* dbl) {
-  if (nq == 0) return IPG_OK;
+int plain_chunk(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const int64_t* off, int64_t q0, int64_t nq,
+                const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species, int64_t a0,
+                int64_t zs, const double2* Z, double2* dU, double* dbl) {
+  if (b1 <= b0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return plain_chunk_j<JJ>(ctx, S, q0, nq, owner, nbr, rij, species, a0, zs, Z, dU, dbl);
+    return plain_chunk_j<JJ>(ctx, S, b0, b1, off, q0, nq, owner, nbr, rij, species, a0, zs, Z, dU, dbl);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
 #undef IPG_J
     default:
@@ -2320,8 +2380,8 @@ int zrows_config(ipg_ctx* ctx, const SnapDev& dev, int* ysm, int* per_sm) {
 }
 
 // Plain dB/dr path on the register chains: per chunk of atoms, Z (row-blocked kernel) and B,
-// E_i; per chunk of the pairs those atoms own, dU (k_snap_dupair) and dbl (k_snap_dbcon).
-// With more than one atom chunk the pair offsets are read back to size the pair chunks.
+// E_i; per run of those atoms whose pairs fit the dU buffer, dU (k_snap_dupair) and dbl
+// (k_snap_dbcon).  With more than one chunk of either kind the pair offsets are read back.
 int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const PairList& pl,
                  const int32_t* d_species, const double2* utot, double* B, double* Ei, double* dbl) {
   ipg_ctx* ctx = s->ctx;
@@ -2329,12 +2389,20 @@ int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const P
   IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
   if (np) IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
   const int64_t C = zrows_chunk(s, dev, n);
+  const int64_t dbytes = 3 * (int64_t)dev.u_half * (int64_t)sizeof(double2);
+  int64_t P = std::max<int64_t>(DBC_P, (((int64_t)4 << 30) / dbytes) / DBC_P * DBC_P);
+  if (s->du_chunk > 0) P = std::max<int64_t>(1, s->du_chunk);
+  std::vector<int64_t> hoff;
+  if (C < n || np > P) {
+    hoff.resize(n + 1);
+    CUDA_RET(ctx, cudaMemcpyAsync(hoff.data(), pl.d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int64_t a = 0; a < n; a++) P = std::max(P, hoff[a + 1] - hoff[a]);  // one atom's pairs always fit
+  }
+  P = std::max<int64_t>(1, std::min(P, np));
   double2 *Z, *dU;
   IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
-  const int64_t dbytes = 3 * (int64_t)dev.u_half * (int64_t)sizeof(double2);
-  int64_t P = std::max<int64_t>(DB_T, (((int64_t)4 << 30) / dbytes) / DB_T * DB_T);
-  if (s->du_chunk > 0) P = std::max<int64_t>(DB_T, s->du_chunk / DB_T * DB_T);
-  P = std::max<int64_t>(1, std::min(P, np));
   IPG_RET(scratch(ctx, "snap_dU", (size_t)P * 3 * dev.u_half + 1, &dU));
   int ysm, yper;
   IPG_RET(zrows_config(ctx, dev, &ysm, &yper));
@@ -2342,13 +2410,6 @@ int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const P
   CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_bdesc, cudaFuncAttributeMaxDynamicSharedMemorySize, bsm));
   int bper = 1;
   CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bper, k_snap_bdesc, GB_WARPS * 32, bsm));
-  std::vector<int64_t> hoff;
-  if (C < n) {
-    hoff.resize(n + 1);
-    CUDA_RET(ctx, cudaMemcpyAsync(hoff.data(), pl.d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
-  }
   for (int64_t a0 = 0; a0 < n; a0 += C) {
     const int64_t nc = std::min(C, n - a0);
     const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
@@ -2358,9 +2419,17 @@ int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const P
     const int64_t bg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, bper));
     IPG_TIMED_LAUNCH(ctx, "snap_bdesc", k_snap_bdesc, (unsigned)bg, GB_WARPS * 32, bsm, dev, a0, nc, d_species, Z,
                      utot, B, Ei);
-    const int64_t pb = C < n ? hoff[a0] : 0, pe = C < n ? hoff[a0 + nc] : np;
-    for (int64_t q0 = pb; q0 < pe; q0 += P)
-      IPG_RET(plain_chunk(ctx, dev, q0, std::min(P, pe - q0), owner, pl.d_j, pl.d_r, d_species, a0, nc, Z, dU, dbl));
+    for (int64_t b0 = a0; b0 < a0 + nc;) {
+      int64_t b1 = a0 + nc, q0 = 0, nq = np;
+      if (!hoff.empty()) {  // the longest run of atoms from b0 whose pairs fit P
+        b1 = std::upper_bound(hoff.begin() + b0 + 1, hoff.begin() + a0 + nc + 1, hoff[b0] + P) - hoff.begin() - 1;
+        b1 = std::max(b1, b0 + 1);
+        q0 = hoff[b0];
+        nq = hoff[b1] - q0;
+      }
+      IPG_RET(plain_chunk(ctx, dev, b0, b1, pl.d_off, q0, nq, owner, pl.d_j, pl.d_r, d_species, a0, nc, Z, dU, dbl));
+      b0 = b1;
+    }
   }
   return IPG_OK;
 }
