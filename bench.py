@@ -189,6 +189,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="size of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and pair-workload lines")
+    ap.add_argument("--extras", default="skin,batch,plain,vjp,desc,pair",
+                    help="comma list of the extra measurements to run (skin, batch, plain, vjp, desc, pair)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-tune", action="store_true", help="skip the (untimed) autotuner and use the default kernel "
                     "configuration, e.g. so that a profiler's launch list holds only the measured steps")
@@ -251,6 +253,11 @@ def main():
                                                    L.ctypes.data_as(vp), beta_b.ctypes.data_as(vp), 0.0, mode,
                                                    vp(E_d.data_ptr()), vp(F_d.data_ptr()), vp(W_d.data_ptr())))
 
+    # per-kernel device timing (ipg_timing_read names); snap_zrows .. snap_gbeta are the plain,
+    # descriptor and pullback kernels of the register-chain path
+    TIMED_KERNELS = ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval",
+                     "snap_zrows", "snap_bdesc", "snap_dupair", "snap_dbcon", "snap_vsum", "snap_gbeta")
+
     def timed(fn, steps, kernel_timing=False):
         for _ in range(args.warmup):
             fn()
@@ -259,7 +266,7 @@ def main():
         torch.cuda.synchronize()
         if kernel_timing:
             ctx.timing(True)
-            for k in ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
+            for k in TIMED_KERNELS:
                 ctx.timing_read(k)
         l0 = ctx.launch_count()
         evs = []
@@ -277,7 +284,7 @@ def main():
         launches = ctx.launch_count() - l0
         kt = {}
         if kernel_timing:
-            for k in ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval"):
+            for k in TIMED_KERNELS:
                 kt[k] = ctx.timing_read(k)
             ctx.timing(False)
         if dist:
@@ -348,7 +355,8 @@ def main():
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "gpu_launches": int(launches),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items() if v[1]}}
 
-    if not args.no_extras:
+    extras = set() if args.no_extras else set(x.strip() for x in args.extras.split(",") if x.strip())
+    if "skin" in extras:
         # MD loops: the neighbor list reused under a 0.3 A Verlet skin (positions unchanged here,
         # so every timed step takes the reuse path: re-measure + filter instead of the cell walk)
         snap.set_skin(0.3)
@@ -356,6 +364,7 @@ def main():
         snap.set_skin(0.0)
         line["adjoint_value_skin_reuse"] = world * n * args.steps / (ms_skin * 1e-3)
         line["skin_kernel_ms_per_step"] = {k: v[0] / args.steps for k, v in kts.items() if v[1]}
+    if "batch" in extras:
         # Batched: 512 configurations (32..2000 atoms, crystals and liquids, ~0.54 M atoms) in one
         # evaluation, eager and as a CUDA-graph replay (ipg_snap_batch_energy_forces_dev), and one
         # force-matching training step (loss and dL/dbeta, host buffers)
@@ -373,11 +382,28 @@ def main():
                             "graph_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_bg * 1e-3),
                             "loss_grad_ms": ms_bl / 2}
         del db
+    if "plain" in extras:
         ms_plain, _, ktp = timed(lambda: step(SNAP_PLAIN), max(2, args.steps // 2), kernel_timing=True)
         plain_value = world * n * max(2, args.steps // 2) / (ms_plain * 1e-3)
         line["plain_value"] = plain_value
         line["adjoint_over_plain"] = value / plain_value
         line["plain_kernel_ms_per_step"] = {k: v[0] / max(2, args.steps // 2) for k, v in ktp.items() if v[1]}
+    if "vjp" in extras:
+        # beta pullback (force-matching gradient, ipg_snap_vjp_beta through host buffers) and the
+        # local descriptors (ipg_snap_descriptors) of the same 54,000 atoms
+        gF = np.random.default_rng(5).normal(size=(n, 3))
+        ms_v, _, ktv = timed(lambda: snap.vjp_beta(system, 0.5, gF), max(2, args.steps // 5), kernel_timing=True)
+        ctx.set_stream(stream.cuda_stream)
+        line["vjp_beta"] = {"ms_per_call": ms_v / max(2, args.steps // 5),
+                            "kernel_ms_per_call": {k: v[0] / max(2, args.steps // 5) for k, v in ktv.items() if v[1]}}
+    if "desc" in extras:
+        ms_d, _, ktd = timed(lambda: ipg.compute_local_descriptors(system, snap), max(2, args.steps // 5),
+                             kernel_timing=True)
+        ctx.set_stream(stream.cuda_stream)
+        line["descriptors"] = {"ms_per_call": ms_d / max(2, args.steps // 5),
+                               "kernel_ms_per_call": {k: v[0] / max(2, args.steps // 5) for k, v in ktd.items()
+                                                      if v[1]}}
+    if "pair" in extras:
         pair = {}
         for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000()), ("lc_scaled", W.lc32000(cells=101))):
             pairs = ipg.api.neighbor_count(s2, p2.get_rcutoff(), ctx=ctx)
