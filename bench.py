@@ -256,7 +256,7 @@ def main():
     # per-kernel device timing (ipg_timing_read names); snap_zrows .. snap_gbeta are the plain,
     # descriptor and pullback kernels of the register-chain path
     TIMED_KERNELS = ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval",
-                     "snap_zrows", "snap_bdesc", "snap_dupair", "snap_dbcon", "snap_vsum", "snap_gbeta")
+                     "snap_zrows", "snap_bdesc", "snap_dbfused", "snap_vsum", "snap_gbeta")
 
     def timed(fn, steps, kernel_timing=False):
         for _ in range(args.warmup):

@@ -1382,10 +1382,9 @@ __global__ void __launch_bounds__(GB_WARPS * 32) k_snap_bdesc(const __grid_const
 // compute_b.jl:207-400).  Every Z triple z belongs to one component jjb(z) with one
 // multiplier m(z) (its coincidence count and, unnormalised, (j1+1)/(j+1)), the same pair the
 // Y coefficients use, so dB[b][k] = 2 sum_{z: jjb(z) = b} m(z) sum_half w Re(conj(dU_k) Z_z).
-// k_snap_dupair writes each pair's dU (all chains in one thread) to a pair-major buffer,
-// k_snap_dbcon contracts it with the owner's Z: one thread per pair, the Z triples of a level
-// unrolled at compile time (their tables below are constexpr restatements of the host's
-// idxz / idxb / y_jjb / y_mult loops), one component k per pass.
+// k_snap_dbfused computes each pair's dU row by row on the register chains and contracts the
+// rows with the owner's Z, the Z triples of a level unrolled at compile time (their tables
+// below are constexpr restatements of the host's idxz / idxb / y_jjb / y_mult loops).
 namespace plaintab {
 constexpr int zrow_count(int j) { return (j / 2 + 1) * (j + 1); }
 constexpr int imin(int a, int b) { return a < b ? a : b; }
@@ -1451,185 +1450,219 @@ constexpr Level level_of(int J, int L, int G = 1, int g = 0) {
 }
 }  // namespace plaintab
 
-constexpr int DB_T = 128;  // threads (pairs) per block of the plain chain kernels
+// Plain dB/dr, one block per owner atom, warp-specialised: warp 0 (the producer) runs every
+// chain of up to 32 of the owner's pairs, one pair per lane, and hands each half-plane row of
+// dU/dr to warps 1..3 (the consumers, one per component k) through a double-buffered row
+// buffer in shared memory; each consumer lane contracts the rows of its pair with the owner's
+// Z (staged in shared memory) into the 55 accumulators of dB[b][k].  dU never leaves the SM.
+// Hand-off by named barriers (ids 1, 2: row buffer b full; 3, 4: row buffer b free), DBF_T
+// threads each: the producer arrives on "full" and waits on "free", the consumers the
+// reverse; both sides walk the same row sequence, so every barrier generation completes.
+constexpr int DBF_T = 128;
+
+template <int ID>
+__device__ __forceinline__ void nbar_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(DBF_T) : "memory");
+}
+template <int ID>
+__device__ __forceinline__ void nbar_arrive() {
+  asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(DBF_T) : "memory");
+}
+// row buffer b: "full" is barrier 1 + b, "free" is barrier 3 + b (immediate ids)
+__device__ __forceinline__ void row_full_arrive(int b) { b ? nbar_arrive<2>() : nbar_arrive<1>(); }
+__device__ __forceinline__ void row_full_wait(int b) { b ? nbar_sync<2>() : nbar_sync<1>(); }
+__device__ __forceinline__ void row_free_arrive(int b) { b ? nbar_arrive<4>() : nbar_arrive<3>(); }
+__device__ __forceinline__ void row_free_wait(int b) { b ? nbar_sync<4>() : nbar_sync<3>(); }
 
 template <int J>
-__global__ void __launch_bounds__(DB_T) k_snap_dupair(const __grid_constant__ SnapDev S, int64_t q0, int64_t nq,
-                                                      const int32_t* __restrict__ owner,
-                                                      const int32_t* __restrict__ nbr,
-                                                      const double* __restrict__ rij,
-                                                      const int32_t* __restrict__ species,
-                                                      double2* __restrict__ dU) {
-  extern __shared__ double2 dsave[];  // saved start rows [4 (J+1)][DB_T]
-  const int64_t t = (int64_t)blockIdx.x * DB_T + threadIdx.x;
-  if (t >= nq) return;  // no block-level synchronisation below
-  const int64_t p = q0 + t;
-  const int si = clamp_sp(species[owner[p]], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
-  const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
-  PairGeom PG;
-  geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
-  snapchain::Geom G;
-  G.a = PG.a;
-  G.b = PG.b;
-  G.sfac = PG.sfac;
+struct DbRowEmit {  // producer side: dU_k[ma] of this lane's pair into row buffer (r & 1)
+  const snapchain::Geom& G;
+  double2* rows;  // [2][3][J+1][32]
+  int lane, r;
+  template <int j>
+  __device__ __forceinline__ void row(const snapchain::Chain<J>& s, int mb) {
+    const int b = r & 1;
+    row_free_wait(b);  // the consumers are done with row r - 2
+    double2* rb = rows + b * 3 * (J + 1) * 32 + lane;
+    const int last = (2 * mb == j) ? mb : j;
 #pragma unroll
-  for (int k = 0; k < 3; k++) {
-    G.da[k] = PG.da[k];
-    G.db[k] = PG.db[k];
-    G.dsu[k] = PG.dsfac * PG.u[k];
+    for (int ma = 0; ma <= j; ma++) {
+      if (ma > last) break;
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        rb[(k * (J + 1) + ma) * 32] = make_double2(fma(G.dsu[k], s.u[ma].x, G.sfac * s.d[k][ma].x),
+                                                   fma(G.dsu[k], s.u[ma].y, G.sfac * s.d[k][ma].y));
+    }
+    row_full_arrive(b);
+    r++;
   }
-  snapchain::all_chains_store<J>(G, dU + t, S.u_half, nq, dsave, DB_T, threadIdx.x);
-}
+};
 
-// Triples Q.. of level L: c[Q] += Re(conj(d) Z_Q[e]) (zp: this pair's owner column at entry
-// e of the staged Z, ZS entries per Z index: compile-time offsets)
-template <int J, int L, int G, int g, int Q, int NQ, int ZS>
-__device__ __forceinline__ void dbcon_terms(double (&c)[NQ], double2 d, const double2* __restrict__ zp) {
+// consumer side: row mb of level L, d = this pair's dU_k of the row (weights applied)
+template <int J, int L, int Q, int NQ, int NB>
+__device__ __forceinline__ void dbf_terms(double (&acc)[NB], const double2 (&d)[L + 1], const double2* __restrict__ zr,
+                                          int last, bool bnorm) {
   if constexpr (Q < NQ) {
-    constexpr int z0 = plaintab::level_of(J, L, G, g).z0[Q];
-    const double2 z = zp[z0 * ZS];
-    c[Q] = fma(d.x, z.x, fma(d.y, z.y, c[Q]));
-    dbcon_terms<J, L, G, g, Q + 1, NQ, ZS>(c, d, zp);
-  }
-}
-
-template <int J, int L, int G, int g, int Q, int NQ, int NB>
-__device__ __forceinline__ void dbcon_add(double (&acc)[NB], const double (&c)[NQ], bool bnorm) {
-  if constexpr (Q < NQ) {
-    constexpr plaintab::Level T = plaintab::level_of(J, L, G, g);
-    constexpr int b = T.jjb[Q];
+    constexpr plaintab::Level T = plaintab::level_of(J, L);
+    constexpr int z0 = T.z0[Q], b = T.jjb[Q];
     constexpr double m = T.m[Q], mn = T.mn[Q];
-    acc[b] = fma(bnorm ? mn : m, c[Q], acc[b]);
-    dbcon_add<J, L, G, g, Q + 1, NQ, NB>(acc, c, bnorm);
+    double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+    for (int ma = 0; ma <= L; ma++) {
+      if (ma > last) break;
+      const double2 z = zr[z0 + ma];
+      c0 = fma(d[ma].x, z.x, c0);
+      c1 = fma(d[ma].y, z.y, c1);
+    }
+    acc[b] = fma(bnorm ? mn : m, c0 + c1, acc[b]);
+    dbf_terms<J, L, Q + 1, NQ, NB>(acc, d, zr, last, bnorm);
   }
 }
 
-// Levels L.. of one component k: dk = dU_k of this pair at half-plane entry 0 (pair stride ps)
-constexpr int DBC_PF = 4;
-template <int J, int L, int G, int g, int NB, int ZS>
-__device__ __forceinline__ void dbcon_levels(double (&acc)[NB], const double2* __restrict__ dk, int64_t ps,
-                                             const double2* __restrict__ zc, bool bnorm) {
-  if constexpr (L <= J && plaintab::level_of(J, L, G, g).n == 0) {
-    dbcon_levels<J, L + 1, G, g, NB, ZS>(acc, dk, ps, zc, bnorm);
-  } else if constexpr (L <= J) {
-    constexpr int NQ = plaintab::level_of(J, L, G, g).n;
-    constexpr int nf = plaintab::nfull_c(L);
-    constexpr int ne = nf + ((L & 1) ? 0 : 1);  // the middle element of an even level, weight 1/2
-    double c[NQ];
+template <int J, int L, int NB>
+__device__ __forceinline__ void dbf_row(double (&acc)[NB], int mb, const double2* __restrict__ rb,
+                                        const double2* __restrict__ zo, bool bnorm) {
+  if constexpr (L <= J) {
+    const int last = (2 * mb == L) ? mb : L;
+    double2 d[L + 1];
 #pragma unroll
-    for (int q = 0; q < NQ; q++) c[q] = 0.0;
-    const double2* d = dk + (int64_t)snapchain::half_block(L) * ps;
-    // dU entries stream from device memory: DBC_PF of them are in flight ahead of their use
-    double2 buf[DBC_PF];
-#pragma unroll
-    for (int i = 0; i < DBC_PF; i++) buf[i] = i < ne ? d[i * ps] : make_double2(0.0, 0.0);
-#pragma unroll 1
-    for (int e0 = 0; e0 < ne; e0 += DBC_PF) {
-#pragma unroll
-      for (int i = 0; i < DBC_PF; i++) {
-        const int e = e0 + i;
-        if (e < ne) {
-          double2 v = buf[i];
-          if (e + DBC_PF < ne) buf[i] = d[(e + DBC_PF) * ps];
-          if (!(L & 1) && e == nf) {
-            v.x *= 0.5;
-            v.y *= 0.5;
-          }
-          dbcon_terms<J, L, G, g, 0, NQ, ZS>(c, v, zc + e * ZS);
-        }
+    for (int ma = 0; ma <= L; ma++) {
+      d[ma] = ma <= last ? rb[ma * 32] : make_double2(0.0, 0.0);
+      if (2 * mb == L && ma == mb) {  // the middle element of an even level: weight 1/2
+        d[ma].x *= 0.5;
+        d[ma].y *= 0.5;
       }
     }
-    dbcon_add<J, L, G, g, 0, NQ, NB>(acc, c, bnorm);
-    dbcon_levels<J, L + 1, G, g, NB, ZS>(acc, dk, ps, zc, bnorm);
+    constexpr int NQ = plaintab::level_of(J, L).n;
+    dbf_terms<J, L, 0, NQ, NB>(acc, d, zo + mb * (L + 1), last, bnorm);
   }
 }
 
-// dbl[p][b][k] for the pairs of owners b0 .. b1-1 (pairs q0.. in the dU buffer, stride ps),
-// the owners' Z in the chunk of atoms a0.. (stride zs).  A block takes DBC_OWN owners, stages
-// their Z in shared memory as [idxz][DBC_OWN] and runs one thread per (pair, component k,
-// group g of the components b = g, g + DBC_G, ...).  One group (all 55 accumulators of
-// twojmax 8 in one thread) measured fastest: more groups shorten the accumulators but repeat
-// every dU load per group, and the kernel is bound by the dU bytes in flight.
-constexpr int DBC_OWN = 4, DBC_P = 128, DBC_G = 1;
-
-template <int J, int g>
-__device__ __forceinline__ void dbcon_pair(const double2* __restrict__ dk, int64_t ps, const double2* __restrict__ zc,
-                                           bool bnorm, double* __restrict__ out) {
-  constexpr int NB = plaintab::nb_of(J);
-  constexpr int NBG = (NB + DBC_G - 1) / DBC_G;
-  double acc[NBG];
-#pragma unroll
-  for (int b = 0; b < NBG; b++) acc[b] = 0.0;
-  dbcon_levels<J, 0, DBC_G, g, NBG, DBC_OWN>(acc, dk, ps, zc, bnorm);
-#pragma unroll
-  for (int b = 0; b < NBG; b++)
-    if (b * DBC_G + g < NB) out[3 * (b * DBC_G + g)] = 2.0 * acc[b];
-}
-
-template <int J, int g>
-__device__ __forceinline__ void dbcon_group(int gr, const double2* __restrict__ dk, int64_t ps,
-                                            const double2* __restrict__ zc, bool bnorm, double* __restrict__ out) {
-  if constexpr (g < DBC_G) {
-    if (gr == g)
-      dbcon_pair<J, g>(dk, ps, zc, bnorm, out);
-    else
-      dbcon_group<J, g + 1>(gr, dk, ps, zc, bnorm, out);
+template <int J, int NB>
+__device__ __forceinline__ void dbf_consume(double (&acc)[NB], int j, int mb, const double2* __restrict__ rb,
+                                            const double2* __restrict__ zo, bool bnorm) {
+  switch (j) {
+#define IPG_L(LL) \
+  case LL:        \
+    dbf_row<J, LL, NB>(acc, mb, rb, zo, bnorm); \
+    break;
+    IPG_L(0) IPG_L(1) IPG_L(2) IPG_L(3) IPG_L(4) IPG_L(5) IPG_L(6) IPG_L(7) IPG_L(8)
+#undef IPG_L
+    default:
+      break;
   }
 }
 
+// dbl[p][b][k] for the pairs of owners b0 .. b1-1; their Z in the chunk of atoms a0.. (stride zs)
 template <int J>
-__global__ void __launch_bounds__(3 * DBC_G * DBC_P) k_snap_dbcon(const __grid_constant__ SnapDev S, int64_t b0,
-                                                                  int64_t b1, const int64_t* __restrict__ off,
-                                                                  const int32_t* __restrict__ owner, int64_t q0,
-                                                                  int64_t ps, int64_t a0, int64_t zs,
-                                                                  const double2* __restrict__ Z,
-                                                                  const double2* __restrict__ dU,
-                                                                  double* __restrict__ dbl) {
-  extern __shared__ double2 zsm[];  // [idxz_max][DBC_OWN]
+__global__ void __launch_bounds__(DBF_T, 2) k_snap_dbfused(const __grid_constant__ SnapDev S, int64_t b0,
+                                                           const int64_t* __restrict__ off,
+                                                           const int32_t* __restrict__ nbr,
+                                                           const double* __restrict__ rij,
+                                                           const int32_t* __restrict__ species, int64_t a0,
+                                                           int64_t zs, const double2* __restrict__ Z,
+                                                           double* __restrict__ dbl) {
+  static_assert(J <= YR_MAX_J, "fused plain kernel covers twojmax <= 8");
   constexpr int NB = plaintab::nb_of(J);
-  const int64_t o0 = b0 + (int64_t)blockIdx.x * DBC_OWN;
-  const int no = (int)((b1 - o0) < DBC_OWN ? (b1 - o0) : DBC_OWN);
-  for (int idx = threadIdx.x; idx < S.idxz_max * DBC_OWN; idx += blockDim.x) {
-    const int z = idx / DBC_OWN, o = idx - z * DBC_OWN;
-    zsm[idx] = o < no ? Z[(size_t)z * zs + (o0 + o - a0)] : make_double2(0.0, 0.0);
-  }
+  extern __shared__ __align__(16) unsigned char fsm[];
+  double2* zo = reinterpret_cast<double2*>(fsm);                 // [idxz_max] the owner's Z
+  double2* rows = zo + ((S.idxz_max + 1) & ~1);                  // [2][3][J+1][32]
+  double2* save = rows + 2 * 3 * (J + 1) * 32;                   // [4 (J+1)][32] producer start rows
+  const int64_t o = b0 + blockIdx.x;
+  for (int z = threadIdx.x; z < S.idxz_max; z += DBF_T) zo[z] = Z[(size_t)z * zs + (o - a0)];
   __syncthreads();
-  const int64_t pb = off[o0], pe = off[o0 + no];
-  const int role = threadIdx.x / DBC_P, tl = threadIdx.x - role * DBC_P;  // warp-uniform role
-  const int k = role / DBC_G, gr = role - k * DBC_G;
-  const bool bnorm = S.bnorm_flag != 0;
-  for (int64_t p = pb + tl; p < pe; p += DBC_P)
-    dbcon_group<J, 0>(gr, dU + (int64_t)k * S.u_half * ps + (p - q0), ps, zsm + (owner[p] - o0), bnorm,
-                      dbl + (size_t)p * NB * 3 + k);
+  const int64_t pb = off[o], pe = off[o + 1];
+  const int npass = (int)((pe - pb + 31) / 32);  // block-uniform
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (npass == 0) return;
+  if (warp == 0) {
+    const int si = clamp_sp(species[o], S.nsp);
+    int r = 0;  // rows handed over so far
+    for (int pass = 0; pass < npass; pass++) {
+      const int64_t p = pb + pass * 32 + lane;
+      snapchain::Geom G;  // idle lanes: the identity rotation with zero weights
+      G.a = make_double2(1.0, 0.0);
+      G.b = make_double2(0.0, 0.0);
+      G.sfac = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        G.da[k] = make_double2(0.0, 0.0);
+        G.db[k] = make_double2(0.0, 0.0);
+        G.dsu[k] = 0.0;
+      }
+      if (p < pe) {
+        const int sj = clamp_sp(species[nbr[p]], S.nsp);
+        const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+        PairGeom PG;
+        geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+        G.a = PG.a;
+        G.b = PG.b;
+        G.sfac = PG.sfac;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          G.da[k] = PG.da[k];
+          G.db[k] = PG.db[k];
+          G.dsu[k] = PG.dsfac * PG.u[k];
+        }
+      }
+      DbRowEmit<J> e{G, rows, lane, r};
+      snapchain::all_chains_rows<J>(G, e, save, 32, lane);
+      r = e.r;
+    }
+    row_free_wait(r & 1);  // the consumers' last two "free" arrivals
+    row_free_wait((r + 1) & 1);
+  } else {
+    const int k = warp - 1;
+    const bool bnorm = S.bnorm_flag != 0;
+    row_free_arrive(0);  // both row buffers start free
+    row_free_arrive(1);
+    int r = 0;
+    for (int pass = 0; pass < npass; pass++) {
+      double acc[NB];
+#pragma unroll
+      for (int b = 0; b < NB; b++) acc[b] = 0.0;
+      for (int mb = -1; mb <= J / 2; mb++) {  // mb = -1: the row (0, 0)
+        const int j0 = mb < 0 ? 0 : (mb == 0 ? 1 : 2 * mb), j1 = mb < 0 ? 0 : J;
+        for (int j = j0; j <= j1; j++, r++) {
+          const int bsel = r & 1;
+          row_full_wait(bsel);
+          dbf_consume<J, NB>(acc, j, mb < 0 ? 0 : mb, rows + (bsel * 3 + k) * (J + 1) * 32 + lane, zo, bnorm);
+          row_free_arrive(bsel);
+        }
+      }
+      const int64_t p = pb + pass * 32 + lane;
+      if (p < pe) {
+        double* out = dbl + (size_t)p * NB * 3 + k;
+#pragma unroll
+        for (int b = 0; b < NB; b++) out[3 * b] = 2.0 * acc[b];
+      }
+    }
+  }
 }
 
 template <int J>
-int plain_chunk_j(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const int64_t* off, int64_t q0, int64_t nq,
-                  const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species, int64_t a0,
-                  int64_t zs, const double2* Z, double2* dU, double* dbl) {
-  if (plaintab::nb_of(J) != S.K) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "plain chain tables disagree");
-  const size_t sm = (size_t)4 * (J + 1) * DB_T * sizeof(double2);
-  if (sm > 48 * 1024)
-    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dupair<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  if (nq > 0)
-    IPG_TIMED_LAUNCH(ctx, "snap_dupair", k_snap_dupair<J>, nblk(nq, DB_T), DB_T, sm, S, q0, nq, owner, nbr, rij,
-                     species, dU);
-  const size_t zsm = (size_t)S.idxz_max * DBC_OWN * sizeof(double2);
-  if (zsm > 48 * 1024)
-    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dbcon<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm));
-  IPG_TIMED_LAUNCH(ctx, "snap_dbcon", k_snap_dbcon<J>, nblk(b1 - b0, DBC_OWN), 3 * DBC_G * DBC_P, zsm, S, b0, b1, off, owner,
-                   q0, nq, a0, zs, Z, dU, dbl);
-  return IPG_OK;
+int plain_fused_j(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const int64_t* off, const int32_t* nbr,
+                  const double* rij, const int32_t* species, int64_t a0, int64_t zs, const double2* Z, double* dbl) {
+  if constexpr (J > YR_MAX_J) {
+    return IPG_ERR_UNSUPPORTED;
+  } else {
+    if (plaintab::nb_of(J) != S.K) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "plain chain tables disagree");
+    const size_t sm = ((size_t)((S.idxz_max + 1) & ~1) + 2 * 3 * (J + 1) * 32 + 4 * (J + 1) * 32) * sizeof(double2);
+    if (sm > 48 * 1024)
+      CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dbfused<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IPG_TIMED_LAUNCH(ctx, "snap_dbfused", k_snap_dbfused<J>, (unsigned)(b1 - b0), DBF_T, sm, S, b0, off, nbr, rij,
+                     species, a0, zs, Z, dbl);
+    return IPG_OK;
+  }
 }
 
-int plain_chunk(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const int64_t* off, int64_t q0, int64_t nq,
-                const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species, int64_t a0,
-                int64_t zs, const double2* Z, double2* dU, double* dbl) {
+int plain_fused(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const int64_t* off, const int32_t* nbr,
+                const double* rij, const int32_t* species, int64_t a0, int64_t zs, const double2* Z, double* dbl) {
   if (b1 <= b0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return plain_chunk_j<JJ>(ctx, S, b0, b1, off, q0, nq, owner, nbr, rij, species, a0, zs, Z, dU, dbl);
+    return plain_fused_j<JJ>(ctx, S, b0, b1, off, nbr, rij, species, a0, zs, Z, dbl);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
 #undef IPG_J
     default:
@@ -2096,7 +2129,6 @@ struct ipg_snap {
   int utot_warps = 4;       // atoms (warps) per block of the per-chain Utot kernels
   bool utot_split = false;  // Utot: one launch per chain (k_snap_utot) instead of k_snap_utot_all
   int64_t vjp_chunk = 0;     // atoms per Z chunk (0: about 4 GiB of Z)
-  int64_t du_chunk = 0;      // pairs per dU chunk of the plain path (0: about 4 GiB of dU)
   bool generic_plain = false;  // plain path: the per-atom block kernel (IPG_GENERIC_PLAIN=1)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
   std::vector<double> beta_host;  // last uploaded beta
@@ -2379,31 +2411,14 @@ int zrows_config(ipg_ctx* ctx, const SnapDev& dev, int* ysm, int* per_sm) {
   return IPG_OK;
 }
 
-// Plain dB/dr path on the register chains: per chunk of atoms, Z (row-blocked kernel) and B,
-// E_i; per run of those atoms whose pairs fit the dU buffer, dU (k_snap_dupair) and dbl
-// (k_snap_dbcon).  With more than one chunk of either kind the pair offsets are read back.
-int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const PairList& pl,
-                 const int32_t* d_species, const double2* utot, double* B, double* Ei, double* dbl) {
+// Plain dB/dr path on the register chains: per chunk of atoms, Z (row-blocked kernel), B and
+// E_i (k_snap_bdesc), then dbl of the pairs those atoms own (k_snap_dbfused).
+int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, const PairList& pl, const int32_t* d_species,
+                 const double2* utot, double* B, double* Ei, double* dbl) {
   ipg_ctx* ctx = s->ctx;
-  int32_t* owner;
-  IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
-  if (np) IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
   const int64_t C = zrows_chunk(s, dev, n);
-  const int64_t dbytes = 3 * (int64_t)dev.u_half * (int64_t)sizeof(double2);
-  int64_t P = std::max<int64_t>(DBC_P, (((int64_t)4 << 30) / dbytes) / DBC_P * DBC_P);
-  if (s->du_chunk > 0) P = std::max<int64_t>(1, s->du_chunk);
-  std::vector<int64_t> hoff;
-  if (C < n || np > P) {
-    hoff.resize(n + 1);
-    CUDA_RET(ctx, cudaMemcpyAsync(hoff.data(), pl.d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
-    for (int64_t a = 0; a < n; a++) P = std::max(P, hoff[a + 1] - hoff[a]);  // one atom's pairs always fit
-  }
-  P = std::max<int64_t>(1, std::min(P, np));
-  double2 *Z, *dU;
+  double2* Z;
   IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
-  IPG_RET(scratch(ctx, "snap_dU", (size_t)P * 3 * dev.u_half + 1, &dU));
   int ysm, yper;
   IPG_RET(zrows_config(ctx, dev, &ysm, &yper));
   const int bsm = (int)((size_t)dev.u_half * YS_ATOMS * sizeof(double2) + (size_t)dev.K * YS_ATOMS * 8);
@@ -2419,17 +2434,7 @@ int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, int64_t np, const P
     const int64_t bg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, bper));
     IPG_TIMED_LAUNCH(ctx, "snap_bdesc", k_snap_bdesc, (unsigned)bg, GB_WARPS * 32, bsm, dev, a0, nc, d_species, Z,
                      utot, B, Ei);
-    for (int64_t b0 = a0; b0 < a0 + nc;) {
-      int64_t b1 = a0 + nc, q0 = 0, nq = np;
-      if (!hoff.empty()) {  // the longest run of atoms from b0 whose pairs fit P
-        b1 = std::upper_bound(hoff.begin() + b0 + 1, hoff.begin() + a0 + nc + 1, hoff[b0] + P) - hoff.begin() - 1;
-        b1 = std::max(b1, b0 + 1);
-        q0 = hoff[b0];
-        nq = hoff[b1] - q0;
-      }
-      IPG_RET(plain_chunk(ctx, dev, b0, b1, pl.d_off, q0, nq, owner, pl.d_j, pl.d_r, d_species, a0, nc, Z, dU, dbl));
-      b0 = b1;
-    }
+    IPG_RET(plain_fused(ctx, dev, a0, a0 + nc, pl.d_off, pl.d_j, pl.d_r, d_species, a0, nc, Z, dbl));
   }
   return IPG_OK;
 }
@@ -2511,7 +2516,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_RET(scratch(ctx, "snap_dbl", (size_t)np * K * 3 + 3, &dbl));
     io.dbl = dbl;
     if (n && chains && dev.J <= YR_MAX_J && s->h.yconst_ok && cap == 0 && !s->generic_plain)
-      IPG_RET(plain_chains(s, dev, n, np, pl, d_species, io.utot_in, out.B, Ei, dbl));
+      IPG_RET(plain_chains(s, dev, n, pl, d_species, io.utot_in, out.B, Ei, dbl));
     else if (n)
       IPG_RET(launch_atoms<MODE_PLAIN>(s, dev, io, n, nullptr));
     if (out.F || out.W6) {
@@ -2845,7 +2850,6 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_Y_ENTRIES")) s->y_entries = g[0] == '1';
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
-  if (const char* g = getenv("IPG_DU_CHUNK")) s->du_chunk = std::max<int64_t>(0, atoll(g));
   if (const char* g = getenv("IPG_GENERIC_PLAIN")) s->generic_plain = g[0] == '1';
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;

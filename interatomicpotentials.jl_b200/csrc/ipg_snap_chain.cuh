@@ -696,43 +696,26 @@ __device__ __forceinline__ void all_chains_v(const Geom& G, double A, const doub
 
 }  // namespace snapchain
 
+
 namespace snapchain {
 
-// ---- dU/dr of one neighbor, every half-plane entry stored (the plain dB/dr path) ----------
-// Row mb of level j: dU_k[ma] = dsfac uhat_k u[ma] + sfac du_k[ma] (compute_duarray,
-// compute_ui.jl:186-326, with the switching function folded in) for ma up to the middle
-// element, to out[(k * uh + h) * ps] (h the half-plane index; ps the pair stride).
-template <int J, int j>
-__device__ __forceinline__ void store_rt(const Chain<J>& s, const Geom& G, int mb, double2* __restrict__ out,
-                                         int uh, int64_t ps) {
-  const int last = (2 * mb == j) ? mb : j;
-  const int hb = half_block(j) + mb * (j + 1);
-#pragma unroll
-  for (int ma = 0; ma <= j; ma++) {
-    if (ma > last) break;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const double2 d = s.d[k][ma], u = s.u[ma];
-      out[((int64_t)k * uh + hb + ma) * ps] = make_double2(fma(G.dsu[k], u.x, G.sfac * d.x),
-                                                           fma(G.dsu[k], u.y, G.sfac * d.y));
-    }
-  }
-}
-
-template <int J, int j>
-__device__ __forceinline__ void level_st(Chain<J>& s, const Geom& G, int mb, double2* __restrict__ out, int uh,
-                                         int64_t ps, double2* save, int nt, int tid) {
+// ---- every half-plane row of one neighbor handed to an emitter, in chain order ------------
+// emit.template row<j>(s, mb) runs after row mb of level j is in registers: row (0, 0) first,
+// then chain 0 over levels 1..J, chain mb over levels 2mb..J.  The rows of all lanes of a warp
+// come in the same order, so the emitter may synchronise the warp with other warps per row.
+template <int J, int j, class Emit>
+__device__ __forceinline__ void level_em(Chain<J>& s, const Geom& G, int mb, Emit& emit, double2* save, int nt,
+                                         int tid) {
   if constexpr (j <= J) {
     advance_rt<J, j>(s, G, mb);
-    store_rt<J, j>(s, G, mb, out, uh, ps);
+    emit.template row<j>(s, mb);
     if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2)
       if (j == 2 * mb + 1) save_mirror<J, j>(s, save, nt, tid);
   }
 }
 
-template <int J>
-__device__ __forceinline__ void all_chains_store(const Geom& G, double2* __restrict__ out, int uh, int64_t ps,
-                                                 double2* save, int nt, int tid) {
+template <int J, class Emit>
+__device__ __forceinline__ void all_chains_rows(const Geom& G, Emit& emit, double2* save, int nt, int tid) {
   static_assert(J <= 12, "level switch covers twojmax <= 12");
   Chain<J> s;
 #pragma unroll
@@ -742,7 +725,7 @@ __device__ __forceinline__ void all_chains_store(const Geom& G, double2* __restr
     for (int k = 0; k < 3; k++) s.d[k][c] = make_double2(0.0, 0.0);
   }
   s.u[0] = make_double2(1.0, 0.0);
-  store_rt<J, 0>(s, G, 0, out, uh, ps);
+  emit.template row<0>(s, 0);
 #pragma unroll 1
   for (int mb = 0; mb <= J / 2; mb++) {
     if (mb > 0) {
@@ -752,7 +735,7 @@ __device__ __forceinline__ void all_chains_store(const Geom& G, double2* __restr
     switch (mb == 0 ? 1 : 2 * mb) {
 #define IPG_LEVEL(JJ) \
   case JJ:            \
-    level_st<J, JJ>(s, G, mb, out, uh, ps, save, nt, tid);
+    level_em<J, JJ>(s, G, mb, emit, save, nt, tid);
       IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
       IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
 #undef IPG_LEVEL

@@ -286,8 +286,8 @@ def test_descriptor_paths_agree(J, monkeypatch):
 
 @pytest.mark.parametrize("J", [3, 6, 8, 9])
 def test_plain_paths_agree(J, monkeypatch):
-    """The plain dB/dr path: for twojmax <= 8 dU from the register chains and the contraction
-    with Z per pair (whole, or in chunks of 40 atoms and 256 pairs), otherwise (or with
+    """The plain dB/dr path: for twojmax <= 8 the fused kernel (dU rows from the register chains
+    contracted with the owner's Z; Z whole or in chunks of 40 atoms), otherwise (or with
     IPG_GENERIC_PLAIN=1) the per-atom block kernel; B, dB, W, E and F all equal the oracle."""
     rng = np.random.default_rng(400 + J)
     pos = rng.uniform(0, 7, (100, 3))
@@ -299,10 +299,9 @@ def test_plain_paths_agree(J, monkeypatch):
     Bo, dBo, Wo = orc.descriptors(s.positions, sp, s.L)
     beta = rng.normal(0, 1e-2, (2, Bo.shape[1]))
     eo, fo, wo = orc.energy_forces(s.positions, sp, s.L, beta, 0.0)
-    for generic, zchunk, pchunk in (("0", "0", "0"), ("0", "40", "256"), ("1", "0", "0")):
+    for generic, zchunk in (("0", "0"), ("0", "40"), ("1", "0")):
         monkeypatch.setenv("IPG_GENERIC_PLAIN", generic)
         monkeypatch.setenv("IPG_VJP_CHUNK", zchunk)
-        monkeypatch.setenv("IPG_DU_CHUNK", pchunk)
         snap, _ = make(prm)
         B, dB, Wd = ipg.compute_all_descriptors(s, snap)
         assert rel_err(B, Bo) <= TOL, (generic, zchunk)
