@@ -208,6 +208,7 @@ int ipg_create(int device, ipg_ctx** out) {
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
   if (const char* e = getenv("IPG_WALK_BY_ATOM")) ctx->walk_by_cell = e[0] != '1';
+  if (const char* e = getenv("IPG_WALK_SINGLE")) ctx->walk_single = e[0] != '0';
   int dev0 = 0;
   cudaGetDevice(&dev0);
   if (cudaSetDevice(device) != cudaSuccess ||

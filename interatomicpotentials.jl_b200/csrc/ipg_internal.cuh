@@ -49,6 +49,10 @@ struct ipg_ctx {
   bool capturing = false;
   uint64_t scratch_gen = 0;
   bool walk_by_cell = true;  // neighbor walk: one warp per cell (false: one warp per atom)
+  // single-pass neighbor walk: per list prefix, the per-atom slot count of the padded
+  // emission (from the largest count of the previous build; 0 = walk twice)
+  std::map<std::string, int> walk_kcap;
+  bool walk_single = true;
 };
 
 // Records a start/stop event pair around a launch when timing is enabled.

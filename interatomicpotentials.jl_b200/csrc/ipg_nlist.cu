@@ -294,12 +294,16 @@ struct WalkAtom {
   int64_t base, end, k;
   int32_t i, pad;
 };
-template <bool EMIT>
+// WM 0: count each atom's hits into cnt (and their maximum into *maxcnt); 1: emit them at
+// off[i]..off[i+1]; 2: both at once, emitting into kcap padded slots per atom (i * kcap ..),
+// hits beyond kcap dropped (the count and *maxcnt still see them).
+template <int WM>
 __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
     int64_t ncells, PairTest t, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ conf,
     const int64_t* __restrict__ cell_start, const int32_t* __restrict__ cell_atoms, const double4* __restrict__ spos,
     int64_t* __restrict__ cnt, const int64_t* __restrict__ off, int32_t* __restrict__ outj,
-    double* __restrict__ outr) {
+    double* __restrict__ outr, int kcap, int* __restrict__ maxcnt) {
+  constexpr bool EMIT = WM != 0;
   __shared__ WalkAtom sa[WALKC_WARPS][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t c = (int64_t)blockIdx.x * WALKC_WARPS + w;
@@ -324,9 +328,12 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
       A[lane].i = i;
       A[lane].x = spos[g0 + lane];
       A[lane].k = 0;
-      if (EMIT) {
+      if (WM == 1) {
         A[lane].base = off[i];
         A[lane].end = off[i + 1];
+      } else if (WM == 2) {
+        A[lane].base = (int64_t)i * kcap;
+        A[lane].end = (int64_t)i * kcap + kcap;
       }
     }
     __syncwarp();
@@ -359,8 +366,31 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
           __syncwarp();
         }
       }
-    if (!EMIT && lane < G) cnt[A[lane].i] = A[lane].k;
+    if (WM != 1) {
+      int km = 0;
+      if (lane < G) {
+        cnt[A[lane].i] = A[lane].k;
+        km = (int)A[lane].k;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) km = max(km, __shfl_xor_sync(0xffffffffu, km, o));
+      if (lane == 0) atomicMax(maxcnt, km);
+    }
   }
+}
+
+// Padded emission (k_pair_walk_cells<2>) to the CSR list: slot t of atom i goes to off[i] + t.
+__global__ void k_pad_compact(int64_t n, int kcap, const int64_t* __restrict__ off, const int32_t* __restrict__ pj,
+                              const double* __restrict__ pr, int32_t* __restrict__ j, double* __restrict__ r) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n * kcap) return;
+  const int64_t i = s / kcap;
+  const int64_t o = off[i] + (s - i * kcap);
+  if (o >= off[i + 1]) return;
+  j[o] = pj[s];
+  r[3 * o] = pr[3 * s];
+  r[3 * o + 1] = pr[3 * s + 1];
+  r[3 * o + 2] = pr[3 * s + 2];
 }
 
 // Sorts each atom's list by neighbor index (insertion sort; lists are short).
@@ -547,32 +577,56 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   cnt = pl.d_off;
   CUDA_RET(ctx, cudaMemsetAsync(cnt, 0, sizeof(int64_t) * (n + 1), ctx->stream));
   const bool by_cell = ctx->walk_by_cell;
+  // One walk instead of two when a previous build of this list gave the per-atom maximum:
+  // emit into padded slots while counting, then compact (or, if an atom overflowed its
+  // slots, emit again at the counted offsets).  Graph capture keeps the two walks.
+  int* maxcnt;
+  IPG_RET(scratch(ctx, (pre + "maxcnt").c_str(), 1, &maxcnt));
+  CUDA_RET(ctx, cudaMemsetAsync(maxcnt, 0, sizeof(int), ctx->stream));
+  int kcap = (by_cell && cap == 0 && !count_only && ctx->walk_single) ? ctx->walk_kcap[pre] : 0;
+  if ((double)n * kcap * 28.0 > 2.0 * (1 << 30)) kcap = 0;  // padded slots within 2 GiB
+  int32_t* pad_j = nullptr;
+  double* pad_r = nullptr;
+  if (kcap > 0 && n > 0) {
+    IPG_RET(scratch(ctx, (pre + "pad_j").c_str(), (size_t)n * kcap + 1, &pad_j));
+    IPG_RET(scratch(ctx, (pre + "pad_r").c_str(), 3 * (size_t)n * kcap + 3, &pad_r));
+  }
   if (n > 0) {
-    if (by_cell)
-      IPG_LAUNCH(ctx, k_pair_walk_cells<false>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
-                 cl.d_grid, cl.d_conf, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
+    if (by_cell && kcap > 0)
+      IPG_LAUNCH(ctx, k_pair_walk_cells<2>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
+                 cl.d_grid, cl.d_conf, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos, cnt, nullptr, pad_j, pad_r, kcap,
+                 maxcnt);
+    else if (by_cell)
+      IPG_LAUNCH(ctx, k_pair_walk_cells<0>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
+                 cl.d_grid, cl.d_conf, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr, 0,
+                 maxcnt);
     else
       IPG_LAUNCH(ctx, k_pair_walk<false>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                  cl.d_cell_atoms, cl.d_spos, cnt, nullptr, nullptr, nullptr);
   }
   IPG_RET(ipg_scan_i64(ctx, cnt, pl.d_off, n + 1));
   pl.d_np = pl.d_off + n;
+  int hmax = 0;
   if (cap > 0) {  // capacity mode: no read-back
     pl.npairs = cap;
     IPG_LAUNCH(ctx, k_clamp_offsets, nblk(n + 1, 256), 256, 0, n, pl.d_off, cap, ctx->d_status);
   } else {
     CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_RET(ctx, cudaMemcpyAsync(&hmax, maxcnt, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+    if (by_cell && !count_only) ctx->walk_kcap[pre] = ((hmax + hmax / 8 + 4 + 7) / 8) * 8;  // next build
   }
   if (pl.npairs >= (int64_t)1 << 40) return ipg_fail(ctx, IPG_ERR_CAPACITY, "pair count overflow");
   if (count_only) return IPG_OK;
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0) {
-    if (by_cell)
-      IPG_LAUNCH(ctx, k_pair_walk_cells<true>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
+    if (by_cell && kcap > 0 && hmax <= kcap)
+      IPG_LAUNCH(ctx, k_pad_compact, nblk(n * kcap, 256), 256, 0, n, kcap, pl.d_off, pad_j, pad_r, pl.d_j, pl.d_r);
+    else if (by_cell)
+      IPG_LAUNCH(ctx, k_pair_walk_cells<1>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
                  cl.d_grid, cl.d_conf, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j,
-                 pl.d_r);
+                 pl.d_r, 0, nullptr);
     else
       IPG_LAUNCH(ctx, k_pair_walk<true>, nblk(32 * n, wt), wt, 0, n, t, cl.d_grid, cl.d_conf, cl.d_cell_start,
                  cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);

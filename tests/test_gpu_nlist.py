@@ -89,3 +89,20 @@ def test_neighbor_count_matches_built_list():
     s2, p2 = W.lc32000(cells=6)
     for s, rc in ((s1, p1.get_rcutoff()), (s2, p2.get_rcutoff())):
         assert ipg.api.neighbor_count(s, rc) == len(ipg.neighborlist(s, rc)._j)
+
+
+def test_single_walk_padded_slots_and_overflow():
+    """After a first build (two walks: count, then emit) a list of the same name is built in one
+    walk into padded per-atom slots sized from the previous maximum, then compacted; a denser
+    system than the slots allow falls back to the emit walk.  Every build equals the oracle."""
+    ctx = ipg.Context(0)
+    rng = np.random.default_rng(5)
+    dense = ipg.System(rng.uniform(0, 20, (1500, 3)), ["Ar"] * 1500, [20.0] * 3)
+    sparse = ipg.System(rng.uniform(0, 40, (900, 3)), ["Ar"] * 900, [40.0] * 3)
+    rc = 4.0
+    for s in (dense, dense, sparse, dense, dense, sparse):
+        nl = ipg.neighborlist(s, rc, ctx=ctx)
+        off, j, r = oracle.nlist_half(s.positions, s.L, rc)
+        assert np.array_equal(nl.offsets, off)
+        assert np.array_equal(nl._j, j)
+        assert np.array_equal(nl._r, r)
