@@ -417,34 +417,35 @@ __global__ void k_pair_sort(int64_t n, const int64_t* __restrict__ off, int32_t*
   }
 }
 
-// Transpose: for every atom k, the pairs p whose neighbor is k, in ascending p.
+// Transpose: for every atom k, the pairs p whose neighbor is k, in ascending p.  The lists it
+// serves (the full SNAP lists) are symmetric with one image per pair, so the pairs whose
+// neighbor is k are those owned by k's own neighbors i, and ascending p is ascending i: pair
+// (i -> k) takes slot #{q owned by k : j[q] < i} of k's in-list.  No atomics, no sort.  (A
+// list cut at a capacity is not symmetric; its slots stay in bounds and the capacity error
+// discards the result.)
 __global__ void k_in_count(const int64_t* __restrict__ d_np, const int32_t* __restrict__ j,
                            int64_t* __restrict__ cnt) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= *d_np) return;
   atomicAdd((unsigned long long*)&cnt[j[p]], 1ull);
 }
-__global__ void k_in_fill(const int64_t* __restrict__ d_np, const int32_t* __restrict__ j,
-                          const int64_t* __restrict__ in_off, int64_t* __restrict__ fill,
-                          int64_t* __restrict__ in_pair) {
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= *d_np) return;
-  int32_t k = j[p];
-  unsigned long long q = atomicAdd((unsigned long long*)&fill[k], 1ull);
-  in_pair[in_off[k] + (int64_t)q] = p;
-}
-__global__ void k_in_sort(int64_t n, const int64_t* __restrict__ in_off, int64_t* __restrict__ in_pair) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  int64_t s = in_off[k], e = in_off[k + 1];
-  for (int64_t a = s + 1; a < e; a++) {
-    int64_t v = in_pair[a];
-    int64_t b = a - 1;
-    while (b >= s && in_pair[b] > v) {
-      in_pair[b + 1] = in_pair[b];
-      b--;
+// One warp per owner i: for each of its pairs (i -> k) the lanes read k's list 32 entries at a
+// time and count the neighbors below i with a ballot.
+__global__ void k_in_rank(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ j,
+                          const int64_t* __restrict__ in_off, int64_t* __restrict__ in_pair) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n) return;  // warp-uniform
+  for (int64_t p = off[i]; p < off[i + 1]; p++) {
+    const int32_t k = j[p];
+    const int64_t q0 = off[k], q1 = off[k + 1];
+    int64_t rank = 0;
+    for (int64_t q = q0; q < q1; q += 32) {
+      const bool below = q + lane < q1 && j[q + lane] < i;
+      rank += __popc(__ballot_sync(0xffffffffu, below));
     }
-    in_pair[b + 1] = v;
+    const int64_t slot = in_off[k] + rank;
+    if (lane == 0 && slot < in_off[k + 1]) in_pair[slot] = p;
   }
 }
 
@@ -545,6 +546,20 @@ int ipg_build_cells(ipg_ctx* ctx, const char* prefix, int64_t n, const double* d
   return IPG_OK;
 }
 
+namespace {
+// The in-lists of a symmetric list (k_in_rank): in_off by counting, in_pair by rank.
+int build_transpose(ipg_ctx* ctx, const std::string& pre, int64_t n, PairList& pl) {
+  IPG_RET(scratch(ctx, (pre + "in_off").c_str(), n + 1, &pl.d_in_off));
+  IPG_RET(scratch(ctx, (pre + "in_pair").c_str(), pl.npairs + 1, &pl.d_in_pair));
+  CUDA_RET(ctx, cudaMemsetAsync(pl.d_in_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
+  if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off);
+  IPG_RET(ipg_scan_i64(ctx, pl.d_in_off, pl.d_in_off, n + 1));
+  if (pl.npairs > 0)
+    IPG_LAUNCH(ctx, k_in_rank, nblk(32 * n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off, pl.d_in_pair);
+  return IPG_OK;
+}
+}  // namespace
+
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
                     const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted, int64_t cap,
                     int walk_warps, bool count_only) {
@@ -632,20 +647,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
                  cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
     if (sorted) IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
   }
-  if (want_transpose) {
-    int64_t* fill;
-    IPG_RET(scratch(ctx, (pre + "in_off").c_str(), n + 1, &pl.d_in_off));
-    IPG_RET(scratch(ctx, (pre + "in_fill").c_str(), n + 1, &fill));
-    IPG_RET(scratch(ctx, (pre + "in_pair").c_str(), pl.npairs + 1, &pl.d_in_pair));
-    CUDA_RET(ctx, cudaMemsetAsync(pl.d_in_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
-    CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (n + 1), ctx->stream));
-    if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off);
-    IPG_RET(ipg_scan_i64(ctx, pl.d_in_off, pl.d_in_off, n + 1));
-    if (pl.npairs > 0) {
-      IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
-      IPG_LAUNCH(ctx, k_in_sort, nblk(n, 128), 128, 0, n, pl.d_in_off, pl.d_in_pair);
-    }
-  }
+  if (want_transpose) IPG_RET(build_transpose(ctx, pre, n, pl));
   return IPG_OK;
 }
 
@@ -698,18 +700,7 @@ int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const
   if (n > 0)
     IPG_LAUNCH(ctx, k_filter_walk<true>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cached.d_off,
                cached.d_j, d_pos, d_species, nsp, nullptr, pl.d_off, pl.d_j, pl.d_r);
-  int64_t* fill;
-  IPG_RET(scratch(ctx, (pre + "in_off").c_str(), n + 1, &pl.d_in_off));
-  IPG_RET(scratch(ctx, (pre + "in_fill").c_str(), n + 1, &fill));
-  IPG_RET(scratch(ctx, (pre + "in_pair").c_str(), pl.npairs + 1, &pl.d_in_pair));
-  CUDA_RET(ctx, cudaMemsetAsync(pl.d_in_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
-  CUDA_RET(ctx, cudaMemsetAsync(fill, 0, sizeof(int64_t) * (n + 1), ctx->stream));
-  if (pl.npairs > 0) IPG_LAUNCH(ctx, k_in_count, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off);
-  IPG_RET(ipg_scan_i64(ctx, pl.d_in_off, pl.d_in_off, n + 1));
-  if (pl.npairs > 0) {
-    IPG_LAUNCH(ctx, k_in_fill, nblk(pl.npairs, 256), 256, 0, pl.d_np, pl.d_j, pl.d_in_off, fill, pl.d_in_pair);
-    IPG_LAUNCH(ctx, k_in_sort, nblk(n, 128), 128, 0, n, pl.d_in_off, pl.d_in_pair);
-  }
+  IPG_RET(build_transpose(ctx, pre, n, pl));
   return IPG_OK;
 }
 
