@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import statistics
@@ -270,6 +271,8 @@ def main():
                 ctx.timing_read(k)
         l0 = ctx.launch_count()
         evs = []
+        gc.collect()  # no collector pause inside the timed loop (the batch extra leaves garbage)
+        gc.disable()
         for _ in range(steps):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -278,6 +281,7 @@ def main():
             e1.record(stream)
             evs.append((e0, e1))
         torch.cuda.synchronize()
+        gc.enable()
         if dist:
             dist.barrier()
         ms = sum(a.elapsed_time(b) for a, b in evs)

@@ -30,7 +30,7 @@ struct PairTerms {
   PairTermDev t[IPG_MAX_PAIR_TERMS];
 };
 
-__constant__ PairTerms c_terms;
+static_assert(sizeof(PairTerms) <= 4096, "the terms travel as a kernel parameter");
 
 // ZBL screening coefficients, src/empirical/zbl.jl:27-28.
 __constant__ double c_zbl_c[4] = {0.18175, 0.50986, 0.28022, 0.02817};
@@ -106,14 +106,14 @@ struct Hit {
   int sj, pad;
 };
 
-__device__ __forceinline__ void eval_hits(const Hit* __restrict__ hb, int nh, int lane, int si, double* acc,
-                                          double& f0, double& f1, double& f2) {
+__device__ __forceinline__ void eval_hits(const PairTerms& TT, const Hit* __restrict__ hb, int nh, int lane, int si,
+                                          double* acc, double& f0, double& f1, double& f2) {
   if (lane >= nh) return;
   const Hit h = hb[lane];
   const double R = sqrt(h.r0 * h.r0 + h.r1 * h.r1 + h.r2 * h.r2);
   double V = 0.0, gsum = 0.0;
-  for (int t = 0; t < c_terms.nterms; t++) {
-    const PairTermDev& T = c_terms.t[t];
+  for (int t = 0; t < TT.nterms; t++) {
+    const PairTermDev& T = TT.t[t];
     if (h.dist > T.rcut) continue;
     if (!((T.mask >> si) & 1ull) || !((T.mask >> h.sj) & 1ull)) continue;
     double v, gg;
@@ -135,7 +135,8 @@ __device__ __forceinline__ void eval_hits(const Hit* __restrict__ hb, int nh, in
   acc[6] += 0.5 * h.r1 * fx;
 }
 
-__global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid* __restrict__ grid,
+__global__ void __launch_bounds__(PAIR_T) k_pair_eval(const __grid_constant__ PairTerms TT, int64_t n,
+                                                      const ConfGrid* __restrict__ grid,
                                                       const int64_t* __restrict__ cell_start,
                                                       const int32_t* __restrict__ cell_atoms,
                                                       const double4* __restrict__ spos, double* __restrict__ F,
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid*
     StencilRanges Rg;
     stencil_ranges(g, c, cell_start, Rg);
     double f0 = 0.0, f1 = 0.0, f2 = 0.0;
-    const double rmax = c_terms.rcut_max;
+    const double rmax = TT.rcut_max;
     Hit* hb = hits[w];
     int nh = 0;
     const unsigned lt = (1u << lane) - 1u;
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid*
             const double p1 = pe_axis_dev(g.L[1], xi.y, xj.y);
             const double p2 = pe_axis_dev(g.L[2], xi.z, xj.z);
             const double d2 = sumsq3_dev(p0, p1, p2);
-            if (d2 <= c_terms.rmax2_hi) {
+            if (d2 <= TT.rmax2_hi) {
               const double dist = sqrt(d2);
               if (dist <= rmax) {
                 ok = true;
@@ -196,14 +197,14 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_eval(int64_t n, const ConfGrid*
         nh += __popc(bal);
         __syncwarp();
         if (nh >= 32) {
-          eval_hits(hb, 32, lane, si, acc, f0, f1, f2);
+          eval_hits(TT, hb, 32, lane, si, acc, f0, f1, f2);
           __syncwarp();
           if (lane < nh - 32) hb[lane] = hb[32 + lane];
           nh -= 32;
           __syncwarp();
         }
       }
-    eval_hits(hb, nh, lane, si, acc, f0, f1, f2);
+    eval_hits(TT, hb, nh, lane, si, acc, f0, f1, f2);
     f0 = warp_sum(f0);
     f1 = warp_sum(f1);
     f2 = warp_sum(f2);
@@ -295,7 +296,6 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
                      uint32_t flags) {
   PairTerms pt;
   IPG_RET(prepare_terms(ctx, terms, nterms, pt));
-  CUDA_RET(ctx, cudaMemcpyToSymbolAsync(c_terms, &pt, sizeof(pt), 0, cudaMemcpyHostToDevice, ctx->stream));
   IPG_RET(ipg_status_reset(ctx));
   int64_t aoff[2] = {0, n};
   CellList cl;
@@ -304,7 +304,7 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
   double *partial, *red;
   IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
   IPG_RET(scratch(ctx, "pair_red", 8, &red));
-  IPG_TIMED_LAUNCH(ctx, "pair_eval", k_pair_eval, (unsigned)nb, PAIR_T, 0, n, cl.d_grid, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos,
+  IPG_TIMED_LAUNCH(ctx, "pair_eval", k_pair_eval, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos,
              (flags & IPG_WANT_F) ? d_F : nullptr, partial, ctx->d_status);
   IPG_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, nb, 7, partial, red);
   if ((flags & IPG_WANT_E) && d_E)
