@@ -92,6 +92,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()  # nvidia-smi takes a while to start: let it sample before the region
+            while not self.lines and time.time() - t0 < 5.0:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self

@@ -429,23 +429,22 @@ __global__ void k_in_count(const int64_t* __restrict__ d_np, const int32_t* __re
   if (p >= *d_np) return;
   atomicAdd((unsigned long long*)&cnt[j[p]], 1ull);
 }
-// One warp per owner i: for each of its pairs (i -> k) the lanes read k's list 32 entries at a
-// time and count the neighbors below i with a ballot.
+// One warp per owner i, one lane per pair (i -> k) (32 at a time); each lane counts the
+// neighbors of k below i on its own, so the lanes' loads overlap.
 __global__ void k_in_rank(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ j,
                           const int64_t* __restrict__ in_off, int64_t* __restrict__ in_pair) {
   const int lane = threadIdx.x & 31;
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;  // warp-uniform
-  for (int64_t p = off[i]; p < off[i + 1]; p++) {
+  const int64_t p1 = off[i + 1];
+  for (int64_t p = off[i] + lane; p < p1; p += 32) {
     const int32_t k = j[p];
     const int64_t q0 = off[k], q1 = off[k + 1];
     int64_t rank = 0;
-    for (int64_t q = q0; q < q1; q += 32) {
-      const bool below = q + lane < q1 && j[q + lane] < i;
-      rank += __popc(__ballot_sync(0xffffffffu, below));
-    }
+#pragma unroll 4
+    for (int64_t q = q0; q < q1; q++) rank += j[q] < i;
     const int64_t slot = in_off[k] + rank;
-    if (lane == 0 && slot < in_off[k + 1]) in_pair[slot] = p;
+    if (slot < in_off[k + 1]) in_pair[slot] = p;
   }
 }
 
