@@ -924,7 +924,8 @@ __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const i
   if (m2 && (mb2 & 1)) cb = -cb;
   const double sx0 = cb, sy0 = m2 ? -cb : cb, sx1 = m2 ? -cb : cb, sy1 = cb;
   cp += ma0;
-  for (int m0 = 0; m0 <= j2; m0 += 2, cp += rs) {
+  int m0 = 0;
+  for (; m0 < j2; m0 += 2, cp += rs) {  // column pairs (m0, m0 + 1) both in range
     const double2 v0 = p2[0], v1 = p2[st2];
     p2 += 2 * st2;
     double2 r[2];
@@ -960,6 +961,28 @@ __device__ __forceinline__ void yr_pair(const double2* __restrict__ usl, const i
         acc[i].x = fma(c, px, acc[i].x);
         acc[i].y = fma(c, py, acc[i].y);
       }
+    }
+  }
+  if (!(j2 & 1)) {  // even j2: the last column (m0 = j2) alone; its partner j2 + 1 is out of range
+    const double2 v0 = p2[0];
+    const double2 w = make_double2(sx0 * v0.x, sy0 * v0.y);
+    const int base = d - m0 - 1 + ma0;
+    const double2* pb = p1 + (M1 ? -base : base) * YS_ATOMS;
+#pragma unroll
+    for (int i = 0; i < NT; i++) {
+      const double2 v = pb[(M1 ? -(i + 1) : (i + 1)) * YS_ATOMS];
+      double px, py;
+      if (M1) {
+        px = fma(v.x, w.x, v.y * w.y);
+        py = fma(v.x, w.y, -(v.y * w.x));
+      } else {
+        px = fma(v.x, w.x, -(v.y * w.y));
+        py = fma(v.x, w.y, v.y * w.x);
+      }
+      const double c0 = cp[i].x;
+      const double c = (M1 && (i & 1)) ? -c0 : c0;
+      acc[i].x = fma(c, px, acc[i].x);
+      acc[i].y = fma(c, py, acc[i].y);
     }
   }
 }
