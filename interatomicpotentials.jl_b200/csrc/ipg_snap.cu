@@ -1521,24 +1521,26 @@ struct DbRowEmit {  // producer side: dU_k[ma] of this lane's pair into row buff
   }
 };
 
-// consumer side: row mb of level L, d = this pair's dU_k of the row (weights applied)
+// consumer side: row mb of level L.  The row's entries ma run in a loop; the level's Z triples
+// are unrolled inside it (one Z load and two FMAs each), so the code per level stays small.
+template <int J, int L, int Q, int NQ>
+__device__ __forceinline__ void dbf_dot(double (&c)[NQ], double2 d, const double2* __restrict__ zr) {
+  if constexpr (Q < NQ) {
+    constexpr int z0 = plaintab::level_of(J, L).z0[Q];
+    const double2 z = zr[z0];
+    c[Q] = fma(d.x, z.x, fma(d.y, z.y, c[Q]));
+    dbf_dot<J, L, Q + 1, NQ>(c, d, zr);
+  }
+}
+
 template <int J, int L, int Q, int NQ, int NB>
-__device__ __forceinline__ void dbf_terms(double (&acc)[NB], const double2 (&d)[L + 1], const double2* __restrict__ zr,
-                                          int last, bool bnorm) {
+__device__ __forceinline__ void dbf_add(double (&acc)[NB], const double (&c)[NQ], bool bnorm) {
   if constexpr (Q < NQ) {
     constexpr plaintab::Level T = plaintab::level_of(J, L);
-    constexpr int z0 = T.z0[Q], b = T.jjb[Q];
+    constexpr int b = T.jjb[Q];
     constexpr double m = T.m[Q], mn = T.mn[Q];
-    double c0 = 0.0, c1 = 0.0;
-#pragma unroll
-    for (int ma = 0; ma <= L; ma++) {
-      if (ma > last) break;
-      const double2 z = zr[z0 + ma];
-      c0 = fma(d[ma].x, z.x, c0);
-      c1 = fma(d[ma].y, z.y, c1);
-    }
-    acc[b] = fma(bnorm ? mn : m, c0 + c1, acc[b]);
-    dbf_terms<J, L, Q + 1, NQ, NB>(acc, d, zr, last, bnorm);
+    acc[b] = fma(bnorm ? mn : m, c[Q], acc[b]);
+    dbf_add<J, L, Q + 1, NQ, NB>(acc, c, bnorm);
   }
 }
 
@@ -1546,18 +1548,22 @@ template <int J, int L, int NB>
 __device__ __forceinline__ void dbf_row(double (&acc)[NB], int mb, const double2* __restrict__ rb,
                                         const double2* __restrict__ zo, bool bnorm) {
   if constexpr (L <= J) {
-    const int last = (2 * mb == L) ? mb : L;
-    double2 d[L + 1];
-#pragma unroll
-    for (int ma = 0; ma <= L; ma++) {
-      d[ma] = ma <= last ? rb[ma * 32] : make_double2(0.0, 0.0);
-      if (2 * mb == L && ma == mb) {  // the middle element of an even level: weight 1/2
-        d[ma].x *= 0.5;
-        d[ma].y *= 0.5;
-      }
-    }
     constexpr int NQ = plaintab::level_of(J, L).n;
-    dbf_terms<J, L, 0, NQ, NB>(acc, d, zo + mb * (L + 1), last, bnorm);
+    const int last = (2 * mb == L) ? mb : L;
+    const double2* zr = zo + mb * (L + 1);
+    double c[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) c[q] = 0.0;
+#pragma unroll 1
+    for (int ma = 0; ma <= last; ma++) {
+      double2 d = rb[ma * 32];
+      if (2 * mb == L && ma == mb) {  // the middle element of an even level: weight 1/2
+        d.x *= 0.5;
+        d.y *= 0.5;
+      }
+      dbf_dot<J, L, 0, NQ>(c, d, zr + ma);
+    }
+    dbf_add<J, L, 0, NQ, NB>(acc, c, bnorm);
   }
 }
 
