@@ -1475,10 +1475,10 @@ constexpr Level level_of(int J, int L, int G = 1, int g = 0) {
 
 // Plain dB/dr, one block per owner atom, warp-specialised: warp 0 (the producer) runs every
 // chain of up to 32 of the owner's pairs, one pair per lane, and hands each half-plane row of
-// dU/dr to warps 1..3 (the consumers, one per component k) through a double-buffered row
-// buffer in shared memory; each consumer lane contracts the rows of its pair with the owner's
+// dU/dr to warps 1..3 (the consumers, one per component k) through three row buffers in
+// shared memory; each consumer lane contracts the rows of its pair with the owner's
 // Z (staged in shared memory) into the 55 accumulators of dB[b][k].  dU never leaves the SM.
-// Hand-off by named barriers (ids 1, 2: row buffer b full; 3, 4: row buffer b free), DBF_T
+// Hand-off by named barriers (ids 1..3: row buffer b full; 4..6: row buffer b free), DBF_T
 // threads each: the producer arrives on "full" and waits on "free", the consumers the
 // reverse; both sides walk the same row sequence, so every barrier generation completes.
 constexpr int DBF_T = 128;
@@ -1491,21 +1491,26 @@ template <int ID>
 __device__ __forceinline__ void nbar_arrive() {
   asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(DBF_T) : "memory");
 }
-// row buffer b: "full" is barrier 1 + b, "free" is barrier 3 + b (immediate ids)
-__device__ __forceinline__ void row_full_arrive(int b) { b ? nbar_arrive<2>() : nbar_arrive<1>(); }
-__device__ __forceinline__ void row_full_wait(int b) { b ? nbar_sync<2>() : nbar_sync<1>(); }
-__device__ __forceinline__ void row_free_arrive(int b) { b ? nbar_arrive<4>() : nbar_arrive<3>(); }
-__device__ __forceinline__ void row_free_wait(int b) { b ? nbar_sync<4>() : nbar_sync<3>(); }
+// DBF_NBUF row buffers; buffer b: "full" is barrier 1 + b, "free" is barrier 4 + b (immediate ids)
+constexpr int DBF_NBUF = 3;
+__device__ __forceinline__ void row_full_arrive(int b) {
+  b == 0 ? nbar_arrive<1>() : (b == 1 ? nbar_arrive<2>() : nbar_arrive<3>());
+}
+__device__ __forceinline__ void row_full_wait(int b) { b == 0 ? nbar_sync<1>() : (b == 1 ? nbar_sync<2>() : nbar_sync<3>()); }
+__device__ __forceinline__ void row_free_arrive(int b) {
+  b == 0 ? nbar_arrive<4>() : (b == 1 ? nbar_arrive<5>() : nbar_arrive<6>());
+}
+__device__ __forceinline__ void row_free_wait(int b) { b == 0 ? nbar_sync<4>() : (b == 1 ? nbar_sync<5>() : nbar_sync<6>()); }
 
 template <int J>
-struct DbRowEmit {  // producer side: dU_k[ma] of this lane's pair into row buffer (r & 1)
+struct DbRowEmit {  // producer side: dU_k[ma] of this lane's pair into row buffer r % DBF_NBUF
   const snapchain::Geom& G;
   double2* rows;  // [2][3][J+1][32]
   int lane, r;
   template <int j>
   __device__ __forceinline__ void row(const snapchain::Chain<J>& s, int mb) {
-    const int b = r & 1;
-    row_free_wait(b);  // the consumers are done with row r - 2
+    const int b = r % DBF_NBUF;
+    row_free_wait(b);  // the consumers are done with row r - DBF_NBUF
     double2* rb = rows + b * 3 * (J + 1) * 32 + lane;
     const int last = (2 * mb == j) ? mb : j;
 #pragma unroll
@@ -1595,8 +1600,8 @@ __global__ void __launch_bounds__(DBF_T, 2) k_snap_dbfused(const __grid_constant
   constexpr int NB = plaintab::nb_of(J);
   extern __shared__ __align__(16) unsigned char fsm[];
   double2* zo = reinterpret_cast<double2*>(fsm);                 // [idxz_max] the owner's Z
-  double2* rows = zo + ((S.idxz_max + 1) & ~1);                  // [2][3][J+1][32]
-  double2* save = rows + 2 * 3 * (J + 1) * 32;                   // [4 (J+1)][32] producer start rows
+  double2* rows = zo + ((S.idxz_max + 1) & ~1);                  // [DBF_NBUF][3][J+1][32]
+  double2* save = rows + DBF_NBUF * 3 * (J + 1) * 32;            // [4 (J+1)][32] producer start rows
   const int64_t o = b0 + blockIdx.x;
   for (int z = threadIdx.x; z < S.idxz_max; z += DBF_T) zo[z] = Z[(size_t)z * zs + (o - a0)];
   __syncthreads();
@@ -1638,13 +1643,13 @@ __global__ void __launch_bounds__(DBF_T, 2) k_snap_dbfused(const __grid_constant
       snapchain::all_chains_rows<J>(G, e, save, 32, lane);
       r = e.r;
     }
-    row_free_wait(r & 1);  // the consumers' last two "free" arrivals
-    row_free_wait((r + 1) & 1);
+#pragma unroll
+    for (int t = 0; t < DBF_NBUF; t++) row_free_wait((r + t) % DBF_NBUF);  // the consumers' last arrivals
   } else {
     const int k = warp - 1;
     const bool bnorm = S.bnorm_flag != 0;
-    row_free_arrive(0);  // both row buffers start free
-    row_free_arrive(1);
+#pragma unroll
+    for (int b = 0; b < DBF_NBUF; b++) row_free_arrive(b);  // every row buffer starts free
     int r = 0;
     for (int pass = 0; pass < npass; pass++) {
       double acc[NB];
@@ -1653,7 +1658,7 @@ __global__ void __launch_bounds__(DBF_T, 2) k_snap_dbfused(const __grid_constant
       for (int mb = -1; mb <= J / 2; mb++) {  // mb = -1: the row (0, 0)
         const int j0 = mb < 0 ? 0 : (mb == 0 ? 1 : 2 * mb), j1 = mb < 0 ? 0 : J;
         for (int j = j0; j <= j1; j++, r++) {
-          const int bsel = r & 1;
+          const int bsel = r % DBF_NBUF;
           row_full_wait(bsel);
           dbf_consume<J, NB>(acc, j, mb < 0 ? 0 : mb, rows + (bsel * 3 + k) * (J + 1) * 32 + lane, zo, bnorm);
           row_free_arrive(bsel);
@@ -1676,7 +1681,8 @@ int plain_fused_j(ipg_ctx* ctx, const SnapDev& S, int64_t b0, int64_t b1, const 
     return IPG_ERR_UNSUPPORTED;
   } else {
     if (plaintab::nb_of(J) != S.K) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "plain chain tables disagree");
-    const size_t sm = ((size_t)((S.idxz_max + 1) & ~1) + 2 * 3 * (J + 1) * 32 + 4 * (J + 1) * 32) * sizeof(double2);
+    const size_t sm =
+        ((size_t)((S.idxz_max + 1) & ~1) + DBF_NBUF * 3 * (J + 1) * 32 + 4 * (J + 1) * 32) * sizeof(double2);
     if (sm > 48 * 1024)
       CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_dbfused<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     IPG_TIMED_LAUNCH(ctx, "snap_dbfused", k_snap_dbfused<J>, (unsigned)(b1 - b0), DBF_T, sm, S, b0, off, nbr, rij,
