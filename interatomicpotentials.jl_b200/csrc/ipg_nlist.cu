@@ -379,6 +379,11 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
   }
 }
 
+// Capacity mode of the padded walk: an atom with more hits than slots is a capacity error.
+__global__ void k_kcap_check(const int* __restrict__ maxcnt, int kcap, int* __restrict__ status) {
+  if (threadIdx.x == 0 && *maxcnt > kcap) atomicExch(status, IPG_ERR_CAPACITY);
+}
+
 // Padded emission (k_pair_walk_cells<2>) to the CSR list: slot t of atom i goes to off[i] + t.
 __global__ void k_pad_compact(int64_t n, int kcap, const int64_t* __restrict__ off, const int32_t* __restrict__ pj,
                               const double* __restrict__ pr, int32_t* __restrict__ j, double* __restrict__ r) {
@@ -593,11 +598,12 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   const bool by_cell = ctx->walk_by_cell;
   // One walk instead of two when a previous build of this list gave the per-atom maximum:
   // emit into padded slots while counting, then compact (or, if an atom overflowed its
-  // slots, emit again at the counted offsets).  Graph capture keeps the two walks.
+  // slots, emit again at the counted offsets).  In capacity mode (graph capture) there is no
+  // read-back: an overflow sets IPG_ERR_CAPACITY in the device status word instead.
   int* maxcnt;
   IPG_RET(scratch(ctx, (pre + "maxcnt").c_str(), 1, &maxcnt));
   CUDA_RET(ctx, cudaMemsetAsync(maxcnt, 0, sizeof(int), ctx->stream));
-  int kcap = (by_cell && cap == 0 && !count_only && ctx->walk_single) ? ctx->walk_kcap[pre] : 0;
+  int kcap = (by_cell && !count_only && ctx->walk_single) ? ctx->walk_kcap[pre] : 0;
   if ((double)n * kcap * 28.0 > 2.0 * (1 << 30)) kcap = 0;  // padded slots within 2 GiB
   int32_t* pad_j = nullptr;
   double* pad_r = nullptr;
@@ -624,6 +630,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   if (cap > 0) {  // capacity mode: no read-back
     pl.npairs = cap;
     IPG_LAUNCH(ctx, k_clamp_offsets, nblk(n + 1, 256), 256, 0, n, pl.d_off, cap, ctx->d_status);
+    if (kcap > 0 && n > 0) IPG_LAUNCH(ctx, k_kcap_check, 1, 32, 0, maxcnt, kcap, ctx->d_status);
   } else {
     CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_RET(ctx, cudaMemcpyAsync(&hmax, maxcnt, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -635,7 +642,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   IPG_RET(scratch(ctx, (pre + "j").c_str(), pl.npairs + 1, &pl.d_j));
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0) {
-    if (by_cell && kcap > 0 && hmax <= kcap)
+    if (by_cell && kcap > 0 && (cap > 0 || hmax <= kcap))
       IPG_LAUNCH(ctx, k_pad_compact, nblk(n * kcap, 256), 256, 0, n, kcap, pl.d_off, pad_j, pad_r, pl.d_j, pl.d_r);
     else if (by_cell)
       IPG_LAUNCH(ctx, k_pair_walk_cells<1>, nblk(cl.ncells, WALKC_WARPS), WALKC_WARPS * 32, 0, cl.ncells, t,
