@@ -157,7 +157,11 @@ def oracle_sample_rate(system, prm, beta, target_s):
     per_atom = max((t_b - t_a) / 192.0, 1e-7)
     m = int(min(len(system), max(256, target_s / per_atom)))
     dt = run(m)
-    return m / dt, m, dt
+    reps = 1
+    while m == len(system) and dt < target_s and reps < 30:  # the whole system is shorter: repeat it
+        dt += run(m)
+        reps += 1
+    return m * reps / dt, m * reps, dt
 
 
 def run_reference(args, rank, world):
@@ -174,8 +178,9 @@ def run_reference(args, rank, world):
         rates.append(r)
         ms, secs = m, secs + dt
     value = float(np.median(rates))
-    sample = (f"first {ms} of the 54,000 centre atoms per step (plain dB/dr path as in compute_all_descriptors, "
-              f"contracted with beta), {cores} OpenMP threads")
+    sample = (f"{ms} centre-atom evaluations of the 54,000-atom workload per step (the first atoms, or repeated "
+              f"passes over all of them; plain dB/dr path as in compute_all_descriptors, contracted with beta), "
+              f"{cores} OpenMP threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * len(system) / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -449,7 +454,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, m, dt = oracle_sample_rate(system, prm, beta_b, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cpu_count(), "kind": "port",
-                                "sample": f"first {m} of {n} centre atoms, plain dB/dr path, {dt:.1f} s, "
+                                "sample": f"{m} centre-atom evaluations of the {n}-atom workload (repeated "
+                                          f"passes when it is shorter), plain dB/dr path, {dt:.1f} s, "
                                           f"{cpu_count()} OpenMP threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
