@@ -62,7 +62,39 @@ int ipg_sync(ipg_ctx* ctx) {
   return IPG_OK;
 }
 
+int ipg_side_begin(ipg_ctx* ctx) {
+  IPG_RET(ipg_side_join(ctx));
+  if (!ctx->side) {
+    CUDA_RET(ctx, cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    CUDA_RET(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    CUDA_RET(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
+  CUDA_RET(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+  CUDA_RET(ctx, cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+  ctx->side_main = ctx->stream;
+  ctx->stream = ctx->side;
+  return IPG_OK;
+}
+
+int ipg_side_end(ipg_ctx* ctx) {
+  if (!ctx->side_main) return IPG_OK;
+  ctx->stream = ctx->side_main;
+  ctx->side_main = nullptr;
+  CUDA_RET(ctx, cudaEventRecord(ctx->ev_join, ctx->side));
+  ctx->side_pending = true;
+  return IPG_OK;
+}
+
+int ipg_side_join(ipg_ctx* ctx) {
+  if (ctx->side_main) IPG_RET(ipg_side_end(ctx));  // an error path left the side stream current
+  if (!ctx->side_pending) return IPG_OK;
+  ctx->side_pending = false;
+  CUDA_RET(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  return IPG_OK;
+}
+
 int ipg_status_check(ipg_ctx* ctx, const char* what) {
+  IPG_RET(ipg_side_join(ctx));
   CUDA_RET(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
   int st = *ctx->h_status;
@@ -230,6 +262,7 @@ int ipg_destroy(ipg_ctx* ctx) {
   if (!ctx) return IPG_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->side) cudaStreamSynchronize(ctx->side);
   for (auto& kv : ctx->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
   for (auto& kv : ctx->timed)
@@ -238,6 +271,9 @@ int ipg_destroy(ipg_ctx* ctx) {
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   delete ctx;
   return IPG_OK;
 }

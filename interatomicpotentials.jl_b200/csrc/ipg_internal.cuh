@@ -53,7 +53,20 @@ struct ipg_ctx {
   // emission (from the largest count of the previous build; 0 = walk twice)
   std::map<std::string, int> walk_kcap;
   bool walk_single = true;
+  // side stream for work that only a later kernel needs (the list transpose): forked from and
+  // joined back into `stream` by events, so it also works inside a graph capture
+  cudaStream_t side = nullptr;
+  cudaStream_t side_main = nullptr;  // `stream` while the side stream stands in for it
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool side_pending = false;
 };
+
+// Runs the launches between ipg_side_begin and ipg_side_end on the side stream (ctx->stream
+// points at it meanwhile), after everything already on the main stream; ipg_side_join makes
+// the main stream wait for them.  ipg_status_check and the list builders join first.
+int ipg_side_begin(ipg_ctx* ctx);
+int ipg_side_end(ipg_ctx* ctx);
+int ipg_side_join(ipg_ctx* ctx);
 
 // Records a start/stop event pair around a launch when timing is enabled.
 int ipg_timing_mark(ipg_ctx* ctx, const char* name, bool start);

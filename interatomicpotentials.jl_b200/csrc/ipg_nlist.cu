@@ -291,7 +291,7 @@ __global__ void k_clamp_offsets(int64_t n, int64_t* __restrict__ off, int64_t ca
 constexpr int WALKC_WARPS = 4;
 struct WalkAtom {
   double4 x;
-  int64_t base, end, k;
+  int64_t base, end;
   int32_t i, pad;
 };
 // WM 0: count each atom's hits into cnt (and their maximum into *maxcnt); 1: emit them at
@@ -327,7 +327,6 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
       const int32_t i = cell_atoms[g0 + lane];
       A[lane].i = i;
       A[lane].x = spos[g0 + lane];
-      A[lane].k = 0;
       if (WM == 1) {
         A[lane].base = off[i];
         A[lane].end = off[i + 1];
@@ -337,6 +336,7 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
       }
     }
     __syncwarp();
+    int64_t myk = 0;  // hits of atom `lane` of this group so far (lane ii owns atom ii's count)
     for (int r = 0; r < R.n; r++)
       for (int64_t q0 = R.beg[r]; q0 < R.end[r]; q0 += 32) {
         const int64_t q = q0 + lane;
@@ -352,25 +352,26 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
           double rr[3];
           const bool ok = inq && pair_ok(t, g.L, i, A[ii].x, j, xj, rr);
           const unsigned bal = __ballot_sync(0xffffffffu, ok);
-          if (EMIT && ok) {
-            const int64_t o = A[ii].base + A[ii].k + __popc(bal & lt);
-            if (o < A[ii].end) {  // a list cut at the capacity (capacity mode) drops its tail
-              outj[o] = j;
-              outr[3 * o] = rr[0];
-              outr[3 * o + 1] = rr[1];
-              outr[3 * o + 2] = rr[2];
+          if (EMIT) {
+            const int64_t kk = __shfl_sync(0xffffffffu, myk, ii);
+            if (ok) {
+              const int64_t o = A[ii].base + kk + __popc(bal & lt);
+              if (o < A[ii].end) {  // a list cut at the capacity (capacity mode) drops its tail
+                outj[o] = j;
+                outr[3 * o] = rr[0];
+                outr[3 * o + 1] = rr[1];
+                outr[3 * o + 2] = rr[2];
+              }
             }
           }
-          __syncwarp();
-          if (lane == 0) A[ii].k += __popc(bal);
-          __syncwarp();
+          if (lane == ii) myk += __popc(bal);
         }
       }
     if (WM != 1) {
       int km = 0;
       if (lane < G) {
-        cnt[A[lane].i] = A[lane].k;
-        km = (int)A[lane].k;
+        cnt[A[lane].i] = myk;
+        km = (int)myk;
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) km = max(km, __shfl_xor_sync(0xffffffffu, km, o));
@@ -569,6 +570,7 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
                     int walk_warps, bool count_only) {
   const int wt = 32 * std::max(1, std::min(4, walk_warps));
   (void)d_species;
+  IPG_RET(ipg_side_join(ctx));
   std::string pre(prefix);
   PairTest t;
   memset(&t, 0, sizeof(t));
@@ -653,7 +655,12 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
                  cl.d_cell_atoms, cl.d_spos, nullptr, pl.d_off, pl.d_j, pl.d_r);
     if (sorted) IPG_LAUNCH(ctx, k_pair_sort, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_r);
   }
-  if (want_transpose) IPG_RET(build_transpose(ctx, pre, n, pl));
+  if (want_transpose) {  // needed only by the force gather: overlaps the first SNAP kernels
+    IPG_RET(ipg_side_begin(ctx));
+    const int st = build_transpose(ctx, pre, n, pl);
+    IPG_RET(ipg_side_end(ctx));
+    IPG_RET(st);
+  }
   return IPG_OK;
 }
 
@@ -675,6 +682,7 @@ int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const d
 int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const PairList& cached,
                      const double* d_pos, const int32_t* d_species, int nsp, const double* h_cut, int mode,
                      PairList& pl) {
+  IPG_RET(ipg_side_join(ctx));
   std::string pre(prefix);
   PairTest t;
   memset(&t, 0, sizeof(t));
@@ -706,7 +714,10 @@ int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const
   if (n > 0)
     IPG_LAUNCH(ctx, k_filter_walk<true>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cached.d_off,
                cached.d_j, d_pos, d_species, nsp, nullptr, pl.d_off, pl.d_j, pl.d_r);
-  IPG_RET(build_transpose(ctx, pre, n, pl));
+  IPG_RET(ipg_side_begin(ctx));
+  const int st = build_transpose(ctx, pre, n, pl);
+  IPG_RET(ipg_side_end(ctx));
+  IPG_RET(st);
   return IPG_OK;
 }
 

@@ -2584,6 +2584,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     if (n) IPG_RET(launch_atoms<MODE_DESC>(s, dev, io, n, nullptr));
   }
   if (out.W6) IPG_RET(scratch(ctx, "snap_w6", 6 * (size_t)n + 6, &w6));
+  IPG_RET(ipg_side_join(ctx));  // the list transpose (side stream) is read from here on
   if ((out.F || out.W6) && fvec && n)
     IPG_TIMED_LAUNCH(ctx, "snap_gather", k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off,
                      pl.d_in_pair, fvec, nch, d_pos, out.F, w6);
@@ -2644,7 +2645,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   }
   if (out.pl_out) *out.pl_out = pl;
   if (out.utot_out) *out.utot_out = io.utot_in;
-  return IPG_OK;
+  return ipg_side_join(ctx);
 }
 
 // ---- CUDA-graph replay of batched evaluations -------------------------------------------
