@@ -79,6 +79,23 @@ int ipg_timing_mark(ipg_ctx* ctx, const char* name, bool start);
   } while (0)
 
 int ipg_fail(ipg_ctx* ctx, int code, const char* fmt, ...);
+
+// Host input checks as single branch-free passes (the compiler vectorises them; the early-exit
+// loops they replace cost ~0.1 ms per 54,000 atoms in front of every host-pointer call).
+inline bool host_all_finite(const double* x, int64_t m) {
+  uint64_t bad = 0;
+  for (int64_t k = 0; k < m; k++) {
+    uint64_t b;
+    memcpy(&b, x + k, sizeof(b));
+    bad |= (uint64_t)(((b >> 52) & 0x7ffu) == 0x7ffu);  // exponent all ones: Inf or NaN
+  }
+  return bad == 0;
+}
+inline bool host_species_ok(const int32_t* sp, int64_t n, int nsp) {
+  uint32_t bad = 0;
+  for (int64_t k = 0; k < n; k++) bad |= (uint32_t)((uint32_t)sp[k] >= (uint32_t)nsp);
+  return bad == 0;
+}
 int ipg_cuda_check(ipg_ctx* ctx, cudaError_t e, const char* what);
 
 #define CUDA_RET(ctx, call) IPG_RET(ipg_cuda_check((ctx), (call), #call))

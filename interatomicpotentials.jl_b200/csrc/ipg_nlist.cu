@@ -740,12 +740,9 @@ int neighbor_pairs(ipg_ctx* ctx, int64_t n, const double* pos, const double L[3]
   if (base != IPG_NLIST_HALF && base != IPG_NLIST_FULL) return ipg_fail(ctx, IPG_ERR_ARG, "bad mode");
   if (base == IPG_NLIST_FULL && !species) return ipg_fail(ctx, IPG_ERR_ARG, "full list needs species");
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
-  for (int64_t k = 0; k < 3 * n; k++)
-    if (!std::isfinite(pos[k])) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite position");
-  if (species)
-    for (int64_t k = 0; k < n; k++)
-      if (species[k] < 0 || species[k] >= std::max(1, (int)nspecies))
-        return ipg_fail(ctx, IPG_ERR_SPECIES, "species id out of range");
+  if (!host_all_finite(pos, 3 * n)) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite position");
+  if (species && !host_species_ok(species, n, std::max(1, (int)nspecies)))
+    return ipg_fail(ctx, IPG_ERR_SPECIES, "species id out of range");
   double *d_pos;
   int32_t* d_sp = nullptr;
   IPG_RET(scratch(ctx, "nl_in_pos", 3 * (size_t)n + 3, &d_pos));

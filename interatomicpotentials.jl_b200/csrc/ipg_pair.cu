@@ -335,10 +335,8 @@ int ipg_pair_eval(ipg_ctx* ctx, int64_t n, const double* pos, const int32_t* spe
                   const ipg_pair_term* terms, int32_t nterms, double* E, double* F, double* W6, uint32_t flags) {
   IPG_RET(check_pair_args(ctx, n, pos, species, L, terms, nterms, E, F, W6, flags));
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
-  for (int64_t k = 0; k < 3 * n; k++)
-    if (!std::isfinite(pos[k])) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite position");
-  for (int64_t k = 0; k < n; k++)
-    if (species[k] < 0 || species[k] >= 64) return ipg_fail(ctx, IPG_ERR_SPECIES, "species id out of range 0..63");
+  if (!host_all_finite(pos, 3 * n)) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite position");
+  if (!host_species_ok(species, n, 64)) return ipg_fail(ctx, IPG_ERR_SPECIES, "species id out of range 0..63");
   double *d_pos, *d_out;
   int32_t* d_sp;
   IPG_RET(scratch(ctx, "pair_in_pos", 3 * (size_t)n + 3, &d_pos));

@@ -2818,10 +2818,9 @@ int check_common(ipg_snap* s, int64_t n, const void* pos, const void* species, c
 }
 
 int check_host_inputs(ipg_snap* s, int64_t n, const double* pos, const int32_t* species) {
-  for (int64_t k = 0; k < 3 * n; k++)
-    if (!std::isfinite(pos[k])) return ipg_fail(s->ctx, IPG_ERR_NONFINITE, "non-finite position");
-  for (int64_t k = 0; k < n; k++)
-    if (species[k] < 0 || species[k] >= s->p.nspecies) return ipg_fail(s->ctx, IPG_ERR_SPECIES, "species id out of range");
+  if (!host_all_finite(pos, 3 * n)) return ipg_fail(s->ctx, IPG_ERR_NONFINITE, "non-finite position");
+  if (!host_species_ok(species, n, s->p.nspecies))
+    return ipg_fail(s->ctx, IPG_ERR_SPECIES, "species id out of range");
   return IPG_OK;
 }
 
