@@ -64,6 +64,7 @@ int ipg_sync(ipg_ctx* ctx) {
 
 int ipg_side_begin(ipg_ctx* ctx) {
   IPG_RET(ipg_side_join(ctx));
+  if (!ctx->side_enabled) return IPG_OK;
   if (!ctx->side) {
     CUDA_RET(ctx, cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
     CUDA_RET(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
@@ -241,6 +242,7 @@ int ipg_create(int device, ipg_ctx** out) {
   ctx->num_sms = prop.multiProcessorCount;
   if (const char* e = getenv("IPG_WALK_BY_ATOM")) ctx->walk_by_cell = e[0] != '1';
   if (const char* e = getenv("IPG_WALK_SINGLE")) ctx->walk_single = e[0] != '0';
+  if (const char* e = getenv("IPG_SIDE_STREAM")) ctx->side_enabled = e[0] != '0';
   int dev0 = 0;
   cudaGetDevice(&dev0);
   if (cudaSetDevice(device) != cudaSuccess ||

@@ -59,6 +59,7 @@ struct ipg_ctx {
   cudaStream_t side_main = nullptr;  // `stream` while the side stream stands in for it
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_pending = false;
+  bool side_enabled = true;  // IPG_SIDE_STREAM=0: everything on `stream`
 };
 
 // Runs the launches between ipg_side_begin and ipg_side_end on the side stream (ctx->stream
