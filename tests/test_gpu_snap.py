@@ -310,6 +310,25 @@ def test_plain_paths_agree(J, monkeypatch):
         assert abs(e - eo) <= TOL * abs(eo) and rel_err(f, fo) <= TOL and rel_err(w, wo) <= TOL, (generic, zchunk)
 
 
+def test_neighbor_switches_bitwise(monkeypatch):
+    """The neighbor build walked once into padded slots or twice (IPG_WALK_SINGLE), and the list
+    transpose on the side stream or in order (IPG_SIDE_STREAM), give bit-identical forces; so do
+    repeated calls on one handle (the first call walks twice, later ones once)."""
+    s, prm, beta = W.snap_j8(cells=5)
+    ref = None
+    for single, side in (("0", "0"), ("1", "1"), ("1", "0"), ("0", "1")):
+        monkeypatch.setenv("IPG_WALK_SINGLE", single)
+        monkeypatch.setenv("IPG_SIDE_STREAM", side)
+        ctx = ipg.Context(0)
+        snap = ipg.SNAP(len(s), prm["twojmax"], prm["species"], prm["rcutfac"], prm["rmin0"], prm["rfac0"],
+                        prm["radii"], prm["weight"], switch_flag=True, ctx=ctx)
+        for _ in range(3):
+            e, f, w = snap.energy_forces(s, beta, mode="adjoint")
+            if ref is None:
+                ref = (e, f, w)
+            assert e == ref[0] and np.array_equal(f, ref[1]) and np.array_equal(w, ref[2]), (single, side)
+
+
 def test_twojmax_beyond_shared_memory_is_unsupported():
     """twojmax 12 needs more than 227 KB of shared memory per block: a clean error."""
     s = ipg.System(np.random.default_rng(0).uniform(0, 5, (10, 3)), ["A"] * 10, [5.0] * 3)
