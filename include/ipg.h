@@ -19,7 +19,9 @@
  *    reference's ustrip.
  *  - Host-pointer entry points copy inputs to the device and results back before they
  *    return.  *_dev entry points take device pointers and run on the context's stream
- *    (set with ipg_set_stream); they synchronise that stream before returning.
+ *    (set with ipg_set_stream); they synchronise that stream before returning.  Inside a
+ *    call the library may fork work onto a second, internal stream of the context (event
+ *    fork and join, also valid inside a graph capture); it is joined before the call returns.
  *  - Ownership: the caller owns every buffer it passes.  The library owns the device
  *    scratch inside a context and grows it on demand.
  *  - Threading: one context per host thread; calls on distinct contexts are independent.
