@@ -1411,7 +1411,6 @@ __global__ void __launch_bounds__(GB_WARPS * 32) k_snap_bdesc(const __grid_const
 namespace plaintab {
 constexpr int zrow_count(int j) { return (j / 2 + 1) * (j + 1); }
 constexpr int imin(int a, int b) { return a < b ? a : b; }
-constexpr int nfull_c(int l) { return ((l + 1) / 2) * (l + 1) + ((l & 1) ? 0 : l / 2); }
 constexpr int idxb_of(int J, int a, int b, int c) {
   int k = 0;
   for (int j1 = 0; j1 <= J; j1++)
