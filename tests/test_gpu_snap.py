@@ -382,3 +382,36 @@ def test_verlet_skin_reuse():
     # the skin list also serves the plain path and the descriptors
     E2, F2, _ = md.energy_forces(s, beta, mode="plain")
     assert rel_err(F2, F0) <= 1e-12
+
+
+@pytest.mark.parametrize("case", ["single", "isolated_and_pair", "sparse"])
+def test_register_chain_paths_edge_cases(case):
+    """Atoms without neighbors (a lone atom, an isolated atom beside a close pair, a sparse gas)
+    through every register-chain path: local descriptors, adjoint and plain energy and forces,
+    and the beta pullback, against the oracle."""
+    rng = np.random.default_rng(500)
+    if case == "single":
+        pos = np.array([[1.0, 2.0, 3.0]])
+    elif case == "isolated_and_pair":
+        pos = np.array([[1.0, 1.0, 1.0], [9.0, 9.0, 9.0], [9.0, 9.0, 10.1]])
+    else:
+        pos = rng.uniform(0, 30, (40, 3))
+    n = len(pos)
+    sym = ["A" if k % 3 else "B" for k in range(n)]
+    s = ipg.System(pos, sym, [30.0] * 3)
+    prm = dict(twojmax=8, species=["A", "B"], rcutfac=2.2, rmin0=0.0, rfac0=0.99363, radii=[1.0, 0.8],
+               weight=[1.0, 0.7], switch_flag=True)
+    snap, orc = make(prm)
+    sp = np.array([0 if x == "A" else 1 for x in sym], np.int32)
+    Bo, _, _ = orc.descriptors(s.positions, sp, s.L)
+    assert rel_err(ipg.compute_local_descriptors(s, snap), Bo) <= TOL
+    beta = rng.normal(0, 1e-2, (2, Bo.shape[1]))
+    eo, fo, _ = orc.energy_forces(s.positions, sp, s.L, beta, 0.0)
+    for mode in ("adjoint", "plain"):
+        e, f, _ = snap.energy_forces(s, beta, 0.0, mode=mode)
+        assert abs(e - eo) <= TOL * max(abs(eo), 1e-300), mode
+        assert np.abs(f - fo).max() <= TOL * max(np.abs(fo).max(), 1.0), mode
+    gF = rng.normal(size=(n, 3))
+    gb, _ = snap.vjp_beta(s, 0.4, gF)
+    go, _ = orc.vjp_beta(s.positions, sp, s.L, 0.4, gF)
+    assert rel_err(gb, go) <= TOL
