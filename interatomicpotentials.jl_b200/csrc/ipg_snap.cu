@@ -1029,7 +1029,7 @@ __device__ __forceinline__ double yr_tile(const SnapDev& S, const YConst& T, con
 }
 
 // Tiles of a row of nma entries: at most YR_TILE wide, as even as possible.
-constexpr int YR_TILE = 6;
+constexpr int YR_TILE = 5;  // widths 4, 5, 6 measured 1.80, 1.77, 1.86 ms at 54,000 atoms
 
 __device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, const YRowDev& row,
                                          const double2* __restrict__ usl, const double* __restrict__ yc,
@@ -1046,7 +1046,7 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, cons
   case NT:         \
     e += yr_tile<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout); \
     break;
-      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5)
 #undef IPG_NT
       default:
         break;
@@ -1102,7 +1102,7 @@ __device__ __forceinline__ void yr_row_z(const SnapDev& S, const YConst& T, cons
   case NT:         \
     yr_tile_z<NT>(S, T, row, ma0, nma, usl, cas, n, atom, valid, zout); \
     break;
-      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5)
 #undef IPG_NT
       default:
         break;
