@@ -508,6 +508,7 @@ __device__ __forceinline__ void advance_u_rt(ChainU<J>& s, double2 a, double2 b,
 // a flush has lane pair (2q, 2q+1) sum the real and imaginary part of slot q over the 32
 // lanes in fixed order and write the Utot entry and its inversion-symmetric mirror.
 constexpr int UT_SLOTS = 16;
+static_assert(2 * UT_SLOTS <= 32, "a flush sums one slot per lane pair: at most 16 slots");
 struct UtStage {
   double2* buf;  // [UT_SLOTS][33] of this warp
   int* dst;      // [UT_SLOTS] packed destination of each slot
