@@ -50,7 +50,7 @@ KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot_all<8>",
 # DRAM bytes (read + write) per atom of one launch, from the ncu --set full captures on the
 # 16,000-atom case summarised in profiles/k_snap_{yrows,pair_adj_all,utot_all}_snap_j8.md;
 # scaled by atoms (pairs per atom are the same).
-NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.971840e6 + 2.481664e6) / 16000,
+NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (52.024064e6 + 2.487296e6) / 16000,
                            "snap_pair": (52.742144e6 + 0.953088e6) / 16000,
                            "snap_utot": (11.558912e6 + 16.316928e6) / 16000}
 
