@@ -205,6 +205,8 @@ def main():
                     "configuration, e.g. so that a profiler's launch list holds only the measured steps")
     ap.add_argument("--cells", type=int, default=30, help="BCC cells per axis (30 -> 54,000 atoms); smaller "
                     "values give the small cases used for profiling")
+    ap.add_argument("--pair-cells", type=int, default=101, help="FCC cells per axis of the scaled linear "
+                    "combination (101 -> 4.12 M atoms); smaller values give the pair kernel's profiling case")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -265,7 +267,7 @@ def main():
     # per-kernel device timing (ipg_timing_read names); snap_zrows .. snap_gbeta are the plain,
     # descriptor and pullback kernels of the register-chain path
     TIMED_KERNELS = ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval",
-                     "snap_zrows", "snap_bdesc", "snap_dbfused", "snap_vsum", "snap_gbeta")
+                     "snap_zrows", "snap_bdesc", "snap_dbfused", "snap_vsum", "snap_gbeta", "snap_hvp")
 
     def timed(fn, steps, kernel_timing=False):
         for _ in range(args.warmup):
@@ -389,10 +391,22 @@ def main():
         Fref_b = np.asarray(db.F.cpu().numpy()) * 1.01
         ms_bl, _, _ = timed(lambda: snap.batch_loss_grad(systems_b, beta_b, Fref_b), 2)
         ctx.set_stream(stream.cuda_stream)
+        # one force-matching training step on device buffers (E, F, loss, dL/dbeta), eager and
+        # as one CUDA-graph launch (ipg_snap_batch_loss_grad_dev)
+        Fref_d = torch.tensor(Fref_b, device=dev)
+        nts = max(2, args.steps // 5)
+        ms_te, _, _ = timed(lambda: db.train_step(beta_b, Fref_d, 0.0, graph=False), nts)
+        db.train_step(beta_b, Fref_d, 0.0, graph=True)  # capture (untimed)
+        l0 = ctx.launch_count()
+        ms_tg, _, _ = timed(lambda: db.train_step(beta_b, Fref_d, 0.0, graph=True), nts)
+        ctx.set_stream(stream.cuda_stream)
         line["batch512"] = {"n_configs": len(systems_b), "n_atoms": nb_atoms,
                             "eager_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_be * 1e-3),
                             "graph_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_bg * 1e-3),
-                            "loss_grad_ms": ms_bl / 2}
+                            "ef_graph_ms": ms_bg / max(2, args.steps // 5),
+                            "loss_grad_ms": ms_bl / 2,
+                            "train_step_eager_ms": ms_te / nts, "train_step_graph_ms": ms_tg / nts,
+                            "train_step_graph_library_launches": (ctx.launch_count() - l0) / (nts + args.warmup)}
         del db
     if "plain" in extras:
         ms_plain, _, ktp = timed(lambda: step(SNAP_PLAIN), max(2, args.steps // 2), kernel_timing=True)
@@ -408,6 +422,11 @@ def main():
         ctx.set_stream(stream.cuda_stream)
         line["vjp_beta"] = {"ms_per_call": ms_v / max(2, args.steps // 5),
                             "kernel_ms_per_call": {k: v[0] / max(2, args.steps // 5) for k, v in ktv.items() if v[1]}}
+        # the full pullback with the exact position term (-gE F - H gF, ipg_snap_vjp)
+        ms_p, _, ktp2 = timed(lambda: snap.vjp(system, beta_b, 0.5, gF), 2, kernel_timing=True)
+        ctx.set_stream(stream.cuda_stream)
+        line["vjp_positions"] = {"ms_per_call": ms_p / 2,
+                                 "kernel_ms_per_call": {k: v[0] / 2 for k, v in ktp2.items() if v[1]}}
     if "desc" in extras:
         ms_d, _, ktd = timed(lambda: ipg.compute_local_descriptors(system, snap), max(2, args.steps // 5),
                              kernel_timing=True)
@@ -417,7 +436,7 @@ def main():
                                                       if v[1]}}
     if "pair" in extras:
         pair = {}
-        for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000()), ("lc_scaled", W.lc32000(cells=101))):
+        for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000()), ("lc_scaled", W.lc32000(cells=args.pair_cells))):
             pairs = ipg.api.neighbor_count(s2, p2.get_rcutoff(), ctx=ctx)
             terms = ipg.empirical.empirical_terms(p2)
             idx = {s: k for k, s in enumerate(s2.unique_symbols())}

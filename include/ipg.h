@@ -76,8 +76,13 @@ IPG_API int ipg_launch_count(const ipg_ctx* ctx, int64_t* out);
 /* Per-kernel device timing (instrumentation with no counterpart in the reference):
  * when enabled, the dominant kernels are bracketed by CUDA events on the context's
  * stream.  ipg_timing_read returns the summed milliseconds and launch count recorded
- * under `kernel` ("snap_atom", "snap_contract", "snap_gather", "pair_eval",
- * "neighbor") since the last read, and resets them. */
+ * under `kernel` since the last read, and resets them.  Names: "neighbor" (the whole
+ * neighbor build), "pair_eval" (pair potentials), and the SNAP kernels "snap_utot" (Utot),
+ * "snap_atom" (the Y kernel of the adjoint path, or the per-atom block kernel),
+ * "snap_pair" (per-neighbor adjoint forces), "snap_gather" (force gather), "snap_zrows" (Z),
+ * "snap_bdesc" (B), "snap_dbfused" (plain dB/dr), "snap_contract" (plain-path contraction),
+ * "snap_vsum" and "snap_gbeta" (beta pullback), "snap_hvp" (the exact Hessian-vector product
+ * of the position pullback).  Unknown names read as zero. */
 IPG_API int ipg_timing_enable(ipg_ctx* ctx, int on);
 IPG_API int ipg_timing_read(ipg_ctx* ctx, const char* kernel, double* total_ms, int64_t* launches);
 
@@ -156,16 +161,30 @@ IPG_API int ipg_pair_eval_dev(ipg_ctx* ctx, int64_t n, const double* d_pos, cons
  * Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream) on the
  * current device and not synchronised.  Calls share the scratch array: calls that overlap
  * on the GPU race, so serialise them (one stream).  The first call on a device resolves
- * the scratch address; make it before any stream capture.  Device-side input errors
- * (non-finite positions) are not reported. */
+ * the scratch address; make it before any stream capture.  That address belongs to the
+ * device's CUDA context at the first call and is kept until exit: do not call this entry
+ * point on a device after cudaDeviceReset there.  Device-side input errors are not reported
+ * (there is no status word to read without a synchronisation): a non-finite position is
+ * placed in an arbitrary cell and gives non-finite results, and a species id outside 0..63
+ * is clamped into that range. */
 IPG_API int ipg_pair_eval_noalloc(void* stream, int64_t n, const double* d_pos, const int32_t* d_species,
                                   const double L[3], const ipg_pair_term* terms, int32_t nterms, double* d_E,
                                   double* d_F, double* d_W6, uint32_t flags);
 
 /* ---- SNAP -------------------------------------------------------------------------------
  * ipg_snap_params mirrors SNAP{S,T} (src/BasisSystems/SNAP/types/types.jl:8-25).
- * chem_flag is not built (IPG_ERR_UNSUPPORTED).  wselfall_flag has no effect without
- * chem_flag (compute_ui.jl:142, compute_b.jl:134-155 with one element).               */
+ * chem_flag (explicit multi-element SNAP; it must equal bnorm_flag, snap.jl:10-13): one Utot
+ *   per element (the neighbor's element, compute_ui.jl:155-175), Z per ordered element pair
+ *   (compute_z.jl:5-61), B and dB/dr per element triple (compute_b.jl:15-95, 104-342), so
+ *   K = idxb_max * nspecies^3 (utl.jl:8-25).  The Z index of compute_z.jl:44-47 writes every
+ *   pair into the first block; literal_chem_z reproduces that, the default keeps one block per
+ *   pair.  bzero shifts the centre element's triple (every triple with wselfall_flag).
+ * quadratic_flag (quadratic SNAP, the option of LAMMPS_SNAP/snap.jl:45-47): the K linear
+ *   components are followed by 0.5 B_k^2 and B_k B_l (l > k), K + K(K+1)/2 in all; beta and
+ *   the descriptors use that length.
+ * With chem_flag or quadratic_flag the evaluation runs the per-atom element-resolved kernel
+ *   (forces through dB/dr in either mode) and ipg_snap_vjp's position pullback returns
+ *   IPG_ERR_UNSUPPORTED.  wselfall_flag puts wself on every element's Utot.                */
 #define IPG_MAX_SNAP_SPECIES 8
 typedef struct ipg_snap_params {
   int32_t twojmax;
@@ -181,6 +200,8 @@ typedef struct ipg_snap_params {
   int32_t switch_flag;
   int32_t wselfall_flag;
   int32_t literal_sqrt_radius; /* reproduce utl.jl:81's sqrt(cutmax) search radius */
+  int32_t quadratic_flag;      /* quadratic SNAP                                       */
+  int32_t literal_chem_z;      /* reproduce compute_z.jl:44-47's Z index with chem_flag */
 } ipg_snap_params;
 
 /* Builds the prebuilt tables of initialize_prebuilt_arrays (prebuilt_arrays.jl:48-247)
@@ -230,10 +251,11 @@ IPG_API int ipg_snap_vjp_beta(ipg_snap* snap, int64_t n, const double* pos, cons
  * for LBasisPotential over SNAP): cotangents gE of E and gF [3n] of F (NULL = 0) give
  *   gbeta [nspecies][K] and gbeta0 as ipg_snap_vjp_beta, and
  *   gpos [3n] = d(gE E + gF . F)/dpos = -gE F - H gF    (H: Hessian of E).
- * -gE F is exact (one adjoint evaluation).  H gF is the derivative of the forces along gF,
- * taken by central differences with Richardson extrapolation (steps 2e-4 and 1e-4 of the
- * largest cutoff along gF / max|gF|; four adjoint evaluations, error O(h^4)).  Any of
- * gbeta, gbeta0, gpos may be NULL; beta [nspecies][K] is needed for gpos.  The reference
+ * Both terms are exact: F from one adjoint evaluation, H gF as the directional derivative of
+ * the adjoint force computation along gF (forward-mode tangents through the Wigner recursion,
+ * Utot, Z, Y and dE/dr; the second-order extension of compute_dij.jl:5-74), in one extra
+ * kernel pass.  Any of gbeta, gbeta0, gpos may be NULL; beta [nspecies][K] is needed for gpos.
+ * twojmax above 8 returns IPG_ERR_UNSUPPORTED for gpos (shared memory).  The reference
  * defines no rrule; this is the pullback that Zygote / ChainRules callers of
  * energy_and_force(s, lbp) need.                                                          */
 IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],
@@ -256,7 +278,9 @@ IPG_API int ipg_snap_autotune(ipg_snap* snap, int64_t n, const double* pos, cons
  * enlarged by `skin` and kept in the handle; later calls with the same atom count,
  * configuration offsets and boxes take their pairs from it (re-measured at the current
  * positions with the same inclusion test as a fresh build) until some atom has moved more
- * than skin/2 since the build, which rebuilds it.  Results equal those of a fresh build up
+ * than skin/2 since the build, a species id differs from the one at the build (the enlarged
+ * cutoffs depend on the species pair) or a position is not finite; any of these rebuilds it,
+ * so bad inputs are reported as by a fresh build.  Results equal those of a fresh build up
  * to the order of summation.  skin = 0 (the default) builds every call; graph replays and
  * the literal search radius always build.  ipg_snap_skin_stats counts builds and reuses.  */
 IPG_API int ipg_snap_set_skin(ipg_snap* snap, double skin);
@@ -297,6 +321,19 @@ IPG_API int ipg_snap_batch_energy_forces_dev(ipg_snap* snap, int32_t nconfig, co
 IPG_API int ipg_snap_batch_loss_grad(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets, const double* pos,
                              const int32_t* species, const double* L, const double* beta, double beta0,
                              const double* F_ref, double* loss, double* gbeta);
+/* One training step of force matching on device buffers: E [nconfig], F [3 n_total] (required),
+ * W6 [nconfig][6] (E and W6 may be NULL), the loss L = sum |F - F_ref|^2 [1] and dL/dbeta
+ * [nspecies][K], from one adjoint evaluation whose pair list, Utot and Z the beta pullback
+ * reuses.  The pullback of the force-matching loss through LBasisPotential's forces
+ * (src/BasisPotentials/linear_potential.jl:37-49) over the fitting rows of
+ * src/BasisSystems/LAMMPS_SNAP/bispectrum.jl:279-387; the reference evaluates it only by
+ * assembling the dB matrix.  graph != 0: as ipg_snap_batch_energy_forces_dev, the whole step
+ * (neighbor build, evaluation, loss, gradient) is captured on the first call and later calls
+ * with the same offsets, boxes and buffers replay it with one graph launch.               */
+IPG_API int ipg_snap_batch_loss_grad_dev(ipg_snap* snap, int32_t nconfig, const int64_t* atom_offsets,
+                                         const double* d_pos, const int32_t* d_species, const double* L,
+                                         const double* beta, double beta0, const double* d_F_ref, int32_t graph,
+                                         double* d_E, double* d_F, double* d_W6, double* d_loss, double* d_gbeta);
 
 #ifdef __cplusplus
 }

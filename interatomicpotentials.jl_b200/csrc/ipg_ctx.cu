@@ -1,4 +1,5 @@
 // ipg_ctx.cu — context lifetime, error reporting, device scratch, status word, scan.
+#include <algorithm>
 #include <cstdarg>
 
 #include <cstdlib>
@@ -104,6 +105,86 @@ int ipg_status_check(ipg_ctx* ctx, const char* what) {
   if (st == IPG_ERR_NONFINITE) return ipg_fail(ctx, st, "%s: non-finite position", what);
   if (st == IPG_ERR_SPECIES) return ipg_fail(ctx, st, "%s: species id out of range", what);
   if (st != IPG_OK) return ipg_fail(ctx, st, "%s: device status %d", what, st);
+  return IPG_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Pinned staging of large host copies.
+namespace {
+constexpr size_t PIN_CHUNK = size_t(8) << 20;   // bytes per ring slot
+constexpr size_t PIN_DIRECT = size_t(1) << 20;  // smaller copies go straight through the driver
+
+// True when p is page-locked host memory that the device can copy from directly.
+bool host_is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+int pinned_ring(ipg_ctx* ctx) {
+  for (int k = 0; k < 2; k++) {
+    if (!ctx->pinned[k]) {
+      void* p = nullptr;
+      if (cudaMallocHost(&p, PIN_CHUNK) != cudaSuccess) {
+        cudaGetLastError();
+        return ipg_fail(ctx, IPG_ERR_NOMEM, "pinned staging allocation failed");
+      }
+      ctx->pinned[k] = static_cast<char*>(p);
+    }
+    if (!ctx->pinned_ev[k]) CUDA_RET(ctx, cudaEventCreateWithFlags(&ctx->pinned_ev[k], cudaEventDisableTiming));
+  }
+  return IPG_OK;
+}
+}  // namespace
+
+int ipg_copy_d2h(ipg_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return IPG_OK;
+  if (bytes < PIN_DIRECT || ctx->capturing || host_is_pinned(dst)) {
+    CUDA_RET(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
+    return IPG_OK;
+  }
+  IPG_RET(pinned_ring(ctx));
+  const size_t nchunk = (bytes + PIN_CHUNK - 1) / PIN_CHUNK;
+  auto issue = [&](size_t c) -> int {
+    const size_t off = c * PIN_CHUNK, len = std::min(PIN_CHUNK, bytes - off);
+    CUDA_RET(ctx, cudaMemcpyAsync(ctx->pinned[c & 1], static_cast<const char*>(src) + off, len,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_RET(ctx, cudaEventRecord(ctx->pinned_ev[c & 1], ctx->stream));
+    return IPG_OK;
+  };
+  IPG_RET(issue(0));
+  if (nchunk > 1) IPG_RET(issue(1));
+  for (size_t c = 0; c < nchunk; c++) {
+    CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[c & 1]));
+    const size_t off = c * PIN_CHUNK, len = std::min(PIN_CHUNK, bytes - off);
+    memcpy(static_cast<char*>(dst) + off, ctx->pinned[c & 1], len);
+    if (c + 2 < nchunk) IPG_RET(issue(c + 2));
+  }
+  return IPG_OK;
+}
+
+int ipg_copy_h2d(ipg_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return IPG_OK;
+  if (bytes < PIN_DIRECT || ctx->capturing || host_is_pinned(src)) {
+    CUDA_RET(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return IPG_OK;
+  }
+  IPG_RET(pinned_ring(ctx));
+  const size_t nchunk = (bytes + PIN_CHUNK - 1) / PIN_CHUNK;
+  for (size_t c = 0; c < nchunk; c++) {
+    if (c >= 2) CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[c & 1]));  // the slot's last DMA is done
+    const size_t off = c * PIN_CHUNK, len = std::min(PIN_CHUNK, bytes - off);
+    memcpy(ctx->pinned[c & 1], static_cast<const char*>(src) + off, len);
+    CUDA_RET(ctx, cudaMemcpyAsync(static_cast<char*>(dst) + off, ctx->pinned[c & 1], len, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CUDA_RET(ctx, cudaEventRecord(ctx->pinned_ev[c & 1], ctx->stream));
+  }
+  // the ring is reused by the next copy: wait until the DMAs out of it are done
+  for (int k = 0; k < 2 && k < (int)nchunk; k++) CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[k]));
   return IPG_OK;
 }
 
@@ -237,10 +318,22 @@ int ipg_create(int device, ipg_ctx** out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return IPG_ERR_CUDA;
   if (prop.major != 10) return IPG_ERR_NODEVICE;  // built for sm_100a only
+  {  // the kernels in this library must be sm_100 code that this device can run
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    cudaFuncAttributes fa;
+    const bool ok = cudaSetDevice(device) == cudaSuccess &&
+                    cudaFuncGetAttributes(&fa, k_scan_add) == cudaSuccess && fa.binaryVersion == 100;
+    cudaGetLastError();
+    cudaSetDevice(dev0);
+    if (!ok) return IPG_ERR_NODEVICE;
+  }
   ipg_ctx* ctx = new ipg_ctx();
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
   if (const char* e = getenv("IPG_WALK_BY_ATOM")) ctx->walk_by_cell = e[0] != '1';
+  if (const char* e = getenv("IPG_PAIR_FULL")) ctx->pair_full_stencil = e[0] == '1';
+  if (const char* e = getenv("IPG_PAIR_MINB")) ctx->pair_minb = std::max(3, std::min(5, atoi(e)));
   if (const char* e = getenv("IPG_WALK_SINGLE")) ctx->walk_single = e[0] != '0';
   if (const char* e = getenv("IPG_SIDE_STREAM")) ctx->side_enabled = e[0] != '0';
   int dev0 = 0;
@@ -276,6 +369,10 @@ int ipg_destroy(ipg_ctx* ctx) {
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  for (int k = 0; k < 2; k++) {
+    if (ctx->pinned[k]) cudaFreeHost(ctx->pinned[k]);
+    if (ctx->pinned_ev[k]) cudaEventDestroy(ctx->pinned_ev[k]);
+  }
   delete ctx;
   return IPG_OK;
 }

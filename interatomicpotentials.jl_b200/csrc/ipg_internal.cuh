@@ -49,6 +49,8 @@ struct ipg_ctx {
   bool capturing = false;
   uint64_t scratch_gen = 0;
   bool walk_by_cell = true;  // neighbor walk: one warp per cell (false: one warp per atom)
+  bool pair_full_stencil = false;  // pair potentials: full-stencil walk even where the half stencil applies
+  int pair_minb = 4;               // pair potentials: register bound of the half-stencil kernel (3, 4, 5)
   // single-pass neighbor walk: per list prefix, the per-atom slot count of the padded
   // emission (from the largest count of the previous build; 0 = walk twice)
   std::map<std::string, int> walk_kcap;
@@ -60,6 +62,10 @@ struct ipg_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_pending = false;
   bool side_enabled = true;  // IPG_SIDE_STREAM=0: everything on `stream`
+  // pinned staging ring for large copies between device memory and the caller's pageable host
+  // buffers (ipg_copy_d2h / ipg_copy_h2d)
+  char* pinned[2] = {nullptr, nullptr};
+  cudaEvent_t pinned_ev[2] = {nullptr, nullptr};
 };
 
 // Runs the launches between ipg_side_begin and ipg_side_end on the side stream (ctx->stream
@@ -110,13 +116,22 @@ int scratch(ipg_ctx* ctx, const char* name, size_t count, T** out) {
   *out = static_cast<T*>(p);
   return IPG_OK;
 }
-// Named pinned host staging buffer.
+// Named host staging buffer (pageable: for small uploads, which the driver copies out of the
+// buffer before cudaMemcpyAsync returns).
 template <class T>
 T* host_scratch(ipg_ctx* ctx, const char* name, size_t count) {
   auto& v = ctx->hbufs[name];
   if (v.size() < count * sizeof(T)) v.resize(count * sizeof(T));
   return reinterpret_cast<T*>(v.data());
 }
+
+// Copies between device memory and a caller's (pageable) host buffer on ctx->stream.  Large
+// copies go through a ring of two pinned chunks, so the DMA of one chunk overlaps the host copy
+// of the other; a copy from pageable memory is staged by the driver at a fraction of the
+// bandwidth.  ipg_copy_d2h returns once `dst` holds the data (it synchronises with the stream);
+// ipg_copy_h2d returns once `src` may be reused.
+int ipg_copy_d2h(ipg_ctx* ctx, void* dst, const void* src, size_t bytes);
+int ipg_copy_h2d(ipg_ctx* ctx, void* dst, const void* src, size_t bytes);
 
 // Kernel launch with accounting and error check.
 #define IPG_LAUNCH(ctx, kernel, grid, block, smem, ...)                                          \
@@ -232,8 +247,10 @@ struct PairList {
 int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const PairList& cached,
                      const double* d_pos, const int32_t* d_species, int nsp, const double* h_cut, int mode,
                      PairList& pl);
-// Largest squared minimum-image displacement of d_pos from d_ref (host value, synchronises).
-int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const double* d_ref, double* out);
+// Largest squared minimum-image displacement of d_pos from d_ref (host value, synchronises);
+// +inf when a position is not finite or a species id differs from d_ref_species.
+int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const double* d_ref,
+                  const int32_t* d_species, const int32_t* d_ref_species, double* out);
 // walk_warps: atoms (warps) per block of the neighbor walk, 1..4.
 int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const int32_t* d_species, int nsp,
                     const double* h_cut, int mode, bool want_transpose, PairList& pl, bool sorted = true,

@@ -213,10 +213,13 @@ __global__ void __launch_bounds__(128) k_filter_walk(int64_t n, PairTest t, cons
                                                      const int32_t* __restrict__ cj, const double* __restrict__ pos,
                                                      const int32_t* __restrict__ species, int nsp,
                                                      int64_t* __restrict__ cnt, const int64_t* __restrict__ off,
-                                                     int32_t* __restrict__ outj, double* __restrict__ outr) {
+                                                     int32_t* __restrict__ outj, double* __restrict__ outr,
+                                                     int* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;  // warp-uniform
+  // ids are clamped so every table read stays in bounds; an id out of range is an error
+  if (!EMIT && lane == 0 && species && (species[i] < 0 || species[i] >= nsp)) dev_raise(status, IPG_ERR_SPECIES);
   const int si = species ? (species[i] < 0 ? 0 : (species[i] >= nsp ? nsp - 1 : species[i])) : 0;
   const double4 xi = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], (double)si);
   const double* L = grid[conf[i]].L;
@@ -247,9 +250,12 @@ __global__ void __launch_bounds__(128) k_filter_walk(int64_t n, PairTest t, cons
 }
 
 // Largest squared minimum-image displacement since the reference positions, as the bit
-// pattern of a non-negative double (ordered like the integers).
+// pattern of a non-negative double (ordered like the integers).  A non-finite position, or a
+// species id that differs from the one at the build, counts as an infinite move, so the
+// caller rebuilds the list (and the fresh build reports the bad input).
 __global__ void k_max_disp2(int64_t n, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ conf,
                             const double* __restrict__ pos, const double* __restrict__ ref,
+                            const int32_t* __restrict__ species, const int32_t* __restrict__ ref_species,
                             unsigned long long* __restrict__ out) {
   __shared__ unsigned long long sm[256];
   double m = 0.0;
@@ -260,6 +266,8 @@ __global__ void k_max_disp2(int64_t n, const ConfGrid* __restrict__ grid, const 
       const double s = pe_axis_dev(L[a], pos[3 * i + a], ref[3 * i + a]);
       d2 += s * s;
     }
+    if (!(d2 <= 1.7976931348623157e308)) d2 = INFINITY;  // NaN or Inf: never reuse
+    if (species && ref_species && species[i] != ref_species[i]) d2 = INFINITY;
     m = fmax(m, d2);
   }
   sm[threadIdx.x] = (unsigned long long)__double_as_longlong(m);
@@ -668,14 +676,16 @@ int ipg_build_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const 
   return IPG_OK;
 }
 
-int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const double* d_ref, double* out) {
+int ipg_max_disp2(ipg_ctx* ctx, const CellList& cl, const double* d_pos, const double* d_ref,
+                  const int32_t* d_species, const int32_t* d_ref_species, double* out) {
   *out = 0.0;
   if (cl.n == 0) return IPG_OK;
   unsigned long long* d_m;
   IPG_RET(scratch(ctx, "skin_maxdisp", 1, &d_m));
   CUDA_RET(ctx, cudaMemsetAsync(d_m, 0, sizeof(unsigned long long), ctx->stream));
   const int64_t grid = std::min<int64_t>(nblk(cl.n, 256), 4 * ctx->num_sms);
-  IPG_LAUNCH(ctx, k_max_disp2, (unsigned)grid, 256, 0, cl.n, cl.d_grid, cl.d_conf, d_pos, d_ref, d_m);
+  IPG_LAUNCH(ctx, k_max_disp2, (unsigned)grid, 256, 0, cl.n, cl.d_grid, cl.d_conf, d_pos, d_ref, d_species,
+             d_ref_species, d_m);
   unsigned long long h = 0;
   CUDA_RET(ctx, cudaMemcpyAsync(&h, d_m, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
@@ -708,7 +718,7 @@ int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const
   CUDA_RET(ctx, cudaMemsetAsync(pl.d_off, 0, sizeof(int64_t) * (n + 1), ctx->stream));
   if (n > 0)
     IPG_LAUNCH(ctx, k_filter_walk<false>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cached.d_off,
-               cached.d_j, d_pos, d_species, nsp, pl.d_off, nullptr, nullptr, nullptr);
+               cached.d_j, d_pos, d_species, nsp, pl.d_off, nullptr, nullptr, nullptr, ctx->d_status);
   IPG_RET(ipg_scan_i64(ctx, pl.d_off, pl.d_off, n + 1));
   pl.d_np = pl.d_off + n;
   CUDA_RET(ctx, cudaMemcpyAsync(&pl.npairs, pl.d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -717,7 +727,7 @@ int ipg_filter_pairs(ipg_ctx* ctx, const char* prefix, const CellList& cl, const
   IPG_RET(scratch(ctx, (pre + "r").c_str(), 3 * pl.npairs + 3, &pl.d_r));
   if (n > 0)
     IPG_LAUNCH(ctx, k_filter_walk<true>, nblk(32 * n, 128), 128, 0, n, t, cl.d_grid, cl.d_conf, cached.d_off,
-               cached.d_j, d_pos, d_species, nsp, nullptr, pl.d_off, pl.d_j, pl.d_r);
+               cached.d_j, d_pos, d_species, nsp, nullptr, pl.d_off, pl.d_j, pl.d_r, ctx->d_status);
   const bool side = cl.nconf == 1;  // as in ipg_build_pairs
   if (side) IPG_RET(ipg_side_begin(ctx));
   const int st = build_transpose(ctx, pre, n, pl);

@@ -19,12 +19,15 @@
 // same device) race on g_scratch; the caller must serialise them, e.g. by using one
 // stream.  The first call on a device looks up the device address of g_scratch
 // (cudaGetSymbolAddress, with that device current) and caches it; that first call
-// should come before any stream capture.  Device-side input errors (non-finite
-// positions) are not reported: there is no status word to read without a
-// synchronisation.
+// should come before any stream capture.  Device-side input errors are not reported:
+// there is no status word to read without a synchronisation.  A non-finite position is
+// placed in cell 0 and gives non-finite results; a species id outside 0..63 is clamped
+// into that range.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
-#include "ipg_internal.cuh"
+#include "ipg_pair.cuh"
 
 namespace {
 
@@ -49,73 +52,6 @@ struct Layout {
 
 // The scratch memory of ipg_pair_eval_noalloc (about 4.3 MB).
 static __device__ __align__(256) unsigned char g_scratch[Layout::total];
-
-struct TermND {
-  int kind;
-  int pad;
-  double coeff, rcut;
-  unsigned long long mask;
-  double p[8];
-};
-struct TermsND {
-  int nterms;
-  double rcut_max, rmax2_hi;
-  TermND t[IPG_MAX_PAIR_TERMS];
-};
-
-// The reference's pair formulas (src/empirical/{lj,bm,coulomb,morse,zbl}.jl, test/mocks.jl),
-// as in ipg_pair.cu; p holds the same precomputed constants.
-__device__ __forceinline__ void term_nd(const TermND& t, double R, double& V, double& g) {
-  const double zc[4] = {0.18175, 0.50986, 0.28022, 0.02817};
-  const double za[4] = {3.19980, 0.94229, 0.40290, 0.20162};
-  switch (t.kind) {
-    case IPG_PAIR_LJ: {
-      const double s = t.p[1] / R, s2 = s * s, s6 = s2 * s2 * s2, s12 = s6 * s6;
-      V = t.p[2] * (s12 - s6);
-      g = t.p[3] * (2.0 * s12 - s6) / (R * R);
-      break;
-    }
-    case IPG_PAIR_BM: {
-      const double ex = t.p[0] * exp((t.p[2] - R) / t.p[1]);
-      const double c = t.p[3] / R, d = t.p[4] / R, c2 = c * c, d2 = d * d;
-      const double c6 = c2 * c2 * c2, d8 = (d2 * d2) * (d2 * d2);
-      V = ex + c6 - d8;
-      g = ex / (t.p[1] * R) + (c6 - d8) / (R * R);
-      break;
-    }
-    case IPG_PAIR_COUL:
-      V = t.p[2] / R;
-      g = t.p[2] / (R * R * R);
-      break;
-    case IPG_PAIR_MORSE: {
-      const double e = exp(-t.p[1] * (R - t.p[2])), om = 1.0 - e;
-      V = t.p[0] * om * om;
-      g = 2.0 * t.p[0] * t.p[1] * om * e / R;
-      break;
-    }
-    case IPG_PAIR_ZBL: {
-      const double d = R / t.p[4];
-      double phi = 0.0, dphi = 0.0;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const double ek = exp(-za[k] * d * t.p[5]);
-        phi += zc[k] * ek;
-        dphi += za[k] * zc[k] * ek;
-      }
-      dphi = -dphi;
-      V = t.p[3] * phi / R;
-      g = t.p[3] * (phi + d * dphi) / (R * R * R);
-      break;
-    }
-    case IPG_PAIR_MOCK_R2:
-      V = R * R * t.p[0];
-      g = R * R * t.p[0];
-      break;
-    default:
-      V = 0.0;
-      g = 0.0;
-  }
-}
 
 // Grid set-up on the device (one block): box, open-axis extents, cell edge >= rcut_max,
 // at most NOALLOC_MAX_CELLS cells; clears the cell counters.
@@ -259,116 +195,21 @@ __global__ void k_na_gather(int64_t n, const double* __restrict__ pos, const int
       make_double4(pos[3 * (int64_t)i], pos[3 * (int64_t)i + 1], pos[3 * (int64_t)i + 2], (double)sp);
 }
 
-struct HitND {
-  double r0, r1, r2, dist;
-  int sj, pad;
-};
-
-__device__ __forceinline__ void eval_nd(const TermsND& T, const HitND* hb, int nh, int lane, int si, double* acc,
-                                        double& f0, double& f1, double& f2) {
-  if (lane >= nh) return;
-  const HitND h = hb[lane];
-  const double R = sqrt(h.r0 * h.r0 + h.r1 * h.r1 + h.r2 * h.r2);
-  double V = 0.0, gs = 0.0;
-  for (int t = 0; t < T.nterms; t++) {
-    const TermND& tt = T.t[t];
-    if (h.dist > tt.rcut) continue;
-    if (!((tt.mask >> si) & 1ull) || !((tt.mask >> h.sj) & 1ull)) continue;
-    double v, gg;
-    term_nd(tt, R, v, gg);
-    V += tt.coeff * v;
-    gs += tt.coeff * gg;
-  }
-  const double fx = gs * h.r0, fy = gs * h.r1, fz = gs * h.r2;
-  f0 += fx;
-  f1 += fy;
-  f2 += fz;
-  acc[0] += 0.5 * V;
-  acc[1] += 0.5 * h.r0 * fx;
-  acc[2] += 0.5 * h.r1 * fy;
-  acc[3] += 0.5 * h.r2 * fz;
-  acc[4] += 0.5 * h.r2 * fy;
-  acc[5] += 0.5 * h.r2 * fx;
-  acc[6] += 0.5 * h.r1 * fx;
-}
-
-// Warp per atom over the stencil ranges (grid-stride over atoms); per-block partials of
+// Warp per atom over the stencil ranges (grid-stride over atoms): the full-stencil walk of
+// ipg_pair.cuh, the same code as the context path's fallback kernel.  Per-block partials of
 // E and the virial go to scratch, forces to F.
-__global__ void __launch_bounds__(NA_T) k_na_pair(const __grid_constant__ TermsND T, int64_t n,
+__global__ void __launch_bounds__(NA_T) k_na_pair(const __grid_constant__ PairTerms T, int64_t n,
                                                   unsigned char* scratch, double* __restrict__ F) {
-  __shared__ HitND hits[NA_WARPS][64];
+  __shared__ PairHit hits[NA_WARPS][64];
   __shared__ double red[NA_WARPS][7];
   const ConfGrid g = *reinterpret_cast<const ConfGrid*>(scratch + Layout::grid);
   const int64_t* cell_start = reinterpret_cast<const int64_t*>(scratch + Layout::count);
   const int32_t* cell_atoms = reinterpret_cast<const int32_t*>(scratch + Layout::atoms);
   const double4* spos = reinterpret_cast<const double4*>(scratch + Layout::spos);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int64_t s = (int64_t)blockIdx.x * NA_WARPS + w; s < n; s += (int64_t)gridDim.x * NA_WARPS) {
-    const int32_t i = cell_atoms[s];
-    const double4 xi = spos[s];
-    const int si = (int)xi.w;
-    int c[3];
-    cell_coords(g, xi.x, xi.y, xi.z, c);
-    StencilRanges Rg;
-    stencil_ranges(g, c, cell_start, Rg);
-    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
-    HitND* hb = hits[w];
-    int nh = 0;
-    for (int r = 0; r < Rg.n; r++)
-      for (int64_t q0 = Rg.beg[r]; q0 < Rg.end[r]; q0 += 32) {
-        const int64_t q = q0 + lane;
-        bool ok = false;
-        HitND h;
-        if (q < Rg.end[r]) {
-          const int32_t j = cell_atoms[q];
-          const double4 xj = spos[q];
-          if (j != i) {
-            const double d2 = sumsq3_dev(pe_axis_dev(g.L[0], xi.x, xj.x), pe_axis_dev(g.L[1], xi.y, xj.y),
-                                         pe_axis_dev(g.L[2], xi.z, xj.z));
-            if (d2 <= T.rmax2_hi) {
-              const double dist = sqrt(d2);
-              if (dist <= T.rcut_max) {
-                ok = true;
-                h.dist = dist;
-                h.sj = (int)xj.w;
-                if (j > i) {
-                  h.r0 = disp_axis_dev(g.L[0], xi.x, xj.x);
-                  h.r1 = disp_axis_dev(g.L[1], xi.y, xj.y);
-                  h.r2 = disp_axis_dev(g.L[2], xi.z, xj.z);
-                } else {
-                  h.r0 = -disp_axis_dev(g.L[0], xj.x, xi.x);
-                  h.r1 = -disp_axis_dev(g.L[1], xj.y, xi.y);
-                  h.r2 = -disp_axis_dev(g.L[2], xj.z, xi.z);
-                }
-              }
-            }
-          }
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, ok);
-        if (ok) hb[nh + __popc(bal & lt)] = h;
-        nh += __popc(bal);
-        __syncwarp();
-        if (nh >= 32) {
-          eval_nd(T, hb, 32, lane, si, acc, f0, f1, f2);
-          __syncwarp();
-          if (lane < nh - 32) hb[lane] = hb[32 + lane];
-          nh -= 32;
-          __syncwarp();
-        }
-      }
-    eval_nd(T, hb, nh, lane, si, acc, f0, f1, f2);
-    __syncwarp();
-    f0 = warp_sum(f0);
-    f1 = warp_sum(f1);
-    f2 = warp_sum(f2);
-    if (F && lane == 0) {
-      F[3 * (int64_t)i] = f0;
-      F[3 * (int64_t)i + 1] = f1;
-      F[3 * (int64_t)i + 2] = f2;
-    }
-  }
+  for (int64_t s = (int64_t)blockIdx.x * NA_WARPS + w; s < n; s += (int64_t)gridDim.x * NA_WARPS)
+    pair_walk_atom(T, g, cell_start, cell_atoms, spos, s, hits[w], lane, acc, F);
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     const double v = warp_sum(acc[k]);
@@ -402,21 +243,31 @@ __global__ void k_na_reduce(int nblocks, const unsigned char* scratch, double* E
   }
 }
 
-// Device address of g_scratch, looked up once per device.
+// Device address of g_scratch, looked up once per device (with that device current) and
+// published through an atomic slot; the lookup itself runs under a mutex, so concurrent first
+// calls from several host threads are safe.  The address belongs to the device's context at
+// the lookup; after cudaDeviceReset it is stale (documented in include/ipg.h).
 constexpr int NA_MAX_DEVICES = 64;
-unsigned char* g_scratch_ptr[NA_MAX_DEVICES] = {};
+std::atomic<unsigned char*> g_scratch_ptr[NA_MAX_DEVICES];
+std::mutex g_scratch_mu;
 
 int scratch_address(int dev, unsigned char** out) {
   if (dev < 0 || dev >= NA_MAX_DEVICES) return IPG_ERR_ARG;
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess) {
-      cudaGetLastError();
-      return IPG_ERR_CUDA;
+  unsigned char* p = g_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    p = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+      void* a = nullptr;
+      if (cudaGetSymbolAddress(&a, g_scratch) != cudaSuccess) {
+        cudaGetLastError();
+        return IPG_ERR_CUDA;
+      }
+      p = static_cast<unsigned char*>(a);
+      g_scratch_ptr[dev].store(p, std::memory_order_release);
     }
-    g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
   }
-  *out = g_scratch_ptr[dev];
+  *out = p;
   return IPG_OK;
 }
 
@@ -434,42 +285,9 @@ int ipg_pair_eval_noalloc(void* stream, int64_t n, const double* d_pos, const in
     return IPG_ERR_ARG;
   for (int a = 0; a < 3; a++)
     if (!(L[a] > 0.0)) return IPG_ERR_ARG;
-  TermsND T;
-  memset(&T, 0, sizeof(T));
-  T.nterms = nterms;
-  for (int k = 0; k < nterms; k++) {
-    const ipg_pair_term& s = terms[k];
-    TermND& d = T.t[k];
-    if (!(s.rcut >= 0.0) || std::isinf(s.rcut)) return IPG_ERR_ARG;
-    d.kind = s.kind;
-    d.coeff = s.coeff;
-    d.rcut = s.rcut;
-    d.mask = s.species_mask;
-    for (int q = 0; q < 8; q++) d.p[q] = s.params[q];
-    switch (s.kind) {
-      case IPG_PAIR_LJ:
-        d.p[2] = 4.0 * s.params[0];
-        d.p[3] = 24.0 * s.params[0];
-        break;
-      case IPG_PAIR_COUL:
-        d.p[2] = 1.0 * s.params[0] * s.params[1];
-        break;
-      case IPG_PAIR_ZBL:
-        if (!(s.params[2] > 0.0)) return IPG_ERR_ARG;
-        d.p[3] = 1.0 * s.params[0] * s.params[1] * s.params[2] * s.params[2];
-        d.p[4] = 0.8854 * 0.529 / (std::pow(s.params[0], 0.23) + std::pow(s.params[1], 0.23));
-        d.p[5] = std::log(s.params[2]);
-        break;
-      case IPG_PAIR_BM:
-      case IPG_PAIR_MORSE:
-      case IPG_PAIR_MOCK_R2:
-        break;
-      default:
-        return IPG_ERR_ARG;
-    }
-    T.rcut_max = std::max(T.rcut_max, s.rcut);
-  }
-  T.rmax2_hi = T.rcut_max * T.rcut_max * (1.0 + 1e-12);
+  PairTerms T;
+  char err[256];
+  if (pair_prepare_terms(terms, nterms, T, err, sizeof(err)) != IPG_OK) return IPG_ERR_ARG;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return IPG_ERR_NODEVICE;
   unsigned char* sc = nullptr;

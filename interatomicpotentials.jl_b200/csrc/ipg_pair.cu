@@ -1,222 +1,51 @@
 // ipg_pair.cu — fused multi-term empirical pair potentials.
 //
 // Replaces, for every term of a LinearCombinationPotential at once, the per-term
-// neighbor build + pair loop of src/types/empirical_potential.jl:20-67 with one walk of
-// the cell list at the largest cutoff.  One thread owns one atom (cell-sorted order, so a
-// warp reads the same neighbor cells), visits every candidate once, and applies each
-// term's own cutoff (PeriodicEuclidean distance <= rcut_t, as the term's own neighbor
-// list would) and species filter (both species in the term's set,
-// empirical_potential.jl:26-43).  Each atom sums its full neighbor set, so forces need no
-// atomics; the half-list energy and virial are recovered as 1/2 of the directed sums.
-// For j < i the displacement is the negated reference displacement of the stored half
-// pair (i.e. -get_displacement(x_j, x_i)), so every force term equals the reference's
-// term bit for bit; only the order of summation differs.
-#include "ipg_internal.cuh"
+// neighbor build + pair loop of src/types/empirical_potential.jl:20-67 with one pass over
+// the cell list at the largest cutoff, each term keeping its own cutoff (PeriodicEuclidean
+// distance <= rcut_t, as the term's own neighbor list would) and species filter (both
+// species in the term's set, empirical_potential.jl:26-43).
+//
+// Half-stencil tiles (k_pair_half).  Like the reference's half list (nnlist.jl:39-40, m > n),
+// every unordered pair is evaluated once.  A work item is a (home cell A, offset k) pair,
+// one warp each: k = 0 is A itself (pairs of slots s < s'), k = 1..13 the 13 neighbor cells
+// of the forward half of the 27-cell stencil.  Lanes own the atoms of the target cell
+// (positions in registers), the warp walks the home cell's atoms one row at a time (a
+// broadcast load), the pairs within the largest cutoff are compacted into a per-warp hit
+// buffer in (row, lane) order, and every 32 hits are evaluated by the whole warp.  The force
+// of each hit goes to its two atoms' owner lanes by a broadcast loop in hit order, so every
+// sum runs in a fixed order (no atomics).  A warp writes its row sums and column sums to its
+// own slots of a partial-force buffer, [14 home offsets + 13 target offsets][slot][3], which
+// k_pair_gather sums per atom in a fixed order.  Each pair's force term is the reference's:
+// with lo < hi the atom ids, r = get_displacement(x_lo, x_hi) (nnlist.jl:18-21), f = g(R) r,
+// F_lo += f, F_hi -= f; only the order of summation differs.
+//
+// The half stencil visits each pair of neighboring cells once only when every periodic axis
+// has at least 3 cells; otherwise the full-stencil walk (ipg_pair.cuh) runs instead.
+#include "ipg_pair.cuh"
 
 namespace {
-
-struct PairTermDev {
-  int kind;
-  int pad;
-  double coeff, rcut;
-  unsigned long long mask;
-  double p[8];  // kind-specific precomputed constants (see prepare_terms)
-};
-
-struct PairTerms {
-  int nterms;
-  double rcut_max;
-  double rmax2_hi;  // rcut_max^2 (1 + 1e-12): candidates beyond it are out for sure
-  PairTermDev t[IPG_MAX_PAIR_TERMS];
-};
-
-static_assert(sizeof(PairTerms) <= 4096, "the terms travel as a kernel parameter");
-
-// ZBL screening coefficients, src/empirical/zbl.jl:27-28.
-__constant__ double c_zbl_c[4] = {0.18175, 0.50986, 0.28022, 0.02817};
-__constant__ double c_zbl_a[4] = {3.19980, 0.94229, 0.40290, 0.20162};
-
-// V(R) and g(R) (force = g r) of one term.
-__device__ __forceinline__ void term_eval(const PairTermDev& t, double R, double& V, double& g) {
-  switch (t.kind) {
-    case IPG_PAIR_LJ: {  // lj.jl:35-36; p = eps, sigma, 4eps, 24eps
-      double s = t.p[1] / R;
-      double s2 = s * s;
-      double s6 = s2 * s2 * s2;
-      double s12 = s6 * s6;
-      V = t.p[2] * (s12 - s6);
-      g = t.p[3] * (2.0 * s12 - s6) / (R * R);
-      break;
-    }
-    case IPG_PAIR_BM: {  // bm.jl:38-39; p = A, rho, sigma, C, D
-      double ex = t.p[0] * exp((t.p[2] - R) / t.p[1]);
-      double c = t.p[3] / R, d = t.p[4] / R;
-      double c2 = c * c, d2 = d * d;
-      double c6 = c2 * c2 * c2, d8 = (d2 * d2) * (d2 * d2);
-      V = ex + c6 - d8;
-      g = ex / (t.p[1] * R) + (c6 - d8) / (R * R);
-      break;
-    }
-    case IPG_PAIR_COUL: {  // coulomb.jl:36-37; p = q1, q2, k_e q1 q2
-      V = t.p[2] / R;
-      g = t.p[2] / (R * R * R);
-      break;
-    }
-    case IPG_PAIR_MORSE: {  // morse.jl:36-39; p = D, alpha, sigma
-      double e = exp(-t.p[1] * (R - t.p[2]));
-      double om = 1.0 - e;
-      V = t.p[0] * om * om;
-      g = 2.0 * t.p[0] * t.p[1] * om * e / R;
-      break;
-    }
-    case IPG_PAIR_ZBL: {  // zbl.jl:29-36; p = Z1, Z2, e, coeff = Z1 Z2 e^2, dden, ln(e)
-      double d = R / t.p[4];
-      double phi = 0.0, dphi = 0.0;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        double ek = exp(-c_zbl_a[k] * d * t.p[5]);  // e^(-a_k d) with base e = p[2]
-        phi += c_zbl_c[k] * ek;
-        dphi += c_zbl_a[k] * c_zbl_c[k] * ek;
-      }
-      dphi = -dphi;
-      V = t.p[3] * phi / R;
-      g = t.p[3] * (phi + d * dphi) / (R * R * R);
-      break;
-    }
-    case IPG_PAIR_MOCK_R2: {  // test/mocks.jl:29-34; p = seed
-      V = R * R * t.p[0];
-      g = R * R * t.p[0];
-      break;
-    }
-    default:
-      V = 0.0;
-      g = 0.0;
-  }
-}
 
 constexpr int PAIR_T = 128;
 constexpr int PAIR_WARPS = PAIR_T / 32;
 
-// One warp per atom (cell-sorted order).  Lanes test consecutive candidates of each
-// stencil range; the pairs within the largest cutoff are compacted into a per-warp
-// shared buffer (ballot prefix, candidate order), and every 32 of them are evaluated by
-// the whole warp, so the term arithmetic (exp, pow) runs on full warps.
-struct Hit {
-  double r0, r1, r2, dist;
-  int sj, pad;
-};
-
-__device__ __forceinline__ void eval_hits(const PairTerms& TT, const Hit* __restrict__ hb, int nh, int lane, int si,
-                                          double* acc, double& f0, double& f1, double& f2) {
-  if (lane >= nh) return;
-  const Hit h = hb[lane];
-  const double R = sqrt(h.r0 * h.r0 + h.r1 * h.r1 + h.r2 * h.r2);
-  double V = 0.0, gsum = 0.0;
-  for (int t = 0; t < TT.nterms; t++) {
-    const PairTermDev& T = TT.t[t];
-    if (h.dist > T.rcut) continue;
-    if (!((T.mask >> si) & 1ull) || !((T.mask >> h.sj) & 1ull)) continue;
-    double v, gg;
-    term_eval(T, R, v, gg);
-    V += T.coeff * v;
-    gsum += T.coeff * gg;
-  }
-  const double fx = gsum * h.r0, fy = gsum * h.r1, fz = gsum * h.r2;
-  f0 += fx;
-  f1 += fy;
-  f2 += fz;
-  acc[0] += 0.5 * V;
-  // empirical_potential.jl:63-64: r * f' -> [xx, yy, zz, zy, zx, yx]
-  acc[1] += 0.5 * h.r0 * fx;
-  acc[2] += 0.5 * h.r1 * fy;
-  acc[3] += 0.5 * h.r2 * fz;
-  acc[4] += 0.5 * h.r2 * fy;
-  acc[5] += 0.5 * h.r2 * fx;
-  acc[6] += 0.5 * h.r1 * fx;
-}
-
+// The full-stencil walk, one warp per atom (the fallback for grids with fewer than 3 cells
+// on a periodic axis).
 __global__ void __launch_bounds__(PAIR_T) k_pair_eval(const __grid_constant__ PairTerms TT, int64_t n,
                                                       const ConfGrid* __restrict__ grid,
                                                       const int64_t* __restrict__ cell_start,
                                                       const int32_t* __restrict__ cell_atoms,
                                                       const double4* __restrict__ spos, double* __restrict__ F,
-                                                      double* __restrict__ partial, int* status) {
-  __shared__ Hit hits[PAIR_WARPS][64];
+                                                      double* __restrict__ partial) {
+  __shared__ PairHit hits[PAIR_WARPS][64];
   __shared__ double red[PAIR_WARPS][7];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t s = (int64_t)blockIdx.x * PAIR_WARPS + w;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // E, W[6]
-  if (s < n) {  // warp-uniform
-    const int32_t i = cell_atoms[s];
-    const double4 xi = spos[s];
-    const int si = (int)xi.w;
-    const ConfGrid g = grid[0];
-    int c[3];
-    cell_coords(g, xi.x, xi.y, xi.z, c);
-    StencilRanges Rg;
-    stencil_ranges(g, c, cell_start, Rg);
-    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
-    const double rmax = TT.rcut_max;
-    Hit* hb = hits[w];
-    int nh = 0;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int r = 0; r < Rg.n; r++)
-      for (int64_t q0 = Rg.beg[r]; q0 < Rg.end[r]; q0 += 32) {
-        const int64_t q = q0 + lane;
-        bool ok = false;
-        Hit h;
-        if (q < Rg.end[r]) {
-          const int32_t j = cell_atoms[q];
-          const double4 xj = spos[q];
-          if (j != i) {
-            const double p0 = pe_axis_dev(g.L[0], xi.x, xj.x);
-            const double p1 = pe_axis_dev(g.L[1], xi.y, xj.y);
-            const double p2 = pe_axis_dev(g.L[2], xi.z, xj.z);
-            const double d2 = sumsq3_dev(p0, p1, p2);
-            if (d2 <= TT.rmax2_hi) {
-              const double dist = sqrt(d2);
-              if (dist <= rmax) {
-                ok = true;
-                h.dist = dist;
-                h.sj = (int)xj.w;
-                if (j > i) {
-                  h.r0 = disp_axis_dev(g.L[0], xi.x, xj.x);
-                  h.r1 = disp_axis_dev(g.L[1], xi.y, xj.y);
-                  h.r2 = disp_axis_dev(g.L[2], xi.z, xj.z);
-                } else {  // -get_displacement(x_j, x_i): the reference's stored half pair
-                  h.r0 = -disp_axis_dev(g.L[0], xj.x, xi.x);
-                  h.r1 = -disp_axis_dev(g.L[1], xj.y, xi.y);
-                  h.r2 = -disp_axis_dev(g.L[2], xj.z, xi.z);
-                }
-              }
-            }
-          }
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, ok);
-        if (ok) hb[nh + __popc(bal & lt)] = h;
-        nh += __popc(bal);
-        __syncwarp();
-        if (nh >= 32) {
-          eval_hits(TT, hb, 32, lane, si, acc, f0, f1, f2);
-          __syncwarp();
-          if (lane < nh - 32) hb[lane] = hb[32 + lane];
-          nh -= 32;
-          __syncwarp();
-        }
-      }
-    eval_hits(TT, hb, nh, lane, si, acc, f0, f1, f2);
-    f0 = warp_sum(f0);
-    f1 = warp_sum(f1);
-    f2 = warp_sum(f2);
-    if (F && lane == 0) {
-      F[3 * (int64_t)i] = f0;
-      F[3 * (int64_t)i + 1] = f1;
-      F[3 * (int64_t)i + 2] = f2;
-    }
-  }
+  if (s < n) pair_walk_atom(TT, grid[0], cell_start, cell_atoms, spos, s, hits[w], lane, acc, F);  // warp-uniform
 #pragma unroll
   for (int k = 0; k < 7; k++) {
-    double v = warp_sum(acc[k]);
+    const double v = warp_sum(acc[k]);
     if (lane == 0) red[w][k] = v;
   }
   __syncthreads();
@@ -225,6 +54,249 @@ __global__ void __launch_bounds__(PAIR_T) k_pair_eval(const __grid_constant__ Pa
     for (int q = 0; q < PAIR_WARPS; q++) v += red[q][threadIdx.x];
     partial[(int64_t)blockIdx.x * 7 + threadIdx.x] = v;
   }
+}
+
+// ---------------------------------------------------------------------------------
+// Half-stencil tiles.
+constexpr int HALF_OFFSETS = 14;  // self + 13 forward neighbors
+constexpr int PBUF_SLOTS = 27;    // partial forces per atom: 14 as a home atom, 13 as a target
+
+// Offset k of the half stencil: 0 = (0,0,0); 1..13 = the (dx,dy,dz) with dz > 0, or dz = 0
+// and dy > 0, or dz = dy = 0 and dx > 0.
+__device__ __forceinline__ void half_offset(int k, int& dx, int& dy, int& dz) {
+  if (k == 0) {
+    dx = dy = dz = 0;
+  } else if (k == 1) {
+    dx = 1, dy = 0, dz = 0;
+  } else if (k <= 4) {
+    dx = k - 3, dy = 1, dz = 0;  // k = 2, 3, 4 -> dx = -1, 0, 1
+  } else {
+    const int q = k - 5;  // 0..8
+    dx = q % 3 - 1, dy = q / 3 - 1, dz = 1;
+  }
+}
+
+// Cell coordinate c + d along an axis of nc cells: wrapped on a periodic axis (nc >= 3 there,
+// so c + d stays a distinct cell), -1 when it leaves an open axis.
+__device__ __forceinline__ int shift_axis(int c, int d, int nc, bool periodic) {
+  int t = c + d;
+  if (periodic) return t < 0 ? t + nc : (t >= nc ? t - nc : t);
+  return (t < 0 || t >= nc) ? -1 : t;
+}
+
+struct HalfHit {
+  double r0, r1, r2, dist;
+  int at;  // row (bits 0-7) and lane (bits 8-15) within the tile
+  int sp;  // species of the row atom (bits 0-7) and of the lane atom (bits 8-15)
+};
+
+// Evaluates the first nh hits (one per lane) and hands each hit's force to its row owner
+// (fa += f) and its lane owner (ft -= f) in hit order.  E and W accumulate lane-wise.
+__device__ __forceinline__ void half_eval(const PairTerms& TT, const HalfHit* __restrict__ hb, int nh, int lane,
+                                          double* acc, double* fa, double* ft) {
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  int at = -1;
+  if (lane < nh) {
+    const HalfHit h = hb[lane];
+    const double R = sqrt(h.r0 * h.r0 + h.r1 * h.r1 + h.r2 * h.r2);
+    double V, g;
+    pair_terms_sum(TT, R, h.dist, h.sp & 0xff, (h.sp >> 8) & 0xff, V, g);
+    fx = g * h.r0;
+    fy = g * h.r1;
+    fz = g * h.r2;
+    acc[0] += V;
+    // empirical_potential.jl:63-64: r * f' -> [xx, yy, zz, zy, zx, yx]
+    acc[1] += h.r0 * fx;
+    acc[2] += h.r1 * fy;
+    acc[3] += h.r2 * fz;
+    acc[4] += h.r2 * fy;
+    acc[5] += h.r2 * fx;
+    acc[6] += h.r1 * fx;
+    at = h.at;
+  }
+  for (int q = 0; q < nh; q++) {
+    const double bx = __shfl_sync(0xffffffffu, fx, q);
+    const double by = __shfl_sync(0xffffffffu, fy, q);
+    const double bz = __shfl_sync(0xffffffffu, fz, q);
+    const int b = __shfl_sync(0xffffffffu, at, q);
+    if (lane == (b & 0xff)) {
+      fa[0] += bx;
+      fa[1] += by;
+      fa[2] += bz;
+    }
+    if (lane == ((b >> 8) & 0xff)) {
+      ft[0] -= bx;
+      ft[1] -= by;
+      ft[2] -= bz;
+    }
+  }
+}
+
+__device__ __forceinline__ void pbuf_put(double* __restrict__ P, int64_t n, int slot_kind, int64_t s, const double* f,
+                                         bool accumulate) {
+  double* q = P + 3 * ((int64_t)slot_kind * n + s);
+  if (accumulate) {
+    q[0] += f[0];
+    q[1] += f[1];
+    q[2] += f[2];
+  } else {
+    q[0] = f[0];
+    q[1] = f[1];
+    q[2] = f[2];
+  }
+}
+
+// MINB: resident blocks per SM the register allocation is bounded for (4: 128 registers).
+template <int MINB>
+__global__ void __launch_bounds__(PAIR_T, MINB) k_pair_half(const __grid_constant__ PairTerms TT, int64_t n,
+                                                         const ConfGrid* __restrict__ grid, int64_t ncells,
+                                                         const int64_t* __restrict__ cell_start,
+                                                         const int32_t* __restrict__ cell_atoms,
+                                                         const double4* __restrict__ spos, double* __restrict__ P,
+                                                         double* __restrict__ partial) {
+  __shared__ HalfHit hits[PAIR_WARPS][64];
+  __shared__ double red[PAIR_WARPS][7];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t item = (int64_t)blockIdx.x * PAIR_WARPS + w;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // E, W[6]
+  if (item < ncells * HALF_OFFSETS) {     // warp-uniform from here on
+    const ConfGrid& g = grid[0];
+    const int64_t A = item / HALF_OFFSETS;
+    const int k = (int)(item - A * HALF_OFFSETS);
+    const int cx = (int)(A % g.nc[0]), cy = (int)((A / g.nc[0]) % g.nc[1]), cz = (int)(A / ((int64_t)g.nc[0] * g.nc[1]));
+    int dx, dy, dz;
+    half_offset(k, dx, dy, dz);
+    const int tx = shift_axis(cx, dx, g.nc[0], !isinf(g.L[0]));
+    const int ty = shift_axis(cy, dy, g.nc[1], !isinf(g.L[1]));
+    const int tz = shift_axis(cz, dz, g.nc[2], !isinf(g.L[2]));
+    if (tx >= 0 && ty >= 0 && tz >= 0) {
+      const int64_t T = ((int64_t)tz * g.nc[1] + ty) * g.nc[0] + tx;
+      const int64_t a0 = cell_start[A], a1 = cell_start[A + 1], t0 = cell_start[T], t1 = cell_start[T + 1];
+      const int home_kind = k, tgt_kind = k == 0 ? 0 : HALF_OFFSETS - 1 + k;
+      // cells of at most 32 atoms are one tile and its sums are stored; larger cells take
+      // several tiles, whose sums accumulate into zeroed slots, as do the row and column
+      // sums of the home cell with itself (each slot is always written by the same lane, in
+      // tile order)
+      const bool multi = (a1 - a0 > 32) || (t1 - t0 > 32) || k == 0;
+      if (multi) {
+        const double z[3] = {0.0, 0.0, 0.0};
+        for (int64_t s = a0 + lane; s < a1; s += 32) pbuf_put(P, n, home_kind, s, z, false);
+        if (k != 0)
+          for (int64_t s = t0 + lane; s < t1; s += 32) pbuf_put(P, n, tgt_kind, s, z, false);
+        __syncwarp();
+      }
+      if (a0 == a1 && k != 0)  // no home atoms: the target atoms still get their (zero) slot
+        for (int64_t s = t0 + lane; s < t1; s += 32) {
+          const double z[3] = {0.0, 0.0, 0.0};
+          pbuf_put(P, n, tgt_kind, s, z, false);
+        }
+      HalfHit* hb = hits[w];
+      const unsigned lt = (1u << lane) - 1u;
+      const double rmax = TT.rcut_max;
+      for (int64_t rc = a0; rc < a1; rc += 32) {
+        const int ra = (int)(a1 - rc < 32 ? a1 - rc : 32);
+        double fa[3] = {0.0, 0.0, 0.0};  // row sums of row rc + lane
+        for (int64_t cc = t0; cc < t1; cc += 32) {
+          const int64_t ts = cc + lane;
+          const bool tv = ts < t1;
+          const double4 xt = tv ? spos[ts] : make_double4(0.0, 0.0, 0.0, 0.0);
+          const int32_t it = tv ? cell_atoms[ts] : -1;
+          double ft[3] = {0.0, 0.0, 0.0};  // column sums of lane atom ts
+          int nh = 0;
+          for (int q = 0; q < ra; q++) {
+            const int64_t as = rc + q;
+            const double4 xa = spos[as];
+            const int32_t ia = cell_atoms[as];
+            bool ok = false;
+            HalfHit h;
+            if (tv && (k != 0 || ts > as)) {
+              const double d2 = sumsq3_dev(pe_axis_dev(g.L[0], xa.x, xt.x), pe_axis_dev(g.L[1], xa.y, xt.y),
+                                           pe_axis_dev(g.L[2], xa.z, xt.z));
+              if (d2 <= TT.rmax2_hi) {
+                const double dist = sqrt(d2);
+                if (dist <= rmax) {
+                  ok = true;
+                  h.dist = dist;
+                  h.at = q | (lane << 8);
+                  h.sp = (int)xa.w | ((int)xt.w << 8);
+                  if (ia < it) {  // r = get_displacement(x_lo, x_hi) with the row atom lo
+                    h.r0 = disp_axis_dev(g.L[0], xa.x, xt.x);
+                    h.r1 = disp_axis_dev(g.L[1], xa.y, xt.y);
+                    h.r2 = disp_axis_dev(g.L[2], xa.z, xt.z);
+                  } else {  // the lane atom is lo: r = -get_displacement(x_lane, x_row)
+                    h.r0 = -disp_axis_dev(g.L[0], xt.x, xa.x);
+                    h.r1 = -disp_axis_dev(g.L[1], xt.y, xa.y);
+                    h.r2 = -disp_axis_dev(g.L[2], xt.z, xa.z);
+                  }
+                }
+              }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) hb[nh + __popc(bal & lt)] = h;
+            nh += __popc(bal);
+            __syncwarp();
+            if (nh >= 32) {
+              half_eval(TT, hb, 32, lane, acc, fa, ft);
+              __syncwarp();
+              if (lane < nh - 32) hb[lane] = hb[32 + lane];
+              nh -= 32;
+              __syncwarp();
+            }
+          }
+          half_eval(TT, hb, nh, lane, acc, fa, ft);
+          __syncwarp();
+          if (tv) pbuf_put(P, n, tgt_kind, ts, ft, multi);
+          __syncwarp();
+        }
+        if (lane < ra) pbuf_put(P, n, home_kind, rc + lane, fa, multi);
+        __syncwarp();
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 7; q++) {
+    const double v = warp_sum(acc[q]);
+    if (lane == 0) red[w][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double v = 0.0;
+    for (int q = 0; q < PAIR_WARPS; q++) v += red[q][threadIdx.x];
+    partial[(int64_t)blockIdx.x * 7 + threadIdx.x] = v;
+  }
+}
+
+// F of every atom: its 14 partial sums as a home atom (offsets k whose target cell exists)
+// and its 13 as a target (offsets k whose home cell, its own cell - offset k, exists), in
+// that fixed order.
+__global__ void k_pair_gather(int64_t n, const ConfGrid* __restrict__ grid, const int32_t* __restrict__ cell_atoms,
+                              const double4* __restrict__ spos, const double* __restrict__ P,
+                              double* __restrict__ F) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const ConfGrid& g = grid[0];
+  const double4 x = spos[s];
+  int c[3];
+  cell_coords(g, x.x, x.y, x.z, c);
+  const bool per[3] = {!isinf(g.L[0]), !isinf(g.L[1]), !isinf(g.L[2])};
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+  for (int kind = 0; kind < PBUF_SLOTS; kind++) {
+    const int k = kind < HALF_OFFSETS ? kind : kind - (HALF_OFFSETS - 1);
+    const int sg = kind < HALF_OFFSETS ? 1 : -1;
+    int d[3];
+    half_offset(k, d[0], d[1], d[2]);
+    bool ok = true;
+    for (int a = 0; a < 3; a++) ok &= shift_axis(c[a], sg * d[a], g.nc[a], per[a]) >= 0;
+    if (!ok) continue;
+    const double* q = P + 3 * ((int64_t)kind * n + s);
+    f0 += q[0];
+    f1 += q[1];
+    f2 += q[2];
+  }
+  const int64_t i = cell_atoms[s];
+  F[3 * i] = f0;
+  F[3 * i + 1] = f1;
+  F[3 * i + 2] = f2;
 }
 
 // Deterministic final reduction of per-block partials: one block, fixed order.
@@ -246,49 +318,9 @@ __global__ void k_reduce_partials(int64_t nblocks, int width, const double* __re
 }
 
 int prepare_terms(ipg_ctx* ctx, const ipg_pair_term* terms, int nterms, PairTerms& pt) {
-  memset(&pt, 0, sizeof(pt));
-  if (nterms < 0 || nterms > IPG_MAX_PAIR_TERMS)
-    return ipg_fail(ctx, IPG_ERR_ARG, "nterms must be in 0..%d", IPG_MAX_PAIR_TERMS);
-  pt.nterms = nterms;
-  pt.rcut_max = 0.0;
-  pt.rmax2_hi = 0.0;
-  for (int k = 0; k < nterms; k++) {
-    const ipg_pair_term& s = terms[k];
-    PairTermDev& d = pt.t[k];
-    d.kind = s.kind;
-    d.coeff = s.coeff;
-    d.rcut = s.rcut;
-    d.mask = s.species_mask;
-    if (!(s.rcut >= 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "term %d: rcut must be >= 0", k);
-    if (std::isinf(s.rcut)) return ipg_fail(ctx, IPG_ERR_ARG, "term %d: rcut must be finite", k);
-    pt.rcut_max = std::max(pt.rcut_max, s.rcut);
-    for (int q = 0; q < 8; q++) d.p[q] = s.params[q];
-    switch (s.kind) {
-      case IPG_PAIR_LJ:
-        d.p[2] = 4.0 * s.params[0];
-        d.p[3] = 24.0 * s.params[0];
-        break;
-      case IPG_PAIR_BM:
-      case IPG_PAIR_MORSE:
-      case IPG_PAIR_MOCK_R2:
-        break;
-      case IPG_PAIR_COUL:
-        d.p[2] = 1.0 * s.params[0] * s.params[1];  // k_e = 1 (src/constants.jl:7)
-        break;
-      case IPG_PAIR_ZBL: {
-        double Z1 = s.params[0], Z2 = s.params[1], e = s.params[2];
-        d.p[3] = 1.0 * Z1 * Z2 * e * e;                                     // _zbl_coeff
-        d.p[4] = 0.8854 * 0.529 / (std::pow(Z1, 0.23) + std::pow(Z2, 0.23));  // _zbl_d divisor
-        d.p[5] = std::log(e);
-        if (!(e > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "term %d: ZBL e must be > 0", k);
-        break;
-      }
-      default:
-        return ipg_fail(ctx, IPG_ERR_ARG, "term %d: unknown kind %d", k, s.kind);
-    }
-  }
-  pt.rmax2_hi = pt.rcut_max * pt.rcut_max * (1.0 + 1e-12);
-  return IPG_OK;
+  char err[256];
+  const int st = pair_prepare_terms(terms, nterms, pt, err, sizeof(err));
+  return st == IPG_OK ? IPG_OK : ipg_fail(ctx, st, "%s", err);
 }
 
 int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
@@ -300,12 +332,39 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
   int64_t aoff[2] = {0, n};
   CellList cl;
   IPG_RET(ipg_build_cells(ctx, "pair_", n, d_pos, d_species, 64, 1, aoff, L, pt.rcut_max, cl));
-  int64_t nb = std::max<int64_t>(1, (n + PAIR_WARPS - 1) / PAIR_WARPS);
-  double *partial, *red;
-  IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
+  const ConfGrid& g = cl.h_grid[0];
+  bool half = n > 0 && !ctx->pair_full_stencil;
+  for (int a = 0; a < 3; a++) half &= std::isinf(g.L[a]) || g.nc[a] >= 3;
+  double* red;
   IPG_RET(scratch(ctx, "pair_red", 8, &red));
-  IPG_TIMED_LAUNCH(ctx, "pair_eval", k_pair_eval, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.d_cell_start, cl.d_cell_atoms, cl.d_spos,
-             (flags & IPG_WANT_F) ? d_F : nullptr, partial, ctx->d_status);
+  double* partial;
+  int64_t nb;
+  IPG_RET(ipg_timing_mark(ctx, "pair_eval", true));
+  if (half) {
+    const int64_t items = cl.ncells * HALF_OFFSETS;
+    nb = std::max<int64_t>(1, (items + PAIR_WARPS - 1) / PAIR_WARPS);
+    double* P;
+    IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
+    IPG_RET(scratch(ctx, "pair_pbuf", (size_t)PBUF_SLOTS * 3 * n, &P));
+    if (ctx->pair_minb == 3)
+      IPG_LAUNCH(ctx, k_pair_half<3>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
+                 cl.d_cell_atoms, cl.d_spos, P, partial);
+    else if (ctx->pair_minb == 5)
+      IPG_LAUNCH(ctx, k_pair_half<5>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
+                 cl.d_cell_atoms, cl.d_spos, P, partial);
+    else
+      IPG_LAUNCH(ctx, k_pair_half<4>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
+                 cl.d_cell_atoms, cl.d_spos, P, partial);
+    if ((flags & IPG_WANT_F) && d_F)
+      IPG_LAUNCH(ctx, k_pair_gather, (unsigned)((n + 255) / 256), 256, 0, n, cl.d_grid, cl.d_cell_atoms, cl.d_spos,
+                 P, d_F);
+  } else {
+    nb = std::max<int64_t>(1, (n + PAIR_WARPS - 1) / PAIR_WARPS);
+    IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
+    IPG_LAUNCH(ctx, k_pair_eval, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.d_cell_start, cl.d_cell_atoms,
+               cl.d_spos, (flags & IPG_WANT_F) ? d_F : nullptr, partial);
+  }
+  IPG_RET(ipg_timing_mark(ctx, "pair_eval", false));
   IPG_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, nb, 7, partial, red);
   if ((flags & IPG_WANT_E) && d_E)
     CUDA_RET(ctx, cudaMemcpyAsync(d_E, red, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -343,16 +402,15 @@ int ipg_pair_eval(ipg_ctx* ctx, int64_t n, const double* pos, const int32_t* spe
   IPG_RET(scratch(ctx, "pair_in_sp", (size_t)n + 1, &d_sp));
   IPG_RET(scratch(ctx, "pair_out", 3 * (size_t)n + 8, &d_out));
   if (n) {
-    CUDA_RET(ctx, cudaMemcpyAsync(d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_RET(ctx, cudaMemcpyAsync(d_sp, species, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    IPG_RET(ipg_copy_h2d(ctx, d_pos, pos, sizeof(double) * 3 * n));
+    IPG_RET(ipg_copy_h2d(ctx, d_sp, species, sizeof(int32_t) * n));
   }
   // d_out layout: [E, W6 (6), pad, F (3n)]
   IPG_RET(pair_eval_device(ctx, n, d_pos, d_sp, L, terms, nterms, d_out, d_out + 8, d_out + 1,
                            flags | IPG_WANT_E | IPG_WANT_W));
   std::vector<double> head(8);
   CUDA_RET(ctx, cudaMemcpyAsync(head.data(), d_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  if ((flags & IPG_WANT_F) && n)
-    CUDA_RET(ctx, cudaMemcpyAsync(F, d_out + 8, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if ((flags & IPG_WANT_F) && n) IPG_RET(ipg_copy_d2h(ctx, F, d_out + 8, sizeof(double) * 3 * n));
   IPG_RET(ipg_status_check(ctx, "ipg_pair_eval"));
   if (flags & IPG_WANT_E) *E = head[0];
   if (flags & IPG_WANT_W) memcpy(W6, head.data() + 1, 6 * sizeof(double));

@@ -599,6 +599,701 @@ __global__ void __launch_bounds__(256) k_snap_atom(const __grid_constant__ SnapD
   }
 }
 
+// ---- exact Hessian-vector product (second-order adjoint) ------------------------------------
+// The position pullback of the forces needs H v (H: the Hessian of E, v: the force cotangent).
+// It is the directional derivative of the adjoint force computation along dx = v: every
+// quantity q of it is carried with its tangent dq/de of x + e v (forward mode over the
+// reverse-mode forces), so the pair terms come out as G_ij = dE_i/dr_ij and its tangent.
+//   r_ij = x_j - x_i                        tangent v_j - v_i
+//   U_ij and dU_ij/dr (Wigner recursion)    recursion of the tangents (product rule, below)
+//   Utot_i = sum_j sfac_j w_j U_ij          tangent by the product rule
+//   Z, Y (bilinear in Utot)                 Zdot = sum cg cg (Udot U + U Udot), Ydot = Y(Zdot)
+//   G_ij = 2 sum_h w_h Re(conj(D_h) Y_h)    Gdot = 2 sum w Re(conj(Ddot) Y + conj(D) Ydot),
+//                                           D_k = dsfac u_k U + sfac dU_k
+// The tangent of the forces is the same gather of Gdot as the forces are of G, and
+// H v = -Fdot.  Design: the second-order extension of compute_dij.jl:5-74 (dE/dr from dU and
+// Y); one block per atom, as k_snap_atom.
+
+// A number with its tangent.
+struct Dual {
+  double v, t;
+};
+__device__ __forceinline__ Dual dd(double v, double t = 0.0) { return Dual{v, t}; }
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual{a.v + b.v, a.t + b.t}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual{a.v - b.v, a.t - b.t}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return Dual{-a.v, -a.t}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual{a.v * b.v, a.t * b.v + a.v * b.t}; }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return Dual{a * b.v, a * b.t}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+  const double q = a.v / b.v;
+  return Dual{q, (a.t - q * b.t) / b.v};
+}
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+  const double r = sqrt(a.v);
+  return Dual{r, a.t / (2.0 * r)};
+}
+
+// The pair geometry of geom_du with tangents along (tx, ty, tz) = dr/de.
+struct PairGeomD {
+  Dual ar, ai, br, bi;            // a, b
+  Dual dar[3], dai[3], dbr[3], dbi[3];  // da/dr_k, db/dr_k
+  Dual u[3];                      // r / |r|
+  Dual sfac, dsfac;               // switching function (times the neighbor weight) and its r-derivative
+};
+
+__device__ __forceinline__ void geom_hvp(const SnapDev& S, double x, double y, double z, double tx, double ty,
+                                         double tz, double rcut, double wj, PairGeomD& G) {
+  const Dual X = dd(x, tx), Y = dd(y, ty), Zc = dd(z, tz);
+  const Dual rsq = X * X + Y * Y + Zc * Zc;
+  const Dual r = dsqrt(rsq);
+  const double rscale0 = S.rfac0 * M_PI / (rcut - S.rmin0);
+  const Dual theta0 = rscale0 * (r - dd(S.rmin0));
+  double sn, cs;
+  sincos(theta0.v, &sn, &cs);
+  const Dual Sn = dd(sn, cs * theta0.t), Cs = dd(cs, -sn * theta0.t);
+  const Dual z0 = r * Cs / Sn;
+  const Dual dz0dr = z0 / r - (rscale0 * r) * (rsq + z0 * z0) / rsq;
+  const Dual rinv = dd(1.0) / r;
+  G.u[0] = X * rinv;
+  G.u[1] = Y * rinv;
+  G.u[2] = Zc * rinv;
+  const Dual r0inv = dd(1.0) / dsqrt(r * r + z0 * z0);
+  G.ar = z0 * r0inv;
+  G.ai = -(Zc * r0inv);
+  G.br = Y * r0inv;
+  G.bi = -(X * r0inv);
+  const Dual dr0invdr = -(r0inv * r0inv * r0inv * (r + z0 * dz0dr));
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const Dual dr0 = dr0invdr * G.u[k];
+    const Dual dz0 = dz0dr * G.u[k];
+    G.dar[k] = dz0 * r0inv + z0 * dr0;
+    G.dai[k] = -(Zc * dr0);
+    G.dbr[k] = Y * dr0;
+    G.dbi[k] = -(X * dr0);
+  }
+  G.dai[2] = G.dai[2] - r0inv;
+  G.dbi[0] = G.dbi[0] - r0inv;
+  G.dbr[1] = G.dbr[1] + r0inv;
+  // compute_sfac / compute_dsfac (compute_ui.jl:350-380, the branches of sfac_of and
+  // dsfac_of) with tangents
+  if (!S.switch_flag || r.v <= S.rmin0) {
+    G.sfac = dd(wj);
+    G.dsfac = dd(0.0);
+  } else {
+    const double rcutfac = M_PI / (rcut - S.rmin0);
+    double s2, c2;
+    sincos((r.v - S.rmin0) * rcutfac, &s2, &c2);
+    const double rt = r.t * rcutfac;
+    G.sfac = r.v > rcut ? dd(0.0) : dd(wj * (0.5 * (c2 + 1.0)), wj * (-0.5 * s2 * rt));
+    G.dsfac = dd(wj * (-0.5 * (s2 * rcutfac)), wj * (-0.5 * c2 * rcutfac * rt));
+  }
+}
+
+// conj(p) * v for complex p = (pr, pi) and v, accumulated with weight c into acc.
+__device__ __forceinline__ void cj_acc(double pr, double pi, double2 v, double c, double2& acc) {
+  acc.x += c * (pr * v.x + pi * v.y);
+  acc.y += c * (pr * v.y - pi * v.x);
+}
+
+// One level of the recursion for the eight components [U, dU/dr_k, Udot, (dU/dr_k)dot] of one
+// pair, lanes over (component, entry); buffers [8][ext_max] (layout of wigner_level).
+//   U_j      = f(a, b, U)
+//   dU_k,j   = f(da_k, db_k, U) + f(a, b, dU_k)
+//   Udot_j   = f(adot, bdot, U) + f(a, b, Udot)
+//   dUdot_k  = f(da_k dot, db_k dot, U) + f(da_k, db_k, Udot) + f(adot, bdot, dU_k) + f(a, b, dUdot_k)
+// with f(A, B, u)[mb][ma] = -rootpq[ma][j-mb] conj(B) u[mb][ma-1] + rootpq[j-ma][j-mb] conj(A) u[mb][ma].
+__device__ __forceinline__ void wigner_level_hvp(const SnapDev& S, const double* rpq, int j, const PairGeomD& G,
+                                                 const double2* __restrict__ prev, double2* __restrict__ cur,
+                                                 int lane) {
+  const int J2 = S.J + 2;
+  const int em = S.ext_max;
+  const int nrec = (j / 2 + 1) * (j + 1);
+  for (int t = lane; t < 8 * nrec; t += 32) {
+    const int comp = t / nrec;
+    const int e = t - comp * nrec;
+    const int mb = e / (j + 1);
+    const int ma = e - mb * (j + 1);
+    const int k = (comp & 3) - 1;  // derivative direction of comps 1..3 and 5..7
+    const bool tangent = comp >= 4;
+    double2 res = make_double2(0.0, 0.0);
+    for (int side = 0; side < 2; side++) {  // side 0: the b term at ma-1; side 1: the a term at ma
+      if (side == 0 && ma == 0) continue;
+      if (side == 1 && ma == j) continue;
+      const int src = side == 0 ? mb * j + ma - 1 : mb * j + ma;
+      const double rp = side == 0 ? -rpq[ma * J2 + (j - mb)] : rpq[(j - ma) * J2 + (j - mb)];
+      const Dual pr = side == 0 ? G.br : G.ar, pi = side == 0 ? G.bi : G.ai;
+      double2 acc = make_double2(0.0, 0.0);
+      // f(a, b, own component)
+      cj_acc(pr.v, pi.v, prev[comp * em + src], 1.0, acc);
+      if (k >= 0) {  // f(da_k, db_k, U): the geometry derivative times U (and its tangent part)
+        const Dual qr = side == 0 ? G.dbr[k] : G.dar[k], qi = side == 0 ? G.dbi[k] : G.dai[k];
+        cj_acc(qr.v, qi.v, prev[(tangent ? 4 : 0) * em + src], 1.0, acc);
+        if (tangent) {
+          cj_acc(qr.t, qi.t, prev[src], 1.0, acc);        // (da_k dot) U
+          cj_acc(pr.t, pi.t, prev[(k + 1) * em + src], 1.0, acc);  // adot dU_k
+        }
+      } else if (tangent) {  // Udot: f(adot, bdot, U)
+        cj_acc(pr.t, pi.t, prev[src], 1.0, acc);
+      }
+      res.x += rp * acc.x;
+      res.y += rp * acc.y;
+    }
+    cur[comp * em + e] = res;
+  }
+  __syncwarp();
+  if (j & 1) {  // mirrored row R = (j+1)/2 of every component (inversion symmetry)
+    const int R = (j + 1) / 2;
+    for (int t = lane; t < 8 * (j + 1); t += 32) {
+      const int comp = t / (j + 1);
+      const int c = t - comp * (j + 1);
+      const double2 src = cur[comp * em + (j - R) * (j + 1) + (j - c)];
+      const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+      cur[comp * em + R * (j + 1) + c] = make_double2(sg * src.x, -sg * src.y);
+    }
+    __syncwarp();
+  }
+}
+
+// Shared memory of k_snap_hvp (doubles): Utot and its tangent [2][idxu_max] complex, the
+// per-warp partial sums of both [2][nwarps][u_half] complex (aliasing Z), Z and Zdot
+// [2][idxz_max] complex, Y and Ydot [2][u_half] complex, sqrt(p/q), the per-warp level
+// buffers [nwarps][2 levels][8][ext_max] complex.
+struct HvpSmem {
+  size_t ut, zs, ys, rpq, lv, total;
+};
+__host__ __device__ inline HvpSmem hvp_smem(const SnapDev& S, int nwarps) {
+  HvpSmem L;
+  size_t o = 0;
+  L.ut = o;
+  o += al16(4 * (size_t)S.idxu_max);
+  L.zs = o;
+  const size_t zsz = 4 * (size_t)S.idxz_max, usz = 4 * (size_t)nwarps * S.u_half;
+  o += al16(zsz > usz ? zsz : usz);
+  L.ys = o;
+  o += al16(4 * (size_t)S.u_half);
+  L.rpq = o;
+  o += al16((size_t)(S.J + 2) * (S.J + 2));
+  L.lv = o;
+  o += al16((size_t)nwarps * 2 * 8 * 2 * S.ext_max);
+  L.total = o * sizeof(double);
+  return L;
+}
+
+// Per pair p = (i, j): fvec[p] = dE_i/dr_ij and fdot[p] = its tangent along the atom
+// displacements v [n][3].  Inputs as k_snap_atom<MODE_ADJ> (beta via S.ycoef).
+__global__ void __launch_bounds__(128) k_snap_hvp(const __grid_constant__ SnapDev S, SnapIO io,
+                                                  const double* __restrict__ v, double* __restrict__ fdot) {
+  extern __shared__ double smem[];
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const HvpSmem L = hvp_smem(S, nwarps);
+  double2* ut = reinterpret_cast<double2*>(smem + L.ut);  // [2][idxu_max]: Utot, Utot dot
+  double2* utd = ut + S.idxu_max;
+  double2* zs = reinterpret_cast<double2*>(smem + L.zs);  // [2][idxz_max]
+  double2* zsd = zs + S.idxz_max;
+  double2* ys = reinterpret_cast<double2*>(smem + L.ys);  // [2][u_half]
+  double2* ysd = ys + S.u_half;
+  double* rpq = smem + L.rpq;
+  const int em = S.ext_max;
+  double2* lv0 = reinterpret_cast<double2*>(smem + L.lv) + (size_t)warp * 2 * 8 * em;
+  double2* lv1 = lv0 + 8 * em;
+  const int J = S.J, uh = S.u_half;
+  for (int q = threadIdx.x; q < (J + 2) * (J + 2); q += blockDim.x) rpq[q] = S.rootpq[q];
+  __syncthreads();
+  for (int64_t i = blockIdx.x; i < io.n; i += gridDim.x) {
+    const int64_t beg = io.off[i], end = io.off[i + 1];
+    const int si = clamp_sp(io.species[i], S.nsp);
+    const double vi[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    // ---- Utot and its tangent (per-warp partials, then a fixed-order sum) ----
+    double2* up = zs;  // [2][nwarps][u_half]
+    for (int q = threadIdx.x; q < 2 * nwarps * uh; q += blockDim.x) up[q] = make_double2(0.0, 0.0);
+    __syncthreads();
+    {
+      double2* upw = up + (size_t)warp * uh;
+      double2* updw = up + (size_t)(nwarps + warp) * uh;
+      for (int64_t p = beg + warp; p < end; p += nwarps) {
+        const int32_t jn = io.nbr[p];
+        const int sj = clamp_sp(io.species[jn], S.nsp);
+        const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+        const double t3[3] = {v[3 * jn] - vi[0], v[3 * jn + 1] - vi[1], v[3 * jn + 2] - vi[2]};
+        PairGeomD G;
+        geom_hvp(S, io.rij[3 * p], io.rij[3 * p + 1], io.rij[3 * p + 2], t3[0], t3[1], t3[2], rcut, S.weight[sj], G);
+        double2* prev = lv0;
+        double2* cur = lv1;
+        for (int j = 0; j <= J; j++) {
+          if (j == 0) {
+            if (lane < 8) cur[lane * em] = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
+            __syncwarp();
+          } else {
+            wigner_level_hvp(S, rpq, j, G, prev, cur, lane);
+          }
+          const int nrec = (j / 2 + 1) * (j + 1);
+          const int hb = S.half_block[j];
+          for (int e = lane; e < nrec; e += 32) {
+            const double2 u = cur[e], ud = cur[4 * em + e];
+            upw[hb + e].x += G.sfac.v * u.x;
+            upw[hb + e].y += G.sfac.v * u.y;
+            updw[hb + e].x += G.sfac.t * u.x + G.sfac.v * ud.x;
+            updw[hb + e].y += G.sfac.t * u.y + G.sfac.v * ud.y;
+          }
+          __syncwarp();
+          double2* tmp = prev;
+          prev = cur;
+          cur = tmp;
+        }
+      }
+    }
+    __syncthreads();
+    for (int h = threadIdx.x; h < uh; h += blockDim.x) {
+      double2 s = make_double2(0.0, 0.0), sd = make_double2(0.0, 0.0);
+      for (int w = 0; w < nwarps; w++) {
+        const double2 a = up[(size_t)w * uh + h], b = up[(size_t)(nwarps + w) * uh + h];
+        s.x += a.x;
+        s.y += a.y;
+        sd.x += b.x;
+        sd.y += b.y;
+      }
+      int j = 0;
+      while (j < J && S.half_block[j + 1] <= h) j++;
+      const int e = h - S.half_block[j];
+      const int mb = e / (j + 1), ma = e - mb * (j + 1);
+      if (ma == mb) s.x += S.wself;
+      const int ub = S.idxu_block[j];
+      const bool middle = (2 * mb == j);
+      if (middle && ma > mb) continue;
+      ut[ub + mb * (j + 1) + ma] = s;
+      utd[ub + mb * (j + 1) + ma] = sd;
+      if (!(middle && ma == mb)) {
+        const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+        ut[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * s.x, -sg * s.y);
+        utd[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * sd.x, -sg * sd.y);
+      }
+    }
+    __syncthreads();
+    // ---- Z and its tangent ----
+    for (int t = threadIdx.x; t < S.idxz_max; t += blockDim.x) {
+      const int jjz = S.zperm[t];
+      const ZDev q = S.idxz[jjz];
+      const double* cgb = S.cglist + q.cgoff;
+      const int j1 = q.j1, j2 = q.j2;
+      double zr = 0.0, zi = 0.0, dr = 0.0, di = 0.0;
+      int i1 = q.u1base, i2 = q.u2base, icgb = q.icgb0;
+      for (int ib = 0; ib < q.nb; ib++) {
+        double sr = 0.0, sim = 0.0, tr = 0.0, tim = 0.0;
+        int icga = q.icga0;
+        for (int ia = 0; ia < q.na; ia++) {
+          const double2 u1 = ut[i1 + ia], u2 = ut[i2 - ia];
+          const double2 d1 = utd[i1 + ia], d2 = utd[i2 - ia];
+          const double c = __ldg(cgb + icga);
+          sr += c * (u1.x * u2.x - u1.y * u2.y);
+          sim += c * (u1.x * u2.y + u1.y * u2.x);
+          tr += c * (d1.x * u2.x - d1.y * u2.y + u1.x * d2.x - u1.y * d2.y);
+          tim += c * (d1.x * u2.y + d1.y * u2.x + u1.x * d2.y + u1.y * d2.x);
+          icga += j2;
+        }
+        const double cb = __ldg(cgb + icgb);
+        zr += cb * sr;
+        zi += cb * sim;
+        dr += cb * tr;
+        di += cb * tim;
+        i1 += j1 + 1;
+        i2 -= j2 + 1;
+        icgb += j2;
+      }
+      if (S.bnorm_flag) {
+        const double f = 1.0 / (q.j + 1);
+        zr *= f;
+        zi *= f;
+        dr *= f;
+        di *= f;
+      }
+      zs[jjz] = make_double2(zr, zi);
+      zsd[jjz] = make_double2(dr, di);
+    }
+    __syncthreads();
+    // ---- Y and its tangent ----
+    {
+      const double* yc = S.ycoef + (size_t)si * S.idxz_max;
+      for (int h = threadIdx.x; h < uh; h += blockDim.x) {
+        double2 y = make_double2(0.0, 0.0), yd = make_double2(0.0, 0.0);
+        for (int q = S.y_off[h]; q < S.y_off[h + 1]; q++) {
+          const int jjz = S.y_jjz[q];
+          const double c = yc[jjz];
+          y.x += c * zs[jjz].x;
+          y.y += c * zs[jjz].y;
+          yd.x += c * zsd[jjz].x;
+          yd.y += c * zsd[jjz].y;
+        }
+        ys[h] = y;
+        ysd[h] = yd;
+      }
+    }
+    __syncthreads();
+    // ---- per neighbor: G = dE_i/dr_ij and its tangent ----
+    for (int64_t p = beg + warp; p < end; p += nwarps) {
+      const int32_t jn = io.nbr[p];
+      const int sj = clamp_sp(io.species[jn], S.nsp);
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+      const double t3[3] = {v[3 * jn] - vi[0], v[3 * jn + 1] - vi[1], v[3 * jn + 2] - vi[2]};
+      PairGeomD G;
+      geom_hvp(S, io.rij[3 * p], io.rij[3 * p + 1], io.rij[3 * p + 2], t3[0], t3[1], t3[2], rcut, S.weight[sj], G);
+      double acc[3] = {0.0, 0.0, 0.0}, accd[3] = {0.0, 0.0, 0.0};
+      double2* prev = lv0;
+      double2* cur = lv1;
+      for (int j = 0; j <= J; j++) {
+        if (j == 0) {
+          if (lane < 8) cur[lane * em] = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
+          __syncwarp();
+        } else {
+          wigner_level_hvp(S, rpq, j, G, prev, cur, lane);
+        }
+        const int nrec = (j / 2 + 1) * (j + 1);
+        const int hb = S.half_block[j];
+        const int nf = nfull_of(j);
+        const int emid = (j & 1) ? -1 : (j / 2) * (j + 1) + j / 2;
+        for (int e = lane; e < nrec; e += 32) {
+          const double w = (e < nf) ? 1.0 : (e == emid ? 0.5 : 0.0);
+          if (w == 0.0) continue;
+          const double2 u = cur[e], ud = cur[4 * em + e];
+          const double2 Yv = ys[hb + e], Yd = ysd[hb + e];
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const double2 du = cur[(k + 1) * em + e], dud = cur[(k + 5) * em + e];
+            // D = dsfac u_k U + sfac dU_k and its tangent
+            const double cu = G.dsfac.v * G.u[k].v, cut = G.dsfac.t * G.u[k].v + G.dsfac.v * G.u[k].t;
+            const double Dx = cu * u.x + G.sfac.v * du.x, Dy = cu * u.y + G.sfac.v * du.y;
+            const double Ddx = cut * u.x + cu * ud.x + G.sfac.t * du.x + G.sfac.v * dud.x;
+            const double Ddy = cut * u.y + cu * ud.y + G.sfac.t * du.y + G.sfac.v * dud.y;
+            acc[k] += w * (Dx * Yv.x + Dy * Yv.y);
+            accd[k] += w * (Ddx * Yv.x + Ddy * Yv.y + Dx * Yd.x + Dy * Yd.y);
+          }
+        }
+        __syncwarp();
+        double2* tmp = prev;
+        prev = cur;
+        cur = tmp;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        acc[k] = warp_sum(acc[k]);
+        accd[k] = warp_sum(accd[k]);
+      }
+      if (lane == 0)
+        for (int k = 0; k < 3; k++) {
+          io.fvec[3 * p + k] = 2.0 * acc[k];
+          fdot[3 * p + k] = 2.0 * accd[k];
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- explicit multi-element SNAP (chem_flag) and quadratic SNAP ---------------------------
+// One block per atom, the phases of k_snap_atom resolved by element (the element of the
+// neighbor for Utot, compute_ui.jl:155-175; ordered element pairs for Z, compute_z.jl:5-61;
+// element triples for B and dB/dr, compute_b.jl:15-95 and :104-342), and the quadratic
+// products of LAMMPS_SNAP/snap.jl:45-47 (0.5 B_k^2 and B_k B_l, l > k, after the klin linear
+// components).  Z of one atom (nelem^2 idxz_max complex) lives in a block-private slice of
+// global memory; the rest in shared memory.
+//   B_ext [n][K] (io.B, when set) and E_i = beta[s_i] . B_ext (io.Ei, bzero already in B);
+//   PLAIN: dB_lin/dr of every pair, io.dbl [np][klin][3]; with quadratic_flag also the linear
+//   coefficients with the same forces, beff [n][klin] (beta_k + sum_l a_kl B_l).
+struct ChemSmem {
+  size_t ut, up, bs, bf, rpq, lv, duf, red, total;
+};
+__host__ __device__ inline ChemSmem chem_smem(const SnapDev& S, int nwarps, bool plain) {
+  ChemSmem L;
+  size_t o = 0;
+  L.ut = o;
+  o += al16(2 * (size_t)S.nelem * S.idxu_max);
+  L.up = o;  // per-warp partial Utot [nwarps][nelem][u_half]
+  o += al16(2 * (size_t)nwarps * S.nelem * S.u_half);
+  L.bs = o;  // linear B [klin]
+  o += al16((size_t)S.klin);
+  L.bf = o;  // effective linear coefficients [klin]
+  o += al16((size_t)S.klin);
+  L.rpq = o;
+  o += al16((size_t)(S.J + 2) * (S.J + 2));
+  L.lv = o;
+  o += al16((size_t)nwarps * 2 * 4 * 2 * S.ext_max);
+  L.duf = o;
+  if (plain) o += al16((size_t)nwarps * 2 * 3 * S.u_half);
+  L.red = o;
+  o += al16(256);
+  L.total = o * sizeof(double);
+  return L;
+}
+
+// First slot of row k of the quadratic block: Klin + sum_{q<k} (Klin - q).
+__device__ __forceinline__ int quad_row(int klin, int k) { return klin + k * klin - k * (k - 1) / 2; }
+
+template <bool PLAIN>
+__global__ void __launch_bounds__(128) k_snap_chem(const __grid_constant__ SnapDev S, SnapIO io,
+                                                   double2* __restrict__ zbuf, double* __restrict__ beff) {
+  extern __shared__ double smem[];
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const ChemSmem L = chem_smem(S, nwarps, PLAIN);
+  double2* ut = reinterpret_cast<double2*>(smem + L.ut);  // [nelem][idxu_max]
+  double2* upart = reinterpret_cast<double2*>(smem + L.up);
+  double* bs = smem + L.bs;
+  double* bfe = smem + L.bf;
+  double* rpq = smem + L.rpq;
+  double* red = smem + L.red;
+  double2* lv0 = reinterpret_cast<double2*>(smem + L.lv) + (size_t)warp * 2 * 4 * S.ext_max;
+  double2* lv1 = lv0 + 4 * S.ext_max;
+  const int J = S.J, K = S.K, KL = S.klin, uh = S.u_half, U = S.idxu_max, M = S.idxz_max;
+  const int ne = S.nelem, KB = KL / (ne * ne * ne);  // components per element triple (idxb_max)
+  double2* zb = zbuf + (size_t)blockIdx.x * ne * ne * M;
+  for (int q = threadIdx.x; q < (J + 2) * (J + 2); q += blockDim.x) rpq[q] = S.rootpq[q];
+  __syncthreads();
+  for (int64_t i = blockIdx.x; i < io.n; i += gridDim.x) {
+    const int64_t beg = io.off[i], end = io.off[i + 1];
+    const int si = clamp_sp(io.species[i], S.nsp);
+    const int ielem = S.chem ? si : 0;
+    // ---- Utot of every element ----
+    for (int q = threadIdx.x; q < nwarps * ne * uh; q += blockDim.x) upart[q] = make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int64_t p = beg + warp; p < end; p += nwarps) {
+      const double x = io.rij[3 * p], y = io.rij[3 * p + 1], z = io.rij[3 * p + 2];
+      const int sj = clamp_sp(io.species[io.nbr[p]], S.nsp);
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+      const double r = sqrt(x * x + y * y + z * z);
+      const double theta0 = (r - S.rmin0) * S.rfac0 * M_PI / (rcut - S.rmin0);
+      const double z0 = r / tan(theta0);
+      const double r0inv = 1.0 / sqrt(r * r + z0 * z0);
+      PairGeom G;
+      G.a = make_double2(r0inv * z0, -r0inv * z);
+      G.b = make_double2(r0inv * y, -r0inv * x);
+      const double sw = sfac_of(S, r, rcut) * S.weight[sj];
+      double2* up = upart + ((size_t)warp * ne + (S.chem ? sj : 0)) * uh;
+      double2* prev = lv0;
+      double2* cur = lv1;
+      if (lane == 0) {
+        prev[0] = make_double2(1.0, 0.0);
+        up[0].x += sw;
+      }
+      __syncwarp();
+      for (int j = 1; j <= J; j++) {
+        wigner_level(S, rpq, j, 1, G, prev, cur, lane);
+        const int nrec = (j / 2 + 1) * (j + 1);
+        double2* upj = up + S.half_block[j];
+        for (int e = lane; e < nrec; e += 32) {
+          upj[e].x += sw * cur[e].x;
+          upj[e].y += sw * cur[e].y;
+        }
+        __syncwarp();
+        double2* t = prev;
+        prev = cur;
+        cur = t;
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < ne * uh; t += blockDim.x) {
+      const int el = t / uh, h = t - el * uh;
+      double2 sacc = make_double2(0.0, 0.0);
+      for (int w = 0; w < nwarps; w++) {
+        const double2 v = upart[((size_t)w * ne + el) * uh + h];
+        sacc.x += v.x;
+        sacc.y += v.y;
+      }
+      int j = 0;
+      while (j < J && S.half_block[j + 1] <= h) j++;
+      const int e = h - S.half_block[j];
+      const int mb = e / (j + 1), ma = e - mb * (j + 1);
+      if (ma == mb && (el == ielem || S.wselfall)) sacc.x += S.wself;  // zero_uarraytot
+      const int ub = el * U + S.idxu_block[j];
+      const bool middle = (2 * mb == j);
+      if (middle && ma > mb) continue;
+      ut[ub + mb * (j + 1) + ma] = sacc;
+      if (!(middle && ma == mb)) {
+        const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+        ut[ub + (j - mb) * (j + 1) + (j - ma)] = make_double2(sg * sacc.x, -sg * sacc.y);
+      }
+    }
+    __syncthreads();
+    // ---- Z of every ordered element pair (literal_chem_z: compute_z.jl's own indexing) ----
+    for (int jjz = threadIdx.x; jjz < M; jjz += blockDim.x) {
+      const ZDev q = S.idxz[jjz];
+      const double* cgb = S.cglist + q.cgoff;
+      const int j1 = q.j1, j2 = q.j2;
+      for (int d = 1; d < ne * ne; d++) zb[(size_t)d * M + jjz] = make_double2(0.0, 0.0);
+      double2 run = make_double2(0.0, 0.0);
+      for (int d = 0; d < ne * ne; d++) {
+        const double2* u1 = ut + (d / ne) * U;
+        const double2* u2 = ut + (d % ne) * U;
+        double zr = S.literal_chem_z ? run.x : 0.0, zi = S.literal_chem_z ? run.y : 0.0;
+        int i1 = q.u1base, i2 = q.u2base, icgb = q.icgb0;
+        for (int ib = 0; ib < q.nb; ib++) {
+          double sr = 0.0, sim = 0.0;
+          int icga = q.icga0;
+          for (int ia = 0; ia < q.na; ia++) {
+            const double2 a1 = u1[i1 + ia], a2 = u2[i2 - ia];
+            const double c = __ldg(cgb + icga);
+            sr += c * (a1.x * a2.x - a1.y * a2.y);
+            sim += c * (a1.x * a2.y + a1.y * a2.x);
+            icga += j2;
+          }
+          const double cb = __ldg(cgb + icgb);
+          zr += cb * sr;
+          zi += cb * sim;
+          i1 += j1 + 1;
+          i2 -= j2 + 1;
+          icgb += j2;
+        }
+        if (S.bnorm_flag) {
+          zr /= (q.j + 1);
+          zi /= (q.j + 1);
+        }
+        run = make_double2(zr, zi);
+        if (!S.literal_chem_z) zb[(size_t)d * M + jjz] = run;
+      }
+      if (S.literal_chem_z) zb[jjz] = run;
+    }
+    __syncthreads();
+    // ---- B of every element triple ----
+    for (int t = threadIdx.x; t < KL; t += blockDim.x) {
+      const int tri = t / KB, b = t - tri * KB;
+      const int e3 = tri % ne, d = tri / ne;  // tri = (e1 ne + e2) ne + e3, d = e1 ne + e2
+      const DBDev db = S.db[b];
+      const int l = db.l[0], u0 = e3 * U + S.idxu_block[l];
+      const double2* zz = zb + (size_t)d * M + db.z0[0];
+      const int nf = nfull_of(l);
+      double sacc = 0.0;
+      for (int e = 0; e < nf; e++) sacc += ut[u0 + e].x * zz[e].x + ut[u0 + e].y * zz[e].y;
+      if (!(l & 1)) {
+        const int e = (l / 2) * (l + 1) + l / 2;
+        sacc += 0.5 * (ut[u0 + e].x * zz[e].x + ut[u0 + e].y * zz[e].y);
+      }
+      double Bv = 2.0 * sacc;
+      if (S.bzero_flag && (S.wselfall || tri == (ielem * ne + ielem) * ne + ielem)) Bv -= S.bzero[l];
+      bs[t] = Bv;
+    }
+    __syncthreads();
+    // ---- B_ext, E_i and the effective linear coefficients ----
+    const double* bt = S.beta + (size_t)si * K;
+    double e = 0.0;
+    for (int k = threadIdx.x; k < KL; k += blockDim.x) {
+      const double bk = bs[k];
+      e += bt[k] * bk;
+      if (io.B) io.B[i * K + k] = bk;
+      if (S.quadratic) {
+        const int r0 = quad_row(KL, k);
+        double g = bt[k] + bt[r0] * bk;  // d/dB_k of beta . B_ext
+        const double q0 = 0.5 * bk * bk;
+        e += bt[r0] * q0;
+        if (io.B) io.B[i * K + r0] = q0;
+        for (int l = k + 1; l < KL; l++) {
+          const double q = bk * bs[l];
+          e += bt[r0 + l - k] * q;
+          if (io.B) io.B[i * K + r0 + l - k] = q;
+          g += bt[r0 + l - k] * bs[l];
+        }
+        for (int l = 0; l < k; l++) g += bt[quad_row(KL, l) + k - l] * bs[l];
+        bfe[k] = g;
+        if (beff) beff[i * KL + k] = g;
+      }
+    }
+    red[threadIdx.x] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)blockDim.x; w++) t += red[w];
+      io.Ei[i] = t;
+    }
+    if (PLAIN) {
+      // ---- per neighbor: dB_lin/dr of every element triple (compute_b.jl:104-342) ----
+      double2* dufw = reinterpret_cast<double2*>(smem + L.duf) + (size_t)warp * 3 * uh;  // [3][u_half]
+      for (int64_t p = beg + warp; p < end; p += nwarps) {
+        const int32_t jn = io.nbr[p];
+        const int sj = clamp_sp(io.species[jn], S.nsp);
+        const int e3 = S.chem ? sj : 0;
+        const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+        PairGeom G;
+        geom_du(S, io.rij[3 * p], io.rij[3 * p + 1], io.rij[3 * p + 2], rcut, S.weight[sj], G);
+        double2* prev = lv0;
+        double2* cur = lv1;
+        const int em = S.ext_max;
+        for (int j = 0; j <= J; j++) {
+          if (j == 0) {
+            if (lane < 4) cur[lane * em] = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
+            __syncwarp();
+          } else {
+            wigner_level(S, rpq, j, 4, G, prev, cur, lane);
+          }
+          const int nrec = (j / 2 + 1) * (j + 1);
+          const int hb = S.half_block[j];
+          for (int ee = lane; ee < nrec; ee += 32) {
+            const double2 u = cur[ee];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              const double2 dd = cur[(k + 1) * em + ee];
+              dufw[k * uh + hb + ee] = make_double2(G.dsfac * u.x * G.u[k] + G.sfac * dd.x,
+                                                    G.dsfac * u.y * G.u[k] + G.sfac * dd.y);
+            }
+          }
+          __syncwarp();
+          double2* t = prev;
+          prev = cur;
+          cur = t;
+        }
+        double* out = io.dbl + (size_t)p * KL * 3;
+        for (int t = lane; t < 3 * KL; t += 32) {
+          const int q = t / 3, k = t - 3 * q;
+          const int tri = q / KB, b = q - tri * KB;
+          const int c3 = tri % ne, b3 = (tri / ne) % ne, a3 = tri / (ne * ne);
+          // the terms that land on triple (a3, b3, c3): term 0 with e3 = c3 and Z(a3, b3),
+          // term 1 with e3 = a3 and Z(c3, b3), term 2 with e3 = b3 and Z(c3, a3)
+          const int cond[3] = {c3 == e3, a3 == e3, b3 == e3};
+          const int zd[3] = {a3 * ne + b3, c3 * ne + b3, c3 * ne + a3};
+          const DBDev db = S.db[b];
+          double tot = 0.0;
+#pragma unroll
+          for (int term = 0; term < 3; term++) {
+            if (!cond[term]) continue;
+            const int l = db.l[term], hb = S.half_block[l];
+            const int nf = nfull_of(l);
+            const double2* du = dufw + k * uh + hb;
+            const double2* zz = zb + (size_t)zd[term] * M + db.z0[term];
+            double sacc = 0.0;
+            for (int ee = 0; ee < nf; ee++) sacc += du[ee].x * zz[ee].x + du[ee].y * zz[ee].y;
+            if (!(l & 1)) {
+              const int ee = (l / 2) * (l + 1) + l / 2;
+              sacc += 0.5 * (du[ee].x * zz[ee].x + du[ee].y * zz[ee].y);
+            }
+            tot += db.fac[term] * sacc;
+          }
+          out[t] = 2.0 * tot;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Quadratic SNAP: the per-pair dB_ext/dr [np][K][3] of the pair's centre i = owner[p] from its
+// linear dB/dr [np][klin][3] and B_ext [n][K] (its first klin entries):
+// d(0.5 B_k^2) = B_k dB_k, d(B_k B_l) = B_l dB_k + B_k dB_l.  Thread per (pair, component k).
+__global__ void k_quad_pairs(int64_t np_cap, const int64_t* __restrict__ d_np, int klin, int K,
+                             const int32_t* __restrict__ owner, const double* __restrict__ Bx,
+                             const double* __restrict__ dbl, double* __restrict__ dbx) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = t / klin;
+  const int k = (int)(t - p * klin);
+  if (p >= np_cap || p >= *d_np) return;
+  const double* b = Bx + (size_t)owner[p] * K;
+  const double* d = dbl + (size_t)p * klin * 3;
+  double* o = dbx + (size_t)p * K * 3;
+  const double bk = b[k];
+  for (int c = 0; c < 3; c++) o[3 * k + c] = d[3 * k + c];
+  const int r0 = klin + k * klin - k * (k - 1) / 2;
+  for (int c = 0; c < 3; c++) o[3 * r0 + c] = bk * d[3 * k + c];
+  for (int l = k + 1; l < klin; l++)
+    for (int c = 0; c < 3; c++) o[3 * (r0 + l - k) + c] = b[l] * d[3 * k + c] + bk * d[3 * l + c];
+}
+
 // Utot of every atom (compute_ui.jl:5-175) from the register chains: one launch per
 // chain MB, one warp per atom, lanes over neighbors (32 at a time).  Each chain's rows
 // (and their mirrors) are disjoint, so the launches write disjoint entries of
@@ -1056,7 +1751,7 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, cons
   return e;
 }
 
-// Z output variant (k_snap_yrows<true>): every item's Z tile goes to zout[jjz][atom]
+// Z output variant (k_snap_yrows<YM_Z>): every item's Z tile goes to zout[jjz][atom]
 // (entries of the half plane; the middle row of an even level up to ma = mb), nothing is
 // summed across items.  Z carries the 1/(j+1) of bnorm_flag (compute_z.jl:49-56).
 template <int NT>
@@ -1111,11 +1806,95 @@ __device__ __forceinline__ void yr_row_z(const SnapDev& S, const YConst& T, cons
   }
 }
 
-template <bool ZOUT>
-__global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_constant__ SnapDev S, const __grid_constant__ YConst T, int64_t n,
+// Y and Z at once (k_snap_yrows<YM_YZ>): each item's Z tile is formed with unit coefficients,
+// written to zout[jjz][atom] as by yr_tile_z, and added into the row's Y with the item's
+// coefficient, so a later beta pullback of the same positions reads Z instead of recomputing
+// it.  Y' and the energy are as from yr_tile.
+template <int NT>
+__device__ __forceinline__ double yr_tile_yz(const SnapDev& S, const YConst& T, const YRowDev& row, int ma0, int nma,
+                                             const double2* __restrict__ usl, const double* __restrict__ yc,
+                                             const double2* __restrict__ cas, int64_t n, int64_t atom, bool valid,
+                                             double2* __restrict__ yout, double2* __restrict__ zout) {
+  double2 acc[NT];
+#pragma unroll
+  for (int i = 0; i < NT; i++) acc[i] = make_double2(0.0, 0.0);
+  const int j = row.j, rs = j + 1;
+  const double bn = S.bnorm_flag ? 1.0 / (j + 1) : 1.0;
+  for (int t = row.t0; t < row.t1; t++) {
+    const YItemDev it = T.items[t];
+    const double c = yc[it.trip];
+    const double2* __restrict__ cp = cas + it.ca / 2;
+    const int j1 = it.j1, j2 = it.j2, d = it.d;
+    double2 z[NT];
+#pragma unroll
+    for (int i = 0; i < NT; i++) z[i] = make_double2(0.0, 0.0);
+    for (int ib = 0; ib < it.nb; ib++) {
+      const int mb1 = it.mb1min + ib, mb2 = it.mb2max - ib;
+      const double cb = bn * T.cb[it.cg + ib];
+      if (2 * mb1 > j1)
+        yr_pair<NT, true>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, z);
+      else
+        yr_pair<NT, false>(usl, S.half_block, cp, rs, ma0, j1, j2, d, mb1, mb2, cb, z);
+    }
+    const int64_t z0 = it.jjz + row.mb * (j + 1) + ma0;
+#pragma unroll
+    for (int i = 0; i < NT; i++) {
+      if (valid && ma0 + i < nma) zout[(size_t)(z0 + i) * n + atom] = z[i];
+      acc[i].x = fma(c, z[i].x, acc[i].x);
+      acc[i].y = fma(c, z[i].y, acc[i].y);
+    }
+  }
+  double e = 0.0;
+#pragma unroll
+  for (int i = 0; i < NT; i++) {
+    const int ma = ma0 + i;
+    if (ma >= nma) break;
+    const double w = (row.mid && ma == nma - 1) ? 0.5 : 1.0;
+    const double2 y = make_double2(w * acc[i].x, w * acc[i].y);
+    const int h = row.h0 + ma;
+    if (valid) yout[(size_t)h * n + atom] = y;
+    const double2 u = usl[(size_t)h * YS_ATOMS];
+    e += u.x * y.x + u.y * y.y;
+  }
+  return e;
+}
+
+__device__ __forceinline__ double yr_row_yz(const SnapDev& S, const YConst& T, const YRowDev& row,
+                                            const double2* __restrict__ usl, const double* __restrict__ yc,
+                                            const double2* __restrict__ cas, int64_t n, int64_t atom, bool valid,
+                                            double2* __restrict__ yout, double2* __restrict__ zout) {
+  const int nma = row.mid ? row.mb + 1 : row.j + 1;
+  const int ntile = (nma + YR_TILE - 1) / YR_TILE;
+  double e = 0.0;
+  int ma0 = 0;
+  for (int k = 0; k < ntile; k++) {
+    const int w = (nma - ma0 + (ntile - k) - 1) / (ntile - k);
+    switch (w) {
+#define IPG_NT(NT) \
+  case NT:         \
+    e += yr_tile_yz<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout, zout); \
+    break;
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5)
+#undef IPG_NT
+      default:
+        break;
+    }
+    ma0 += w;
+  }
+  return e;
+}
+
+// YM: YM_Y writes Y' (yout [u_half][n]) and E_i; YM_Z writes Z (yout [idxz_max][n], nothing
+// summed across items); YM_YZ writes both (Z to zout).
+// NW: warps per block (the Utot tile of 32 atoms is shared by all of them; two blocks per SM).
+constexpr int YM_Y = 0, YM_Z = 1, YM_YZ = 2;
+template <int YM, int NW = YS_WARPS>
+__global__ void __launch_bounds__(NW * 32, 2) k_snap_yrows(const __grid_constant__ SnapDev S, const __grid_constant__ YConst T, int64_t n,
                                                                  const int32_t* __restrict__ species,
                                                                  const double2* __restrict__ utot,
-                                                                 double2* __restrict__ yout, double* __restrict__ Ei) {
+                                                                 double2* __restrict__ yout, double* __restrict__ Ei,
+                                                                 double2* __restrict__ zout) {
+  constexpr bool ZOUT = YM == YM_Z;
   extern __shared__ __align__(16) unsigned char ysh[];  // layout: yr_smem
   __shared__ int next_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1160,6 +1939,8 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
       const YRowDev row = T.rows[r];
       if (ZOUT)
         yr_row_z(S, T, row, usl, cas, n, atom, valid, yout);  // yout: Z [idxz_max][n]
+      else if (YM == YM_YZ)
+        erow[r * YS_ATOMS + lane] = yr_row_yz(S, T, row, usl, yc, cas, n, atom, valid, yout, zout);
       else
         erow[r * YS_ATOMS + lane] = yr_row(S, T, row, usl, yc, cas, n, atom, valid, yout);
     }
@@ -1180,7 +1961,7 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yrows(const __grid_co
 //   V_i = sum over neighbors j of (g_i - g_j) . dU_ij/dr_ij      (half plane of every level),
 // the terms t, levels and factors of each component being those of dB/dr (compute_b.jl:
 // 207-400).  V comes from k_snap_vsum (every chain of a neighbor per lane), Z from
-// k_snap_yrows<true>, and k_snap_gbeta contracts them with the atoms in lanes.
+// k_snap_yrows<YM_Z>, and k_snap_gbeta contracts them with the atoms in lanes.
 
 // V of atoms a0 .. a0+nc-1 as V[h][nc]: one warp per atom, lanes over neighbors (32 at a
 // time), v_h = A u_h + sum_k B_k du_k,h with A = dsfac gv.uhat, B_k = sfac gv_k, gv = g_i - g_j;
@@ -1355,7 +2136,7 @@ __global__ void __launch_bounds__(GB_WARPS * 32) k_snap_gbeta(const __grid_const
   for (int q = threadIdx.x; q < nsp * K; q += blockDim.x) gpart[(size_t)blockIdx.x * nsp * K + q] = gacc[q];
 }
 
-// Bispectrum components from Z (k_snap_yrows<true>) and Utot for atoms a0 .. a0+nc-1
+// Bispectrum components from Z (k_snap_yrows<YM_Z>) and Utot for atoms a0 .. a0+nc-1
 // (compute_b.jl:17-94): B_b = 2 sum_half w Re(conj(U_j) Z(j1,j2,j)) - bzero_j, 32 atoms per
 // tile in lanes, the warps over components; Ei = beta[s_i] . B_i (the bzero shift inside B).
 // B [n][K] (optional) and Ei [n] are indexed by the global atom.
@@ -1853,14 +2634,16 @@ int launch_pair_adj(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d
 }
 
 // Plain path contraction: f_p = dB_i/dr_ij . beta[s_i] from the materialised dB/dr.
+// fvec[p] = dbl[p] . beta of the pair's centre atom i: K components of dbl [np][K][3]; beta per
+// atom (atom_stride > 0: beta + i*atom_stride) or per species (beta + s_i*sp_stride).
 __global__ void k_snap_contract(int64_t n, const int64_t* __restrict__ off, const int32_t* __restrict__ species,
                                 int nsp, const double* __restrict__ dbl, const double* __restrict__ beta, int K,
-                                double* __restrict__ fvec) {
+                                int64_t atom_stride, int64_t sp_stride, double* __restrict__ fvec) {
   // one warp per atom; lanes over (pair, component) rows
   int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (i >= n) return;
-  const double* bt = beta + (size_t)clamp_sp(species[i], nsp) * K;
+  const double* bt = atom_stride > 0 ? beta + (size_t)i * atom_stride : beta + (size_t)clamp_sp(species[i], nsp) * sp_stride;
   for (int64_t p = off[i]; p < off[i + 1]; p++) {
     const double* d = dbl + (size_t)p * K * 3;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
@@ -2096,6 +2879,44 @@ __global__ void k_sum_partials(int64_t nblocks, int width, const double* __restr
   out[q] = s;
 }
 
+// Beta pullback from the descriptors (chem_flag / quadratic SNAP): block b sums the atoms of
+// its contiguous range, threads over the (species block, component) columns:
+// part[b][s][q] = sum_a [s_a = s] gE B_a[q] + g_a . dB_a[s K + q]  (dB_a [K*nsp][3]).
+__global__ void k_gbeta_desc(int64_t n, int K, int nsp, const int32_t* __restrict__ species,
+                             const double* __restrict__ B, const double* __restrict__ dB, const double* __restrict__ g,
+                             double gE, double* __restrict__ part) {
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t a0 = (int64_t)blockIdx.x * per, a1 = a0 + per < n ? a0 + per : n;
+  const int KN = K * nsp;
+  for (int col = threadIdx.x; col < KN; col += blockDim.x) {
+    const int sp = col / K, q = col - sp * K;
+    double acc = 0.0;
+    for (int64_t a = a0; a < a1; a++) {
+      if (species[a] == sp) acc += gE * B[(size_t)a * K + q];
+      const double* d = dB + ((size_t)a * KN + col) * 3;
+      acc += g[3 * a] * d[0] + g[3 * a + 1] * d[1] + g[3 * a + 2] * d[2];
+    }
+    part[(size_t)blockIdx.x * KN + col] = acc;
+  }
+}
+
+// Per-block sums of x[0 .. n) over contiguous ranges of ceil(n / gridDim.x) items, each in a
+// fixed order (blockDim.x = 256).
+__global__ void k_sum_partials_strided(int64_t n, const double* __restrict__ x, double* __restrict__ out) {
+  __shared__ double sm[256];
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t b = (int64_t)blockIdx.x * per, e = b + per < n ? b + per : n;
+  double v = 0.0;
+  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) v += x[i];
+  sm[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sm[0];
+}
+
 // ycoef[s][z] = y_mult[z] * beta[s][y_jjb[z]]
 __global__ void k_ycoef(int nsp, int nz, int K, const double* __restrict__ ymult, const int32_t* __restrict__ yjjb,
                         const double* __restrict__ beta, double* __restrict__ ycoef) {
@@ -2106,24 +2927,14 @@ __global__ void k_ycoef(int nsp, int nz, int K, const double* __restrict__ ymult
 }
 
 // out = x + t u (3n coordinates).
-__global__ void k_shift(int64_t m, const double* __restrict__ x, const double* __restrict__ u, double t,
-                        double* __restrict__ out) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < m) out[k] = x[k] + t * u[k];
-}
-
-// Position pullback: gpos = -gE F0 + s R, R the Richardson-extrapolated central difference
-// of the forces along the unit direction (steps h and h/2).  Fh = {F(+h), F(-h), F(+h/2), F(-h/2)}.
-__global__ void k_vjp_pos(int64_t m, const double* __restrict__ F0, double gE, const double* __restrict__ Fp,
-                          const double* __restrict__ Fm, const double* __restrict__ Fp2, const double* __restrict__ Fm2,
-                          double h, double s, double* __restrict__ gpos) {
+// gpos = -gE F + Fdot: the position pullback d(gE E + gF . F)/dx = -gE F - H gF, with
+// H gF = -Fdot the tangent of the forces along gF.
+__global__ void k_vjp_pos(int64_t m, const double* __restrict__ F0, double gE, const double* __restrict__ Fdot,
+                          double* __restrict__ gpos) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= m) return;
   double g = -gE * F0[k];
-  if (Fp) {
-    const double d1 = (Fp[k] - Fm[k]) / (2.0 * h), d2 = (Fp2[k] - Fm2[k]) / h;
-    g += s * (4.0 * d2 - d1) / 3.0;
-  }
+  if (Fdot) g += Fdot[k];
   gpos[k] = g;
 }
 
@@ -2165,6 +2976,7 @@ struct ipg_snap {
   int64_t vjp_chunk = 0;     // atoms per Z chunk (0: about 4 GiB of Z)
   bool generic_plain = false;  // plain path: the per-atom block kernel (IPG_GENERIC_PLAIN=1)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
+  int yr_warps = 8;         // warps per block of the adjoint Y kernel (8 or 10)
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
   int64_t last_np = 0;
@@ -2179,6 +2991,8 @@ struct ipg_snap {
     std::vector<double> L;
     const void *pos = nullptr, *sp = nullptr;
     void *E = nullptr, *F = nullptr, *W6 = nullptr;
+    const void* Fref = nullptr;  // training steps: F_ref, loss, dL/dbeta buffers
+    void *loss = nullptr, *gbeta = nullptr;
     bool pair_split = false, y_entries = false;
     int utot_warps = 0, walk_warps = 0;
     cudaGraphExec_t exec = nullptr;
@@ -2199,7 +3013,8 @@ struct ipg_snap {
     std::vector<double> L;
     CellList cl;      // buffers under the "skin_" prefix
     PairList pairs;   // the list with enlarged cutoffs
-    double* ref = nullptr;  // positions at the build
+    double* ref = nullptr;     // positions at the build
+    int32_t* ref_sp = nullptr;  // species at the build (a change rebuilds the list)
   } sk;
   int64_t skin_builds = 0, skin_reuses = 0;
 };
@@ -2254,7 +3069,13 @@ int upload_tables(ipg_snap* s) {
   memset(&d, 0, sizeof(d));
   d.J = h.J;
   d.nsp = s->p.nspecies;
-  d.K = h.idxb_max;
+  d.chem = s->p.chem_flag ? 1 : 0;
+  d.nelem = d.chem ? s->p.nspecies : 1;
+  d.wselfall = s->p.wselfall_flag ? 1 : 0;
+  d.literal_chem_z = s->p.literal_chem_z ? 1 : 0;
+  d.quadratic = s->p.quadratic_flag ? 1 : 0;
+  d.klin = h.idxb_max * d.nelem * d.nelem * d.nelem;
+  d.K = d.quadratic ? d.klin + d.klin * (d.klin + 1) / 2 : d.klin;
   d.idxu_max = h.idxu_max;
   d.idxz_max = h.idxz_max;
   d.u_half = h.u_half;
@@ -2325,7 +3146,8 @@ int launch_atoms(ipg_snap* s, const SnapDev& dev, const SnapIO& io, int64_t nato
 // set (the replay path uploads before each launch).
 int set_beta(ipg_snap* s, const double* beta, double beta0, SnapDev& dev) {
   ipg_ctx* ctx = s->ctx;
-  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  const int K = dev.K, nsp = s->p.nspecies;
+  const bool chemq = dev.chem || dev.quadratic;  // bzero is inside B there: no energy shift
   double *d_beta, *d_ycoef;
   const size_t nb = (size_t)nsp * K;
   IPG_RET(scratch(ctx, "snap_beta", nb + IPG_MAX_SNAP_SPECIES + 1, &d_beta));
@@ -2339,7 +3161,7 @@ int set_beta(ipg_snap* s, const double* beta, double beta0, SnapDev& dev) {
   for (size_t k = 0; k < nb; k++) hb[k] = beta ? beta[k] : 0.0;
   for (int q = 0; q < IPG_MAX_SNAP_SPECIES; q++) {  // -beta[s] . bzero[j(k)] (compute_b.jl:134-155)
     double t = 0.0;
-    if (q < nsp)
+    if (q < nsp && !chemq)
       for (int k = 0; k < K; k++) t += hb[(size_t)q * K + k] * s->h.bzero[s->h.idxb[3 * k + 2]];
     hb[nb + q] = -t;
   }
@@ -2374,7 +3196,7 @@ int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int3
                  memcmp(C.L.data(), h_L, sizeof(double) * 3 * nconf) == 0;
     if (valid) {
       double d2;
-      IPG_RET(ipg_max_disp2(s->ctx, C.cl, d_pos, C.ref, &d2));
+      IPG_RET(ipg_max_disp2(s->ctx, C.cl, d_pos, C.ref, d_species, C.ref_sp, &d2));
       valid = d2 <= 0.25 * s->skin * s->skin;
     }
     if (!valid) {
@@ -2389,7 +3211,10 @@ int snap_neighbors_inner(ipg_snap* s, int64_t n, const double* d_pos, const int3
       IPG_RET(ipg_build_pairs(s->ctx, "skin_", C.cl, d_species, nsp, cut2.data(), IPG_NLIST_FULL, false, C.pairs,
                               false, 0, s->walk_warps));
       IPG_RET(scratch(s->ctx, "skin_ref", 3 * (size_t)n, &C.ref));
+      IPG_RET(scratch(s->ctx, "skin_ref_sp", (size_t)n, &C.ref_sp));
       CUDA_RET(s->ctx, cudaMemcpyAsync(C.ref, d_pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice,
+                                       s->ctx->stream));
+      CUDA_RET(s->ctx, cudaMemcpyAsync(C.ref_sp, d_species, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice,
                                        s->ctx->stream));
       C.valid = true;
       C.n = n;
@@ -2426,6 +3251,8 @@ struct EvalOut {
   double* Aw = nullptr;  // [nconf][6][K*nsp] fitting virial rows (device)
   PairList* pl_out = nullptr;          // receives the pair list (stays valid until the next build)
   const double2** utot_out = nullptr;  // receives Utot [n][idxu_max] when the chain kernel made it
+  double2* zall = nullptr;  // adjoint mode: also write Z [idxz_max][n] here (row-blocked Y kernel only)
+  bool* zall_done = nullptr;  // set when zall was written
 };
 
 // Atoms per chunk of the Z buffer (idxz_max entries per atom): about 4 GiB, or IPG_VJP_CHUNK.
@@ -2436,12 +3263,12 @@ int64_t zrows_chunk(const ipg_snap* s, const SnapDev& dev, int64_t n) {
   return std::max<int64_t>(1, std::min(C, n));
 }
 
-// Shared memory and blocks per SM of k_snap_yrows<true>.
+// Shared memory and blocks per SM of k_snap_yrows<YM_Z>.
 int zrows_config(ipg_ctx* ctx, const SnapDev& dev, int* ysm, int* per_sm) {
   *ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
-  CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yrows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, *ysm));
+  CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_yrows<YM_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, *ysm));
   *per_sm = 1;
-  CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_snap_yrows<true>, YS_WARPS * 32, *ysm));
+  CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_snap_yrows<YM_Z>, YS_WARPS * 32, *ysm));
   return IPG_OK;
 }
 
@@ -2463,8 +3290,8 @@ int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, const PairList& pl,
     const int64_t nc = std::min(C, n - a0);
     const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
     const int64_t yg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, yper));
-    IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<true>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
-                     d_species + a0, utot + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr);
+    IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<YM_Z>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
+                     d_species + a0, utot + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr, (double2*)nullptr);
     const int64_t bg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, bper));
     IPG_TIMED_LAUNCH(ctx, "snap_bdesc", k_snap_bdesc, (unsigned)bg, GB_WARPS * 32, bsm, dev, a0, nc, d_species, Z,
                      utot, B, Ei);
@@ -2499,7 +3326,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   io.B = out.B;
   io.status = ctx->d_status;
   const bool need_plain = (mode == MODE_PLAIN) || out.dB || out.Wd || out.Aw;
-  const bool chains = dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint;
+  const bool chemq = dev.chem || dev.quadratic;  // element-resolved / quadratic SNAP kernel
+  const bool chains = dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && !chemq;
   if (chains && n) {  // Utot from the register-chain kernel
     double2* utot;
     IPG_RET(scratch(ctx, "snap_utot", (size_t)n * dev.idxu_max + 1, &utot));
@@ -2507,7 +3335,56 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     io.utot_in = utot;
   }
   int nch = 1;
-  if (mode == MODE_ADJ && chains) {
+  if (chemq) {
+    // chem_flag / quadratic_flag: B (and E_i), and dB_lin/dr of every pair when forces or
+    // force descriptors are wanted; the forces contract dB/dr with beta (quadratic: with each
+    // atom's effective linear coefficients), the descriptors read the extended dB/dr.
+    const int KL = dev.klin;
+    const bool forces = mode != MODE_DESC && (out.F || out.W6);
+    const bool want_db = out.dB || out.Wd || out.Aw;
+    const bool plain = forces || want_db;
+    double* Bx = out.B;
+    if (dev.quadratic && want_db && !Bx) IPG_RET(scratch(ctx, "snap_Bx", (size_t)n * K + 1, &Bx));
+    io.B = Bx;
+    double *dlin = nullptr, *beff = nullptr;
+    if (plain) IPG_RET(scratch(ctx, "snap_dbl", (size_t)np * KL * 3 + 3, &dlin));
+    if (dev.quadratic && forces) IPG_RET(scratch(ctx, "snap_beff", (size_t)n * KL + 1, &beff));
+    io.dbl = dlin;
+    const ChemSmem CL = chem_smem(dev, 4, plain);
+    if (CL.total > 227 * 1024)
+      return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "chem/quadratic SNAP needs %zu bytes of shared memory", CL.total);
+    const void* kfn = plain ? (const void*)k_snap_chem<true> : (const void*)k_snap_chem<false>;
+    CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL.total));
+    int per_sm = 1;
+    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 128, CL.total));
+    const int64_t grid = std::min<int64_t>(std::max<int64_t>(n, 1), (int64_t)ctx->num_sms * std::max(1, per_sm));
+    double2* zbuf;
+    IPG_RET(scratch(ctx, "snap_chem_z", (size_t)grid * dev.nelem * dev.nelem * dev.idxz_max + 1, &zbuf));
+    if (n) {
+      if (plain)
+        IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_chem<true>, (unsigned)grid, 128, CL.total, dev, io, zbuf, beff);
+      else
+        IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_chem<false>, (unsigned)grid, 128, CL.total, dev, io, zbuf, beff);
+    }
+    if (forces) {
+      IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
+      if (n)
+        IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, nsp,
+                         dlin, beff ? beff : dev.beta, KL, beff ? (int64_t)KL : (int64_t)0, (int64_t)K, fvec);
+    }
+    if (want_db) {
+      dbl = dlin;
+      if (dev.quadratic) {  // the extended dB/dr of every pair
+        int32_t* owner;
+        IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
+        IPG_RET(scratch(ctx, "snap_dbx", (size_t)np * K * 3 + 3, &dbl));
+        if (n) {
+          IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
+          IPG_LAUNCH(ctx, k_quad_pairs, nblk(np * KL, 256), 256, 0, np, pl.d_np, KL, K, owner, Bx, dlin, dbl);
+        }
+      }
+    }
+  } else if (mode == MODE_ADJ && chains) {
     // per-atom kernel writes the weighted Y; the register-chain kernel does the neighbors
     nch = s->pair_split ? dev.J / 2 + 1 : 1;
     double2* yout;
@@ -2521,16 +3398,28 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
         const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
-        const void* kfn = rows ? (const void*)k_snap_yrows<false> : (const void*)k_snap_yatoms;
+        const bool withz = rows && out.zall;
+        const bool w10 = rows && !withz && s->yr_warps == 10;  // ten warps per block (IPG_YR_WARPS=10)
+        const int ythreads = (w10 ? 10 : YS_WARPS) * 32;
+        const void* kfn = !rows ? (const void*)k_snap_yatoms
+                                : (withz ? (const void*)k_snap_yrows<YM_YZ>
+                                         : (w10 ? (const void*)k_snap_yrows<YM_Y, 10> : (const void*)k_snap_yrows<YM_Y>));
         if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
         CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
-        CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, YS_WARPS * 32, ysm));
+        CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, ythreads, ysm));
         const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
         const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
-        if (rows)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<false>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
-                           d_species, io.utot_in, yout, Ei);
+        if (withz) {
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<YM_YZ>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst,
+                           n, d_species, io.utot_in, yout, Ei, out.zall);
+          if (out.zall_done) *out.zall_done = true;
+        } else if (w10)
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 10>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
+                           n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
+        else if (rows)
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<YM_Y>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
+                           d_species, io.utot_in, yout, Ei, (double2*)nullptr);
         else
           IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
                            io.utot_in, yout, Ei);
@@ -2556,7 +3445,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     if (out.F || out.W6) {
       IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
       if (n) IPG_TIMED_LAUNCH(ctx, "snap_contract", k_snap_contract, nblk(32 * n, 256), 256, 0, n, pl.d_off, d_species, nsp, dbl, dev.beta, K,
-                               fvec);
+                               (int64_t)0, (int64_t)K, fvec);
     }
   } else if (chains && n && dev.J <= YR_MAX_J && s->h.yconst_ok && cap == 0) {
     // Z from the row-blocked kernel per chunk of atoms, then B (and E_i) per atom tile
@@ -2573,8 +3462,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       const int64_t nc = std::min(C, n - a0);
       const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
       const int64_t yg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, yper));
-      IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<true>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
-                       d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr);
+      IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<YM_Z>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
+                       d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr, (double2*)nullptr);
       const int64_t bg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, bper));
       IPG_TIMED_LAUNCH(ctx, "snap_bdesc", k_snap_bdesc, (unsigned)bg, GB_WARPS * 32, bsm, dev, a0, nc, d_species, Z,
                        io.utot_in, out.B, Ei);
@@ -2647,14 +3536,73 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
   return ipg_side_join(ctx);
 }
 
+int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
+                    const int64_t* h_atom_off, const double* h_L, const double* beta, double gE, const double* d_g,
+                    double* d_gbeta, const PairList* reuse_pl, const double2* reuse_utot, const double2* reuse_Z);
+
+// Graph mode of a whole force-matching training step (snap_train_step).
+constexpr int MODE_TRAIN = 100;
+// Z of a training step is kept for the pullback when it takes at most this many bytes.
+constexpr size_t TRAIN_Z_MAX = size_t(48) << 30;
+
+// One force-matching training step over a batch (the fitting loop of PotentialLearning over
+// the descriptors of src/BasisSystems/LAMMPS_SNAP/bispectrum.jl:279-387):
+//   E, F, W6 of the adjoint path (o; F is required), L = sum_atoms |F - F_ref|^2 (d_loss) and
+//   dL/dbeta = the beta pullback with cotangent 2 (F - F_ref) (d_gbeta [nspecies][K]).
+// The pullback reuses the evaluation's pair list and Utot, and the Z the Y kernel wrote beside
+// Y (when it fits TRAIN_Z_MAX).  Device buffers only, no synchronisation, so the whole step can
+// be captured as one CUDA graph (cap > 0: capacity mode, as snap_eval).
+int snap_train_step(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_sp, int nconf, const int64_t* off,
+                    const double* L, const double* beta, double beta0, const double* d_Fref, const EvalOut& o,
+                    double* d_loss, double* d_gbeta, int64_t cap) {
+  ipg_ctx* ctx = s->ctx;
+  const SnapDev& dev = s->dev;
+  double *d_g, *d_li, *d_lpart;
+  IPG_RET(scratch(ctx, "loss_g", 3 * (size_t)n + 3, &d_g));
+  IPG_RET(scratch(ctx, "loss_li", (size_t)n + 1, &d_li));
+  const int64_t lblk = std::max<int64_t>(1, std::min<int64_t>((n + 1023) / 1024, 4096));
+  IPG_RET(scratch(ctx, "loss_part", (size_t)lblk, &d_lpart));
+  EvalOut oo = o;
+  PairList pl;
+  const double2* utot = nullptr;
+  oo.pl_out = &pl;
+  oo.utot_out = &utot;
+  double2* Z = nullptr;
+  bool zdone = false;
+  const bool chains = dev.J <= PAIR_CHAIN_MAX_J && !s->generic_adjoint && !dev.chem && !dev.quadratic;
+  if (chains && dev.J <= YR_MAX_J && s->h.yconst_ok && !s->y_entries && n &&
+      (size_t)n * dev.idxz_max * sizeof(double2) <= TRAIN_Z_MAX) {
+    IPG_RET(scratch(ctx, "train_Z", (size_t)n * dev.idxz_max + 1, &Z));
+    oo.zall = Z;
+    oo.zall_done = &zdone;
+  }
+  IPG_RET(snap_eval(s, n, d_pos, d_sp, nconf, off, L, beta, beta0, MODE_ADJ, oo, cap));
+  if (n) {
+    IPG_LAUNCH(ctx, k_loss_grad, nblk(n, 256), 256, 0, n, o.F, d_Fref, d_g, d_li);
+    IPG_LAUNCH(ctx, k_sum_partials_strided, (unsigned)lblk, 256, 0, n, d_li, d_lpart);
+    IPG_LAUNCH(ctx, k_sum_partials, 1, 32, 0, lblk, 1, d_lpart, d_loss, 0.0);
+  } else {
+    CUDA_RET(ctx, cudaMemsetAsync(d_loss, 0, sizeof(double), ctx->stream));
+  }
+  return snap_vjp_device(s, n, d_pos, d_sp, nconf, off, L, beta, 0.0, d_g, d_gbeta, &pl, utot, zdone ? Z : nullptr);
+}
+
 // ---- CUDA-graph replay of batched evaluations -------------------------------------------
 constexpr int IPG_ERR_NOT_CAPTURED = 1;  // internal: no graph for this key (not an API code)
 
+// The device buffers of a force-matching training step (MODE_TRAIN graphs).
+struct TrainBufs {
+  const double* Fref = nullptr;
+  double* loss = nullptr;
+  double* gbeta = nullptr;
+};
+
 ipg_snap::Graph* find_graph(ipg_snap* s, int32_t nconfig, const int64_t* off, const double* L, int mode,
-                            const void* pos, const void* sp, const EvalOut& o) {
+                            const void* pos, const void* sp, const EvalOut& o, const TrainBufs& tb) {
   for (auto& g : s->graphs) {
     if (g.nconfig != nconfig || g.mode != mode || g.pos != pos || g.sp != sp || g.E != o.E || g.F != o.F ||
-        g.W6 != o.W6 || g.pair_split != s->pair_split || g.y_entries != s->y_entries ||
+        g.W6 != o.W6 || g.Fref != tb.Fref || g.loss != tb.loss || g.gbeta != tb.gbeta ||
+        g.pair_split != s->pair_split || g.y_entries != s->y_entries ||
         g.utot_warps != s->utot_warps || g.walk_warps != s->walk_warps)
       continue;
     if (memcmp(g.off.data(), off, sizeof(int64_t) * (nconfig + 1)) != 0) continue;
@@ -2674,9 +3622,10 @@ void drop_graph(ipg_snap* s, ipg_snap::Graph* g) {
 // Returns IPG_ERR_NOT_CAPTURED when there is no usable graph, IPG_ERR_CAPACITY when the
 // pair count outgrew the captured capacity (the graph is dropped; the caller re-runs).
 int batch_graph_replay(ipg_snap* s, int32_t nconfig, const int64_t* off, const double* d_pos, const int32_t* d_sp,
-                       const double* L, const double* beta, double beta0, int mode, const EvalOut& o) {
+                       const double* L, const double* beta, double beta0, int mode, const EvalOut& o,
+                       const TrainBufs& tb = TrainBufs()) {
   ipg_ctx* ctx = s->ctx;
-  ipg_snap::Graph* g = find_graph(s, nconfig, off, L, mode, d_pos, d_sp, o);
+  ipg_snap::Graph* g = find_graph(s, nconfig, off, L, mode, d_pos, d_sp, o, tb);
   if (!g) return IPG_ERR_NOT_CAPTURED;
   if (g->gen != ctx->scratch_gen) {  // a scratch buffer moved since the capture
     drop_graph(s, g);
@@ -2709,13 +3658,17 @@ int batch_graph_replay(ipg_snap* s, int32_t nconfig, const int64_t* off, const d
 // every scratch buffer first, so nothing allocates while capturing.  Failures only mean
 // that later calls run eagerly.
 void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const double* d_pos, const int32_t* d_sp,
-                         const double* L, const double* beta, double beta0, int mode, const EvalOut& o) {
+                         const double* L, const double* beta, double beta0, int mode, const EvalOut& o,
+                         const TrainBufs& tb = TrainBufs()) {
   ipg_ctx* ctx = s->ctx;
   const int64_t n = off[nconfig];
   const int64_t cap = s->last_np + s->last_np / 4 + 1024;
-  if (ipg_status_reset(ctx) || snap_eval(s, n, d_pos, d_sp, nconfig, off, L, beta, beta0, mode, o, cap) ||
-      ipg_status_check(ctx, "graph warm-up"))
-    return;
+  auto body = [&]() {
+    return mode == MODE_TRAIN ? snap_train_step(s, n, d_pos, d_sp, nconfig, off, L, beta, beta0, tb.Fref, o, tb.loss,
+                                                tb.gbeta, cap)
+                              : snap_eval(s, n, d_pos, d_sp, nconfig, off, L, beta, beta0, mode, o, cap);
+  };
+  if (ipg_status_reset(ctx) || body() || ipg_status_check(ctx, "graph warm-up")) return;
   if (s->graphs.size() >= 8) drop_graph(s, &s->graphs.front());
   ipg_snap::Graph g;
   g.nconfig = nconfig;
@@ -2727,6 +3680,9 @@ void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const
   g.E = o.E;
   g.F = o.F;
   g.W6 = o.W6;
+  g.Fref = tb.Fref;
+  g.loss = tb.loss;
+  g.gbeta = tb.gbeta;
   g.pair_split = s->pair_split;
   g.y_entries = s->y_entries;
   g.utot_warps = s->utot_warps;
@@ -2742,7 +3698,7 @@ void batch_graph_capture(ipg_snap* s, int32_t nconfig, const int64_t* off, const
   if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
     st = IPG_ERR_CUDA;
   } else {
-    st = snap_eval(s, n, d_pos, d_sp, nconfig, off, L, beta, beta0, mode, o, cap);
+    st = body();
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     if (st == IPG_OK && e != cudaSuccess) st = IPG_ERR_CUDA;
   }
@@ -2816,6 +3772,13 @@ int check_common(ipg_snap* s, int64_t n, const void* pos, const void* species, c
   return IPG_OK;
 }
 
+int check_offsets(ipg_ctx* ctx, int32_t nconfig, const int64_t* atom_offsets) {
+  if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
+  for (int c = 0; c < nconfig; c++)
+    if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
+  return IPG_OK;
+}
+
 int check_host_inputs(ipg_snap* s, int64_t n, const double* pos, const int32_t* species) {
   if (!host_all_finite(pos, 3 * n)) return ipg_fail(s->ctx, IPG_ERR_NONFINITE, "non-finite position");
   if (!host_species_ok(species, n, s->p.nspecies))
@@ -2829,8 +3792,8 @@ int upload_inputs(ipg_snap* s, int64_t n, const double* pos, const int32_t* spec
   IPG_RET(scratch(ctx, "snap_in_pos", 3 * (size_t)n + 3, d_pos));
   IPG_RET(scratch(ctx, "snap_in_sp", (size_t)n + 1, d_sp));
   if (n) {
-    CUDA_RET(ctx, cudaMemcpyAsync(*d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_RET(ctx, cudaMemcpyAsync(*d_sp, species, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    IPG_RET(ipg_copy_h2d(ctx, *d_pos, pos, sizeof(double) * 3 * n));
+    IPG_RET(ipg_copy_h2d(ctx, *d_sp, species, sizeof(int32_t) * n));
   }
   return IPG_OK;
 }
@@ -2850,7 +3813,6 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
     return ipg_fail(ctx, IPG_ERR_ARG, "nspecies must be in 1..%d", IPG_MAX_SNAP_SPECIES);
   if (p.chem_flag != p.bnorm_flag)  // snap.jl:10-13
     return ipg_fail(ctx, IPG_ERR_ARG, "chem_flag and bnorm_flag should be the same");
-  if (p.chem_flag) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "chem_flag is not built");
   if (!(p.rcutfac > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "rcutfac must be > 0");
   for (int q = 0; q < p.nspecies; q++)
     if (!(p.radii[q] > 0.0)) return ipg_fail(ctx, IPG_ERR_ARG, "radii must be > 0");
@@ -2885,6 +3847,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
   if (const char* g = getenv("IPG_GENERIC_PLAIN")) s->generic_plain = g[0] == '1';
+  if (const char* g = getenv("IPG_YR_WARPS")) s->yr_warps = atoi(g) == 10 ? 10 : 8;
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);
@@ -2917,7 +3880,7 @@ int ipg_snap_destroy(ipg_snap* s) {
 
 int ipg_snap_ncoeff(const ipg_snap* s, int32_t* K) {
   if (!s || !K) return IPG_ERR_ARG;
-  *K = s->h.idxb_max;
+  *K = s->dev.K;
   return IPG_OK;
 }
 
@@ -2933,7 +3896,7 @@ int ipg_snap_descriptors(ipg_snap* s, int64_t n, const double* pos, const int32_
   int32_t* d_sp;
   IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
   IPG_RET(ipg_status_reset(ctx));
-  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  const int K = s->dev.K, nsp = s->p.nspecies;
   EvalOut o;
   double *dB_d = nullptr, *B_d = nullptr, *W_d = nullptr;
   if (what & IPG_DESC_B) IPG_RET(scratch(ctx, "snap_out_B", (size_t)n * K + 1, &B_d));
@@ -2944,9 +3907,8 @@ int ipg_snap_descriptors(ipg_snap* s, int64_t n, const double* pos, const int32_
   o.Wd = W_d;
   int64_t aoff[2] = {0, n};
   IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, nullptr, 0.0, MODE_DESC, o));
-  if (B_d && n) CUDA_RET(ctx, cudaMemcpyAsync(B, B_d, sizeof(double) * n * K, cudaMemcpyDeviceToHost, ctx->stream));
-  if (dB_d && n)
-    CUDA_RET(ctx, cudaMemcpyAsync(dB, dB_d, sizeof(double) * n * K * nsp * 3, cudaMemcpyDeviceToHost, ctx->stream));
+  if (B_d && n) IPG_RET(ipg_copy_d2h(ctx, B, B_d, sizeof(double) * n * K));
+  if (dB_d && n) IPG_RET(ipg_copy_d2h(ctx, dB, dB_d, sizeof(double) * n * K * nsp * 3));
   if (W_d) {
     if (n) CUDA_RET(ctx, cudaMemcpyAsync(W, W_d, sizeof(double) * K * nsp * 6, cudaMemcpyDeviceToHost, ctx->stream));
     else memset(W, 0, sizeof(double) * K * nsp * 6);
@@ -2983,7 +3945,7 @@ int ipg_snap_batch_descriptors(ipg_snap* s, int32_t nconfig, const int64_t* atom
   double* d_pos;
   int32_t* d_sp;
   IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
-  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  const int K = s->dev.K, nsp = s->p.nspecies;
   const size_t KN = (size_t)K * nsp;
   double *B_d, *Ae_d = nullptr, *Af_d = nullptr, *Aw_d = nullptr;
   IPG_RET(scratch(ctx, "fit_B", (size_t)n * K + 1, &B_d));
@@ -3002,7 +3964,7 @@ int ipg_snap_batch_descriptors(ipg_snap* s, int32_t nconfig, const int64_t* atom
     if (n) CUDA_RET(ctx, cudaMemcpyAsync(Ae, Ae_d, sizeof(double) * nconfig * KN, cudaMemcpyDeviceToHost, ctx->stream));
     else memset(Ae, 0, sizeof(double) * nconfig * KN);
   }
-  if (Af && n) CUDA_RET(ctx, cudaMemcpyAsync(Af, Af_d, sizeof(double) * 3 * n * KN, cudaMemcpyDeviceToHost, ctx->stream));
+  if (Af && n) IPG_RET(ipg_copy_d2h(ctx, Af, Af_d, sizeof(double) * 3 * n * KN));
   if (Aw) {
     if (n) CUDA_RET(ctx, cudaMemcpyAsync(Aw, Aw_d, sizeof(double) * 6 * nconfig * KN, cudaMemcpyDeviceToHost, ctx->stream));
     else memset(Aw, 0, sizeof(double) * 6 * nconfig * KN);
@@ -3052,7 +4014,7 @@ int ipg_snap_energy_forces(ipg_snap* s, int64_t n, const double* pos, const int3
                     o));
   double head[8];
   CUDA_RET(ctx, cudaMemcpyAsync(head, d_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  if (F && n) CUDA_RET(ctx, cudaMemcpyAsync(F, d_out + 8, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (F && n) IPG_RET(ipg_copy_d2h(ctx, F, d_out + 8, sizeof(double) * 3 * n));
   IPG_RET(ipg_status_check(ctx, "ipg_snap_energy_forces"));
   if (E) *E = head[0];
   if (W6) memcpy(W6, head + 1, 6 * sizeof(double));
@@ -3068,11 +4030,29 @@ namespace {
 // resident.  g = cotangent of forces [3n] (device), gE scalar.
 // reuse_pl / reuse_utot: the pair list and Utot of an evaluation of the same positions just
 // before (snap_eval's pl_out / utot_out), or null to build them here.
+// reuse_Z: Z [idxz_max][n] of the same positions (k_snap_yrows<YM_YZ>), or null to form it here.
 int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
                     const int64_t* h_atom_off, const double* h_L, const double* beta, double gE, const double* d_g,
-                    double* d_gbeta, const PairList* reuse_pl = nullptr, const double2* reuse_utot = nullptr) {
+                    double* d_gbeta, const PairList* reuse_pl, const double2* reuse_utot, const double2* reuse_Z) {
   ipg_ctx* ctx = s->ctx;
   SnapDev dev = s->dev;
+  if (dev.chem || dev.quadratic) {
+    // element-resolved / quadratic SNAP: B and dB of every atom (compute_all_descriptors'
+    // layouts), then gbeta[s][q] = gE sum_{i in s} B_i[q] + sum_a g_a . dB_a[s K + q]
+    const int K = dev.K, nsp = dev.nsp;
+    double *Bx, *dBx, *part;
+    IPG_RET(scratch(ctx, "vjp_Bx", (size_t)n * K + 1, &Bx));
+    IPG_RET(scratch(ctx, "vjp_dBx", (size_t)n * K * nsp * 3 + 1, &dBx));
+    EvalOut o;
+    o.B = Bx;
+    o.dB = dBx;
+    IPG_RET(snap_eval(s, n, d_pos, d_species, nconf, h_atom_off, h_L, beta, 0.0, MODE_DESC, o));
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, 1024));
+    IPG_RET(scratch(ctx, "vjp_gpart", (size_t)grid * nsp * K + 1, &part));
+    IPG_LAUNCH(ctx, k_gbeta_desc, (unsigned)grid, 128, 0, n, K, nsp, d_species, Bx, dBx, d_g, gE, part);
+    IPG_LAUNCH(ctx, k_sum_partials, nblk((int64_t)nsp * K, 128), 128, 0, grid, nsp * K, part, d_gbeta, 0.0);
+    return IPG_OK;
+  }
   IPG_RET(set_beta(s, beta, 0.0, dev));
   PairList pl;
   if (reuse_pl)
@@ -3104,10 +4084,14 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
   if (io.utot_in && dev.J <= YR_MAX_J && s->h.yconst_ok) {
     // register-chain path: Z (row-blocked kernel) and V per chunk of atoms, then the
     // contraction
-    const int64_t C = zrows_chunk(s, dev, n);
+    const bool zgiven = reuse_Z && reuse_pl && reuse_utot;
+    const int64_t C = zgiven ? n : zrows_chunk(s, dev, n);
     const int64_t nchunk = (n + C - 1) / C;
     double2 *Z, *V;
-    IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
+    if (zgiven)
+      Z = const_cast<double2*>(reuse_Z);
+    else
+      IPG_RET(scratch(ctx, "snap_Z", (size_t)C * dev.idxz_max + 1, &Z));
     IPG_RET(scratch(ctx, "snap_vjp_V", (size_t)C * dev.u_half + 1, &V));
     int ysm, yper, gper = 1;
     IPG_RET(zrows_config(ctx, dev, &ysm, &yper));
@@ -3123,8 +4107,10 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
       const int64_t a0 = c * C, nc = std::min(C, n - a0);
       const int64_t tiles = (nc + YS_ATOMS - 1) / YS_ATOMS;
       const int64_t yg = std::min<int64_t>(tiles, (int64_t)ctx->num_sms * std::max(1, yper));
-      IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<true>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst, nc,
-                       d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr);
+      if (!zgiven)
+        IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<YM_Z>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst,
+                         nc, d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr,
+                         (double2*)nullptr);
       IPG_RET(launch_vsum(ctx, dev, a0, nc, pl.d_off, pl.d_j, pl.d_r, d_species, d_g, V));
       const int64_t gg = std::min(tiles, gmax);
       IPG_TIMED_LAUNCH(ctx, "snap_gbeta", k_snap_gbeta, (unsigned)gg, GB_WARPS * 32, gsm, dev, a0, nc, d_species, Z,
@@ -3167,17 +4153,17 @@ int ipg_snap_vjp_beta(ipg_snap* s, int64_t n, const double* pos, const int32_t* 
   int32_t* d_sp;
   IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
   IPG_RET(ipg_status_reset(ctx));
-  const int K = s->h.idxb_max, nsp = s->p.nspecies;
+  const int K = s->dev.K, nsp = s->p.nspecies;
   double *d_g, *d_gb;
   IPG_RET(scratch(ctx, "snap_vjp_g", 3 * (size_t)n + 3, &d_g));
   IPG_RET(scratch(ctx, "snap_vjp_gb", (size_t)nsp * K, &d_gb));
   if (n) {
-    if (gF) CUDA_RET(ctx, cudaMemcpyAsync(d_g, gF, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (gF) IPG_RET(ipg_copy_h2d(ctx, d_g, gF, sizeof(double) * 3 * n));
     else CUDA_RET(ctx, cudaMemsetAsync(d_g, 0, sizeof(double) * 3 * n, ctx->stream));
   }
   int64_t aoff[2] = {0, n};
   std::vector<double> zero_beta((size_t)nsp * K, 0.0);
-  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, 1, aoff, L, zero_beta.data(), gE, d_g, d_gb));
+  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, 1, aoff, L, zero_beta.data(), gE, d_g, d_gb, nullptr, nullptr, nullptr));
   CUDA_RET(ctx, cudaMemcpyAsync(gbeta, d_gb, sizeof(double) * nsp * K, cudaMemcpyDeviceToHost, ctx->stream));
   IPG_RET(ipg_status_check(ctx, "ipg_snap_vjp_beta"));
   if (gbeta0) *gbeta0 = gE;
@@ -3194,48 +4180,58 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
   if (!gpos || n == 0) return IPG_OK;
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
   IPG_RET(check_host_inputs(s, n, pos, species));
-  double scale = 0.0;  // max |gF|: the difference step is taken along gF / scale
-  if (gF)
-    for (int64_t k = 0; k < 3 * n; k++) {
-      if (!std::isfinite(gF[k])) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite force cotangent");
-      scale = std::max(scale, std::fabs(gF[k]));
-    }
+  if (gF && !host_all_finite(gF, 3 * n)) return ipg_fail(ctx, IPG_ERR_NONFINITE, "non-finite force cotangent");
   double* d_pos;
   int32_t* d_sp;
   IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
   const size_t m = 3 * (size_t)n;
-  double *F0, *Fs, *x, *dir, *gp;
+  double *F0, *Fd = nullptr, *gp;
   IPG_RET(scratch(ctx, "vjp_F0", m, &F0));
-  IPG_RET(scratch(ctx, "vjp_Fs", 4 * m, &Fs));
-  IPG_RET(scratch(ctx, "vjp_x", m, &x));
-  IPG_RET(scratch(ctx, "vjp_dir", m, &dir));
   IPG_RET(scratch(ctx, "vjp_gpos", m, &gp));
   IPG_RET(ipg_status_reset(ctx));
   int64_t aoff[2] = {0, n};
   EvalOut o;
   o.F = F0;
+  PairList pl;
+  o.pl_out = &pl;
   IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, o));
-  // step: 2e-4 of the largest cutoff (1e-3 for a 5 A cutoff), in the caller's length unit
-  double rmax = 0.0;
-  for (int q = 0; q < s->p.nspecies; q++) rmax = std::max(rmax, 2.0 * s->p.radii[q] * s->p.rcutfac);
-  const double h = 2e-4 * rmax;
-  if (scale > 0.0) {
-    std::vector<double> u(m);
-    for (size_t k = 0; k < m; k++) u[k] = gF[k] / scale;
-    CUDA_RET(ctx, cudaMemcpyAsync(dir, u.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
-    const double steps[4] = {h, -h, 0.5 * h, -0.5 * h};
-    for (int q = 0; q < 4; q++) {
-      IPG_LAUNCH(ctx, k_shift, nblk((int64_t)m, 256), 256, 0, (int64_t)m, d_pos, dir, steps[q], x);
-      EvalOut oq;
-      oq.F = Fs + q * m;
-      IPG_RET(snap_eval(s, n, x, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, oq));
-    }
-    CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));  // u is released on return
+  if (gF) {
+    // H gF: the tangent of the forces along gF, exact (k_snap_hvp, second-order adjoint)
+    SnapDev dev = s->dev;
+    if (dev.chem || dev.quadratic)
+      return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "the position pullback of chem_flag / quadratic SNAP is not built");
+    IPG_RET(set_beta(s, beta, 0.0, dev));
+    const int nw = 4;
+    const HvpSmem HL = hvp_smem(dev, nw);
+    if (HL.total > 227 * 1024)
+      return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "twojmax %d: the position pullback needs %zu bytes of shared memory",
+                      dev.J, HL.total);
+    double *d_v, *fv, *fd;
+    IPG_RET(scratch(ctx, "vjp_v", m, &d_v));
+    IPG_RET(scratch(ctx, "vjp_Fdot", m, &Fd));
+    IPG_RET(scratch(ctx, "vjp_fvec", 3 * (size_t)pl.npairs + 3, &fv));
+    IPG_RET(scratch(ctx, "vjp_fdot", 3 * (size_t)pl.npairs + 3, &fd));
+    IPG_RET(ipg_copy_h2d(ctx, d_v, gF, sizeof(double) * m));
+    SnapIO io;
+    memset(&io, 0, sizeof(io));
+    io.n = n;
+    io.off = pl.d_off;
+    io.nbr = pl.d_j;
+    io.rij = pl.d_r;
+    io.species = d_sp;
+    io.fvec = fv;
+    io.status = ctx->d_status;
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_hvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HL.total));
+    int per_sm = 1;
+    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_hvp, nw * 32, HL.total));
+    const int64_t grid = std::min<int64_t>(n, (int64_t)ctx->num_sms * std::max(1, per_sm));
+    IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_snap_hvp, (unsigned)grid, nw * 32, HL.total, dev, io, d_v, fd);
+    IPG_RET(ipg_side_join(ctx));
+    IPG_LAUNCH(ctx, k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off, pl.d_in_pair, fd, 1,
+               d_pos, Fd, (double*)nullptr);
   }
-  const bool fd = scale > 0.0;
-  IPG_LAUNCH(ctx, k_vjp_pos, nblk((int64_t)m, 256), 256, 0, (int64_t)m, F0, gE, fd ? Fs : nullptr,
-             fd ? Fs + m : nullptr, fd ? Fs + 2 * m : nullptr, fd ? Fs + 3 * m : nullptr, h, scale, gp);
-  CUDA_RET(ctx, cudaMemcpyAsync(gpos, gp, sizeof(double) * m, cudaMemcpyDeviceToHost, ctx->stream));
+  IPG_LAUNCH(ctx, k_vjp_pos, nblk((int64_t)m, 256), 256, 0, (int64_t)m, F0, gE, Fd, gp);
+  IPG_RET(ipg_copy_d2h(ctx, gpos, gp, sizeof(double) * m));
   return ipg_status_check(ctx, "ipg_snap_vjp");
 }
 
@@ -3394,7 +4390,7 @@ int ipg_snap_batch_energy_forces(ipg_snap* s, int32_t nconfig, const int64_t* at
                     mode == IPG_SNAP_ADJOINT ? MODE_ADJ : MODE_PLAIN, o));
   if (E) CUDA_RET(ctx, cudaMemcpyAsync(E, d_out, sizeof(double) * nconfig, cudaMemcpyDeviceToHost, ctx->stream));
   if (W6) CUDA_RET(ctx, cudaMemcpyAsync(W6, d_out + nconfig, sizeof(double) * 6 * nconfig, cudaMemcpyDeviceToHost, ctx->stream));
-  if (F && n) CUDA_RET(ctx, cudaMemcpyAsync(F, d_out + 7 * nconfig, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (F && n) IPG_RET(ipg_copy_d2h(ctx, F, d_out + 7 * nconfig, sizeof(double) * 3 * n));
   return ipg_status_check(ctx, "ipg_snap_batch_energy_forces");
 }
 
@@ -3404,9 +4400,7 @@ int ipg_snap_batch_loss_grad(ipg_snap* s, int32_t nconfig, const int64_t* atom_o
   if (!s || nconfig < 1 || !atom_offsets || !L || !beta || !F_ref || !loss || !gbeta)
     return s ? ipg_fail(s->ctx, IPG_ERR_ARG, "bad batch args") : IPG_ERR_ARG;
   ipg_ctx* ctx = s->ctx;
-  if (atom_offsets[0] != 0) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets[0] must be 0");
-  for (int c = 0; c < nconfig; c++)
-    if (atom_offsets[c + 1] < atom_offsets[c]) return ipg_fail(ctx, IPG_ERR_ARG, "atom_offsets must be non-decreasing");
+  IPG_RET(check_offsets(ctx, nconfig, atom_offsets));
   int64_t n = atom_offsets[nconfig];
   IPG_RET(check_common(s, n, pos, species, L));
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
@@ -3414,35 +4408,54 @@ int ipg_snap_batch_loss_grad(ipg_snap* s, int32_t nconfig, const int64_t* atom_o
   double* d_pos;
   int32_t* d_sp;
   IPG_RET(upload_inputs(s, n, pos, species, &d_pos, &d_sp));
-  const int K = s->h.idxb_max, nsp = s->p.nspecies;
-  double *d_F, *d_Fref, *d_g, *d_li, *d_gb, *d_l;
+  const int K = s->dev.K, nsp = s->p.nspecies;
+  double *d_F, *d_Fref, *d_gb, *d_l;
   IPG_RET(scratch(ctx, "loss_F", 3 * (size_t)n + 3, &d_F));
   IPG_RET(scratch(ctx, "loss_Fref", 3 * (size_t)n + 3, &d_Fref));
-  IPG_RET(scratch(ctx, "loss_g", 3 * (size_t)n + 3, &d_g));
-  IPG_RET(scratch(ctx, "loss_li", (size_t)n + 1, &d_li));
   IPG_RET(scratch(ctx, "loss_gb", (size_t)nsp * K, &d_gb));
   IPG_RET(scratch(ctx, "loss_l", 1, &d_l));
-  if (n) CUDA_RET(ctx, cudaMemcpyAsync(d_Fref, F_ref, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  if (n) IPG_RET(ipg_copy_h2d(ctx, d_Fref, F_ref, sizeof(double) * 3 * n));
   IPG_RET(ipg_status_reset(ctx));
   EvalOut o;
   o.F = d_F;
-  PairList pl;
-  const double2* utot = nullptr;
-  o.pl_out = &pl;
-  o.utot_out = &utot;
-  IPG_RET(snap_eval(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, beta0, MODE_ADJ, o));
-  if (n) {
-    IPG_LAUNCH(ctx, k_loss_grad, nblk(n, 256), 256, 0, n, d_F, d_Fref, d_g, d_li);
-    IPG_LAUNCH(ctx, k_sum_partials, 1, 32, 0, n, 1, d_li, d_l, 0.0);
-  } else {
-    CUDA_RET(ctx, cudaMemsetAsync(d_l, 0, sizeof(double), ctx->stream));
-  }
-  // same positions: the pullback reuses the evaluation's pair list and Utot
-  IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, 0.0, d_g, d_gb, &pl, utot));
+  IPG_RET(snap_train_step(s, n, d_pos, d_sp, nconfig, atom_offsets, L, beta, beta0, d_Fref, o, d_l, d_gb, 0));
   CUDA_RET(ctx, cudaMemcpyAsync(gbeta, d_gb, sizeof(double) * nsp * K, cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_RET(ctx, cudaMemcpyAsync(loss, d_l, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  (void)beta0;
   return ipg_status_check(ctx, "ipg_snap_batch_loss_grad");
+}
+
+int ipg_snap_batch_loss_grad_dev(ipg_snap* s, int32_t nconfig, const int64_t* atom_offsets, const double* d_pos,
+                                 const int32_t* d_species, const double* L, const double* beta, double beta0,
+                                 const double* d_Fref, int32_t graph, double* d_E, double* d_F, double* d_W6,
+                                 double* d_loss, double* d_gbeta) {
+  if (!s || nconfig < 1 || !atom_offsets || !L || !beta || !d_Fref || !d_F || !d_loss || !d_gbeta)
+    return s ? ipg_fail(s->ctx, IPG_ERR_ARG, "bad batch args") : IPG_ERR_ARG;
+  ipg_ctx* ctx = s->ctx;
+  IPG_RET(check_offsets(ctx, nconfig, atom_offsets));
+  const int64_t n = atom_offsets[nconfig];
+  if (n > 0 && (!d_pos || !d_species)) return ipg_fail(ctx, IPG_ERR_ARG, "null positions or species");
+  CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  EvalOut o;
+  o.E = d_E;
+  o.F = d_F;
+  o.W6 = d_W6;
+  TrainBufs tb;
+  tb.Fref = d_Fref;
+  tb.loss = d_loss;
+  tb.gbeta = d_gbeta;
+  bool periodic = true;
+  for (int k = 0; k < 3 * nconfig; k++) periodic &= std::isfinite(L[k]);
+  const bool use_graph = graph != 0 && periodic && n > 0;
+  if (use_graph) {
+    int st = batch_graph_replay(s, nconfig, atom_offsets, d_pos, d_species, L, beta, beta0, MODE_TRAIN, o, tb);
+    if (st != IPG_ERR_CAPACITY && st != IPG_ERR_NOT_CAPTURED) return st;
+  }
+  IPG_RET(ipg_status_reset(ctx));
+  IPG_RET(snap_train_step(s, n, d_pos, d_species, nconfig, atom_offsets, L, beta, beta0, d_Fref, o, d_loss, d_gbeta,
+                          0));
+  IPG_RET(ipg_status_check(ctx, "ipg_snap_batch_loss_grad_dev"));
+  if (use_graph) batch_graph_capture(s, nconfig, atom_offsets, d_pos, d_species, L, beta, beta0, MODE_TRAIN, o, tb);
+  return IPG_OK;
 }
 
 }  // extern "C"

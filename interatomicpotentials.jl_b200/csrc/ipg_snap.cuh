@@ -85,6 +85,10 @@ struct SnapDev {
   const YItemDev* yitems;
   const double* yca;
   const int32_t* ytrip_jjz;  // [n_ytrip] first Z entry of each triple
+  // explicit multi-element SNAP (chem_flag) and quadratic SNAP: K is then the number of
+  // components per species block, klin of them linear (idxb_max per element triple), the rest
+  // the products B_k B_l (k <= l) of quadratic_flag
+  int chem, nelem, wselfall, literal_chem_z, quadratic, klin;
   const double* beta0;  // [1] energy offset of LBasisPotential (device, like ebias)
   const double* ebias;  // [nsp] -beta[s] . bzero (energy shift of bzero_flag), device memory so that
                         // a captured graph sees the beta of each replay

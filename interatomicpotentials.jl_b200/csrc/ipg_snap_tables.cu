@@ -1,4 +1,4 @@
-// ipg_snap_tables.cpp — host construction of the SNAP index and Clebsch–Gordan tables.
+// ipg_snap_tables.cu — host construction of the SNAP index and Clebsch–Gordan tables.
 //
 // The tables are those of initialize_prebuilt_arrays
 // (src/BasisSystems/SNAP/types/prebuilt_arrays.jl:48-321): the same enumeration order of

@@ -34,6 +34,7 @@ API_SYMBOLS = (
     "ipg_snap_descriptors", "ipg_snap_energy_forces", "ipg_snap_energy_forces_dev", "ipg_snap_vjp_beta",
     "ipg_snap_vjp", "ipg_snap_autotune", "ipg_snap_batch_descriptors", "ipg_snap_set_skin", "ipg_snap_skin_stats",
     "ipg_snap_batch_energy_forces", "ipg_snap_batch_energy_forces_dev", "ipg_snap_batch_loss_grad",
+    "ipg_snap_batch_loss_grad_dev",
 )
 
 
@@ -53,7 +54,7 @@ class SnapParams(C.Structure):
                 ("rfac0", C.c_double), ("radii", C.c_double * MAX_SNAP_SPECIES),
                 ("weight", C.c_double * MAX_SNAP_SPECIES), ("chem_flag", C.c_int32), ("bzero_flag", C.c_int32),
                 ("bnorm_flag", C.c_int32), ("switch_flag", C.c_int32), ("wselfall_flag", C.c_int32),
-                ("literal_sqrt_radius", C.c_int32)]
+                ("literal_sqrt_radius", C.c_int32), ("quadratic_flag", C.c_int32), ("literal_chem_z", C.c_int32)]
 
 
 _lib = None
@@ -101,6 +102,7 @@ def lib():
         "ipg_snap_batch_energy_forces": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, i32, vp, vp, vp]),
         "ipg_snap_batch_energy_forces_dev": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, i32, i32, vp, vp, vp]),
         "ipg_snap_batch_loss_grad": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, vp, vp, vp]),
+        "ipg_snap_batch_loss_grad_dev": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, d, vp, i32, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

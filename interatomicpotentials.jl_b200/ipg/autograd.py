@@ -4,8 +4,8 @@ Julia shim defines for the same library calls.
 ``snap_energy_forces(snap, system, positions, beta, beta0)`` returns (E, F) as tensors that
 carry gradients to ``positions`` (n, 3) and ``beta`` (nsp, K): the pullback is
 ``ipg_snap_vjp`` (include/ipg.h), i.e. dE/dbeta = sum_i B_i, dE/dpos = -F, and the force
-cotangent through dF/dbeta (exact, linear in beta) and -H gF (Richardson-extrapolated central
-differences of the adjoint forces).  ``snap_loss`` is the force-matching loss
+cotangent through dF/dbeta (exact, linear in beta) and -H gF (exact: the directional
+derivative of the adjoint force computation along gF, a second-order adjoint).  ``snap_loss`` is the force-matching loss
 L = sum |F - F_ref|^2 over a batch with its exact beta gradient (``ipg_snap_batch_loss_grad``).
 """
 from __future__ import annotations

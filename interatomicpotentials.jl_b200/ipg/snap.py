@@ -23,8 +23,8 @@ def _vp(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def get_num_snap_coeffs(twojmax, n_elems, chem_flag):
-    """src/BasisSystems/SNAP/utilities/utl.jl:8-25."""
+def get_num_snap_coeffs(twojmax, n_elems, chem_flag, quadratic_flag=False):
+    """src/BasisSystems/SNAP/utilities/utl.jl:8-25 (quadratic_flag: plus K(K+1)/2 products)."""
     J = twojmax
     if J % 2 == 0:
         m = J // 2 + 1
@@ -32,21 +32,25 @@ def get_num_snap_coeffs(twojmax, n_elems, chem_flag):
     else:
         m = (J + 1) // 2
         nc = m * (m + 1) * (m + 2) // 3
-    return nc * n_elems ** 3 if chem_flag else nc
+    k = nc * n_elems ** 3 if chem_flag else nc
+    return k + k * (k + 1) // 2 if quadratic_flag else k
 
 
 class SNAP:
     """SNAP{S,T} (src/BasisSystems/SNAP/types/types.jl:8-25).
 
     Keyword flags follow the reference constructors (snap.jl:6-97); chem_flag must equal
-    bnorm_flag (snap.jl:10-13) and chem_flag itself is not built (IPGError UNSUPPORTED).
+    bnorm_flag (snap.jl:10-13).  chem_flag resolves the descriptors by element triple
+    (K = idxb_max * nspecies^3); literal_chem_z reproduces compute_z.jl's Z index with it.
+    quadratic_flag appends the products 0.5 B_k^2 and B_k B_l (l > k) to the K linear
+    components (the quadratic option of LAMMPS_SNAP/snap.jl:45-47).
     literal_sqrt_radius=True reproduces the sqrt(cutmax) neighbor search radius of
     utl.jl:81 literally; the default searches within cutmax.
     """
 
     def __init__(self, n_atoms, twojmax, species, rcutfac, rmin0, rfac0, radii, weight, chem_flag=False,
                  bzero_flag=False, bnorm_flag=False, switch_flag=False, wselfall_flag=False,
-                 literal_sqrt_radius=False, ctx=None):
+                 literal_sqrt_radius=False, quadratic_flag=False, literal_chem_z=False, ctx=None):
         if chem_flag != bnorm_flag:
             raise ValueError("chem_flag and bnorm_flag should be the same")
         self.n_atoms = n_atoms
@@ -71,6 +75,9 @@ class SNAP:
         p.chem_flag, p.bzero_flag, p.bnorm_flag = int(chem_flag), int(bzero_flag), int(bnorm_flag)
         p.switch_flag, p.wselfall_flag = int(switch_flag), int(wselfall_flag)
         p.literal_sqrt_radius = int(literal_sqrt_radius)
+        p.quadratic_flag = int(quadratic_flag)
+        p.literal_chem_z = int(literal_chem_z)
+        self.quadratic_flag = bool(quadratic_flag)
         h = C.c_void_p()
         self.ctx.check(lib().ipg_snap_create(self.ctx.handle, C.byref(p), C.byref(h)))
         self._h = h
@@ -263,6 +270,24 @@ class DeviceBatch:
     def set_positions(self, pos):
         import torch
         self.pos.copy_(torch.as_tensor(pos, dtype=torch.float64).reshape(-1, 3))
+
+    def train_step(self, beta, F_ref, beta0=0.0, graph=True):
+        """One force-matching training step (``ipg_snap_batch_loss_grad_dev``): fills E, F, W
+        and returns the device tensors (loss (1,), dL/dbeta (nsp, K)); with ``graph=True`` the
+        whole step is one CUDA-graph launch after the first call.  F_ref: a device tensor
+        (n_total, 3) that must stay the same buffer across graph replays."""
+        import torch
+        beta = self.snap.beta_blocks(beta)
+        if not hasattr(self, "loss"):
+            dev = self.pos.device
+            self.loss = torch.zeros(1, dtype=torch.float64, device=dev)
+            self.gbeta = torch.zeros((len(self.snap.species), self.snap.K), dtype=torch.float64, device=dev)
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        self.snap.ctx.check(lib().ipg_snap_batch_loss_grad_dev(
+            self.snap._h, self.nconfig, _vp(self.off), ptr(self.pos), ptr(self.species), _vp(self.L), _vp(beta),
+            float(beta0), ptr(F_ref), int(bool(graph)), ptr(self.E), ptr(self.F), ptr(self.W), ptr(self.loss),
+            ptr(self.gbeta)))
+        return self.loss, self.gbeta
 
     def evaluate(self, beta, beta0=0.0, mode="adjoint", graph=True):
         """Fills (and returns) the device tensors E (nconf,), F (n_total, 3), W (nconf, 6)."""

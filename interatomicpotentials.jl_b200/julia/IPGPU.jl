@@ -112,6 +112,8 @@ struct SnapParams
     switch_flag::Int32
     wselfall_flag::Int32
     literal_sqrt_radius::Int32
+    quadratic_flag::Int32   # quadratic SNAP (the LAMMPS_SNAP keyword); the reference SNAP has none
+    literal_chem_z::Int32   # compute_z.jl's own Z index with chem_flag
 end
 
 pad8(v) = ntuple(i -> i <= length(v) ? Float64(v[i]) : 0.0, 8)
@@ -119,7 +121,7 @@ pad8(v) = ntuple(i -> i <= length(v) ? Float64(v[i]) : 0.0, 8)
 function handle(snap::SNAP)
     p = SnapParams(snap.twojmax, length(snap.species), snap.rcutfac, snap.rmin0, snap.rfac0,
                    pad8(snap.radii), pad8(snap.weight), snap.chem_flag, snap.bzero_flag,
-                   snap.bnorm_flag, snap.switch_flag, snap.wselfall_flag, 0)
+                   snap.bnorm_flag, snap.switch_flag, snap.wselfall_flag, 0, 0, 0)
     h = Ref{Ptr{Cvoid}}(C_NULL)
     check(ccall((:ipg_snap_create, libipg), Cint, (Ctx, Ref{SnapParams}, Ref{Ptr{Cvoid}}), context(), p, h))
     h[]

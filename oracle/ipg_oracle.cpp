@@ -330,6 +330,12 @@ struct Snap {
   double rcutfac, rmin0, rfac0;
   std::vector<double> radii, weight;
   int bzero_flag, bnorm_flag, switch_flag, literal_sqrt;
+  int chem_flag = 0, wselfall_flag = 0, literal_chem_z = 0, quadratic_flag = 0;
+  int nelem = 1;  // elements resolved by the descriptors: nsp with chem_flag, else 1
+  // linear components per species block (get_num_snap_coeffs, utl.jl:8-25), and with the
+  // quadratic products B_k B_l (k <= l) appended (LAMMPS_SNAP/snap.jl:45-47)
+  int nlin() const { return idxb_max * nelem * nelem * nelem; }
+  int ncoef() const { return quadratic_flag ? nlin() + nlin() * (nlin() + 1) / 2 : nlin(); }
   int idxcg_max, idxu_max, idxb_max, idxz_max;
   std::vector<int> idxcg_block, idxu_block, idxb_block, idxz_block;  // [(J+1)^3], [J+1]
   std::vector<int> idxb;                                            // 3 per jjb
@@ -617,28 +623,34 @@ void compute_duidrj(const Snap& s, const double* rij, double wj, double rcut, co
 
 // Per-atom state of compute_all_descriptors (snap.jl:251-310).
 struct AtomWork {
-  std::vector<double> utr, uti;  // Utot [idxu_max]
+  std::vector<double> utr, uti;  // Utot [nelem][idxu_max]
   std::vector<double> ulr, uli;  // per-neighbor U [nnbr][idxu_max]
-  std::vector<double> zr, zi;    // Z [idxz_max]
+  std::vector<double> zr, zi;    // Z [nelem^2][idxz_max]
   std::vector<double> yr, yi;    // Y [idxu_max] (adjoint restatement)
-  std::vector<double> b;         // B [idxb_max]
+  std::vector<double> b;         // B [nlin]
   std::vector<double> dur, dui;  // dU [idxu_max][3]
-  std::vector<double> db;        // dB [idxb_max][3]
+  std::vector<double> db;        // dB [nlin][3]
 };
 
-// compute_ui.jl:5-44, 131-175: Utot for atom i from its neighbor rows.
+// compute_ui.jl:5-44, 131-175: Utot for atom i from its neighbor rows; with chem_flag one
+// Utot per element (the neighbor's element, add_uarraytot :155-175), wself on the diagonal of
+// the centre's element or, with wselfall_flag, of every element (zero_uarraytot :131-152).
 void compute_ui(const Snap& s, int64_t nn, const double* r, const int32_t* jn, int32_t si, const int32_t* species,
                 AtomWork& w) {
   int U = s.idxu_max;
-  w.utr.assign(U, 0.0);
-  w.uti.assign(U, 0.0);
-  for (int j = 0; j <= s.J; j++) {  // zero_uarraytot: wself on the diagonal
-    int jju = s.idxu_block[j];
-    for (int mb = 0; mb <= j; mb++)
-      for (int ma = 0; ma <= j; ma++) {
-        if (ma == mb) w.utr[jju] = s.wself;
-        jju++;
-      }
+  w.utr.assign((size_t)s.nelem * U, 0.0);
+  w.uti.assign((size_t)s.nelem * U, 0.0);
+  const int ielem = s.chem_flag ? si : 0;
+  for (int e = 0; e < s.nelem; e++) {
+    if (!(e == ielem || s.wselfall_flag)) continue;
+    for (int j = 0; j <= s.J; j++) {  // zero_uarraytot: wself on the diagonal
+      int jju = s.idxu_block[j];
+      for (int mb = 0; mb <= j; mb++)
+        for (int ma = 0; ma <= j; ma++) {
+          if (ma == mb) w.utr[(size_t)e * U + jju] = s.wself;
+          jju++;
+        }
+    }
   }
   w.ulr.assign((size_t)nn * U, 0.0);
   w.uli.assign((size_t)nn * U, 0.0);
@@ -655,84 +667,123 @@ void compute_ui(const Snap& s, int64_t nn, const double* r, const int32_t* jn, i
     double* ui = &w.uli[(size_t)k * U];
     compute_uarray(s, x, y, z, z0, rr, ur, ui);
     double sfac = compute_sfac(s, rr, rcutij) * wj;
+    const size_t eo = (size_t)(s.chem_flag ? sj : 0) * U;
     for (int q = 0; q < U; q++) {
-      w.utr[q] += sfac * ur[q];
-      w.uti[q] += sfac * ui[q];
+      w.utr[eo + q] += sfac * ur[q];
+      w.uti[eo + q] += sfac * ui[q];
     }
   }
 }
 
-// compute_z.jl:1-62 (chem_flag off: idouble = 0)
+// compute_z.jl:1-62: Z of every ordered element pair (elem1, elem2), idouble = elem1*nelem
+// + elem2, at Z[idouble*idxz_max + jjz].  literal_chem_z reproduces the reference's indexing
+// (:19-20 zero the slot idouble*idxz_max + jjz, :44-47 accumulate into and divide slot jjz):
+// every pair then sums into the first block, dividing the running sum by j+1 after each pair
+// when bnorm_flag is set, and the other blocks stay zero.
 void compute_zi(const Snap& s, AtomWork& w) {
-  w.zr.assign(s.idxz_max, 0.0);
-  w.zi.assign(s.idxz_max, 0.0);
-  for (int jjz = 0; jjz < s.idxz_max; jjz++) {
-    const ZIdx& q = s.idxz[jjz];
-    const double* cgblock = &s.cglist[s.idxcg_block[s.blk(q.j1, q.j2, q.j)]];
-    double zr = 0.0, zi = 0.0;
-    int jju1 = s.idxu_block[q.j1] + (q.j1 + 1) * q.mb1min;
-    int jju2 = s.idxu_block[q.j2] + (q.j2 + 1) * q.mb2max;
-    int icgb = q.mb1min * (q.j2 + 1) + q.mb2max;
-    for (int ib = 0; ib < q.nb; ib++) {
-      double sr = 0.0, si = 0.0;
-      int ma1 = q.ma1min, ma2 = q.ma2max;
-      int icga = q.ma1min * (q.j2 + 1) + q.ma2max;
-      for (int ia = 0; ia < q.na; ia++) {
-        double u1r = w.utr[jju1 + ma1], u1i = w.uti[jju1 + ma1];
-        double u2r = w.utr[jju2 + ma2], u2i = w.uti[jju2 + ma2];
-        sr += cgblock[icga] * (u1r * u2r - u1i * u2i);
-        si += cgblock[icga] * (u1r * u2i + u1i * u2r);
-        ma1++;
-        ma2--;
-        icga += q.j2;
+  const int M = s.idxz_max, U = s.idxu_max;
+  w.zr.assign((size_t)s.nelem * s.nelem * M, 0.0);
+  w.zi.assign((size_t)s.nelem * s.nelem * M, 0.0);
+  int idouble = 0;
+  for (int e1 = 0; e1 < s.nelem; e1++)
+    for (int e2 = 0; e2 < s.nelem; e2++) {
+      const double* u1r = &w.utr[(size_t)e1 * U];
+      const double* u1i = &w.uti[(size_t)e1 * U];
+      const double* u2r = &w.utr[(size_t)e2 * U];
+      const double* u2i = &w.uti[(size_t)e2 * U];
+      for (int jjz = 0; jjz < M; jjz++) {
+        const ZIdx& q = s.idxz[jjz];
+        const double* cgblock = &s.cglist[s.idxcg_block[s.blk(q.j1, q.j2, q.j)]];
+        const size_t zslot = s.literal_chem_z ? (size_t)jjz : (size_t)idouble * M + jjz;
+        w.zr[(size_t)idouble * M + jjz] = 0.0;
+        w.zi[(size_t)idouble * M + jjz] = 0.0;
+        double zr = w.zr[zslot], zi = w.zi[zslot];
+        int jju1 = s.idxu_block[q.j1] + (q.j1 + 1) * q.mb1min;
+        int jju2 = s.idxu_block[q.j2] + (q.j2 + 1) * q.mb2max;
+        int icgb = q.mb1min * (q.j2 + 1) + q.mb2max;
+        for (int ib = 0; ib < q.nb; ib++) {
+          double sr = 0.0, si = 0.0;
+          int ma1 = q.ma1min, ma2 = q.ma2max;
+          int icga = q.ma1min * (q.j2 + 1) + q.ma2max;
+          for (int ia = 0; ia < q.na; ia++) {
+            double a1r = u1r[jju1 + ma1], a1i = u1i[jju1 + ma1];
+            double a2r = u2r[jju2 + ma2], a2i = u2i[jju2 + ma2];
+            sr += cgblock[icga] * (a1r * a2r - a1i * a2i);
+            si += cgblock[icga] * (a1r * a2i + a1i * a2r);
+            ma1++;
+            ma2--;
+            icga += q.j2;
+          }
+          zr += cgblock[icgb] * sr;
+          zi += cgblock[icgb] * si;
+          jju1 += q.j1 + 1;
+          jju2 -= q.j2 + 1;
+          icgb += q.j2;
+        }
+        if (s.bnorm_flag) {
+          zr /= (q.j + 1);
+          zi /= (q.j + 1);
+        }
+        w.zr[zslot] = zr;
+        w.zi[zslot] = zi;
       }
-      zr += cgblock[icgb] * sr;
-      zi += cgblock[icgb] * si;
-      jju1 += q.j1 + 1;
-      jju2 -= q.j2 + 1;
-      icgb += q.j2;
+      idouble++;
     }
-    if (s.bnorm_flag) {
-      zr /= (q.j + 1);
-      zi /= (q.j + 1);
-    }
-    w.zr[jjz] = zr;
-    w.zi[jjz] = zi;
-  }
 }
 
-// compute_b.jl:67-157 (chem_flag off)
-void compute_bi(const Snap& s, AtomWork& w) {
-  w.b.assign(s.idxb_max, 0.0);
-  for (int jjb = 0; jjb < s.idxb_max; jjb++) {
-    int j1 = s.idxb[3 * jjb], j2 = s.idxb[3 * jjb + 1], j = s.idxb[3 * jjb + 2];
-    int jjz = s.idxz_block[s.blk(j1, j2, j)];
-    int jju = s.idxu_block[j];
-    double sumzu = 0.0;
-    for (int mb = 0; 2 * mb < j; mb++)
-      for (int ma = 0; ma <= j; ma++) {
-        sumzu += w.utr[jju] * w.zr[jjz] + w.uti[jju] * w.zi[jjz];
-        jjz++;
-        jju++;
+// compute_b.jl:5-95: B of every element triple (elem1, elem2, elem3), itriple =
+// (elem1*nelem + elem2)*nelem + elem3, at B[itriple*idxb_max + jjb]: Utot of elem3 against Z of
+// (elem1, elem2).  bzero: the centre element's triple (ielem, ielem, ielem), or every triple with
+// wselfall_flag, as LAMMPS' compute_bi(ielem).  (The reference wraps the whole computation in a
+// loop over ielem that recomputes B each time, so only the last element's triple would keep its
+// shift; the per-centre shift is taken here.)
+void compute_bi(const Snap& s, AtomWork& w, int32_t si) {
+  const int K = s.idxb_max, U = s.idxu_max, M = s.idxz_max, n = s.nelem;
+  w.b.assign((size_t)s.nlin(), 0.0);
+  int itriple = 0;
+  for (int e1 = 0; e1 < n; e1++)
+    for (int e2 = 0; e2 < n; e2++) {
+      const size_t zo = (size_t)(e1 * n + e2) * M;
+      for (int e3 = 0; e3 < n; e3++) {
+        const double* ur = &w.utr[(size_t)e3 * U];
+        const double* ui = &w.uti[(size_t)e3 * U];
+        for (int jjb = 0; jjb < K; jjb++) {
+          int j1 = s.idxb[3 * jjb], j2 = s.idxb[3 * jjb + 1], j = s.idxb[3 * jjb + 2];
+          size_t jjz = zo + s.idxz_block[s.blk(j1, j2, j)];
+          int jju = s.idxu_block[j];
+          double sumzu = 0.0;
+          for (int mb = 0; 2 * mb < j; mb++)
+            for (int ma = 0; ma <= j; ma++) {
+              sumzu += ur[jju] * w.zr[jjz] + ui[jju] * w.zi[jjz];
+              jjz++;
+              jju++;
+            }
+          if (j % 2 == 0) {
+            int mb = j / 2;
+            for (int ma = 0; ma < mb; ma++) {
+              sumzu += ur[jju] * w.zr[jjz] + ui[jju] * w.zi[jjz];
+              jjz++;
+              jju++;
+            }
+            sumzu += 0.5 * (ur[jju] * w.zr[jjz] + ui[jju] * w.zi[jjz]);
+          }
+          w.b[(size_t)itriple * K + jjb] = 2.0 * sumzu;
+        }
+        itriple++;
       }
-    if (j % 2 == 0) {
-      int mb = j / 2;
-      for (int ma = 0; ma < mb; ma++) {
-        sumzu += w.utr[jju] * w.zr[jjz] + w.uti[jju] * w.zi[jjz];
-        jjz++;
-        jju++;
-      }
-      sumzu += 0.5 * (w.utr[jju] * w.zr[jjz] + w.uti[jju] * w.zi[jjz]);
     }
-    w.b[jjb] = 2.0 * sumzu;
+  if (s.bzero_flag) {
+    const int ielem = s.chem_flag ? si : 0;
+    for (int t = 0; t < n * n * n; t++) {
+      if (!s.wselfall_flag && t != (ielem * n + ielem) * n + ielem) continue;
+      for (int jjb = 0; jjb < K; jjb++) w.b[(size_t)t * K + jjb] -= s.bzero[s.idxb[3 * jjb + 2]];
+    }
   }
-  if (s.bzero_flag)
-    for (int jjb = 0; jjb < s.idxb_max; jjb++) w.b[jjb] -= s.bzero[s.idxb[3 * jjb + 2]];
 }
 
 // Half-plane sum of Re(conj(du[:,k]) * z) over level j starting at Z index jjz
 // (the inner loops of compute_b.jl:225-266).
-inline void sum_half(const Snap& s, const AtomWork& w, int j, int jjz, double* out3) {
+inline void sum_half(const Snap& s, const AtomWork& w, int j, size_t jjz, double* out3) {
   int jju = s.idxu_block[j];
   double acc[3] = {0.0, 0.0, 0.0};
   for (int mb = 0; 2 * mb < j; mb++)
@@ -753,20 +804,71 @@ inline void sum_half(const Snap& s, const AtomWork& w, int j, int jjz, double* o
   for (int k = 0; k < 3; k++) out3[k] = acc[k];
 }
 
-// compute_b.jl:166-404 compute_dbidrj (chem_flag off: every itriple is 0)
-void compute_dbidrj(const Snap& s, AtomWork& w) {
-  w.db.assign((size_t)s.idxb_max * 3, 0.0);
-  for (int jjb = 0; jjb < s.idxb_max; jjb++) {
+// compute_b.jl:104-342 compute_dbidrj for a neighbor of element jelem (elem3 = jelem with
+// chem_flag, else 0): for every element pair, the three terms of each component land in their
+// own triples (:196, :250, :305).
+void compute_dbidrj(const Snap& s, AtomWork& w, int32_t jelem) {
+  const int K = s.idxb_max, M = s.idxz_max, n = s.nelem;
+  const int e3 = s.chem_flag ? jelem : 0;
+  w.db.assign((size_t)s.nlin() * 3, 0.0);
+  for (int jjb = 0; jjb < K; jjb++) {
     int j1 = s.idxb[3 * jjb], j2 = s.idxb[3 * jjb + 1], j = s.idxb[3 * jjb + 2];
-    double t[3];
-    sum_half(s, w, j, s.idxz_block[s.blk(j1, j2, j)], t);
-    for (int k = 0; k < 3; k++) w.db[3 * jjb + k] = 2.0 * t[k];
-    double j1fac = (j + 1) / (j1 + 1.0);
-    sum_half(s, w, j1, s.idxz_block[s.blk(j, j2, j1)], t);
-    for (int k = 0; k < 3; k++) w.db[3 * jjb + k] += s.bnorm_flag ? 2.0 * t[k] : 2.0 * t[k] * j1fac;
-    double j2fac = (j + 1) / (j2 + 1.0);
-    sum_half(s, w, j2, s.idxz_block[s.blk(j, j1, j2)], t);
-    for (int k = 0; k < 3; k++) w.db[3 * jjb + k] += s.bnorm_flag ? 2.0 * t[k] : 2.0 * t[k] * j2fac;
+    for (int e1 = 0; e1 < n; e1++)
+      for (int e2 = 0; e2 < n; e2++) {
+        double t[3];
+        size_t it = (size_t)((e1 * n + e2) * n + e3);
+        sum_half(s, w, j, (size_t)(e1 * n + e2) * M + s.idxz_block[s.blk(j1, j2, j)], t);
+        for (int k = 0; k < 3; k++) w.db[3 * (it * K + jjb) + k] = 2.0 * t[k];
+        double j1fac = (j + 1) / (j1 + 1.0);
+        it = (size_t)((e3 * n + e2) * n + e1);
+        sum_half(s, w, j1, (size_t)(e1 * n + e2) * M + s.idxz_block[s.blk(j, j2, j1)], t);
+        for (int k = 0; k < 3; k++) w.db[3 * (it * K + jjb) + k] += s.bnorm_flag ? 2.0 * t[k] : 2.0 * t[k] * j1fac;
+        double j2fac = (j + 1) / (j2 + 1.0);
+        it = (size_t)((e1 * n + e3) * n + e2);
+        sum_half(s, w, j2, (size_t)(e2 * n + e1) * M + s.idxz_block[s.blk(j, j1, j2)], t);
+        for (int k = 0; k < 3; k++) w.db[3 * (it * K + jjb) + k] += s.bnorm_flag ? 2.0 * t[k] : 2.0 * t[k] * j2fac;
+      }
+  }
+}
+
+// Quadratic SNAP (the quadratic option of LAMMPS_SNAP/snap.jl:45-47, LAMMPS' layout): the
+// linear components b [nlin] are followed by 0.5 b_k b_k and b_k b_l (l > k), k outer.
+void quad_extend(const Snap& s, const double* b, double* out) {
+  const int K = s.nlin();
+  std::memcpy(out, b, sizeof(double) * K);
+  size_t q = K;
+  for (int k = 0; k < K; k++) {
+    out[q++] = 0.5 * b[k] * b[k];
+    for (int l = k + 1; l < K; l++) out[q++] = b[k] * b[l];
+  }
+}
+// Their derivative for one pair: d(0.5 b_k^2) = b_k db_k, d(b_k b_l) = b_l db_k + b_k db_l.
+void quad_extend_d(const Snap& s, const double* b, const double* db, double* out) {
+  const int K = s.nlin();
+  std::memcpy(out, db, sizeof(double) * 3 * K);
+  size_t q = K;
+  for (int k = 0; k < K; k++) {
+    for (int c = 0; c < 3; c++) out[3 * q + c] = b[k] * db[3 * k + c];
+    q++;
+    for (int l = k + 1; l < K; l++) {
+      for (int c = 0; c < 3; c++) out[3 * q + c] = b[l] * db[3 * k + c] + b[k] * db[3 * l + c];
+      q++;
+    }
+  }
+}
+// The linear coefficients that give the same forces: beta_eff[k] = beta[k] + sum_l a_kl b_l with
+// a the symmetric matrix of the quadratic coefficients (a_kk from 0.5 b_k^2).
+void quad_beta_eff(const Snap& s, const double* beta, const double* b, double* out) {
+  const int K = s.nlin();
+  for (int k = 0; k < K; k++) out[k] = beta[k];
+  size_t q = K;
+  for (int k = 0; k < K; k++) {
+    out[k] += beta[q++] * b[k];
+    for (int l = k + 1; l < K; l++) {
+      out[k] += beta[q] * b[l];
+      out[l] += beta[q] * b[k];
+      q++;
+    }
   }
 }
 
@@ -922,7 +1024,8 @@ int orc_pair_eval(int64_t n, const double* pos, const int32_t* species, const do
 // ----- SNAP -------------------------------------------------------------------------
 void* orc_snap_create(int32_t twojmax, int32_t nsp, double rcutfac, double rmin0, double rfac0, const double* radii,
                       const double* weight, int32_t bzero_flag, int32_t bnorm_flag, int32_t switch_flag,
-                      int32_t literal_sqrt) {
+                      int32_t literal_sqrt, int32_t chem_flag, int32_t wselfall_flag, int32_t literal_chem_z,
+                      int32_t quadratic_flag) {
   if (twojmax < 0 || twojmax > 14 || nsp < 1 || nsp > 64) return nullptr;
   Snap* s = new Snap();
   s->J = twojmax;
@@ -936,9 +1039,17 @@ void* orc_snap_create(int32_t twojmax, int32_t nsp, double rcutfac, double rmin0
   s->bnorm_flag = bnorm_flag;
   s->switch_flag = switch_flag;
   s->literal_sqrt = literal_sqrt;
+  s->chem_flag = chem_flag;
+  s->wselfall_flag = wselfall_flag;
+  s->literal_chem_z = literal_chem_z;
+  s->quadratic_flag = quadratic_flag;
+  s->nelem = chem_flag ? nsp : 1;
   init_tables(*s);
   return s;
 }
+
+// Components per species block: get_num_snap_coeffs (utl.jl:8-25), with the quadratic products.
+int32_t orc_snap_ncoef(void* h) { return static_cast<Snap*>(h)->ncoef(); }
 
 void orc_snap_destroy(void* h) { delete static_cast<Snap*>(h); }
 
@@ -984,10 +1095,11 @@ int orc_snap_descriptors(void* h, int64_t n, const double* pos, const int32_t* s
   if (st) return st;
   PairList pl;
   snap_list(n, pos, L, species, s.nsp, s.radii.data(), s.rcutfac, s.literal_sqrt, pl);
-  int K = s.idxb_max, Kn = K * s.nsp;
+  int K = s.ncoef(), Kn = K * s.nsp;
   if (dB) std::memset(dB, 0, sizeof(double) * (size_t)n * 3 * Kn);
   if (W) std::memset(W, 0, sizeof(double) * 6 * Kn);
   AtomWork w;
+  std::vector<double> bx(K), dbx(3 * (size_t)K);
   for (int64_t i = 0; i < n; i++) {
     int64_t nn = pl.off[i + 1] - pl.off[i];
     const double* r = &pl.r[3 * pl.off[i]];
@@ -1000,8 +1112,12 @@ int orc_snap_descriptors(void* h, int64_t n, const double* pos, const int32_t* s
         utot_out[((size_t)i * s.idxu_max + q) * 2 + 1] = w.uti[q];
       }
     compute_zi(s, w);
-    compute_bi(s, w);
-    if (B) std::memcpy(B + (size_t)i * K, w.b.data(), sizeof(double) * K);
+    compute_bi(s, w, si);
+    if (s.quadratic_flag)
+      quad_extend(s, w.b.data(), bx.data());
+    else
+      bx = w.b;
+    if (B) std::memcpy(B + (size_t)i * K, bx.data(), sizeof(double) * K);
     if (!dB && !W) continue;
     int ioff = K * si;
     w.dur.assign((size_t)s.idxu_max * 3, 0.0);
@@ -1012,18 +1128,22 @@ int orc_snap_descriptors(void* h, int64_t n, const double* pos, const int32_t* s
       double rcut = (s.radii[si] + s.radii[sj]) * s.rcutfac;
       compute_duidrj(s, r + 3 * k, s.weight[sj], rcut, &w.ulr[(size_t)k * s.idxu_max],
                      &w.uli[(size_t)k * s.idxu_max], w.dur.data(), w.dui.data());
-      compute_dbidrj(s, w);
+      compute_dbidrj(s, w, sj);
+      if (s.quadratic_flag)
+        quad_extend_d(s, w.b.data(), w.db.data(), dbx.data());
+      else
+        dbx = w.db;
       if (dB)
         for (int q = 0; q < K; q++)
           for (int c = 0; c < 3; c++) {
-            dB[((size_t)i * Kn + ioff + q) * 3 + c] += w.db[3 * q + c];
-            dB[((size_t)jj * Kn + ioff + q) * 3 + c] -= w.db[3 * q + c];
+            dB[((size_t)i * Kn + ioff + q) * 3 + c] += dbx[3 * q + c];
+            dB[((size_t)jj * Kn + ioff + q) * 3 + c] -= dbx[3 * q + c];
           }
       if (W) {
         const double* xi = pos + 3 * i;
         const double* xj = pos + 3 * jj;
         for (int q = 0; q < K; q++) {
-          const double* d = &w.db[3 * q];
+          const double* d = &dbx[3 * q];
           double* wc = W + (size_t)(ioff + q) * 6;
           wc[0] += d[0] * xi[0] - d[0] * xj[0];
           wc[1] += d[1] * xi[1] - d[1] * xj[1];
@@ -1053,7 +1173,7 @@ int orc_snap_energy_forces(void* h, int64_t n, const double* pos, const int32_t*
   if (i1 > n) i1 = n;
   PairList pl;
   snap_list(n, pos, L, species, s.nsp, s.radii.data(), s.rcutfac, s.literal_sqrt, pl);
-  int K = s.idxb_max;
+  int K = s.ncoef(), KL = s.nlin();
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
   int nt = omp_get_max_threads();
@@ -1070,6 +1190,7 @@ int orc_snap_energy_forces(void* h, int64_t n, const double* pos, const int32_t*
     int tid = 0;
 #endif
     AtomWork w;
+    std::vector<double> bx(K), beff(KL);
 #pragma omp for schedule(dynamic, 4)
     for (int64_t i = i0; i < i1; i++) {
       int64_t nn = pl.off[i + 1] - pl.off[i];
@@ -1079,13 +1200,23 @@ int orc_snap_energy_forces(void* h, int64_t n, const double* pos, const int32_t*
       const double* bs = beta + (size_t)K * si;
       compute_ui(s, nn, r, jn, si, species, w);
       compute_zi(s, w);
-      compute_bi(s, w);
+      compute_bi(s, w, si);
+      if (s.quadratic_flag)
+        quad_extend(s, w.b.data(), bx.data());
+      else
+        bx = w.b;
       double ei = 0.0;
-      for (int q = 0; q < K; q++) ei += bs[q] * w.b[q];
+      for (int q = 0; q < K; q++) ei += bs[q] * bx[q];
       Eth[tid] += ei;
       if (Ei) Ei[i] = ei;
       if (!F && !W6) continue;
-      if (mode == 1) compute_yi(s, bs, w);
+      // forces need the linear coefficients only (quadratic: per-atom effective ones)
+      if (s.quadratic_flag)
+        quad_beta_eff(s, bs, w.b.data(), beff.data());
+      else
+        std::memcpy(beff.data(), bs, sizeof(double) * KL);
+      const bool adj = mode == 1 && !s.chem_flag;  // the Y restatement covers one element
+      if (adj) compute_yi(s, beff.data(), w);
       w.dur.assign((size_t)s.idxu_max * 3, 0.0);
       w.dui.assign((size_t)s.idxu_max * 3, 0.0);
       for (int64_t k = 0; k < nn; k++) {
@@ -1095,12 +1226,12 @@ int orc_snap_energy_forces(void* h, int64_t n, const double* pos, const int32_t*
         compute_duidrj(s, r + 3 * k, s.weight[sj], rcut, &w.ulr[(size_t)k * s.idxu_max],
                        &w.uli[(size_t)k * s.idxu_max], w.dur.data(), w.dui.data());
         double f[3] = {0.0, 0.0, 0.0};
-        if (mode == 1) {
+        if (adj) {
           compute_deidrj(s, w, f);
         } else {
-          compute_dbidrj(s, w);
-          for (int q = 0; q < K; q++)
-            for (int c = 0; c < 3; c++) f[c] += w.db[3 * q + c] * bs[q];
+          compute_dbidrj(s, w, sj);
+          for (int q = 0; q < KL; q++)
+            for (int c = 0; c < 3; c++) f[c] += w.db[3 * q + c] * beff[q];
         }
         if (F)
           for (int c = 0; c < 3; c++) {
@@ -1137,22 +1268,72 @@ int orc_snap_energy_forces(void* h, int64_t n, const double* pos, const int32_t*
 }
 
 // Vector-Jacobian product of (E, F) with respect to beta: gbeta[s][k] =
-// gE * sum_{i in s} B_i[k] + sum_k gF_k . dB_k[:, block s][k]; gbeta0 = gE.
+// gE * sum_{i in s} B_i[k] + sum_k gF_k . dB_k[:, block s][k]; gbeta0 = gE.  The force part is
+// sum over pairs (i, j) of (gF_i - gF_j) . dB_i/dr_ij in the block of s_i (the dB of
+// compute_all_descriptors gathered per atom, snap.jl:276-277), summed per OpenMP thread.
 int orc_snap_vjp_beta(void* h, int64_t n, const double* pos, const int32_t* species, const double* L, double gE,
                       const double* gF, double* gbeta, double* gbeta0) {
   Snap& s = *static_cast<Snap*>(h);
   int st = snap_check(s, n, pos, species, L);
   if (st) return st;
-  int K = s.idxb_max, Kn = K * s.nsp;
-  std::vector<double> B((size_t)n * K), dB((size_t)n * 3 * Kn);
-  orc_snap_descriptors(h, n, pos, species, L, B.data(), gF ? dB.data() : nullptr, nullptr, nullptr);
-  std::memset(gbeta, 0, sizeof(double) * Kn);
-  for (int64_t i = 0; i < n; i++)
-    for (int q = 0; q < K; q++) gbeta[K * species[i] + q] += gE * B[(size_t)i * K + q];
-  if (gF)
-    for (int64_t i = 0; i < n; i++)
-      for (int c = 0; c < Kn; c++)
-        for (int k = 0; k < 3; k++) gbeta[c] += gF[3 * i + k] * dB[((size_t)i * Kn + c) * 3 + k];
+  PairList pl;
+  snap_list(n, pos, L, species, s.nsp, s.radii.data(), s.rcutfac, s.literal_sqrt, pl);
+  const int K = s.ncoef(), Kn = K * s.nsp;
+#ifdef _OPENMP
+  int nt = omp_get_max_threads();
+#else
+  int nt = 1;
+#endif
+  std::vector<std::vector<double>> gth(nt, std::vector<double>(Kn, 0.0));
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    int tid = omp_get_thread_num();
+#else
+    int tid = 0;
+#endif
+    AtomWork w;
+    std::vector<double> bx(K), dbx(3 * (size_t)K);
+    double* g = gth[tid].data();
+#pragma omp for schedule(dynamic, 4)
+    for (int64_t i = 0; i < n; i++) {
+      int64_t nn = pl.off[i + 1] - pl.off[i];
+      const double* r = &pl.r[3 * pl.off[i]];
+      const int32_t* jn = &pl.j[pl.off[i]];
+      int32_t si = species[i];
+      compute_ui(s, nn, r, jn, si, species, w);
+      compute_zi(s, w);
+      compute_bi(s, w, si);
+      if (s.quadratic_flag)
+        quad_extend(s, w.b.data(), bx.data());
+      else
+        bx = w.b;
+      double* gs = g + (size_t)K * si;
+      for (int q = 0; q < K; q++) gs[q] += gE * bx[q];
+      if (!gF) continue;
+      w.dur.assign((size_t)s.idxu_max * 3, 0.0);
+      w.dui.assign((size_t)s.idxu_max * 3, 0.0);
+      for (int64_t k = 0; k < nn; k++) {
+        int32_t jj = jn[k];
+        int32_t sj = species[jj];
+        double rcut = (s.radii[si] + s.radii[sj]) * s.rcutfac;
+        compute_duidrj(s, r + 3 * k, s.weight[sj], rcut, &w.ulr[(size_t)k * s.idxu_max],
+                       &w.uli[(size_t)k * s.idxu_max], w.dur.data(), w.dui.data());
+        compute_dbidrj(s, w, sj);
+        if (s.quadratic_flag)
+          quad_extend_d(s, w.b.data(), w.db.data(), dbx.data());
+        else
+          dbx = w.db;
+        const double gv[3] = {gF[3 * i] - gF[3 * jj], gF[3 * i + 1] - gF[3 * jj + 1], gF[3 * i + 2] - gF[3 * jj + 2]};
+        for (int q = 0; q < K; q++) gs[q] += gv[0] * dbx[3 * q] + gv[1] * dbx[3 * q + 1] + gv[2] * dbx[3 * q + 2];
+      }
+    }
+  }
+  for (int c = 0; c < Kn; c++) {
+    double t = 0.0;
+    for (int q = 0; q < nt; q++) t += gth[q][c];
+    gbeta[c] = t;
+  }
   if (gbeta0) *gbeta0 = gE;
   return 0;
 }

@@ -51,7 +51,9 @@ def lib():
         _lib.orc_pair_eval.restype = C.c_int
         _lib.orc_pair_eval.argtypes = [i64, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
         _lib.orc_snap_create.restype = vp
-        _lib.orc_snap_create.argtypes = [i32, i32, d, d, d, vp, vp, i32, i32, i32, i32]
+        _lib.orc_snap_create.argtypes = [i32, i32, d, d, d, vp, vp, i32, i32, i32, i32, i32, i32, i32, i32]
+        _lib.orc_snap_ncoef.restype = i32
+        _lib.orc_snap_ncoef.argtypes = [vp]
         _lib.orc_snap_destroy.restype = None
         _lib.orc_snap_destroy.argtypes = [vp]
         _lib.orc_snap_sizes.restype = None
@@ -143,7 +145,8 @@ class Snap:
     """Oracle SNAP basis (prebuilt tables of prebuilt_arrays.jl:48-321)."""
 
     def __init__(self, twojmax, radii, weight, rcutfac, rmin0=0.0, rfac0=0.99363, bzero=False, bnorm=False,
-                 switch=False, literal_sqrt=False):
+                 switch=False, literal_sqrt=False, chem=False, wselfall=False, literal_chem_z=False,
+                 quadratic=False):
         self.radii = _f64(radii)
         self.weight = _f64(weight)
         self.nsp = len(self.radii)
@@ -151,13 +154,14 @@ class Snap:
         self.rcutfac = float(rcutfac)
         self.literal_sqrt = bool(literal_sqrt)
         self.h = lib().orc_snap_create(twojmax, self.nsp, rcutfac, rmin0, rfac0, _p(self.radii), _p(self.weight),
-                                       int(bzero), int(bnorm), int(switch), int(literal_sqrt))
+                                       int(bzero), int(bnorm), int(switch), int(literal_sqrt), int(chem),
+                                       int(wselfall), int(literal_chem_z), int(quadratic))
         if not self.h:
             raise ValueError("oracle rejected SNAP parameters")
         sz = np.zeros(4, np.int32)
         lib().orc_snap_sizes(self.h, _p(sz))
         self.idxu_max, self.idxz_max, self.idxb_max, self.idxcg_max = (int(x) for x in sz)
-        self.K = self.idxb_max
+        self.K = int(lib().orc_snap_ncoef(self.h))  # components per species block
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -1,6 +1,6 @@
 """Generates tests/golden/reference_fixtures.npz from the reference's own test files.
 
-    python tests/golden/make_golden.py [/path/to/InteratomicPotentials.jl]
+    python tests/golden/make_golden.py /path/to/InteratomicPotentials.jl
 
 The reference (cesmix-mit/InteratomicPotentials.jl) is Julia and cannot run here, so
 its golden vectors are read from its test sources as text:
@@ -16,7 +16,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py /path/to/InteratomicPotentials.jl")
+REF = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_fixtures.npz")
 
 NUM = r"-?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?"

@@ -167,3 +167,45 @@ def test_fitting_matrices(batch):
     b = beta.reshape(-1)
     assert rel_err(Ae @ b + 0.25, E) <= 1e-12
     assert rel_err(Af @ b, F.reshape(-1)) <= 1e-12
+
+
+def test_train_step_graph(batch):
+    """ipg_snap_batch_loss_grad_dev: E, F, the loss and dL/dbeta of one force-matching step;
+    with graph=1 the first call captures the whole step and later calls replay it with one graph
+    launch (new positions and beta read from the buffers), bitwise equal to eager steps and
+    equal to the host-pointer loss gradient and to the oracle."""
+    import torch
+    systems, snap, orc, beta = batch
+    rng = np.random.default_rng(9)
+    _, F0, _ = snap.batch_energy_forces(systems, beta + rng.normal(0, 1e-3, beta.shape), 0.0)
+    Fref_h = F0 + rng.normal(0, 0.01, F0.shape)
+    db = ipg.DeviceBatch(snap, systems)
+    Fref = torch.tensor(Fref_h, device=db.pos.device)
+    loss_e, g_e = db.train_step(beta, Fref, 0.2, graph=False)
+    loss_e, g_e = loss_e.item(), g_e.cpu().numpy().copy()
+    E_e, F_e = db.E.cpu().numpy().copy(), db.F.cpu().numpy().copy()
+    loss_h, g_h = snap.batch_loss_grad(systems, beta, Fref_h, 0.2)
+    assert abs(loss_e - loss_h) <= 1e-13 * loss_h and rel_err(g_e, g_h) <= 1e-13
+    off = np.concatenate([[0], np.cumsum([len(s) for s in systems])])
+    go = np.zeros_like(g_e)
+    for c, s in enumerate(systems):
+        eo, fo, _ = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.2)
+        assert abs(E_e[c] - eo) <= TOL * abs(eo)
+        gF = 2.0 * (fo - Fref_h[off[c]:off[c + 1]])
+        go += orc.vjp_beta(s.positions, snap.species_ids(s), s.L, 0.0, gF)[0]
+    assert rel_err(g_e, go) <= TOL
+    for call in range(3):
+        l0 = snap.ctx.launch_count()
+        loss, g = db.train_step(beta, Fref, 0.2, graph=True)
+        torch.cuda.synchronize()
+        if call > 0:  # k_ycoef through the library, the rest is one graph launch
+            assert snap.ctx.launch_count() - l0 <= 2
+        assert loss.item() == loss_e and np.array_equal(g.cpu().numpy(), g_e)
+        assert np.array_equal(db.E.cpu().numpy(), E_e) and np.array_equal(db.F.cpu().numpy(), F_e)
+    moved = _moved(systems, np.random.default_rng(10))
+    db.set_positions(np.concatenate([s.positions for s in moved]))
+    beta2 = 0.9 * beta
+    loss, g = db.train_step(beta2, Fref, 0.0, graph=True)
+    torch.cuda.synchronize()
+    loss_h2, g_h2 = snap.batch_loss_grad(moved, beta2, Fref_h, 0.0)
+    assert abs(loss.item() - loss_h2) <= 1e-13 * loss_h2 and rel_err(g.cpu().numpy(), g_h2) <= 1e-13

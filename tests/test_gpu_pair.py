@@ -156,3 +156,37 @@ def test_dev_entry_point_with_torch():
     e, f = ipg.energy_and_force(s, p)
     assert abs(E.item() - e) <= 1e-13 * abs(e)
     assert rel_err(F.cpu().numpy(), f) <= 1e-13
+
+
+@pytest.mark.parametrize("case", ["dense_cells", "mixed_boundaries", "two_cells_periodic", "open_cluster",
+                                  "empty_cells"])
+@pytest.mark.parametrize("full", ["0", "1"])
+def test_half_and_full_stencil_paths(case, full, monkeypatch):
+    """The half-stencil tiles (each pair once; every periodic axis with >= 3 cells) and the
+    full-stencil walk (IPG_PAIR_FULL=1, and the fallback for fewer cells) against the oracle:
+    cells of more than 32 atoms (several tiles per cell pair), open and periodic axes mixed,
+    2 cells on a periodic axis, one open cell, and a sparse gas with empty cells."""
+    monkeypatch.setenv("IPG_PAIR_FULL", full)
+    ctx = ipg.Context(0)
+    rng = np.random.default_rng(77)
+    if case == "dense_cells":  # ~74 atoms per cell
+        s = ipg.System(rng.uniform(0, 12, (2000, 3)), list(np.where(rng.random(2000) < 0.5, "Ar", "Xe")), [12.0] * 3)
+        p = ipg.LennardJones(0.01, 1.0, 4.0, ["Ar"]) + ipg.Morse(0.1, 1.0, 1.5, 3.5, ["Ar", "Xe"])
+    elif case == "mixed_boundaries":
+        s = ipg.System(rng.uniform(0, 30, (900, 3)), list(np.where(rng.random(900) < 0.5, "Ar", "Xe")),
+                       [30.0, 30.0, 30.0], (True, False, True))
+        p = ipg.LennardJones(0.01, 3.0, 6.0, ["Ar", "Xe"]) + ipg.ZBL(18, 54, W.EULER_E, 5.0, ["Ar", "Xe"])
+    elif case == "two_cells_periodic":
+        s = ipg.System(rng.uniform(0, 10, (300, 3)), ["Ar"] * 300, [10.0, 30.0, 30.0])
+        p = ipg.LennardJones(0.01, 2.0, 4.5, ["Ar"])
+    elif case == "open_cluster":
+        s = ipg.System(rng.normal(0, 3, (200, 3)), ["Ar"] * 200, [10.0] * 3, (False, False, False))
+        p = ipg.BornMayer(2.0, 0.5, 1.0, 0.8, 0.7, 50.0, ["Ar"])
+    else:
+        s = ipg.System(rng.uniform(0, 200, (300, 3)), ["Ar"] * 300, [200.0] * 3)
+        p = ipg.LennardJones(0.01, 3.0, 12.0, ["Ar"])
+    e, f, w = ipg.empirical.pair_eval(s, ipg.empirical.empirical_terms(p), ctx=ctx)
+    eo, fo, wo = oracle_eval(s, p)
+    assert abs(e - eo) <= TOL * max(abs(eo), 1e-300), (e, eo)
+    assert rel_err(f, fo) <= TOL
+    assert rel_err(w, wo) <= TOL

@@ -197,10 +197,17 @@ def test_species_out_of_range_rejected():
     assert st == -7
 
 
-def test_chem_flag_unsupported():
-    with pytest.raises(ipg.IPGError) as e:
-        ipg.SNAP(1, 4, ["A"], 1.0, 0.0, 0.99, [1.0], [1.0], chem_flag=True, bnorm_flag=True)
-    assert e.value.status == -8
+def test_chem_flag_requires_bnorm():
+    """snap.jl:10-13: chem_flag and bnorm_flag must be the same."""
+    with pytest.raises(ValueError):
+        ipg.SNAP(1, 4, ["A"], 1.0, 0.0, 0.99, [1.0], [1.0], chem_flag=True, bnorm_flag=False)
+    import ctypes as C
+    p = ipg._lib.SnapParams()
+    p.twojmax, p.nspecies, p.rcutfac, p.rfac0 = 4, 1, 1.0, 0.99
+    p.radii[0], p.weight[0] = 1.0, 1.0
+    p.chem_flag, p.bnorm_flag = 1, 0
+    h = C.c_void_p()
+    assert ipg._lib.lib().ipg_snap_create(ipg.default_context().handle, C.byref(p), C.byref(h)) == -1
 
 
 def test_lbasis_potential_api():
@@ -415,3 +422,62 @@ def test_register_chain_paths_edge_cases(case):
     gb, _ = snap.vjp_beta(s, 0.4, gF)
     go, _ = orc.vjp_beta(s.positions, sp, s.L, 0.4, gF)
     assert rel_err(gb, go) <= TOL
+
+
+def test_verlet_skin_reuse_checks_inputs():
+    """With a skin set, a device-pointer call that would reuse the list still reports a
+    non-finite position (IPG_ERR_NONFINITE) and an out-of-range species id (IPG_ERR_SPECIES),
+    as a fresh build does, and a call that keeps the positions but changes species rebuilds
+    the list (its enlarged cutoffs depend on the species pair) and equals a fresh evaluation."""
+    import ctypes as C
+    import torch
+    system, prm, beta = W.snap_j8(cells=5)
+    fresh, _ = make(prm, switch_flag=True)
+    md, _ = make(prm, switch_flag=True)
+    md.set_skin(0.4)
+    n = len(system)
+    bb = md.beta_blocks(beta)
+    L = system.L
+    vp = C.c_void_p
+    E = torch.zeros(1, dtype=torch.float64, device="cuda")
+    F = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    Wv = torch.zeros(6, dtype=torch.float64, device="cuda")
+
+    def dev_call(pos, sp):
+        p = torch.tensor(pos, dtype=torch.float64, device="cuda")
+        q = torch.tensor(sp, dtype=torch.int32, device="cuda")
+        st = ipg._lib.lib().ipg_snap_energy_forces_dev(md.handle, n, vp(p.data_ptr()), vp(q.data_ptr()),
+                                                       L.ctypes.data_as(vp), bb.ctypes.data_as(vp), 0.0, 1,
+                                                       vp(E.data_ptr()), vp(F.data_ptr()), vp(Wv.data_ptr()))
+        torch.cuda.synchronize()
+        return st, E.item(), F.cpu().numpy()
+
+    md.ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        sp0 = md.species_ids(system)
+        assert dev_call(system.positions, sp0)[0] == 0
+        assert dev_call(system.positions, sp0)[0] == 0
+        assert md.skin_stats() == (1, 1)
+        bad = system.positions.copy()
+        bad[7, 1] = np.nan
+        assert dev_call(bad, sp0)[0] == -6
+        E0, F0, _ = fresh.energy_forces(system, beta)
+        st, E1, F1 = dev_call(system.positions, sp0)
+        assert st == 0 and abs(E1 - E0) <= 1e-12 * abs(E0) and rel_err(F1, F0) <= 1e-12
+        # same positions, species swapped on a tenth of the atoms
+        sym = list(system.symbols)
+        for k in range(0, len(sym), 10):
+            sym[k] = "B" if sym[k] == "A" else "A"
+        s2 = ipg.System(system.positions, sym, system.box, system.periodic)
+        sp2 = md.species_ids(s2)
+        b0 = md.skin_stats()[0]
+        E0, F0, _ = fresh.energy_forces(s2, beta)
+        st, E1, F1 = dev_call(system.positions, sp2)
+        assert st == 0 and md.skin_stats()[0] == b0 + 1
+        assert abs(E1 - E0) <= 1e-12 * abs(E0) and rel_err(F1, F0) <= 1e-12
+        assert dev_call(system.positions, sp2)[0] == 0  # reuse again
+        sp3 = sp2.copy()
+        sp3[3] = 5
+        assert dev_call(system.positions, sp3)[0] == -7
+    finally:
+        md.ctx.set_stream(None)

@@ -126,3 +126,108 @@ def test_snap_literal_radius_finds_no_neighbors():
     assert len(j) == 0
     off, j, r = oracle.nlist_snap(s.positions, s.L, sp, prm["radii"], prm["rcutfac"], literal_sqrt=False)
     assert 20 < np.diff(off).mean() < 30
+
+
+# ---- chem_flag and quadratic SNAP (oracle known answers; no reference values exist) ------
+def _cluster(seed, n=24, nsp=2):
+    rng = np.random.default_rng(seed)
+    pos = rng.normal(0, 1.6, (n, 3))
+    sp = rng.integers(0, nsp, n).astype(np.int32)
+    return pos, sp
+
+
+@pytest.mark.parametrize("bzero", [False, True])
+def test_chem_components_sum_to_single_element_descriptors(bzero):
+    """With chem_flag the element-resolved Utot of an atom sum to the single-element Utot (wself
+    once, on the centre's element), Z is bilinear and B trilinear in them, so B and dB summed
+    over all element triples equal the single-element B and dB with the same bnorm (and the
+    bzero shift, taken once on the centre's triple)."""
+    J = 6
+    pos, sp = _cluster(31)
+    L = np.full(3, np.inf)
+    kw = dict(rmin0=0.0, rfac0=0.99363, switch=True, bzero=bzero, bnorm=True)
+    one = oracle.Snap(J, [0.5, 0.45], [1.0, 0.6], 2.2, **kw)
+    chem = oracle.Snap(J, [0.5, 0.45], [1.0, 0.6], 2.2, chem=True, **kw)
+    K = one.K
+    assert chem.K == 8 * K
+    B1, dB1, W1 = one.descriptors(pos, sp, L)
+    Bc, dBc, Wc = chem.descriptors(pos, sp, L)
+    Bsum = Bc.reshape(len(pos), 8, K).sum(axis=1)
+    assert np.abs(Bsum - B1).max() <= 1e-12 * np.abs(B1).max()
+    # dB [n][K*nsp][3]: the species blocks keep their order, the triples sum inside each block
+    dsum = dBc.reshape(len(pos), 2, 8, K, 3).sum(axis=2).reshape(len(pos), 2 * K, 3)
+    assert np.abs(dsum - dB1).max() <= 1e-12 * np.abs(dB1).max()
+    wsum = Wc.reshape(2, 8, K, 6).sum(axis=1).reshape(2 * K, 6)
+    assert np.abs(wsum - W1).max() <= 1e-12 * np.abs(W1).max()
+
+
+def test_chem_single_species_equals_plain_bnorm():
+    """One species: the chem_flag descriptors are the single-element ones."""
+    pos, _ = _cluster(32)
+    sp = np.zeros(len(pos), np.int32)
+    L = np.full(3, np.inf)
+    a = oracle.Snap(8, [0.5], [1.0], 2.0, switch=True, bnorm=True)
+    b = oracle.Snap(8, [0.5], [1.0], 2.0, switch=True, bnorm=True, chem=True)
+    Ba, dBa, _ = a.descriptors(pos, sp, L)
+    Bb, dBb, _ = b.descriptors(pos, sp, L)
+    assert np.array_equal(Ba, Bb) and np.array_equal(dBa, dBb)
+
+
+def test_chem_literal_z_index():
+    """compute_z.jl:19-20,44-47 taken literally: every element pair sums into the first Z block
+    (the running sum divided by j+1 after each pair with bnorm) and the other blocks stay zero,
+    so B of every triple whose element pair is not the first vanishes."""
+    pos, sp = _cluster(33)
+    L = np.full(3, np.inf)
+    s = oracle.Snap(4, [0.5, 0.45], [1.0, 0.6], 2.2, switch=True, bnorm=True, chem=True, literal_chem_z=True)
+    K = s.idxb_max
+    B, _, _ = s.descriptors(pos, sp, L)
+    B = B.reshape(len(pos), 4, 2, K)  # (elem1 elem2), elem3, component
+    assert np.all(B[:, 1:] == 0.0)
+    assert np.abs(B[:, 0]).max() > 0.0
+
+
+def test_chem_forces_are_energy_gradient():
+    pos, sp = _cluster(34, n=16)
+    L = np.full(3, np.inf)
+    s = oracle.Snap(6, [0.5, 0.45], [1.0, 0.6], 2.2, switch=True, bnorm=True, chem=True, bzero=True)
+    beta = np.random.default_rng(3).normal(0, 1e-2, (2, s.K))
+    e, f, _ = s.energy_forces(pos, sp, L, beta, 0.1)
+    h = 1e-5
+    for a, c in [(0, 0), (7, 2), (11, 1)]:
+        pp = pos.copy(); pp[a, c] += h
+        pm = pos.copy(); pm[a, c] -= h
+        fd = -(s.energy_forces(pp, sp, L, beta)[0] - s.energy_forces(pm, sp, L, beta)[0]) / (2 * h)
+        assert abs(fd - f[a, c]) <= 1e-7 * np.abs(f).max()
+
+
+@pytest.mark.parametrize("chem", [False, True])
+def test_quadratic_descriptors_and_forces(chem):
+    """Quadratic SNAP: B is followed by 0.5 B_k^2 and B_k B_l (l > k); E = beta . B_ext, and the
+    forces (through the per-atom effective linear coefficients) are -dE/dx."""
+    pos, sp = _cluster(35, n=14)
+    L = np.full(3, np.inf)
+    kw = dict(switch=True, bnorm=chem, chem=chem)
+    lin = oracle.Snap(4, [0.5, 0.45], [1.0, 0.6], 2.2, **kw)
+    q = oracle.Snap(4, [0.5, 0.45], [1.0, 0.6], 2.2, quadratic=True, **kw)
+    K = lin.K
+    assert q.K == K + K * (K + 1) // 2
+    Bl, dBl, _ = lin.descriptors(pos, sp, L)
+    Bq, dBq, _ = q.descriptors(pos, sp, L)
+    assert np.array_equal(Bq[:, :K], Bl)
+    iu = np.triu_indices(K)
+    outer = Bl[:, :, None] * Bl[:, None, :]
+    outer[:, np.arange(K), np.arange(K)] *= 0.5
+    assert np.abs(Bq[:, K:] - outer[:, iu[0], iu[1]]).max() <= 1e-14 * np.abs(Bq).max()
+    beta = np.random.default_rng(4).normal(0, 1e-2, (2, q.K))
+    e, f, _ = q.energy_forces(pos, sp, L, beta, 0.0)
+    assert abs(e - np.einsum("ik,ik->", Bq, beta[sp])) <= 1e-12 * abs(e)
+    # compute_all_descriptors' dB is -d(sum B)/dx per centre-species block, so F = dB . beta
+    fd_b = np.einsum("ikc,k->ic", dBq[:, :q.K], beta[0]) + np.einsum("ikc,k->ic", dBq[:, q.K:], beta[1])
+    assert np.abs(f - fd_b).max() <= 1e-12 * np.abs(f).max()
+    h = 1e-5
+    for a, c in [(0, 0), (9, 2)]:
+        pp = pos.copy(); pp[a, c] += h
+        pm = pos.copy(); pm[a, c] -= h
+        fd = -(q.energy_forces(pp, sp, L, beta)[0] - q.energy_forces(pm, sp, L, beta)[0]) / (2 * h)
+        assert abs(fd - f[a, c]) <= 1e-7 * np.abs(f).max()
