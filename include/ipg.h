@@ -47,7 +47,7 @@ extern "C" {
 #define IPG_ERR_CUDA (-2)         /* CUDA runtime error                                  */
 #define IPG_ERR_NOMEM (-3)        /* device allocation failed                            */
 #define IPG_ERR_CAPACITY (-4)     /* a device-side capacity was exceeded                 */
-#define IPG_ERR_TIMEOUT (-5)      /* a bounded device wait ran out                       */
+                                  /* (-5 is not used: no kernel waits on another)         */
 #define IPG_ERR_NONFINITE (-6)    /* NaN or Inf in positions                             */
 #define IPG_ERR_SPECIES (-7)      /* species id out of range                             */
 #define IPG_ERR_UNSUPPORTED (-8)  /* valid in the reference but not built here           */
@@ -64,8 +64,6 @@ IPG_API int ipg_create(int device, ipg_ctx** out);
 IPG_API int ipg_destroy(ipg_ctx* ctx);
 /* Message of the last error on ctx ("" if none).  Valid until the next call on ctx. */
 IPG_API const char* ipg_last_error(const ipg_ctx* ctx);
-/* Upper bound, in milliseconds, for every bounded device-side wait (default 2000). */
-IPG_API int ipg_set_timeout_ms(ipg_ctx* ctx, uint32_t ms);
 /* Runs subsequent *_dev calls on `stream` (a cudaStream_t, or NULL for the context's own). */
 IPG_API int ipg_set_stream(ipg_ctx* ctx, void* stream);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */

@@ -101,7 +101,6 @@ int ipg_status_check(ipg_ctx* ctx, const char* what) {
   CUDA_RET(ctx, cudaStreamSynchronize(ctx->stream));
   int st = *ctx->h_status;
   if (st == IPG_ERR_CAPACITY) return ipg_fail(ctx, st, "%s: device capacity exceeded", what);
-  if (st == IPG_ERR_TIMEOUT) return ipg_fail(ctx, st, "%s: bounded device wait timed out", what);
   if (st == IPG_ERR_NONFINITE) return ipg_fail(ctx, st, "%s: non-finite position", what);
   if (st == IPG_ERR_SPECIES) return ipg_fail(ctx, st, "%s: species id out of range", what);
   if (st != IPG_OK) return ipg_fail(ctx, st, "%s: device status %d", what, st);
@@ -378,12 +377,6 @@ int ipg_destroy(ipg_ctx* ctx) {
 }
 
 const char* ipg_last_error(const ipg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
-
-int ipg_set_timeout_ms(ipg_ctx* ctx, uint32_t ms) {
-  if (!ctx || ms == 0) return IPG_ERR_ARG;
-  ctx->timeout_ms = ms;
-  return IPG_OK;
-}
 
 int ipg_set_stream(ipg_ctx* ctx, void* stream) {
   if (!ctx) return IPG_ERR_ARG;

@@ -27,7 +27,6 @@ struct ipg_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
-  uint32_t timeout_ms = 2000;
   int64_t launches = 0;
   int* d_status = nullptr;  // device status word (IPG_OK or a negative code)
   int* h_status = nullptr;  // pinned mirror

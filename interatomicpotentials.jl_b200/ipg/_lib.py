@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libipg.so")
 
 IPG_OK = 0
 STATUS = {
-    -1: "IPG_ERR_ARG", -2: "IPG_ERR_CUDA", -3: "IPG_ERR_NOMEM", -4: "IPG_ERR_CAPACITY", -5: "IPG_ERR_TIMEOUT",
+    -1: "IPG_ERR_ARG", -2: "IPG_ERR_CUDA", -3: "IPG_ERR_NOMEM", -4: "IPG_ERR_CAPACITY",
     -6: "IPG_ERR_NONFINITE", -7: "IPG_ERR_SPECIES", -8: "IPG_ERR_UNSUPPORTED", -9: "IPG_ERR_NODEVICE",
 }
 
@@ -28,7 +28,7 @@ MAX_PAIR_TERMS = 16
 
 # Every symbol include/ipg.h declares.
 API_SYMBOLS = (
-    "ipg_create", "ipg_destroy", "ipg_last_error", "ipg_set_timeout_ms", "ipg_set_stream", "ipg_version",
+    "ipg_create", "ipg_destroy", "ipg_last_error", "ipg_set_stream", "ipg_version",
     "ipg_launch_count", "ipg_timing_enable", "ipg_timing_read", "ipg_neighbor_build", "ipg_neighbor_count", "ipg_nlist_size", "ipg_nlist_export", "ipg_nlist_free",
     "ipg_pair_eval", "ipg_pair_eval_dev", "ipg_pair_eval_noalloc", "ipg_snap_create", "ipg_snap_destroy", "ipg_snap_ncoeff",
     "ipg_snap_descriptors", "ipg_snap_energy_forces", "ipg_snap_energy_forces_dev", "ipg_snap_vjp_beta",
@@ -73,7 +73,6 @@ def lib():
         "ipg_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
         "ipg_destroy": (C.c_int, [vp]),
         "ipg_last_error": (C.c_char_p, [vp]),
-        "ipg_set_timeout_ms": (C.c_int, [vp, u32]),
         "ipg_set_stream": (C.c_int, [vp, vp]),
         "ipg_version": (C.c_int, []),
         "ipg_launch_count": (C.c_int, [vp, C.POINTER(i64)]),

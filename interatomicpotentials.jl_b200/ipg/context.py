@@ -27,9 +27,6 @@ class Context:
         """Runs *_dev calls on a CUDA stream given as an integer handle (e.g. torch's)."""
         self.check(lib().ipg_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 
-    def set_timeout_ms(self, ms: int):
-        self.check(lib().ipg_set_timeout_ms(self._h, int(ms)))
-
     def launch_count(self) -> int:
         v = C.c_int64()
         self.check(lib().ipg_launch_count(self._h, C.byref(v)))
