@@ -20,10 +20,10 @@ int ipg_fail(ipg_ctx* ctx, int code, const char* fmt, ...) {
 
 int ipg_cuda_check(ipg_ctx* ctx, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return IPG_OK;
-  if (e == cudaErrorMemoryAllocation) {
-    cudaGetLastError();
-    return ipg_fail(ctx, IPG_ERR_NOMEM, "%s: %s", what, cudaGetErrorString(e));
-  }
+  // clear the runtime's last-error state, so that a failed call (a launch configuration or an
+  // attribute the device refuses) is not reported again by the next launch's check
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation) return ipg_fail(ctx, IPG_ERR_NOMEM, "%s: %s", what, cudaGetErrorString(e));
   return ipg_fail(ctx, IPG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 

@@ -49,7 +49,7 @@ struct ipg_ctx {
   uint64_t scratch_gen = 0;
   bool walk_by_cell = true;  // neighbor walk: one warp per cell (false: one warp per atom)
   bool pair_full_stencil = false;  // pair potentials: full-stencil walk even where the half stencil applies
-  int pair_minb = 4;               // pair potentials: register bound of the half-stencil kernel (3, 4, 5)
+  int pair_minb = 3;               // pair potentials: register bound of the half-stencil kernel (3, 4, 5)
   // single-pass neighbor walk: per list prefix, the per-atom slot count of the padded
   // emission (from the largest count of the previous build; 0 = walk twice)
   std::map<std::string, int> walk_kcap;

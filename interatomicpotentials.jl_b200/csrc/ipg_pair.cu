@@ -90,13 +90,25 @@ struct HalfHit {
   int sp;  // species of the row atom (bits 0-7) and of the lane atom (bits 8-15)
 };
 
+// Per-warp staging of half_eval: a force per row and per column of the tile.
+struct HalfStage {
+  double row[32][3];
+  double col[32][3];
+};
+
 // Evaluates the first nh hits (one per lane) and hands each hit's force to its row owner
-// (fa += f) and its lane owner (ft -= f) in hit order.  E and W accumulate lane-wise.
+// (fa += f) and its column owner (ft -= f).  Rows: the hits of a row are contiguous (they are
+// appended in row order), so a segmented scan over the lanes (a fixed tree) leaves each row's
+// total at its last hit, which stages it for the row's owner lane.  Columns: a row's hits have
+// distinct columns, so the rows of the batch are handed over one after another (row order),
+// each hit staging its force for its column's owner lane.  E and W accumulate lane-wise.
 __device__ __forceinline__ void half_eval(const PairTerms& TT, const HalfHit* __restrict__ hb, int nh, int lane,
-                                          double* acc, double* fa, double* ft) {
+                                          HalfStage& st, double* acc, double* fa, double* ft) {
+  constexpr unsigned FULL = 0xffffffffu;
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  int at = -1;
-  if (lane < nh) {
+  int row = 64 + lane, col = 0;  // idle lanes: rows that match no hit
+  const bool act = lane < nh;
+  if (act) {
     const HalfHit h = hb[lane];
     const double R = sqrt(h.r0 * h.r0 + h.r1 * h.r1 + h.r2 * h.r2);
     double V, g;
@@ -112,23 +124,56 @@ __device__ __forceinline__ void half_eval(const PairTerms& TT, const HalfHit* __
     acc[4] += h.r2 * fy;
     acc[5] += h.r2 * fx;
     acc[6] += h.r1 * fx;
-    at = h.at;
+    row = h.at & 0xff;
+    col = (h.at >> 8) & 0xff;
   }
-  for (int q = 0; q < nh; q++) {
-    const double bx = __shfl_sync(0xffffffffu, fx, q);
-    const double by = __shfl_sync(0xffffffffu, fy, q);
-    const double bz = __shfl_sync(0xffffffffu, fz, q);
-    const int b = __shfl_sync(0xffffffffu, at, q);
-    if (lane == (b & 0xff)) {
-      fa[0] += bx;
-      fa[1] += by;
-      fa[2] += bz;
+  // rows: segmented inclusive scan over the lanes
+  double sx = fx, sy = fy, sz = fz;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double ox = __shfl_up_sync(FULL, sx, off), oy = __shfl_up_sync(FULL, sy, off),
+                 oz = __shfl_up_sync(FULL, sz, off);
+    const int orow = __shfl_up_sync(FULL, row, off);
+    if (lane >= off && orow == row) {
+      sx += ox;
+      sy += oy;
+      sz += oz;
     }
-    if (lane == ((b >> 8) & 0xff)) {
-      ft[0] -= bx;
-      ft[1] -= by;
-      ft[2] -= bz;
+  }
+  const int nrow = __shfl_down_sync(FULL, row, 1);
+  const bool last = act && (lane == nh - 1 || nrow != row);
+  if (last) {
+    st.row[row][0] = sx;
+    st.row[row][1] = sy;
+    st.row[row][2] = sz;
+  }
+  const unsigned rows = __reduce_or_sync(FULL, last ? 1u << row : 0u);
+  __syncwarp();
+  if ((rows >> lane) & 1u) {
+    fa[0] += st.row[lane][0];
+    fa[1] += st.row[lane][1];
+    fa[2] += st.row[lane][2];
+  }
+  // columns: one row of the batch at a time
+  unsigned pend = __ballot_sync(FULL, act);
+  while (pend) {
+    const int r = __shfl_sync(FULL, row, __ffs(pend) - 1);
+    const bool in = act && row == r;
+    const unsigned seg = __ballot_sync(FULL, in);
+    if (in) {
+      st.col[col][0] = fx;
+      st.col[col][1] = fy;
+      st.col[col][2] = fz;
     }
+    const unsigned cols = __reduce_or_sync(FULL, in ? 1u << col : 0u);
+    __syncwarp();
+    if ((cols >> lane) & 1u) {
+      ft[0] -= st.col[lane][0];
+      ft[1] -= st.col[lane][1];
+      ft[2] -= st.col[lane][2];
+    }
+    __syncwarp();
+    pend &= ~seg;
   }
 }
 
@@ -146,7 +191,8 @@ __device__ __forceinline__ void pbuf_put(double* __restrict__ P, int64_t n, int 
   }
 }
 
-// MINB: resident blocks per SM the register allocation is bounded for (4: 128 registers).
+// MINB: resident blocks per SM the register allocation is bounded for (3: 168 registers, the
+// default; 4: 128; 5: 96, with spills; 36.0 / 36.6 / 66 ms at 4.1 M atoms, five terms).
 template <int MINB>
 __global__ void __launch_bounds__(PAIR_T, MINB) k_pair_half(const __grid_constant__ PairTerms TT, int64_t n,
                                                          const ConfGrid* __restrict__ grid, int64_t ncells,
@@ -155,63 +201,72 @@ __global__ void __launch_bounds__(PAIR_T, MINB) k_pair_half(const __grid_constan
                                                          const double4* __restrict__ spos, double* __restrict__ P,
                                                          double* __restrict__ partial) {
   __shared__ HalfHit hits[PAIR_WARPS][64];
+  __shared__ HalfStage stage[PAIR_WARPS];
   __shared__ double red[PAIR_WARPS][7];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t item = (int64_t)blockIdx.x * PAIR_WARPS + w;
-  double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // E, W[6]
-  if (item < ncells * HALF_OFFSETS) {     // warp-uniform from here on
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // E, W[6] of every item this warp takes
+  const double L0 = grid[0].L[0], L1 = grid[0].L[1], L2 = grid[0].L[2];
+  // grid-stride over the items (a fixed assignment, so E and W sum in a fixed order); the
+  // block's warps meet at a barrier only once, at the end
+  const int64_t nitems = ncells * HALF_OFFSETS;
+  const int64_t wstride = (int64_t)gridDim.x * PAIR_WARPS;
+  for (int64_t item = (int64_t)blockIdx.x * PAIR_WARPS + w; item < nitems; item += wstride) {  // warp-uniform
     const ConfGrid& g = grid[0];
-    const int64_t A = item / HALF_OFFSETS;
-    const int k = (int)(item - A * HALF_OFFSETS);
-    const int cx = (int)(A % g.nc[0]), cy = (int)((A / g.nc[0]) % g.nc[1]), cz = (int)(A / ((int64_t)g.nc[0] * g.nc[1]));
+    // cells number below 2^31 (ipg_build_cells): 32-bit index arithmetic
+    const int A = (int)(item / HALF_OFFSETS);
+    const int k = (int)(item - (int64_t)A * HALF_OFFSETS);
+    const int nxy = g.nc[0] * g.nc[1];
+    const int cz = A / nxy, rem = A - cz * nxy;
+    const int cy = rem / g.nc[0], cx = rem - cy * g.nc[0];
     int dx, dy, dz;
     half_offset(k, dx, dy, dz);
-    const int tx = shift_axis(cx, dx, g.nc[0], !isinf(g.L[0]));
-    const int ty = shift_axis(cy, dy, g.nc[1], !isinf(g.L[1]));
-    const int tz = shift_axis(cz, dz, g.nc[2], !isinf(g.L[2]));
-    if (tx >= 0 && ty >= 0 && tz >= 0) {
-      const int64_t T = ((int64_t)tz * g.nc[1] + ty) * g.nc[0] + tx;
-      const int64_t a0 = cell_start[A], a1 = cell_start[A + 1], t0 = cell_start[T], t1 = cell_start[T + 1];
-      const int home_kind = k, tgt_kind = k == 0 ? 0 : HALF_OFFSETS - 1 + k;
-      // cells of at most 32 atoms are one tile and its sums are stored; larger cells take
-      // several tiles, whose sums accumulate into zeroed slots, as do the row and column
-      // sums of the home cell with itself (each slot is always written by the same lane, in
-      // tile order)
-      const bool multi = (a1 - a0 > 32) || (t1 - t0 > 32) || k == 0;
-      if (multi) {
+    const int tx = shift_axis(cx, dx, g.nc[0], !isinf(L0));
+    const int ty = shift_axis(cy, dy, g.nc[1], !isinf(L1));
+    const int tz = shift_axis(cz, dz, g.nc[2], !isinf(L2));
+    if (tx < 0 || ty < 0 || tz < 0) continue;
+    const int64_t T = ((int64_t)tz * g.nc[1] + ty) * g.nc[0] + tx;
+    const int64_t a0 = cell_start[A], a1 = cell_start[A + 1], t0 = cell_start[T], t1 = cell_start[T + 1];
+    const int home_kind = k, tgt_kind = k == 0 ? 0 : HALF_OFFSETS - 1 + k;
+    // cells of at most 32 atoms are one tile and its sums are stored; larger cells take
+    // several tiles, whose sums accumulate into zeroed slots, as do the row and column sums
+    // of the home cell with itself (each slot is always written by the same lane, in tile
+    // order)
+    const bool multi = (a1 - a0 > 32) || (t1 - t0 > 32) || k == 0;
+    if (multi) {
+      const double z[3] = {0.0, 0.0, 0.0};
+      for (int64_t s = a0 + lane; s < a1; s += 32) pbuf_put(P, n, home_kind, s, z, false);
+      if (k != 0)
+        for (int64_t s = t0 + lane; s < t1; s += 32) pbuf_put(P, n, tgt_kind, s, z, false);
+      __syncwarp();
+    }
+    if (a0 == a1 && k != 0)  // no home atoms: the target atoms still get their (zero) slot
+      for (int64_t s = t0 + lane; s < t1; s += 32) {
         const double z[3] = {0.0, 0.0, 0.0};
-        for (int64_t s = a0 + lane; s < a1; s += 32) pbuf_put(P, n, home_kind, s, z, false);
-        if (k != 0)
-          for (int64_t s = t0 + lane; s < t1; s += 32) pbuf_put(P, n, tgt_kind, s, z, false);
-        __syncwarp();
+        pbuf_put(P, n, tgt_kind, s, z, false);
       }
-      if (a0 == a1 && k != 0)  // no home atoms: the target atoms still get their (zero) slot
-        for (int64_t s = t0 + lane; s < t1; s += 32) {
-          const double z[3] = {0.0, 0.0, 0.0};
-          pbuf_put(P, n, tgt_kind, s, z, false);
-        }
-      HalfHit* hb = hits[w];
-      const unsigned lt = (1u << lane) - 1u;
-      const double rmax = TT.rcut_max;
-      for (int64_t rc = a0; rc < a1; rc += 32) {
-        const int ra = (int)(a1 - rc < 32 ? a1 - rc : 32);
-        double fa[3] = {0.0, 0.0, 0.0};  // row sums of row rc + lane
-        for (int64_t cc = t0; cc < t1; cc += 32) {
-          const int64_t ts = cc + lane;
-          const bool tv = ts < t1;
-          const double4 xt = tv ? spos[ts] : make_double4(0.0, 0.0, 0.0, 0.0);
-          const int32_t it = tv ? cell_atoms[ts] : -1;
-          double ft[3] = {0.0, 0.0, 0.0};  // column sums of lane atom ts
-          int nh = 0;
-          for (int q = 0; q < ra; q++) {
+    HalfHit* hb = hits[w];
+    const unsigned lt = (1u << lane) - 1u;
+    const double rmax = TT.rcut_max;
+    for (int64_t rc = a0; rc < a1; rc += 32) {
+      const int ra = (int)(a1 - rc < 32 ? a1 - rc : 32);
+      double fa[3] = {0.0, 0.0, 0.0};  // row sums of row rc + lane
+      for (int64_t cc = t0; cc < t1; cc += 32) {
+        const int64_t ts = cc + lane;
+        const bool tv = ts < t1;
+        const double4 xt = tv ? spos[ts] : make_double4(0.0, 0.0, 0.0, 0.0);
+        const int32_t it = tv ? cell_atoms[ts] : -1;
+        double ft[3] = {0.0, 0.0, 0.0};  // column sums of lane atom ts
+        int nh = 0;
+        for (int q = 0; q <= ra; q++) {  // q == ra: evaluate what is left
+          if (q < ra) {
             const int64_t as = rc + q;
             const double4 xa = spos[as];
             const int32_t ia = cell_atoms[as];
             bool ok = false;
             HalfHit h;
             if (tv && (k != 0 || ts > as)) {
-              const double d2 = sumsq3_dev(pe_axis_dev(g.L[0], xa.x, xt.x), pe_axis_dev(g.L[1], xa.y, xt.y),
-                                           pe_axis_dev(g.L[2], xa.z, xt.z));
+              const double d2 = sumsq3_dev(pe_axis_dev(L0, xa.x, xt.x), pe_axis_dev(L1, xa.y, xt.y),
+                                           pe_axis_dev(L2, xa.z, xt.z));
               if (d2 <= TT.rmax2_hi) {
                 const double dist = sqrt(d2);
                 if (dist <= rmax) {
@@ -220,13 +275,13 @@ __global__ void __launch_bounds__(PAIR_T, MINB) k_pair_half(const __grid_constan
                   h.at = q | (lane << 8);
                   h.sp = (int)xa.w | ((int)xt.w << 8);
                   if (ia < it) {  // r = get_displacement(x_lo, x_hi) with the row atom lo
-                    h.r0 = disp_axis_dev(g.L[0], xa.x, xt.x);
-                    h.r1 = disp_axis_dev(g.L[1], xa.y, xt.y);
-                    h.r2 = disp_axis_dev(g.L[2], xa.z, xt.z);
+                    h.r0 = disp_axis_dev(L0, xa.x, xt.x);
+                    h.r1 = disp_axis_dev(L1, xa.y, xt.y);
+                    h.r2 = disp_axis_dev(L2, xa.z, xt.z);
                   } else {  // the lane atom is lo: r = -get_displacement(x_lane, x_row)
-                    h.r0 = -disp_axis_dev(g.L[0], xt.x, xa.x);
-                    h.r1 = -disp_axis_dev(g.L[1], xt.y, xa.y);
-                    h.r2 = -disp_axis_dev(g.L[2], xt.z, xa.z);
+                    h.r0 = -disp_axis_dev(L0, xt.x, xa.x);
+                    h.r1 = -disp_axis_dev(L1, xt.y, xa.y);
+                    h.r2 = -disp_axis_dev(L2, xt.z, xa.z);
                   }
                 }
               }
@@ -235,22 +290,22 @@ __global__ void __launch_bounds__(PAIR_T, MINB) k_pair_half(const __grid_constan
             if (ok) hb[nh + __popc(bal & lt)] = h;
             nh += __popc(bal);
             __syncwarp();
-            if (nh >= 32) {
-              half_eval(TT, hb, 32, lane, acc, fa, ft);
-              __syncwarp();
-              if (lane < nh - 32) hb[lane] = hb[32 + lane];
-              nh -= 32;
-              __syncwarp();
-            }
           }
-          half_eval(TT, hb, nh, lane, acc, fa, ft);
-          __syncwarp();
-          if (tv) pbuf_put(P, n, tgt_kind, ts, ft, multi);
-          __syncwarp();
+          // one call site of the term code: full batches, then the rest after the last row
+          while (nh >= 32 || (q == ra && nh > 0)) {
+            const int m = nh < 32 ? nh : 32;
+            half_eval(TT, hb, m, lane, stage[w], acc, fa, ft);
+            __syncwarp();
+            if (lane < nh - m) hb[lane] = hb[m + lane];
+            nh -= m;
+            __syncwarp();
+          }
         }
-        if (lane < ra) pbuf_put(P, n, home_kind, rc + lane, fa, multi);
+        if (tv) pbuf_put(P, n, tgt_kind, ts, ft, multi);
         __syncwarp();
       }
+      if (lane < ra) pbuf_put(P, n, home_kind, rc + lane, fa, multi);
+      __syncwarp();
     }
   }
 #pragma unroll
@@ -299,9 +354,10 @@ __global__ void k_pair_gather(int64_t n, const ConfGrid* __restrict__ grid, cons
   F[3 * i + 2] = f2;
 }
 
-// Deterministic final reduction of per-block partials: one block, fixed order.
+// Deterministic final reduction of per-block partials (E and W6): one block, fixed order;
+// component 0 goes to E, 1..6 to W6 (either may be null).
 __global__ void k_reduce_partials(int64_t nblocks, int width, const double* __restrict__ partial,
-                                  double* __restrict__ out) {
+                                  double* __restrict__ E, double* __restrict__ W6) {
   __shared__ double sm[256];
   for (int k = 0; k < width; k++) {
     double v = 0.0;
@@ -312,7 +368,10 @@ __global__ void k_reduce_partials(int64_t nblocks, int width, const double* __re
       if ((int)threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
       __syncthreads();
     }
-    if (threadIdx.x == 0) out[k] = sm[0];
+    if (threadIdx.x == 0) {
+      if (k == 0 && E) *E = sm[0];
+      if (k > 0 && W6) W6[k - 1] = sm[0];
+    }
     __syncthreads();
   }
 }
@@ -335,25 +394,26 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
   const ConfGrid& g = cl.h_grid[0];
   bool half = n > 0 && !ctx->pair_full_stencil;
   for (int a = 0; a < 3; a++) half &= std::isinf(g.L[a]) || g.nc[a] >= 3;
-  double* red;
-  IPG_RET(scratch(ctx, "pair_red", 8, &red));
   double* partial;
   int64_t nb;
   IPG_RET(ipg_timing_mark(ctx, "pair_eval", true));
   if (half) {
     const int64_t items = cl.ncells * HALF_OFFSETS;
-    nb = std::max<int64_t>(1, (items + PAIR_WARPS - 1) / PAIR_WARPS);
+    // grid-stride: a fixed grid of a few waves of resident blocks (the kernel's register bound
+    // allows pair_minb blocks of four warps per SM)
+    nb = std::max<int64_t>(1, std::min<int64_t>((items + PAIR_WARPS - 1) / PAIR_WARPS,
+                                                (int64_t)ctx->num_sms * ctx->pair_minb * 4));
     double* P;
     IPG_RET(scratch(ctx, "pair_partial", (size_t)nb * 7, &partial));
     IPG_RET(scratch(ctx, "pair_pbuf", (size_t)PBUF_SLOTS * 3 * n, &P));
-    if (ctx->pair_minb == 3)
-      IPG_LAUNCH(ctx, k_pair_half<3>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
+    if (ctx->pair_minb == 4)
+      IPG_LAUNCH(ctx, k_pair_half<4>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
                  cl.d_cell_atoms, cl.d_spos, P, partial);
     else if (ctx->pair_minb == 5)
       IPG_LAUNCH(ctx, k_pair_half<5>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
                  cl.d_cell_atoms, cl.d_spos, P, partial);
     else
-      IPG_LAUNCH(ctx, k_pair_half<4>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
+      IPG_LAUNCH(ctx, k_pair_half<3>, (unsigned)nb, PAIR_T, 0, pt, n, cl.d_grid, cl.ncells, cl.d_cell_start,
                  cl.d_cell_atoms, cl.d_spos, P, partial);
     if ((flags & IPG_WANT_F) && d_F)
       IPG_LAUNCH(ctx, k_pair_gather, (unsigned)((n + 255) / 256), 256, 0, n, cl.d_grid, cl.d_cell_atoms, cl.d_spos,
@@ -365,11 +425,8 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
                cl.d_spos, (flags & IPG_WANT_F) ? d_F : nullptr, partial);
   }
   IPG_RET(ipg_timing_mark(ctx, "pair_eval", false));
-  IPG_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, nb, 7, partial, red);
-  if ((flags & IPG_WANT_E) && d_E)
-    CUDA_RET(ctx, cudaMemcpyAsync(d_E, red, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  if ((flags & IPG_WANT_W) && d_W6)
-    CUDA_RET(ctx, cudaMemcpyAsync(d_W6, red + 1, 6 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  IPG_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, nb, 7, partial, (flags & IPG_WANT_E) ? d_E : nullptr,
+             (flags & IPG_WANT_W) ? d_W6 : nullptr);
   return IPG_OK;
 }
 

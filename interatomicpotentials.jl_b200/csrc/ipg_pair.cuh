@@ -55,14 +55,16 @@ inline int pair_prepare_terms(const ipg_pair_term* terms, int nterms, PairTerms&
         d.p[2] = 4.0 * s.params[0];
         d.p[3] = 24.0 * s.params[0];
         break;
-      case IPG_PAIR_BM:
+      case IPG_PAIR_BM:  // p = A, rho, sigma, C, D, 1/rho
+        d.p[5] = 1.0 / s.params[1];
+        break;
       case IPG_PAIR_MORSE:
       case IPG_PAIR_MOCK_R2:
         break;
       case IPG_PAIR_COUL:  // p = q1, q2, k_e q1 q2 with k_e = 1 (src/constants.jl:7)
         d.p[2] = 1.0 * s.params[0] * s.params[1];
         break;
-      case IPG_PAIR_ZBL: {  // p = Z1, Z2, e, Z1 Z2 e^2, the screening length, ln(e)
+      case IPG_PAIR_ZBL: {  // p = Z1, Z2, e, Z1 Z2 e^2, the screening length, ln(e), 1/length
         const double Z1 = s.params[0], Z2 = s.params[1], e = s.params[2];
         if (!(e > 0.0)) {
           snprintf(err, errlen, "term %d: ZBL e must be > 0", k);
@@ -71,6 +73,7 @@ inline int pair_prepare_terms(const ipg_pair_term* terms, int nterms, PairTerms&
         d.p[3] = 1.0 * Z1 * Z2 * e * e;
         d.p[4] = 0.8854 * 0.529 / (std::pow(Z1, 0.23) + std::pow(Z2, 0.23));
         d.p[5] = std::log(e);
+        d.p[6] = 1.0 / d.p[4];
         break;
       }
       default:
@@ -82,42 +85,45 @@ inline int pair_prepare_terms(const ipg_pair_term* terms, int nterms, PairTerms&
   return IPG_OK;
 }
 
-// V(R) and g(R) (force = g r) of one term.
-__device__ __forceinline__ void pair_term_eval(const PairTermDev& t, double R, double& V, double& g) {
+// V(R) and g(R) (force = g r) of one term; ir = 1/R and ir2 = 1/R^2 are formed once per pair,
+// so every division by R of the reference formulas is a product with ir (the results differ
+// from the literal divisions by rounding only).
+__device__ __forceinline__ void pair_term_eval(const PairTermDev& t, double R, double ir, double ir2, double& V,
+                                               double& g) {
   switch (t.kind) {
-    case IPG_PAIR_LJ: {  // lj.jl:35-36
-      const double s = t.p[1] / R;
+    case IPG_PAIR_LJ: {  // lj.jl:35-36; p = eps, sigma, 4 eps, 24 eps
+      const double s = t.p[1] * ir;
       const double s2 = s * s;
       const double s6 = s2 * s2 * s2;
       const double s12 = s6 * s6;
       V = t.p[2] * (s12 - s6);
-      g = t.p[3] * (2.0 * s12 - s6) / (R * R);
+      g = t.p[3] * (2.0 * s12 - s6) * ir2;
       break;
     }
-    case IPG_PAIR_BM: {  // bm.jl:38-39; p = A, rho, sigma, C, D
-      const double ex = t.p[0] * exp((t.p[2] - R) / t.p[1]);
-      const double c = t.p[3] / R, d = t.p[4] / R;
+    case IPG_PAIR_BM: {  // bm.jl:38-39; p = A, rho, sigma, C, D, 1/rho
+      const double ex = t.p[0] * exp((t.p[2] - R) * t.p[5]);
+      const double c = t.p[3] * ir, d = t.p[4] * ir;
       const double c2 = c * c, d2 = d * d;
       const double c6 = c2 * c2 * c2, d8 = (d2 * d2) * (d2 * d2);
       V = ex + c6 - d8;
-      g = ex / (t.p[1] * R) + (c6 - d8) / (R * R);
+      g = ex * t.p[5] * ir + (c6 - d8) * ir2;
       break;
     }
-    case IPG_PAIR_COUL:  // coulomb.jl:36-37
-      V = t.p[2] / R;
-      g = t.p[2] / (R * R * R);
+    case IPG_PAIR_COUL:  // coulomb.jl:36-37; p = q1, q2, k_e q1 q2
+      V = t.p[2] * ir;
+      g = t.p[2] * ir * ir2;
       break;
     case IPG_PAIR_MORSE: {  // morse.jl:36-39; p = D, alpha, sigma
       const double e = exp(-t.p[1] * (R - t.p[2]));
       const double om = 1.0 - e;
       V = t.p[0] * om * om;
-      g = 2.0 * t.p[0] * t.p[1] * om * e / R;
+      g = 2.0 * t.p[0] * t.p[1] * om * e * ir;
       break;
     }
     case IPG_PAIR_ZBL: {  // zbl.jl:27-36: e^(-a_k d) with base e = p[2]
       const double zc[4] = {0.18175, 0.50986, 0.28022, 0.02817};
       const double za[4] = {3.19980, 0.94229, 0.40290, 0.20162};
-      const double d = R / t.p[4];
+      const double d = R * t.p[6];
       double phi = 0.0, dphi = 0.0;
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -126,8 +132,8 @@ __device__ __forceinline__ void pair_term_eval(const PairTermDev& t, double R, d
         dphi += za[k] * zc[k] * ek;
       }
       dphi = -dphi;
-      V = t.p[3] * phi / R;
-      g = t.p[3] * (phi + d * dphi) / (R * R * R);
+      V = t.p[3] * phi * ir;
+      g = t.p[3] * (phi + d * dphi) * ir * ir2;
       break;
     }
     case IPG_PAIR_MOCK_R2:  // test/mocks.jl:29-34; p = seed
@@ -147,12 +153,13 @@ __device__ __forceinline__ void pair_terms_sum(const PairTerms& TT, double R, do
                                                double& g) {
   V = 0.0;
   g = 0.0;
+  const double ir = 1.0 / R, ir2 = ir * ir;
   for (int t = 0; t < TT.nterms; t++) {
     const PairTermDev& T = TT.t[t];
     if (dist > T.rcut) continue;
     if (!((T.mask >> si) & 1ull) || !((T.mask >> sj) & 1ull)) continue;
     double v, gg;
-    pair_term_eval(T, R, v, gg);
+    pair_term_eval(T, R, ir, ir2, v, gg);
     V += T.coeff * v;
     g += T.coeff * gg;
   }
@@ -210,12 +217,12 @@ __device__ __forceinline__ void pair_walk_atom(const PairTerms& TT, const ConfGr
   const double rmax = TT.rcut_max;
   int nh = 0;
   const unsigned lt = (1u << lane) - 1u;
-  for (int r = 0; r < Rg.n; r++)
-    for (int64_t q0 = Rg.beg[r]; q0 < Rg.end[r]; q0 += 32) {
+  for (int r = 0; r <= Rg.n; r++)  // r == Rg.n: evaluate what is left
+    for (int64_t q0 = r < Rg.n ? Rg.beg[r] : 0; q0 < (r < Rg.n ? Rg.end[r] : 1); q0 += 32) {
       const int64_t q = q0 + lane;
       bool ok = false;
       PairHit h;
-      if (q < Rg.end[r]) {
+      if (r < Rg.n && q < Rg.end[r]) {
         const int32_t j = cell_atoms[q];
         const double4 xj = spos[q];
         if (j != i) {
@@ -244,16 +251,16 @@ __device__ __forceinline__ void pair_walk_atom(const PairTerms& TT, const ConfGr
       if (ok) hb[nh + __popc(bal & lt)] = h;
       nh += __popc(bal);
       __syncwarp();
-      if (nh >= 32) {
-        pair_eval_hits(TT, hb, 32, lane, si, acc, f0, f1, f2);
+      // one call site of the term code: full batches, then the rest after the last range
+      while (nh >= 32 || (r == Rg.n && nh > 0)) {
+        const int m = nh < 32 ? nh : 32;
+        pair_eval_hits(TT, hb, m, lane, si, acc, f0, f1, f2);
         __syncwarp();
-        if (lane < nh - 32) hb[lane] = hb[32 + lane];
-        nh -= 32;
+        if (lane < nh - m) hb[lane] = hb[m + lane];
+        nh -= m;
         __syncwarp();
       }
     }
-  pair_eval_hits(TT, hb, nh, lane, si, acc, f0, f1, f2);
-  __syncwarp();
   f0 = warp_sum(f0);
   f1 = warp_sum(f1);
   f2 = warp_sum(f2);

@@ -703,14 +703,16 @@ __device__ __forceinline__ void cj_acc(double pr, double pi, double2 v, double c
 //   Udot_j   = f(adot, bdot, U) + f(a, b, Udot)
 //   dUdot_k  = f(da_k dot, db_k dot, U) + f(da_k, db_k, Udot) + f(adot, bdot, dU_k) + f(a, b, dUdot_k)
 // with f(A, B, u)[mb][ma] = -rootpq[ma][j-mb] conj(B) u[mb][ma-1] + rootpq[j-ma][j-mb] conj(A) u[mb][ma].
+// values_only: the two components U and Udot (Utot needs no derivative), else all eight.
 __device__ __forceinline__ void wigner_level_hvp(const SnapDev& S, const double* rpq, int j, const PairGeomD& G,
                                                  const double2* __restrict__ prev, double2* __restrict__ cur,
-                                                 int lane) {
+                                                 int lane, bool values_only) {
   const int J2 = S.J + 2;
   const int em = S.ext_max;
   const int nrec = (j / 2 + 1) * (j + 1);
-  for (int t = lane; t < 8 * nrec; t += 32) {
-    const int comp = t / nrec;
+  const int ncomp = values_only ? 2 : 8;
+  for (int t = lane; t < ncomp * nrec; t += 32) {
+    const int comp = values_only ? (t / nrec) * 4 : t / nrec;
     const int e = t - comp * nrec;
     const int mb = e / (j + 1);
     const int ma = e - mb * (j + 1);
@@ -744,8 +746,8 @@ __device__ __forceinline__ void wigner_level_hvp(const SnapDev& S, const double*
   __syncwarp();
   if (j & 1) {  // mirrored row R = (j+1)/2 of every component (inversion symmetry)
     const int R = (j + 1) / 2;
-    for (int t = lane; t < 8 * (j + 1); t += 32) {
-      const int comp = t / (j + 1);
+    for (int t = lane; t < ncomp * (j + 1); t += 32) {
+      const int comp = values_only ? (t / (j + 1)) * 4 : t / (j + 1);
       const int c = t - comp * (j + 1);
       const double2 src = cur[comp * em + (j - R) * (j + 1) + (j - c)];
       const double sg = ((c + R) & 1) ? -1.0 : 1.0;
@@ -782,7 +784,7 @@ __host__ __device__ inline HvpSmem hvp_smem(const SnapDev& S, int nwarps) {
 
 // Per pair p = (i, j): fvec[p] = dE_i/dr_ij and fdot[p] = its tangent along the atom
 // displacements v [n][3].  Inputs as k_snap_atom<MODE_ADJ> (beta via S.ycoef).
-__global__ void __launch_bounds__(128) k_snap_hvp(const __grid_constant__ SnapDev S, SnapIO io,
+__global__ void __launch_bounds__(256) k_snap_hvp(const __grid_constant__ SnapDev S, SnapIO io,
                                                   const double* __restrict__ v, double* __restrict__ fdot) {
   extern __shared__ double smem[];
   const int nwarps = blockDim.x >> 5;
@@ -826,7 +828,7 @@ __global__ void __launch_bounds__(128) k_snap_hvp(const __grid_constant__ SnapDe
             if (lane < 8) cur[lane * em] = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
             __syncwarp();
           } else {
-            wigner_level_hvp(S, rpq, j, G, prev, cur, lane);
+            wigner_level_hvp(S, rpq, j, G, prev, cur, lane, true);
           }
           const int nrec = (j / 2 + 1) * (j + 1);
           const int hb = S.half_block[j];
@@ -946,7 +948,7 @@ __global__ void __launch_bounds__(128) k_snap_hvp(const __grid_constant__ SnapDe
           if (lane < 8) cur[lane * em] = make_double2(lane == 0 ? 1.0 : 0.0, 0.0);
           __syncwarp();
         } else {
-          wigner_level_hvp(S, rpq, j, G, prev, cur, lane);
+          wigner_level_hvp(S, rpq, j, G, prev, cur, lane, false);
         }
         const int nrec = (j / 2 + 1) * (j + 1);
         const int hb = S.half_block[j];
@@ -2870,6 +2872,34 @@ __global__ void k_snap_W_desc(int64_t n, int K, int nsp, const int64_t* __restri
   for (int q = threadIdx.x; q < nsp * K * 6; q += blockDim.x) part[(size_t)blockIdx.x * nsp * K * 6 + q] = wsm[q];
 }
 
+// The W descriptors when their [nsp][K][6] sums do not fit shared memory (quadratic SNAP):
+// one thread per component b sums every atom and pair in order, straight into W.
+__global__ void k_snap_W_cols(int64_t n, int K, int nsp, const int64_t* __restrict__ off,
+                              const int32_t* __restrict__ nbr, const int32_t* __restrict__ species,
+                              const double* __restrict__ pos, const double* __restrict__ dbl, double* __restrict__ W) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= K) return;
+  for (int s = 0; s < nsp; s++)
+    for (int c = 0; c < 6; c++) W[((size_t)s * K + b) * 6 + c] = 0.0;
+  for (int64_t i = 0; i < n; i++) {
+    const int s = clamp_sp(species[i], nsp);
+    const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+    double w[6] = {0, 0, 0, 0, 0, 0};
+    for (int64_t p = off[i]; p < off[i + 1]; p++) {
+      const double* d = dbl + ((size_t)p * K + b) * 3;
+      const int64_t jn = nbr[p];
+      const double dx = xi - pos[3 * jn], dy = yi - pos[3 * jn + 1], dz = zi - pos[3 * jn + 2];
+      w[0] += d[0] * dx;
+      w[1] += d[1] * dy;
+      w[2] += d[2] * dz;
+      w[3] += d[1] * dz;
+      w[4] += d[0] * dz;
+      w[5] += d[0] * dy;
+    }
+    for (int c = 0; c < 6; c++) W[((size_t)s * K + b) * 6 + c] += w[c];
+  }
+}
+
 __global__ void k_sum_partials(int64_t nblocks, int width, const double* __restrict__ part, double* __restrict__ out,
                                double scale_add_base) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2976,7 +3006,7 @@ struct ipg_snap {
   int64_t vjp_chunk = 0;     // atoms per Z chunk (0: about 4 GiB of Z)
   bool generic_plain = false;  // plain path: the per-atom block kernel (IPG_GENERIC_PLAIN=1)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
-  int yr_warps = 8;         // warps per block of the adjoint Y kernel (8 or 10)
+  int yr_warps = 10;        // warps per block of the adjoint Y kernel (10, or 8)
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
   int64_t last_np = 0;
@@ -3399,11 +3429,12 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
         const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
         const bool withz = rows && out.zall;
-        const bool w10 = rows && !withz && s->yr_warps == 10;  // ten warps per block (IPG_YR_WARPS=10)
+        const bool w10 = rows && !withz && s->yr_warps == 10;  // ten warps per block (IPG_YR_WARPS=8: eight)
         const int ythreads = (w10 ? 10 : YS_WARPS) * 32;
         const void* kfn = !rows ? (const void*)k_snap_yatoms
-                                : (withz ? (const void*)k_snap_yrows<YM_YZ>
-                                         : (w10 ? (const void*)k_snap_yrows<YM_Y, 10> : (const void*)k_snap_yrows<YM_Y>));
+                          : withz ? (const void*)k_snap_yrows<YM_YZ>
+                          : w10   ? (const void*)k_snap_yrows<YM_Y, 10>
+                                  : (const void*)k_snap_yrows<YM_Y>;
         if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
         CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
@@ -3520,7 +3551,9 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_LAUNCH(ctx, k_snap_fit_rows, (unsigned)nconf, 128, 0, nconf, d_coff, K, nsp, d_species, out.B, pl.d_off,
                pl.d_j, d_pos, dbl, out.Ae, out.Aw);
   }
-  if (out.Wd) {
+  if (out.Wd && (size_t)nsp * K * 6 * 8 > 200 * 1024) {
+    IPG_LAUNCH(ctx, k_snap_W_cols, nblk(K, 128), 128, 0, n, K, nsp, pl.d_off, pl.d_j, d_species, d_pos, dbl, out.Wd);
+  } else if (out.Wd) {
     const int width = nsp * K * 6;
     int64_t grid = std::min<int64_t>(std::max<int64_t>(n, 1), 2 * ctx->num_sms);
     double* part;
@@ -3847,7 +3880,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
   if (const char* g = getenv("IPG_GENERIC_PLAIN")) s->generic_plain = g[0] == '1';
-  if (const char* g = getenv("IPG_YR_WARPS")) s->yr_warps = atoi(g) == 10 ? 10 : 8;
+  if (const char* g = getenv("IPG_YR_WARPS")) s->yr_warps = atoi(g) == 8 ? 8 : 10;
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);
@@ -4201,7 +4234,7 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
     if (dev.chem || dev.quadratic)
       return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "the position pullback of chem_flag / quadratic SNAP is not built");
     IPG_RET(set_beta(s, beta, 0.0, dev));
-    const int nw = 4;
+    const int nw = 8;
     const HvpSmem HL = hvp_smem(dev, nw);
     if (HL.total > 227 * 1024)
       return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "twojmax %d: the position pullback needs %zu bytes of shared memory",

@@ -99,9 +99,11 @@ class SNAP:
         return max(2.0 * r * self.rcutfac for r in self.radii)
 
     def species_ids(self, system):
+        """0-based species ids of the system's atoms, by their position in snap.species."""
+        lut = {s: k for k, s in enumerate(self.species)}
         try:
-            return np.ascontiguousarray([self.species.index(s) for s in system.symbols], dtype=np.int32)
-        except ValueError as e:
+            return np.fromiter((lut[s] for s in system.symbols), dtype=np.int32, count=len(system.symbols))
+        except KeyError as e:
             raise ValueError(f"system has a species not in snap.species: {e}") from None
 
     def close(self):

@@ -481,3 +481,19 @@ def test_verlet_skin_reuse_checks_inputs():
         assert dev_call(system.positions, sp3)[0] == -7
     finally:
         md.ctx.set_stream(None)
+
+
+@pytest.mark.parametrize("env", [dict(IPG_YR_WARPS="8")])
+def test_y_kernel_variants_agree(env, monkeypatch):
+    """The adjoint Y kernel with eight warps per block (the default has ten) gives the forces of
+    the default kernel to rounding and the oracle's to 1e-10."""
+    s, prm, beta = W.snap_j8(cells=6)
+    ref, orc = make(prm, switch_flag=True)
+    e0, f0, w0 = ref.energy_forces(s, beta, 0.1)
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    snap, _ = make(prm, switch_flag=True)
+    e, f, w = snap.energy_forces(s, beta, 0.1)
+    assert abs(e - e0) <= 1e-13 * abs(e0) and rel_err(f, f0) <= 1e-13 and rel_err(w, w0) <= 1e-13
+    eo, fo, _ = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.1)
+    assert abs(e - eo) <= TOL * abs(eo) and rel_err(f, fo) <= TOL
