@@ -712,8 +712,9 @@ __device__ __forceinline__ void wigner_level_hvp(const SnapDev& S, const double*
   const int nrec = (j / 2 + 1) * (j + 1);
   const int ncomp = values_only ? 2 : 8;
   for (int t = lane; t < ncomp * nrec; t += 32) {
-    const int comp = values_only ? (t / nrec) * 4 : t / nrec;
-    const int e = t - comp * nrec;
+    const int grp = t / nrec;  // component group: U, Udot (values_only) or all eight
+    const int comp = values_only ? grp * 4 : grp;
+    const int e = t - grp * nrec;
     const int mb = e / (j + 1);
     const int ma = e - mb * (j + 1);
     const int k = (comp & 3) - 1;  // derivative direction of comps 1..3 and 5..7
@@ -747,8 +748,9 @@ __device__ __forceinline__ void wigner_level_hvp(const SnapDev& S, const double*
   if (j & 1) {  // mirrored row R = (j+1)/2 of every component (inversion symmetry)
     const int R = (j + 1) / 2;
     for (int t = lane; t < ncomp * (j + 1); t += 32) {
-      const int comp = values_only ? (t / (j + 1)) * 4 : t / (j + 1);
-      const int c = t - comp * (j + 1);
+      const int grp = t / (j + 1);
+      const int comp = values_only ? grp * 4 : grp;
+      const int c = t - grp * (j + 1);
       const double2 src = cur[comp * em + (j - R) * (j + 1) + (j - c)];
       const double sg = ((c + R) & 1) ? -1.0 : 1.0;
       cur[comp * em + R * (j + 1) + c] = make_double2(sg * src.x, -sg * src.y);
@@ -1373,6 +1375,7 @@ __global__ void __launch_bounds__(UTA_WARPS * 32) k_snap_utot_all(const __grid_c
       sw = sfac_of(S, r, rcut) * S.weight[sj];
     }
     st.first = p0 == beg;
+    st.nact = end - p0 < 32 ? (int)(end > p0 ? end - p0 : 0) : 32;
     snapchain::all_chains_utot<J>(a, b, sw, st);
   }
 }
@@ -2026,6 +2029,7 @@ __global__ void __launch_bounds__(VS_WARPS * 32) k_snap_vsum(const __grid_consta
       }
     }
     st.first = p0 == beg;
+    st.nact = end - p0 < 32 ? (int)(end > p0 ? end - p0 : 0) : 32;
     snapchain::all_chains_v<J>(G, A, Bk, st, vsh, NT, threadIdx.x);
   }
 }
