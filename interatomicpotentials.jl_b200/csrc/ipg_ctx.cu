@@ -1,8 +1,12 @@
 // ipg_ctx.cu — context lifetime, error reporting, device scratch, status word, scan.
 #include <algorithm>
 #include <cstdarg>
-
 #include <cstdlib>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+
+#include <unistd.h>
 
 #include "ipg_internal.cuh"
 
@@ -109,9 +113,80 @@ int ipg_status_check(ipg_ctx* ctx, const char* what) {
 
 // ---------------------------------------------------------------------------------
 // Pinned staging of large host copies.
+
+// A fixed team of host threads that splits one large memcpy: the caller copies the first
+// share, each worker one of the others.  Created at a context's first large copy, joined when
+// the context is destroyed.  A process forked after the team started has no workers, so the
+// team copies on the caller's thread alone there.
+struct HostCopyTeam {
+  explicit HostCopyTeam(int nthreads) : pid_(getpid()), parts_(nthreads) {
+    for (int k = 1; k < nthreads; k++) th_.emplace_back([this, k] { work(k); });
+  }
+  ~HostCopyTeam() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    go_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  void copy(void* dst, const void* src, size_t bytes) {
+    if (th_.empty() || bytes < (size_t(1) << 20) || getpid() != pid_) {
+      memcpy(dst, src, bytes);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      dst_ = static_cast<char*>(dst);
+      src_ = static_cast<const char*>(src);
+      bytes_ = bytes;
+      left_ = (int)th_.size();
+      gen_++;
+    }
+    go_.notify_all();
+    part(0);
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [this] { return left_ == 0; });
+  }
+
+ private:
+  // share k of the current copy (shares are whole multiples of 4 KiB; the last takes the rest)
+  void part(int k) {
+    const size_t share = ((bytes_ / parts_) + 4095) & ~size_t(4095);
+    const size_t lo = std::min(bytes_, share * k), hi = k == parts_ - 1 ? bytes_ : std::min(bytes_, lo + share);
+    if (hi > lo) memcpy(dst_ + lo, src_ + lo, hi - lo);
+  }
+  void work(int k) {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        go_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      part(k);
+      std::lock_guard<std::mutex> lk(m_);
+      if (--left_ == 0) done_.notify_one();
+    }
+  }
+  const pid_t pid_;
+  const int parts_;
+  std::vector<std::thread> th_;
+  std::mutex m_;
+  std::condition_variable go_, done_;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t bytes_ = 0;
+  uint64_t gen_ = 0;
+  int left_ = 0;
+  bool stop_ = false;
+};
+
 namespace {
-constexpr size_t PIN_CHUNK = size_t(8) << 20;   // bytes per ring slot
+constexpr size_t PIN_CHUNK = size_t(4) << 20;   // bytes per ring slot
 constexpr size_t PIN_DIRECT = size_t(1) << 20;  // smaller copies go straight through the driver
+constexpr int SLOTS = ipg_ctx::PIN_SLOTS;
 
 // True when p is page-locked host memory that the device can copy from directly.
 bool host_is_pinned(const void* p) {
@@ -124,7 +199,7 @@ bool host_is_pinned(const void* p) {
 }
 
 int pinned_ring(ipg_ctx* ctx) {
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < SLOTS; k++) {
     if (!ctx->pinned[k]) {
       void* p = nullptr;
       if (cudaMallocHost(&p, PIN_CHUNK) != cudaSuccess) {
@@ -135,9 +210,22 @@ int pinned_ring(ipg_ctx* ctx) {
     }
     if (!ctx->pinned_ev[k]) CUDA_RET(ctx, cudaEventCreateWithFlags(&ctx->pinned_ev[k], cudaEventDisableTiming));
   }
+  if (!ctx->copy_team) {
+    int nt = ctx->copy_threads;
+    if (nt <= 0) {  // half the host's hardware threads, at most 8: a memcpy saturates well before
+      const unsigned hw = std::thread::hardware_concurrency();
+      nt = (int)std::max(1u, std::min(8u, hw / 2));
+    }
+    ctx->copy_team = new HostCopyTeam(nt);
+  }
   return IPG_OK;
 }
 }  // namespace
+
+void ipg_copy_team_free(ipg_ctx* ctx) {
+  delete ctx->copy_team;
+  ctx->copy_team = nullptr;
+}
 
 int ipg_copy_d2h(ipg_ctx* ctx, void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return IPG_OK;
@@ -150,18 +238,17 @@ int ipg_copy_d2h(ipg_ctx* ctx, void* dst, const void* src, size_t bytes) {
   const size_t nchunk = (bytes + PIN_CHUNK - 1) / PIN_CHUNK;
   auto issue = [&](size_t c) -> int {
     const size_t off = c * PIN_CHUNK, len = std::min(PIN_CHUNK, bytes - off);
-    CUDA_RET(ctx, cudaMemcpyAsync(ctx->pinned[c & 1], static_cast<const char*>(src) + off, len,
+    CUDA_RET(ctx, cudaMemcpyAsync(ctx->pinned[c % SLOTS], static_cast<const char*>(src) + off, len,
                                   cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_RET(ctx, cudaEventRecord(ctx->pinned_ev[c & 1], ctx->stream));
+    CUDA_RET(ctx, cudaEventRecord(ctx->pinned_ev[c % SLOTS], ctx->stream));
     return IPG_OK;
   };
-  IPG_RET(issue(0));
-  if (nchunk > 1) IPG_RET(issue(1));
+  for (size_t c = 0; c < nchunk && c < (size_t)SLOTS; c++) IPG_RET(issue(c));
   for (size_t c = 0; c < nchunk; c++) {
-    CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[c & 1]));
+    CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[c % SLOTS]));
     const size_t off = c * PIN_CHUNK, len = std::min(PIN_CHUNK, bytes - off);
-    memcpy(static_cast<char*>(dst) + off, ctx->pinned[c & 1], len);
-    if (c + 2 < nchunk) IPG_RET(issue(c + 2));
+    ctx->copy_team->copy(static_cast<char*>(dst) + off, ctx->pinned[c % SLOTS], len);
+    if (c + SLOTS < nchunk) IPG_RET(issue(c + SLOTS));
   }
   return IPG_OK;
 }
@@ -175,15 +262,15 @@ int ipg_copy_h2d(ipg_ctx* ctx, void* dst, const void* src, size_t bytes) {
   IPG_RET(pinned_ring(ctx));
   const size_t nchunk = (bytes + PIN_CHUNK - 1) / PIN_CHUNK;
   for (size_t c = 0; c < nchunk; c++) {
-    if (c >= 2) CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[c & 1]));  // the slot's last DMA is done
+    if (c >= (size_t)SLOTS) CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[c % SLOTS]));  // slot's DMA done
     const size_t off = c * PIN_CHUNK, len = std::min(PIN_CHUNK, bytes - off);
-    memcpy(ctx->pinned[c & 1], static_cast<const char*>(src) + off, len);
-    CUDA_RET(ctx, cudaMemcpyAsync(static_cast<char*>(dst) + off, ctx->pinned[c & 1], len, cudaMemcpyHostToDevice,
-                                  ctx->stream));
-    CUDA_RET(ctx, cudaEventRecord(ctx->pinned_ev[c & 1], ctx->stream));
+    ctx->copy_team->copy(ctx->pinned[c % SLOTS], static_cast<const char*>(src) + off, len);
+    CUDA_RET(ctx, cudaMemcpyAsync(static_cast<char*>(dst) + off, ctx->pinned[c % SLOTS], len,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_RET(ctx, cudaEventRecord(ctx->pinned_ev[c % SLOTS], ctx->stream));
   }
   // the ring is reused by the next copy: wait until the DMAs out of it are done
-  for (int k = 0; k < 2 && k < (int)nchunk; k++) CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[k]));
+  for (int k = 0; k < SLOTS && k < (int)nchunk; k++) CUDA_RET(ctx, cudaEventSynchronize(ctx->pinned_ev[k]));
   return IPG_OK;
 }
 
@@ -335,6 +422,7 @@ int ipg_create(int device, ipg_ctx** out) {
   if (const char* e = getenv("IPG_PAIR_MINB")) ctx->pair_minb = std::max(3, std::min(5, atoi(e)));
   if (const char* e = getenv("IPG_WALK_SINGLE")) ctx->walk_single = e[0] != '0';
   if (const char* e = getenv("IPG_SIDE_STREAM")) ctx->side_enabled = e[0] != '0';
+  if (const char* e = getenv("IPG_COPY_THREADS")) ctx->copy_threads = std::max(1, std::min(64, atoi(e)));
   int dev0 = 0;
   cudaGetDevice(&dev0);
   if (cudaSetDevice(device) != cudaSuccess ||
@@ -368,7 +456,8 @@ int ipg_destroy(ipg_ctx* ctx) {
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
-  for (int k = 0; k < 2; k++) {
+  ipg_copy_team_free(ctx);
+  for (int k = 0; k < ipg_ctx::PIN_SLOTS; k++) {
     if (ctx->pinned[k]) cudaFreeHost(ctx->pinned[k]);
     if (ctx->pinned_ev[k]) cudaEventDestroy(ctx->pinned_ev[k]);
   }

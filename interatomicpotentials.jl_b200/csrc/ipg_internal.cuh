@@ -62,9 +62,12 @@ struct ipg_ctx {
   bool side_pending = false;
   bool side_enabled = true;  // IPG_SIDE_STREAM=0: everything on `stream`
   // pinned staging ring for large copies between device memory and the caller's pageable host
-  // buffers (ipg_copy_d2h / ipg_copy_h2d)
-  char* pinned[2] = {nullptr, nullptr};
-  cudaEvent_t pinned_ev[2] = {nullptr, nullptr};
+  // buffers (ipg_copy_d2h / ipg_copy_h2d), and the host threads that split each slot's memcpy
+  static constexpr int PIN_SLOTS = 4;
+  char* pinned[PIN_SLOTS] = {};
+  cudaEvent_t pinned_ev[PIN_SLOTS] = {};
+  struct HostCopyTeam* copy_team = nullptr;
+  int copy_threads = 0;  // threads per host memcpy, the caller included (0: chosen at first use)
 };
 
 // Runs the launches between ipg_side_begin and ipg_side_end on the side stream (ctx->stream
@@ -125,12 +128,14 @@ T* host_scratch(ipg_ctx* ctx, const char* name, size_t count) {
 }
 
 // Copies between device memory and a caller's (pageable) host buffer on ctx->stream.  Large
-// copies go through a ring of two pinned chunks, so the DMA of one chunk overlaps the host copy
-// of the other; a copy from pageable memory is staged by the driver at a fraction of the
-// bandwidth.  ipg_copy_d2h returns once `dst` holds the data (it synchronises with the stream);
+// copies go through a ring of four pinned chunks, so the DMAs of some chunks overlap the host
+// copy of another, and each chunk's host copy is split over a team of host threads; a copy
+// from pageable memory is staged by the driver at a fraction of the bandwidth.  ipg_copy_d2h returns once `dst` holds the data (it synchronises with the stream);
 // ipg_copy_h2d returns once `src` may be reused.
 int ipg_copy_d2h(ipg_ctx* ctx, void* dst, const void* src, size_t bytes);
 int ipg_copy_h2d(ipg_ctx* ctx, void* dst, const void* src, size_t bytes);
+// Joins the host copy threads (ipg_ctx_destroy).
+void ipg_copy_team_free(ipg_ctx* ctx);
 
 // Kernel launch with accounting and error check.
 #define IPG_LAUNCH(ctx, kernel, grid, block, smem, ...)                                          \
@@ -276,7 +281,7 @@ __device__ __forceinline__ int stencil_axis(int c, int nc, bool per, int* out) {
 // at most 9 rows of at most 3 ranges (usually 9 ranges in all).
 struct StencilRanges {
   int n;
-  int64_t beg[27], end[27];
+  int32_t beg[27], end[27];  // slots (every entry point keeps n below 2^31)
 };
 __device__ __forceinline__ void stencil_ranges(const ConfGrid& g, const int* c, const int64_t* __restrict__ cell_start,
                                                StencilRanges& R) {
@@ -299,8 +304,8 @@ __device__ __forceinline__ void stencil_ranges(const ConfGrid& g, const int* c, 
       while (d < nx) {
         int e = d;
         while (e + 1 < nx && sx[e + 1] == sx[e] + 1) e++;
-        R.beg[R.n] = cell_start[row + sx[d]];
-        R.end[R.n] = cell_start[row + sx[e] + 1];
+        R.beg[R.n] = (int32_t)cell_start[row + sx[d]];
+        R.end[R.n] = (int32_t)cell_start[row + sx[e] + 1];
         R.n++;
         d = e + 1;
       }

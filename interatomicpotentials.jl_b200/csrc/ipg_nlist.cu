@@ -293,15 +293,41 @@ __global__ void k_clamp_offsets(int64_t n, int64_t* __restrict__ off, int64_t ca
 }
 
 // The same walk with one warp per cell: every atom of a cell has the same stencil, so each
-// chunk of 32 candidates is loaded once and tested against every atom of the cell (their
-// positions, ids and output cursors staged in shared memory, read as broadcasts).  Each
-// atom's hits come out in the same order as from k_pair_walk.
+// chunk of 32 candidates is loaded once and tested against every atom of a group of up to 32
+// atoms of the cell, in two phases.  Phase 1 applies only the first test of pair_ok (the
+// periodic distance against the candidate radius, with the same arithmetic, so the same
+// decision; a separation of a box length or more is left to the full test), WALK_ILP atoms at
+// a time so that their independent FP64 chains overlap, and queues the (atom, candidate) pairs
+// that pass in (atom, lane) order in a per-warp ring.  Phase 2 runs the full pair_ok on 32
+// queued pairs at a time, one per lane, and emits the members after each atom's running count
+// (shared memory).  One test in eight passes: with the member path inside the chunk loop, the
+// few members of a chunk made every lane run it.  Each atom's hits come out in candidate order,
+// as from k_pair_walk.
 constexpr int WALKC_WARPS = 4;
+constexpr int WALK_ILP = 4;    // atoms per phase-1 step
+constexpr int WALK_RING = 256;  // queue entries per warp (a step adds at most 32 * WALK_ILP to fewer than 32)
 struct WalkAtom {
   double4 x;
   int64_t base, end;
-  int32_t i, pad;
+  int32_t i, cnt;  // atom id, hits so far
 };
+struct WalkQ {
+  int32_t slot, ii;  // candidate slot, group atom
+};
+
+// The first test of pair_ok: false only when pair_ok is false.  Branch-free: every term is
+// formed, and the flags are combined bitwise.
+__device__ __forceinline__ bool walk_prefilter(const PairTest& t, const double* L, int32_t i, double4 xi, int32_t j,
+                                               double4 xj) {
+  const bool other = t.mode == IPG_NLIST_HALF ? j > i : j != i;
+  // pe_axis_dev for |a - b| < L (an open axis has L = inf, where min(s1, inf) = s1)
+  const double s0 = fabs(__dsub_rn(xi.x, xj.x)), s1 = fabs(__dsub_rn(xi.y, xj.y)), s2 = fabs(__dsub_rn(xi.z, xj.z));
+  const bool far = !(s0 < L[0]) | !(s1 < L[1]) | !(s2 < L[2]);  // fmod case or NaN: full test
+  const double m0 = fmin(s0, __dsub_rn(L[0], s0)), m1 = fmin(s1, __dsub_rn(L[1], s1)),
+               m2 = fmin(s2, __dsub_rn(L[2], s2));
+  return other & (far | (sumsq3_dev(m0, m1, m2) <= t.rcut2_hi));
+}
+
 // WM 0: count each atom's hits into cnt (and their maximum into *maxcnt); 1: emit them at
 // off[i]..off[i+1]; 2: both at once, emitting into kcap padded slots per atom (i * kcap ..),
 // hits beyond kcap dropped (the count and *maxcnt still see them).
@@ -313,6 +339,7 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
     double* __restrict__ outr, int kcap, int* __restrict__ maxcnt) {
   constexpr bool EMIT = WM != 0;
   __shared__ WalkAtom sa[WALKC_WARPS][32];
+  __shared__ WalkQ sq[WALKC_WARPS][WALK_RING];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t c = (int64_t)blockIdx.x * WALKC_WARPS + w;
   if (c >= ncells) return;  // warp-uniform; the kernel synchronises only within a warp
@@ -328,58 +355,106 @@ __global__ void __launch_bounds__(WALKC_WARPS * 32) k_pair_walk_cells(
   stencil_ranges(g, cc, cell_start, R);
   const unsigned lt = (1u << lane) - 1u;
   WalkAtom* A = sa[w];
+  WalkQ* Q = sq[w];
   for (int64_t g0 = s0; g0 < s1; g0 += 32) {
     const int G = (int)((s1 - g0) < 32 ? (s1 - g0) : 32);
     __syncwarp();
     if (lane < G) {
       const int32_t i = cell_atoms[g0 + lane];
       A[lane].i = i;
+      A[lane].cnt = 0;
       A[lane].x = spos[g0 + lane];
       if (WM == 1) {
         A[lane].base = off[i];
         A[lane].end = off[i + 1];
-      } else if (WM == 2) {
+      } else {
         A[lane].base = (int64_t)i * kcap;
         A[lane].end = (int64_t)i * kcap + kcap;
       }
     }
     __syncwarp();
-    int64_t myk = 0;  // hits of atom `lane` of this group so far (lane ii owns atom ii's count)
-    for (int r = 0; r < R.n; r++)
-      for (int64_t q0 = R.beg[r]; q0 < R.end[r]; q0 += 32) {
-        const int64_t q = q0 + lane;
-        const bool inq = q < R.end[r];
-        int32_t j = 0;
-        double4 xj = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (inq) {
-          j = cell_atoms[q];
-          xj = spos[q];
-        }
-        for (int ii = 0; ii < G; ii++) {
-          const int32_t i = A[ii].i;
-          double rr[3];
-          const bool ok = inq && pair_ok(t, g.L, i, A[ii].x, j, xj, rr);
-          const unsigned bal = __ballot_sync(0xffffffffu, ok);
-          if (EMIT) {
-            const int64_t kk = __shfl_sync(0xffffffffu, myk, ii);
-            if (ok) {
-              const int64_t o = A[ii].base + kk + __popc(bal & lt);
-              if (o < A[ii].end) {  // a list cut at the capacity (capacity mode) drops its tail
-                outj[o] = j;
-                outr[3 * o] = rr[0];
-                outr[3 * o + 1] = rr[1];
-                outr[3 * o + 2] = rr[2];
-              }
-            }
+    // the (range, chunk, atoms) sequence flattened, so that phase 2 has one call site: each
+    // pass takes one step of phase 1, then drains full batches, and the remainder after the
+    // last step
+    int r = 0;
+    while (r < R.n && R.beg[r] >= R.end[r]) r++;
+    int64_t q0 = r < R.n ? R.beg[r] : 0, q = 0;
+    int ii = 0;
+    unsigned head = 0, tail = 0;  // ring positions (mod WALK_RING) of the first and next entries
+    bool inq = false;
+    int32_t j = 0;
+    double4 xj = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (;;) {
+      const bool more = r < R.n;  // warp-uniform
+      if (more) {
+        if (ii == 0) {  // a new chunk of candidates
+          q = q0 + lane;
+          inq = q < R.end[r];
+          if (inq) {
+            j = cell_atoms[q];
+            xj = spos[q];
           }
-          if (lane == ii) myk += __popc(bal);
+        }
+        bool cand[WALK_ILP];
+#pragma unroll
+        for (int k = 0; k < WALK_ILP; k++) {
+          const int a = ii + k < G ? ii + k : ii;
+          cand[k] = inq & (ii + k < G) & walk_prefilter(t, g.L, A[a].i, A[a].x, j, xj);
+        }
+#pragma unroll
+        for (int k = 0; k < WALK_ILP; k++) {
+          const unsigned bal = __ballot_sync(0xffffffffu, cand[k]);
+          if (cand[k]) Q[(tail + __popc(bal & lt)) % WALK_RING] = WalkQ{(int32_t)q, ii + k};
+          tail += __popc(bal);
+        }
+        ii += WALK_ILP;
+        if (ii >= G) {
+          ii = 0;
+          q0 += 32;
+          if (q0 >= R.end[r]) {
+            do r++;
+            while (r < R.n && R.beg[r] >= R.end[r]);
+            if (r < R.n) q0 = R.beg[r];
+          }
         }
       }
+      while (tail - head >= 32u || (!more && tail != head)) {  // phase 2 on the next m queued pairs
+        __syncwarp();
+        const int m = tail - head < 32u ? (int)(tail - head) : 32;
+        bool ok = false;
+        int e_ii = 0;
+        int32_t e_j = 0;
+        double rr[3];
+        if (lane < m) {
+          const WalkQ e = Q[(head + lane) % WALK_RING];
+          e_ii = e.ii;
+          e_j = cell_atoms[e.slot];
+          ok = pair_ok(t, g.L, A[e_ii].i, A[e_ii].x, e_j, spos[e.slot], rr);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        // lanes of the same atom: its members rank after the atom's running count
+        const unsigned grp = __match_any_sync(0xffffffffu, lane < m ? e_ii : 32 + lane);
+        if (EMIT && ok) {
+          const int64_t o = A[e_ii].base + A[e_ii].cnt + __popc(bal & grp & lt);
+          if (o < A[e_ii].end) {  // a list cut at the capacity (capacity mode) drops its tail
+            outj[o] = e_j;
+            outr[3 * o] = rr[0];
+            outr[3 * o + 1] = rr[1];
+            outr[3 * o + 2] = rr[2];
+          }
+        }
+        __syncwarp();
+        if (lane < m && (grp >> lane) == 1u) A[e_ii].cnt += __popc(bal & grp);  // the group's last lane
+        head += m;
+        __syncwarp();
+      }
+      if (!more) break;
+    }
     if (WM != 1) {
       int km = 0;
       if (lane < G) {
-        cnt[A[lane].i] = myk;
-        km = (int)myk;
+        km = A[lane].cnt;
+        cnt[A[lane].i] = km;
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) km = max(km, __shfl_xor_sync(0xffffffffu, km, o));

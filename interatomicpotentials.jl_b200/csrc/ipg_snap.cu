@@ -1375,7 +1375,6 @@ __global__ void __launch_bounds__(UTA_WARPS * 32) k_snap_utot_all(const __grid_c
       sw = sfac_of(S, r, rcut) * S.weight[sj];
     }
     st.first = p0 == beg;
-    st.nact = end - p0 < 32 ? (int)(end > p0 ? end - p0 : 0) : 32;
     snapchain::all_chains_utot<J>(a, b, sw, st);
   }
 }
@@ -1729,7 +1728,10 @@ __device__ __forceinline__ double yr_tile(const SnapDev& S, const YConst& T, con
 }
 
 // Tiles of a row of nma entries: at most YR_TILE wide, as even as possible.
-constexpr int YR_TILE = 5;  // widths 4, 5, 6 measured 1.80, 1.77, 1.86 ms at 54,000 atoms
+#ifndef IPG_YR_TILE
+#define IPG_YR_TILE 5  // widths 4, 5, 6 measured 1.80, 1.77, 1.86 ms at 54,000 atoms (eight warps)
+#endif
+constexpr int YR_TILE = IPG_YR_TILE;
 
 __device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, const YRowDev& row,
                                          const double2* __restrict__ usl, const double* __restrict__ yc,
@@ -1744,9 +1746,9 @@ __device__ __forceinline__ double yr_row(const SnapDev& S, const YConst& T, cons
     switch (w) {
 #define IPG_NT(NT) \
   case NT:         \
-    e += yr_tile<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout); \
+    if constexpr (NT <= YR_TILE) e += yr_tile<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout); \
     break;
-      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5)
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
 #undef IPG_NT
       default:
         break;
@@ -1800,9 +1802,9 @@ __device__ __forceinline__ void yr_row_z(const SnapDev& S, const YConst& T, cons
     switch (w) {
 #define IPG_NT(NT) \
   case NT:         \
-    yr_tile_z<NT>(S, T, row, ma0, nma, usl, cas, n, atom, valid, zout); \
+    if constexpr (NT <= YR_TILE) yr_tile_z<NT>(S, T, row, ma0, nma, usl, cas, n, atom, valid, zout); \
     break;
-      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5)
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
 #undef IPG_NT
       default:
         break;
@@ -1877,9 +1879,9 @@ __device__ __forceinline__ double yr_row_yz(const SnapDev& S, const YConst& T, c
     switch (w) {
 #define IPG_NT(NT) \
   case NT:         \
-    e += yr_tile_yz<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout, zout); \
+    if constexpr (NT <= YR_TILE) e += yr_tile_yz<NT>(S, T, row, ma0, nma, usl, yc, cas, n, atom, valid, yout, zout); \
     break;
-      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5)
+      IPG_NT(1) IPG_NT(2) IPG_NT(3) IPG_NT(4) IPG_NT(5) IPG_NT(6)
 #undef IPG_NT
       default:
         break;
@@ -2029,7 +2031,6 @@ __global__ void __launch_bounds__(VS_WARPS * 32) k_snap_vsum(const __grid_consta
       }
     }
     st.first = p0 == beg;
-    st.nact = end - p0 < 32 ? (int)(end > p0 ? end - p0 : 0) : 32;
     snapchain::all_chains_v<J>(G, A, Bk, st, vsh, NT, threadIdx.x);
   }
 }
@@ -3010,7 +3011,7 @@ struct ipg_snap {
   int64_t vjp_chunk = 0;     // atoms per Z chunk (0: about 4 GiB of Z)
   bool generic_plain = false;  // plain path: the per-atom block kernel (IPG_GENERIC_PLAIN=1)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
-  int yr_warps = 10;        // warps per block of the adjoint Y kernel (10, or 8)
+  int yr_warps = 12;        // warps per block of the adjoint Y kernel (8, 10, 12 or 16)
   std::vector<double> beta_host;  // last uploaded beta
   // last evaluation's pair count, cell grids and chunk table (host), for graph capture
   int64_t last_np = 0;
@@ -3433,12 +3434,15 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
         const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
         const bool withz = rows && out.zall;
-        const bool w10 = rows && !withz && s->yr_warps == 10;  // ten warps per block (IPG_YR_WARPS=8: eight)
-        const int ythreads = (w10 ? 10 : YS_WARPS) * 32;
-        const void* kfn = !rows ? (const void*)k_snap_yatoms
-                          : withz ? (const void*)k_snap_yrows<YM_YZ>
-                          : w10   ? (const void*)k_snap_yrows<YM_Y, 10>
-                                  : (const void*)k_snap_yrows<YM_Y>;
+        // warps per block of the Y-only kernel (IPG_YR_WARPS: 8, 10, 12 or 16)
+        const int yw = rows && !withz ? s->yr_warps : YS_WARPS;
+        const int ythreads = yw * 32;
+        const void* kfn = !rows       ? (const void*)k_snap_yatoms
+                          : withz     ? (const void*)k_snap_yrows<YM_YZ>
+                          : yw == 10  ? (const void*)k_snap_yrows<YM_Y, 10>
+                          : yw == 12  ? (const void*)k_snap_yrows<YM_Y, 12>
+                          : yw == 16  ? (const void*)k_snap_yrows<YM_Y, 16>
+                                      : (const void*)k_snap_yrows<YM_Y>;
         if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
         CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
         int per_sm = 1;
@@ -3449,8 +3453,14 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
           IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<YM_YZ>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst,
                            n, d_species, io.utot_in, yout, Ei, out.zall);
           if (out.zall_done) *out.zall_done = true;
-        } else if (w10)
+        } else if (rows && yw == 10)
           IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 10>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
+                           n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
+        else if (rows && yw == 12)
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 12>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
+                           n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
+        else if (rows && yw == 16)
+          IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 16>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
                            n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
         else if (rows)
           IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<YM_Y>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
@@ -3884,7 +3894,10 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
   if (const char* g = getenv("IPG_GENERIC_PLAIN")) s->generic_plain = g[0] == '1';
-  if (const char* g = getenv("IPG_YR_WARPS")) s->yr_warps = atoi(g) == 8 ? 8 : 10;
+  if (const char* g = getenv("IPG_YR_WARPS")) {
+    const int w = atoi(g);
+    s->yr_warps = (w == 8 || w == 10 || w == 16) ? w : 12;
+  }
   // cutoffs, utl.jl:41-56
   const int ns = p.nspecies;
   s->cutsq.assign(ns * ns, 0.0);

@@ -515,7 +515,6 @@ struct UtStage {
   double* ut;    // this atom's entry 0, as doubles; entry e at ut[2 e stride + c]
   int64_t stride = 1;
   int lane, nslot;
-  int nact = 32;  // lanes of this chunk that hold a neighbor (the others stage zeros)
   bool first;    // first chunk of neighbors: write (with wself on the diagonal), else add
   double wself;
   // packed destination: entry e | mirror e' << 12 | mirror sign << 24 | diagonal << 25 | has mirror << 26
@@ -534,9 +533,8 @@ struct UtStage {
     if (q < nslot) {
       const double* col = reinterpret_cast<const double*>(buf + q * 33) + c;
       double t4[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a shorter dependency chain
-      // the lanes past nact staged exact zeros: leaving them out changes no sum
-#pragma unroll 4
-      for (int k = 0; k < nact; k++) t4[k & 3] += col[2 * k];
+#pragma unroll
+      for (int k = 0; k < 32; k++) t4[k & 3] += col[2 * k];
       const double t = (t4[0] + t4[1]) + (t4[2] + t4[3]);
       const int pk = dst[q];
       const int e = pk & 0xfff;

@@ -483,10 +483,10 @@ def test_verlet_skin_reuse_checks_inputs():
         md.ctx.set_stream(None)
 
 
-@pytest.mark.parametrize("env", [dict(IPG_YR_WARPS="8")])
+@pytest.mark.parametrize("env", [dict(IPG_YR_WARPS="8"), dict(IPG_YR_WARPS="10"), dict(IPG_YR_WARPS="16")])
 def test_y_kernel_variants_agree(env, monkeypatch):
-    """The adjoint Y kernel with eight warps per block (the default has ten) gives the forces of
-    the default kernel to rounding and the oracle's to 1e-10."""
+    """The adjoint Y kernel with 8, 10 or 16 warps per block (the default has twelve) gives the
+    forces of the default kernel to rounding and the oracle's to 1e-10."""
     s, prm, beta = W.snap_j8(cells=6)
     ref, orc = make(prm, switch_flag=True)
     e0, f0, w0 = ref.energy_forces(s, beta, 0.1)
