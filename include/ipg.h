@@ -79,8 +79,10 @@ IPG_API int ipg_launch_count(const ipg_ctx* ctx, int64_t* out);
  * "snap_atom" (the Y kernel of the adjoint path, or the per-atom block kernel),
  * "snap_pair" (per-neighbor adjoint forces), "snap_gather" (force gather), "snap_zrows" (Z),
  * "snap_bdesc" (B), "snap_dbfused" (plain dB/dr), "snap_contract" (plain-path contraction),
- * "snap_vsum" and "snap_gbeta" (beta pullback), "snap_hvp" (the exact Hessian-vector product
- * of the position pullback).  Unknown names read as zero. */
+ * "snap_vsum" and "snap_gbeta" (beta pullback; "snap_vsum" also carries the Utot tangent of
+ * the position pullback), "snap_hvp" (the rest of the exact Hessian-vector product of the
+ * position pullback: the polarized Y evaluations and the second-order pair chains).  Unknown
+ * names read as zero. */
 IPG_API int ipg_timing_enable(ipg_ctx* ctx, int on);
 IPG_API int ipg_timing_read(ipg_ctx* ctx, const char* kernel, double* total_ms, int64_t* launches);
 
@@ -250,10 +252,14 @@ IPG_API int ipg_snap_vjp_beta(ipg_snap* snap, int64_t n, const double* pos, cons
  *   gbeta [nspecies][K] and gbeta0 as ipg_snap_vjp_beta, and
  *   gpos [3n] = d(gE E + gF . F)/dpos = -gE F - H gF    (H: Hessian of E).
  * Both terms are exact: F from one adjoint evaluation, H gF as the directional derivative of
- * the adjoint force computation along gF (forward-mode tangents through the Wigner recursion,
- * Utot, Z, Y and dE/dr; the second-order extension of compute_dij.jl:5-74), in one extra
- * kernel pass.  Any of gbeta, gbeta0, gpos may be NULL; beta [nspecies][K] is needed for gpos.
- * twojmax above 8 returns IPG_ERR_UNSUPPORTED for gpos (shared memory).  The reference
+ * the adjoint force computation along gF (the second-order extension of compute_dij.jl:5-74):
+ * the tangent of Utot (the beta pullback's V kernel), the tangent of Y by polarization of the
+ * quadratic form Y(Utot) (two Y evaluations at Utot +/- s Utot_dot, s a power of two; no
+ * truncation term), and forward-mode tangents through the Wigner recursion and dE/dr per pair.
+ * Environment IPG_GENERIC_HVP=1 at ipg_snap_create selects the per-atom kernel that carries
+ * every phase in forward mode instead (same results to rounding).  Any of gbeta, gbeta0, gpos
+ * may be NULL; beta [nspecies][K] is needed for gpos.  twojmax above 8 returns
+ * IPG_ERR_UNSUPPORTED for gpos.  The reference
  * defines no rrule; this is the pullback that Zygote / ChainRules callers of
  * energy_and_force(s, lbp) need.                                                          */
 IPG_API int ipg_snap_vjp(ipg_snap* snap, int64_t n, const double* pos, const int32_t* species, const double L[3],

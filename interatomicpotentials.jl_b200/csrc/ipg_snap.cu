@@ -2612,6 +2612,181 @@ int launch_pair_adj_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_
   }
 }
 
+// ---- exact Hessian-vector product on the register chains -------------------------------
+// The position pullback needs Hv, the tangent of the forces along a displacement v of the
+// atoms.  dE_i/dr_ij = 2 sum_h w Re(conj(D_k,h) Y_h), D_k = dsfac uhat_k U + sfac dU/dr_k,
+// depends on the pair geometry and on the centre atom's Y.  Its tangent along rdot = v_j - v_i
+// has a pair-local part (U, dU and the geometry along rdot: the second-order chain of
+// snapchain::all_chains_hvp) and a Y part (Ydot).  Y is a quadratic form in Utot, so
+// Ydot = [Y(U + s Udot) - Y(U - s Udot)] / (2s) exactly in exact arithmetic (the terms in s^2
+// cancel identically; no truncation term), with s a power of two per atom that gives U and
+// s Udot the same magnitude; Udot comes from k_snap_vsum (V with g = v is -Udot).
+
+// Per atom (one warp): s = 2^k with s max|Udot| ~ max|U| over the half plane, and the half
+// plane of U -/+ s V into Up / Um (full Utot layout; the Y kernel reads only these entries).
+// V holds the half plane up to the middle element of an even level; the entries beyond it are
+// the inversion-symmetric mirrors of entries of the same row (compute_ui.jl:105-125).
+__global__ void k_hvp_split(const __grid_constant__ SnapDev S, int64_t n, const double2* __restrict__ utot,
+                            const double2* __restrict__ V, double2* __restrict__ Up, double2* __restrict__ Um,
+                            double* __restrict__ scale) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;  // warp-uniform
+  const int U = S.idxu_max, UH = S.u_half;
+  auto vdot = [&](int h) -> double2 {  // Udot = -V, mirrored where V is not stored
+    int j = 0;
+    while (j < S.J && S.half_block[j + 1] <= h) j++;
+    const int e = h - S.half_block[j], mb = e / (j + 1), ma = e - mb * (j + 1);
+    if (2 * mb == j && ma > mb) {
+      const double2 m = V[(size_t)(S.half_block[j] + mb * (j + 1) + (j - ma)) * n + i];
+      const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+      return make_double2(-sg * m.x, sg * m.y);  // -( (-1)^(ma+mb) conj(m) )
+    }
+    const double2 v = V[(size_t)h * n + i];
+    return make_double2(-v.x, -v.y);
+  };
+  double mu = 0.0, mv = 0.0;
+  for (int h = lane; h < UH; h += 32) {
+    const double2 u = utot[(size_t)i * U + S.u_of_h[h]], d = vdot(h);
+    mu = fmax(mu, fmax(fabs(u.x), fabs(u.y)));
+    mv = fmax(mv, fmax(fabs(d.x), fabs(d.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = fmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+  }
+  int ex = 0;
+  if (mv > 0.0 && mu > 0.0) {  // s = 2^round(log2(mu / mv)), exact to multiply and divide by
+    int eu, ev;
+    frexp(mu, &eu);
+    frexp(mv, &ev);
+    ex = eu - ev;
+  }
+  const double s = ldexp(1.0, ex);
+  if (lane == 0) scale[i] = s;
+  for (int h = lane; h < UH; h += 32) {
+    const size_t e = (size_t)i * U + S.u_of_h[h];
+    const double2 u = utot[e], d = vdot(h);
+    Up[e] = make_double2(fma(s, d.x, u.x), fma(s, d.y, u.y));
+    Um[e] = make_double2(fma(-s, d.x, u.x), fma(-s, d.y, u.y));
+  }
+}
+
+// Ydot[h][i] = (Yp - Ym) / (2 s_i)
+__global__ void k_hvp_ydot(int64_t n, int uh, const double2* __restrict__ Yp, const double2* __restrict__ Ym,
+                           const double* __restrict__ scale, double2* __restrict__ Yd) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)uh * n) return;
+  const int64_t i = t % n;
+  const double f = 0.5 / scale[i];
+  const double2 a = Yp[t], b = Ym[t];
+  Yd[t] = make_double2((a.x - b.x) * f, (a.y - b.y) * f);
+}
+
+// fdot[p][k] = the tangent of dE_i/dr_ij[k] along v (one (pair, k) per thread, k = blockIdx.y):
+//   2 (cudot T0 + cu T2 + sfacdot T1 + sfac T3 + cu T4 + sfac T5),  cu = dsfac uhat_k,
+// T as in snapchain::all_chains_hvp.  Each block stages Y and Ydot of its pairs' few owner
+// atoms in shared memory, as k_snap_pair_adj_all does.
+constexpr int HVP_T = 128;
+constexpr int HVP_Y_ATOMS = 7;
+template <int J>
+__global__ void __launch_bounds__(HVP_T) k_snap_pair_hvp(const __grid_constant__ SnapDev S,
+                                                         const int64_t* __restrict__ d_np, int64_t natoms,
+                                                         const int32_t* __restrict__ owner,
+                                                         const int32_t* __restrict__ nbr,
+                                                         const double* __restrict__ rij,
+                                                         const int32_t* __restrict__ species,
+                                                         const double* __restrict__ v,
+                                                         const double2* __restrict__ Yw,
+                                                         const double2* __restrict__ Yd, double* __restrict__ fdot,
+                                                         int ystage) {
+  extern __shared__ double2 save[];  // [4 (J+1)][HVP_T], then Y and Ydot [2][u_half][HVP_Y_ATOMS]
+  const int64_t np = *d_np;
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
+  if (p0 >= np) return;  // block-uniform
+  const int k = blockIdx.y;
+  const int first = owner[p0];
+  const int nat = owner[(p0 + blockDim.x - 1 < np ? p0 + blockDim.x : np) - 1] - first + 1;
+  const bool staged = nat <= ystage;
+  double2* ysm = save + 4 * (J + 1) * HVP_T;
+  double2* ydm = ysm + S.u_half * HVP_Y_ATOMS;
+  if (staged) {
+    for (int idx = threadIdx.x; idx < S.u_half * nat; idx += blockDim.x) {
+      const int h = idx / nat, a = idx - h * nat;
+      ysm[h * HVP_Y_ATOMS + a] = Yw[(size_t)h * natoms + first + a];
+      ydm[h * HVP_Y_ATOMS + a] = Yd[(size_t)h * natoms + first + a];
+    }
+  }
+  __syncthreads();
+  if (p >= np) return;
+  const int i = owner[p];
+  const int32_t jn = nbr[p];
+  const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[jn], S.nsp);
+  const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+  PairGeomD PG;
+  geom_hvp(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], v[3 * jn] - v[3 * i], v[3 * jn + 1] - v[3 * i + 1],
+           v[3 * jn + 2] - v[3 * i + 2], rcut, S.weight[sj], PG);
+  snapchain::Geom2 G;
+  G.a = make_double2(PG.ar.v, PG.ai.v);
+  G.at = make_double2(PG.ar.t, PG.ai.t);
+  G.b = make_double2(PG.br.v, PG.bi.v);
+  G.bt = make_double2(PG.br.t, PG.bi.t);
+  Dual uk = PG.u[0];
+  G.da = make_double2(PG.dar[0].v, PG.dai[0].v);
+  G.dat = make_double2(PG.dar[0].t, PG.dai[0].t);
+  G.db = make_double2(PG.dbr[0].v, PG.dbi[0].v);
+  G.dbt = make_double2(PG.dbr[0].t, PG.dbi[0].t);
+#pragma unroll
+  for (int q = 1; q < 3; q++)  // direction k by selects (a runtime index would put PG in local memory)
+    if (q == k) {
+      uk = PG.u[q];
+      G.da = make_double2(PG.dar[q].v, PG.dai[q].v);
+      G.dat = make_double2(PG.dar[q].t, PG.dai[q].t);
+      G.db = make_double2(PG.dbr[q].v, PG.dbi[q].v);
+      G.dbt = make_double2(PG.dbr[q].t, PG.dbi[q].t);
+    }
+  double T[6];
+  if (staged)
+    snapchain::all_chains_hvp<J>(G, ysm + (i - first), ydm + (i - first), HVP_Y_ATOMS, T, save, HVP_T, threadIdx.x);
+  else
+    snapchain::all_chains_hvp<J>(G, Yw + i, Yd + i, natoms, T, save, HVP_T, threadIdx.x);
+  const double cu = PG.dsfac.v * uk.v, cut = PG.dsfac.t * uk.v + PG.dsfac.v * uk.t;
+  fdot[3 * p + k] = 2.0 * (cut * T[0] + cu * T[2] + PG.sfac.t * T[1] + PG.sfac.v * T[3] + cu * T[4] +
+                           PG.sfac.v * T[5]);
+}
+
+template <int J>
+int launch_pair_hvp_j(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms,
+                      const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species,
+                      const double* v, const double2* Yw, const double2* Yd, double* fdot) {
+  const size_t base = (size_t)4 * (J + 1) * HVP_T * sizeof(double2);
+  const size_t with_y = base + (size_t)2 * S.u_half * HVP_Y_ATOMS * sizeof(double2);
+  const int ystage = with_y <= 113 * 1024 ? HVP_Y_ATOMS : 0;  // two blocks per SM still fit
+  const size_t sm = ystage ? with_y : base;
+  if (sm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_pair_hvp<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const dim3 grid((unsigned)nblk(np, HVP_T), 3);
+  IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_snap_pair_hvp<J>, grid, HVP_T, sm, S, d_np, natoms, owner, nbr, rij, species,
+                   v, Yw, Yd, fdot, ystage);
+  return IPG_OK;
+}
+
+int launch_pair_hvp(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms,
+                    const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species,
+                    const double* v, const double2* Yw, const double2* Yd, double* fdot) {
+  if (np == 0) return IPG_OK;
+  switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_pair_hvp_j<JJ>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, v, Yw, Yd, fdot);
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
+  }
+}
+
 constexpr int PAIR_CHAIN_MAX_J = 10;  // twojmax handled by the register-chain kernel
 
 template <int J, int MB>
@@ -2728,7 +2903,7 @@ __global__ void k_snap_gather(int64_t n, const int64_t* __restrict__ off, const 
 // Per-configuration sums in fixed order: chunks of atoms (chunk table on the host:
 // config, first atom, end) are reduced by one block each, then the chunks of each
 // configuration are added in order: E[c] = beta0 + sum Ei, W6[c] = sum w6.
-constexpr int RED_CHUNK = 4096;
+constexpr int RED_CHUNK = 1024;
 __global__ void k_chunk_reduce(const int64_t* __restrict__ chunks, const double* __restrict__ Ei,
                                const double* __restrict__ w6, double* __restrict__ part) {
   __shared__ double sm[7][128];
@@ -2749,17 +2924,27 @@ __global__ void k_chunk_reduce(const int64_t* __restrict__ chunks, const double*
   if (threadIdx.x < 7) part[7 * blockIdx.x + threadIdx.x] = sm[threadIdx.x][0];
 }
 
-__global__ void k_conf_reduce(int nconf, const int64_t* __restrict__ conf_chunk, const double* __restrict__ part,
-                              const double* __restrict__ beta0p, double* __restrict__ E, double* __restrict__ W6) {
-  const double beta0 = *beta0p;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nconf) return;
+// One block of CONF_T threads per configuration: thread t sums chunks t, t + CONF_T, ... of
+// its configuration, then a fixed-order tree over the threads.
+constexpr int CONF_T = 64;
+__global__ void __launch_bounds__(CONF_T) k_conf_reduce(int nconf, const int64_t* __restrict__ conf_chunk,
+                                                        const double* __restrict__ part,
+                                                        const double* __restrict__ beta0p, double* __restrict__ E,
+                                                        double* __restrict__ W6) {
+  __shared__ double sm[7][CONF_T];
+  const int c = blockIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int64_t k = conf_chunk[c]; k < conf_chunk[c + 1]; k++)
+  for (int64_t k = conf_chunk[c] + threadIdx.x; k < conf_chunk[c + 1]; k += CONF_T)
     for (int q = 0; q < 7; q++) acc[q] += part[7 * k + q];
-  if (E) E[c] = beta0 + acc[0];
-  if (W6)
-    for (int q = 0; q < 6; q++) W6[6 * c + q] = acc[1 + q];
+  for (int q = 0; q < 7; q++) sm[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int o = CONF_T / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int q = 0; q < 7; q++) sm[q][threadIdx.x] += sm[q][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && E) E[c] = *beta0p + sm[0][0];
+  if (threadIdx.x < 6 && W6) W6[6 * c + threadIdx.x] = sm[1 + threadIdx.x][0];
 }
 
 // Per-atom force descriptors: dB_k[block s][b][c] = sum_{p in out(k), s_k = s} dbl_p -
@@ -2838,10 +3023,11 @@ __global__ void k_snap_fit_rows(int nconf, const int64_t* __restrict__ conf_off,
   }
 }
 
+// owner[p] = the centre atom of pair p: one warp per atom, lanes over its pairs (coalesced).
 __global__ void k_pair_owner(int64_t n, const int64_t* __restrict__ off, int32_t* __restrict__ owner) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;
-  for (int64_t p = off[i]; p < off[i + 1]; p++) owner[p] = (int32_t)i;
+  for (int64_t p = off[i] + (threadIdx.x & 31); p < off[i + 1]; p += 32) owner[p] = (int32_t)i;
 }
 
 // Virial descriptors W[block s][b][6] = sum over pairs of dB_i/dr_ij (x) (x_i - x_j)
@@ -3010,6 +3196,7 @@ struct ipg_snap {
   bool utot_split = false;  // Utot: one launch per chain (k_snap_utot) instead of k_snap_utot_all
   int64_t vjp_chunk = 0;     // atoms per Z chunk (0: about 4 GiB of Z)
   bool generic_plain = false;  // plain path: the per-atom block kernel (IPG_GENERIC_PLAIN=1)
+  bool generic_hvp = false;    // position pullback: the per-atom forward-mode kernel (IPG_GENERIC_HVP=1)
   int walk_warps = 4;       // atoms (warps) per block of the neighbor walk
   int yr_warps = 12;        // warps per block of the adjoint Y kernel (8, 10, 12 or 16)
   std::vector<double> beta_host;  // last uploaded beta
@@ -3286,6 +3473,7 @@ struct EvalOut {
   double* Aw = nullptr;  // [nconf][6][K*nsp] fitting virial rows (device)
   PairList* pl_out = nullptr;          // receives the pair list (stays valid until the next build)
   const double2** utot_out = nullptr;  // receives Utot [n][idxu_max] when the chain kernel made it
+  const double2** yw_out = nullptr;    // adjoint mode: receives the weighted Y [u_half][n] of the chain path
   double2* zall = nullptr;  // adjoint mode: also write Z [idxz_max][n] here (row-blocked Y kernel only)
   bool* zall_done = nullptr;  // set when zall was written
 };
@@ -3332,6 +3520,56 @@ int plain_chains(ipg_snap* s, const SnapDev& dev, int64_t n, const PairList& pl,
                      utot, B, Ei);
     IPG_RET(plain_fused(ctx, dev, a0, a0 + nc, pl.d_off, pl.d_j, pl.d_r, d_species, a0, nc, Z, dbl));
   }
+  return IPG_OK;
+}
+
+// The Y kernel on the Utot of n atoms (full layout [n][idxu_max]): yout = weighted Y
+// [u_half][n] and Ei = the energy of each atom; zall (optional) also receives Z (and
+// *zall_done is set).  *done stays false when neither atoms-in-lanes kernel fits (the caller
+// runs the generic per-atom kernel).  tname: the timing name of the launch.
+int launch_y(ipg_snap* s, const SnapDev& dev, const char* tname, int64_t n, const int32_t* d_species,
+             const double2* utot, double2* yout, double* Ei, double2* zall, bool* zall_done, bool* done) {
+  ipg_ctx* ctx = s->ctx;
+  *done = false;
+  size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
+  if (n == 0 || ysm > 200 * 1024) return IPG_OK;  // atoms-in-lanes: the Utot of 32 atoms in shared memory
+  const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
+  const bool withz = rows && zall;
+  // warps per block of the Y-only kernel (IPG_YR_WARPS: 8, 10, 12 or 16)
+  const int yw = rows && !withz ? s->yr_warps : YS_WARPS;
+  const int ythreads = yw * 32;
+  const void* kfn = !rows       ? (const void*)k_snap_yatoms
+                    : withz     ? (const void*)k_snap_yrows<YM_YZ>
+                    : yw == 10  ? (const void*)k_snap_yrows<YM_Y, 10>
+                    : yw == 12  ? (const void*)k_snap_yrows<YM_Y, 12>
+                    : yw == 16  ? (const void*)k_snap_yrows<YM_Y, 16>
+                                : (const void*)k_snap_yrows<YM_Y>;
+  if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
+  CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
+  int per_sm = 1;
+  CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, ythreads, ysm));
+  const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
+  const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
+  if (withz) {
+    IPG_TIMED_LAUNCH(ctx, tname, k_snap_yrows<YM_YZ>, (unsigned)grid, ythreads, ysm, dev, s->h.yconst, n, d_species,
+                     utot, yout, Ei, zall);
+    if (zall_done) *zall_done = true;
+  } else if (rows && yw == 10) {
+    IPG_TIMED_LAUNCH(ctx, tname, (k_snap_yrows<YM_Y, 10>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst, n,
+                     d_species, utot, yout, Ei, (double2*)nullptr);
+  } else if (rows && yw == 12) {
+    IPG_TIMED_LAUNCH(ctx, tname, (k_snap_yrows<YM_Y, 12>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst, n,
+                     d_species, utot, yout, Ei, (double2*)nullptr);
+  } else if (rows && yw == 16) {
+    IPG_TIMED_LAUNCH(ctx, tname, (k_snap_yrows<YM_Y, 16>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst, n,
+                     d_species, utot, yout, Ei, (double2*)nullptr);
+  } else if (rows) {
+    IPG_TIMED_LAUNCH(ctx, tname, k_snap_yrows<YM_Y>, (unsigned)grid, ythreads, ysm, dev, s->h.yconst, n, d_species,
+                     utot, yout, Ei, (double2*)nullptr);
+  } else {
+    IPG_TIMED_LAUNCH(ctx, tname, k_snap_yatoms, (unsigned)grid, ythreads, ysm, dev, n, d_species, utot, yout, Ei);
+  }
+  *done = true;
   return IPG_OK;
 }
 
@@ -3414,7 +3652,7 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
         IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
         IPG_RET(scratch(ctx, "snap_dbx", (size_t)np * K * 3 + 3, &dbl));
         if (n) {
-          IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
+          IPG_LAUNCH(ctx, k_pair_owner, nblk(32 * n, 256), 256, 0, n, pl.d_off, owner);
           IPG_LAUNCH(ctx, k_quad_pairs, nblk(np * KL, 256), 256, 0, np, pl.d_np, KL, K, owner, Bx, dlin, dbl);
         }
       }
@@ -3429,48 +3667,11 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
     IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np * nch + 3, &fvec));
     io.yout = yout;
     if (n) {
-      IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
-      size_t ysm = (size_t)dev.u_half * YS_ATOMS * sizeof(double2);
-      if (ysm <= 200 * 1024) {  // atoms-in-lanes Y kernel (Utot of 32 atoms in shared memory)
-        const bool rows = dev.J <= YR_MAX_J && !s->y_entries && s->h.yconst_ok;
-        const bool withz = rows && out.zall;
-        // warps per block of the Y-only kernel (IPG_YR_WARPS: 8, 10, 12 or 16)
-        const int yw = rows && !withz ? s->yr_warps : YS_WARPS;
-        const int ythreads = yw * 32;
-        const void* kfn = !rows       ? (const void*)k_snap_yatoms
-                          : withz     ? (const void*)k_snap_yrows<YM_YZ>
-                          : yw == 10  ? (const void*)k_snap_yrows<YM_Y, 10>
-                          : yw == 12  ? (const void*)k_snap_yrows<YM_Y, 12>
-                          : yw == 16  ? (const void*)k_snap_yrows<YM_Y, 16>
-                                      : (const void*)k_snap_yrows<YM_Y>;
-        if (rows) ysm = yr_smem(dev.J, dev.nsp, dev.n_ytrip, dev.n_yca, dev.u_half, dev.n_yrows).total();
-        CUDA_RET(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysm));
-        int per_sm = 1;
-        CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, ythreads, ysm));
-        const int64_t groups = (n + YS_ATOMS - 1) / YS_ATOMS;
-        const int64_t grid = std::min<int64_t>(groups, (int64_t)ctx->num_sms * std::max(1, per_sm));
-        if (withz) {
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<YM_YZ>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst,
-                           n, d_species, io.utot_in, yout, Ei, out.zall);
-          if (out.zall_done) *out.zall_done = true;
-        } else if (rows && yw == 10)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 10>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
-                           n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
-        else if (rows && yw == 12)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 12>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
-                           n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
-        else if (rows && yw == 16)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", (k_snap_yrows<YM_Y, 16>), (unsigned)grid, ythreads, ysm, dev, s->h.yconst,
-                           n, d_species, io.utot_in, yout, Ei, (double2*)nullptr);
-        else if (rows)
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yrows<YM_Y>, (unsigned)grid, YS_WARPS * 32, ysm, dev, s->h.yconst, n,
-                           d_species, io.utot_in, yout, Ei, (double2*)nullptr);
-        else
-          IPG_TIMED_LAUNCH(ctx, "snap_atom", k_snap_yatoms, (unsigned)grid, YS_WARPS * 32, ysm, dev, n, d_species,
-                           io.utot_in, yout, Ei);
-      } else {
-        IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
-      }
+      IPG_LAUNCH(ctx, k_pair_owner, nblk(32 * n, 256), 256, 0, n, pl.d_off, owner);
+      bool ydone = false;
+      IPG_RET(launch_y(s, dev, "snap_atom", n, d_species, io.utot_in, yout, Ei, out.zall, out.zall_done, &ydone));
+      if (!ydone) IPG_RET(launch_atoms<MODE_ADJY>(s, dev, io, n, nullptr));
+      if (out.yw_out) *out.yw_out = yout;
       if (s->pair_split)
         IPG_RET(launch_pair_adj(ctx, dev, np, pl.d_np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
       else
@@ -3548,12 +3749,13 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
                                     ctx->stream));
     d_cc = d_ch + ch.size();
     IPG_LAUNCH(ctx, k_chunk_reduce, (unsigned)nchunk, 128, 0, d_ch, Ei, w6, part);
-    IPG_LAUNCH(ctx, k_conf_reduce, nblk(nconf, 128), 128, 0, nconf, d_cc, part, dev.beta0, out.E, out.W6);
+    if (nconf > 0)
+      IPG_LAUNCH(ctx, k_conf_reduce, (unsigned)nconf, CONF_T, 0, nconf, d_cc, part, dev.beta0, out.E, out.W6);
   }
   if (out.dB && n) {
     int32_t* owner;
     IPG_RET(scratch(ctx, "snap_owner", (size_t)np + 1, &owner));
-    IPG_LAUNCH(ctx, k_pair_owner, nblk(n, 256), 256, 0, n, pl.d_off, owner);
+    IPG_LAUNCH(ctx, k_pair_owner, nblk(32 * n, 256), 256, 0, n, pl.d_off, owner);
     IPG_LAUNCH(ctx, k_snap_dB_atoms, nblk(n * 3 * K, 128), 128, 0, n, K, nsp, pl.d_off, pl.d_in_off, pl.d_in_pair,
                owner, d_species, dbl, out.dB, out.dB_rows ? 1 : 0);
   }
@@ -3894,6 +4096,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));
   if (const char* g = getenv("IPG_GENERIC_PLAIN")) s->generic_plain = g[0] == '1';
+  if (const char* g = getenv("IPG_GENERIC_HVP")) s->generic_hvp = g[0] == '1';
   if (const char* g = getenv("IPG_YR_WARPS")) {
     const int w = atoi(g);
     s->yr_warps = (w == 8 || w == 10 || w == 16) ? w : 12;
@@ -4244,39 +4447,71 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
   o.F = F0;
   PairList pl;
   o.pl_out = &pl;
+  const double2 *utot = nullptr, *yw = nullptr;
+  o.utot_out = &utot;
+  o.yw_out = &yw;
   IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, o));
   if (gF) {
-    // H gF: the tangent of the forces along gF, exact (k_snap_hvp, second-order adjoint)
+    // H gF: the tangent of the forces along gF, exact
     SnapDev dev = s->dev;
     if (dev.chem || dev.quadratic)
       return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "the position pullback of chem_flag / quadratic SNAP is not built");
     IPG_RET(set_beta(s, beta, 0.0, dev));
-    const int nw = 8;
-    const HvpSmem HL = hvp_smem(dev, nw);
-    if (HL.total > 227 * 1024)
-      return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "twojmax %d: the position pullback needs %zu bytes of shared memory",
-                      dev.J, HL.total);
-    double *d_v, *fv, *fd;
+    double *d_v, *fd;
     IPG_RET(scratch(ctx, "vjp_v", m, &d_v));
     IPG_RET(scratch(ctx, "vjp_Fdot", m, &Fd));
-    IPG_RET(scratch(ctx, "vjp_fvec", 3 * (size_t)pl.npairs + 3, &fv));
     IPG_RET(scratch(ctx, "vjp_fdot", 3 * (size_t)pl.npairs + 3, &fd));
     IPG_RET(ipg_copy_h2d(ctx, d_v, gF, sizeof(double) * m));
-    SnapIO io;
-    memset(&io, 0, sizeof(io));
-    io.n = n;
-    io.off = pl.d_off;
-    io.nbr = pl.d_j;
-    io.rij = pl.d_r;
-    io.species = d_sp;
-    io.fvec = fv;
-    io.status = ctx->d_status;
-    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_hvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HL.total));
-    int per_sm = 1;
-    CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_hvp, nw * 32, HL.total));
-    const int64_t grid = std::min<int64_t>(n, (int64_t)ctx->num_sms * std::max(1, per_sm));
-    IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_snap_hvp, (unsigned)grid, nw * 32, HL.total, dev, io, d_v, fd);
     IPG_RET(ipg_side_join(ctx));
+    if (utot && yw && dev.J <= YR_MAX_J && !s->generic_hvp) {
+      // register chains: Udot (k_snap_vsum), Ydot by polarization (two Y launches), the
+      // second-order pair chains (k_snap_pair_hvp)
+      const int U = dev.idxu_max, UH = dev.u_half;
+      double2 *V, *Up, *Um, *Yp, *Ym, *Yd;
+      double *sc, *ebuf;
+      int32_t* owner;
+      IPG_RET(scratch(ctx, "hvp_V", (size_t)UH * n + 1, &V));
+      IPG_RET(scratch(ctx, "hvp_Up", (size_t)U * n + 1, &Up));
+      IPG_RET(scratch(ctx, "hvp_Um", (size_t)U * n + 1, &Um));
+      IPG_RET(scratch(ctx, "hvp_Yp", (size_t)UH * n + 1, &Yp));
+      IPG_RET(scratch(ctx, "hvp_Ym", (size_t)UH * n + 1, &Ym));
+      IPG_RET(scratch(ctx, "hvp_Yd", (size_t)UH * n + 1, &Yd));
+      IPG_RET(scratch(ctx, "hvp_scale", (size_t)n, &sc));
+      IPG_RET(scratch(ctx, "hvp_E", (size_t)n, &ebuf));
+      IPG_RET(scratch(ctx, "snap_owner", (size_t)pl.npairs + 1, &owner));
+      IPG_RET(launch_vsum(ctx, dev, 0, n, pl.d_off, pl.d_j, pl.d_r, d_sp, d_v, V));
+      IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_hvp_split, nblk(32 * n, 256), 256, 0, dev, n, utot, V, Up, Um, sc);
+      bool d1 = false, d2 = false;
+      IPG_RET(launch_y(s, dev, "snap_hvp", n, d_sp, Up, Yp, ebuf, nullptr, nullptr, &d1));
+      IPG_RET(launch_y(s, dev, "snap_hvp", n, d_sp, Um, Ym, ebuf, nullptr, nullptr, &d2));
+      if (!d1 || !d2) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "position pullback: no atoms-in-lanes Y kernel");
+      IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_hvp_ydot, nblk((int64_t)UH * n, 256), 256, 0, n, UH, Yp, Ym, sc, Yd);
+      IPG_LAUNCH(ctx, k_pair_owner, nblk(32 * n, 256), 256, 0, n, pl.d_off, owner);
+      IPG_RET(launch_pair_hvp(ctx, dev, pl.npairs, pl.d_np, n, owner, pl.d_j, pl.d_r, d_sp, d_v, yw, Yd, fd));
+    } else {
+      // one block per atom, every phase in forward mode (k_snap_hvp)
+      const int nw = 8;
+      const HvpSmem HL = hvp_smem(dev, nw);
+      if (HL.total > 227 * 1024)
+        return ipg_fail(ctx, IPG_ERR_UNSUPPORTED,
+                        "twojmax %d: the position pullback needs %zu bytes of shared memory", dev.J, HL.total);
+      double* fv;
+      IPG_RET(scratch(ctx, "vjp_fvec", 3 * (size_t)pl.npairs + 3, &fv));
+      SnapIO io;
+      memset(&io, 0, sizeof(io));
+      io.n = n;
+      io.off = pl.d_off;
+      io.nbr = pl.d_j;
+      io.rij = pl.d_r;
+      io.species = d_sp;
+      io.fvec = fv;
+      io.status = ctx->d_status;
+      CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_hvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HL.total));
+      int per_sm = 1;
+      CUDA_RET(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_hvp, nw * 32, HL.total));
+      const int64_t grid = std::min<int64_t>(n, (int64_t)ctx->num_sms * std::max(1, per_sm));
+      IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_snap_hvp, (unsigned)grid, nw * 32, HL.total, dev, io, d_v, fd);
+    }
     IPG_LAUNCH(ctx, k_snap_gather, nblk(n, 128), 128, 0, n, pl.d_off, pl.d_j, pl.d_in_off, pl.d_in_pair, fd, 1,
                d_pos, Fd, (double*)nullptr);
   }

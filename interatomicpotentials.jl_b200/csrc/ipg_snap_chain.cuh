@@ -747,3 +747,169 @@ __device__ __forceinline__ void all_chains_rows(const Geom& G, Emit& emit, doubl
 }
 
 }  // namespace snapchain
+
+namespace snapchain {
+
+// ---- second order: the tangent of dE_i/dr_ij[k] along a displacement ---------------------
+// One (pair, direction k) per thread.  With a dot the derivative along the pair's displacement
+// tangent rdot = v_j - v_i, the chain carries U, Udot, dU = dU/dr_k and its tangent dUdot:
+//   U_j     = f(a, b, U)
+//   Udot_j  = f(adot, bdot, U) + f(a, b, Udot)
+//   dU_j    = f(da, db, U) + f(a, b, dU)
+//   dUdot_j = f(dadot, dbdot, U) + f(da, db, Udot) + f(adot, bdot, dU) + f(a, b, dUdot)
+// with f(A, B, u)[ma] = -rootpq[ma][j-mb] conj(B) u[ma-1] + rootpq[j-ma][j-mb] conj(A) u[ma]
+// (the product rule on the recursion of compute_ui.jl:66-101, 224-267), and contracts them
+// with the weighted Y of the centre atom and its tangent Ydot:
+//   T[0] = sum Re(conj(U) Y),    T[1] = sum Re(conj(dU) Y),    T[2] = sum Re(conj(Udot) Y),
+//   T[3] = sum Re(conj(dUdot) Y), T[4] = sum Re(conj(U) Ydot), T[5] = sum Re(conj(dU) Ydot).
+template <int J>
+struct Chain2 {
+  double2 u[J + 1], ut[J + 1], d[J + 1], dt[J + 1];
+};
+struct Geom2 {
+  double2 a, at, b, bt, da, dat, db, dbt;
+};
+
+__device__ __forceinline__ void cmac(double2 A, double2 v, double2& acc) {  // acc += conj(A) v
+  acc.x = fma(A.x, v.x, fma(A.y, v.y, acc.x));
+  acc.y = fma(A.x, v.y, fma(-A.y, v.x, acc.y));
+}
+__device__ __forceinline__ double2 scl(double r, double2 v) { return make_double2(r * v.x, r * v.y); }
+
+template <int J, int j>
+__device__ __forceinline__ void advance2(Chain2<J>& s, const Geom2& G, int mb) {
+  const int col = j - mb;
+#pragma unroll
+  for (int ma = j; ma >= 0; --ma) {
+    double2 nu = make_double2(0.0, 0.0), nut = nu, nd = nu, ndt = nu;
+    if (ma > 0) {  // - rootpq[ma][j-mb] conj(B) u[ma-1]
+      const double rp = -c_rpq[ma * RPQ_STRIDE + col];
+      const double2 B = scl(rp, G.b), Bt = scl(rp, G.bt), dB = scl(rp, G.db), dBt = scl(rp, G.dbt);
+      const double2 v = s.u[ma - 1], vt = s.ut[ma - 1], dv = s.d[ma - 1], dvt = s.dt[ma - 1];
+      cmac(B, v, nu);
+      cmac(Bt, v, nut);
+      cmac(B, vt, nut);
+      cmac(dB, v, nd);
+      cmac(B, dv, nd);
+      cmac(dBt, v, ndt);
+      cmac(dB, vt, ndt);
+      cmac(Bt, dv, ndt);
+      cmac(B, dvt, ndt);
+    }
+    if (ma < j) {  // + rootpq[j-ma][j-mb] conj(A) u[ma]
+      const double rp = c_rpq[(j - ma) * RPQ_STRIDE + col];
+      const double2 A = scl(rp, G.a), At = scl(rp, G.at), dA = scl(rp, G.da), dAt = scl(rp, G.dat);
+      const double2 v = s.u[ma], vt = s.ut[ma], dv = s.d[ma], dvt = s.dt[ma];
+      cmac(A, v, nu);
+      cmac(At, v, nut);
+      cmac(A, vt, nut);
+      cmac(dA, v, nd);
+      cmac(A, dv, nd);
+      cmac(dAt, v, ndt);
+      cmac(dA, vt, ndt);
+      cmac(At, dv, ndt);
+      cmac(A, dvt, ndt);
+    }
+    s.u[ma] = nu;
+    s.ut[ma] = nut;
+    s.d[ma] = nd;
+    s.dt[ma] = ndt;
+  }
+}
+
+// Yw / Yd point at the centre atom's entry of h = 0 in [h][atom] arrays of stride ys.
+template <int J, int j>
+__device__ __forceinline__ void contract2(const Chain2<J>& s, const double2* __restrict__ Yw,
+                                          const double2* __restrict__ Yd, int64_t ys, int mb, double (&T)[6]) {
+  const int last = (2 * mb == j) ? mb : j;  // middle row of an even level stops at ma = j/2
+  const int64_t h0 = half_block(j) + mb * (j + 1);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > last) break;
+    const double2 y = Yw[(h0 + ma) * ys], yd = Yd[(h0 + ma) * ys];
+    T[0] = fma(s.u[ma].x, y.x, fma(s.u[ma].y, y.y, T[0]));
+    T[1] = fma(s.d[ma].x, y.x, fma(s.d[ma].y, y.y, T[1]));
+    T[2] = fma(s.ut[ma].x, y.x, fma(s.ut[ma].y, y.y, T[2]));
+    T[3] = fma(s.dt[ma].x, y.x, fma(s.dt[ma].y, y.y, T[3]));
+    T[4] = fma(s.u[ma].x, yd.x, fma(s.u[ma].y, yd.y, T[4]));
+    T[5] = fma(s.d[ma].x, yd.x, fma(s.d[ma].y, yd.y, T[5]));
+  }
+}
+
+// Chain mb+1 starts from the mirror of chain mb's row at level 2mb+1 (inversion symmetry,
+// compute_ui.jl:105-125), saved as save[(comp (J+1) + c) nt + tid].
+template <int J, int j>
+__device__ __forceinline__ void save_mirror2(const Chain2<J>& s, double2* __restrict__ save, int nt, int tid) {
+  constexpr int R = (j + 1) / 2;
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+    const double2 src[4] = {s.u[j - c], s.ut[j - c], s.d[j - c], s.dt[j - c]};
+#pragma unroll
+    for (int q = 0; q < 4; q++) save[(q * (J + 1) + c) * nt + tid] = make_double2(sg * src[q].x, -sg * src[q].y);
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void load_row2(Chain2<J>& s, const double2* __restrict__ save, int nt, int tid, int count) {
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    if (c >= count) break;
+    s.u[c] = save[(0 * (J + 1) + c) * nt + tid];
+    s.ut[c] = save[(1 * (J + 1) + c) * nt + tid];
+    s.d[c] = save[(2 * (J + 1) + c) * nt + tid];
+    s.dt[c] = save[(3 * (J + 1) + c) * nt + tid];
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level2(Chain2<J>& s, const Geom2& G, const double2* __restrict__ Yw,
+                                       const double2* __restrict__ Yd, int64_t ys, int mb, double (&T)[6],
+                                       double2* save, int nt, int tid) {
+  if constexpr (j <= J) {
+    advance2<J, j>(s, G, mb);
+    contract2<J, j>(s, Yw, Yd, ys, mb, T);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2)
+      if (j == 2 * mb + 1) save_mirror2<J, j>(s, save, nt, tid);
+  }
+}
+
+// All chains of one (pair, direction): every half-plane entry once (runtime-row level code, as
+// all_chains_adjoint).
+template <int J>
+__device__ __forceinline__ void all_chains_hvp(const Geom2& G, const double2* __restrict__ Yw,
+                                               const double2* __restrict__ Yd, int64_t ys, double (&T)[6],
+                                               double2* save, int nt, int tid) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
+  Chain2<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+    s.ut[c] = s.u[c];
+    s.d[c] = s.u[c];
+    s.dt[c] = s.u[c];
+  }
+  s.u[0] = make_double2(1.0, 0.0);  // level 0: U = 1, every derivative and tangent 0
+#pragma unroll
+  for (int q = 0; q < 6; q++) T[q] = 0.0;
+  contract2<J, 0>(s, Yw, Yd, ys, 0, T);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+      asm volatile("" ::: "memory");  // this chain's loads stay after the previous chain's saves
+      load_row2<J>(s, save, nt, tid, 2 * mb);  // row mb of level 2mb-1
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {  // chain mb runs levels 2mb (1 for chain 0) .. J
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level2<J, JJ>(s, G, Yw, Yd, ys, mb, T, save, nt, tid);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
+}
+
+}  // namespace snapchain

@@ -154,3 +154,24 @@ def test_torch_autograd(case):
     l_ref, g_ref = snap.batch_loss_grad(systems, beta, Fref)
     assert abs(lval.item() - l_ref) <= 1e-14 * l_ref
     assert rel_err(bl.grad.numpy(), g_ref) <= 1e-14
+
+
+@pytest.mark.parametrize("J", [2, 5, 8])
+def test_chain_hvp_matches_forward_mode_kernel(J, monkeypatch):
+    """The register-chain Hessian-vector product (Udot by k_snap_vsum, Ydot by polarization of
+    the quadratic Y, the second-order pair chains) equals the per-atom forward-mode kernel
+    (IPG_GENERIC_HVP=1) to rounding, at twojmax 2, 5 and 8."""
+    rng = np.random.default_rng(70 + J)
+    n = 90
+    pos = rng.uniform(0, 10.0, (n, 3))
+    sym = list(np.where(rng.random(n) < 0.5, "A", "B"))
+    s = ipg.System(pos, sym, [10.0] * 3)
+    args = (1, J, ["A", "B"], 2.2, 0.0, 0.97, [1.0, 0.8], [1.0, 0.6])
+    fast = ipg.SNAP(*args, switch_flag=True)
+    monkeypatch.setenv("IPG_GENERIC_HVP", "1")
+    slow = ipg.SNAP(*args, switch_flag=True)
+    beta = rng.normal(0, 1e-2, (2, len(fast)))
+    gF = rng.normal(size=(n, 3))
+    _, _, g1 = fast.vjp(s, beta, 0.25, gF)
+    _, _, g2 = slow.vjp(s, beta, 0.25, gF)
+    assert rel_err(g1, g2) <= 1e-12, rel_err(g1, g2)
