@@ -50,7 +50,7 @@ KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot_all<8>",
 # DRAM bytes (read + write) per atom of one launch, from the ncu --set full captures on the
 # 16,000-atom case summarised in profiles/k_snap_{yrows,pair_adj_all,utot_all}_snap_j8.md;
 # scaled by atoms (pairs per atom are the same).
-NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (52.024064e6 + 2.487296e6) / 16000,
+NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.886336e6 + 2.899200e6) / 16000,
                            "snap_pair": (52.742144e6 + 0.953088e6) / 16000,
                            "snap_utot": (11.558912e6 + 16.316928e6) / 16000}
 
@@ -267,7 +267,7 @@ def main():
     # per-kernel device timing (ipg_timing_read names); snap_zrows .. snap_gbeta are the plain,
     # descriptor and pullback kernels of the register-chain path
     TIMED_KERNELS = ("snap_atom", "snap_utot", "snap_pair", "snap_gather", "snap_contract", "neighbor", "pair_eval",
-                     "snap_zrows", "snap_bdesc", "snap_dbfused", "snap_vsum", "snap_gbeta", "snap_hvp")
+                     "snap_zrows", "snap_bdesc", "snap_dbfused", "snap_vsum", "snap_gbeta", "snap_hvp", "snap_hvp_y")
 
     def timed(fn, steps, kernel_timing=False):
         for _ in range(args.warmup):
@@ -482,6 +482,11 @@ def main():
                 pair[name]["hbm"] = {"algorithmic_bytes": nbytes, "kernel_ms": k_ms, "achieved_GBps": gbps,
                                      "peak_GBps": HBM_PEAK, "frac": gbps / HBM_PEAK if gbps else None,
                                      "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+                # what bounds it instead: the ncu counters of k_pair_half<3> on the 1 M-atom
+                # case of the same lattice (profiles/k_pair_half_lc_1m.md)
+                pair[name]["ncu_pipes"] = {"kernel": "k_pair_half<3>", "fp64_pipe_pct": 19.7, "issue_active_pct": 40.2,
+                                           "dram_pct_of_peak": 1.05, "bound": "FP64 latency (wait stalls)",
+                                           "source": "profiles/k_pair_half_lc_1m.md"}
         line["lj_pairs_per_s"] = pair
 
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -3787,7 +3787,8 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
 
 int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
                     const int64_t* h_atom_off, const double* h_L, const double* beta, double gE, const double* d_g,
-                    double* d_gbeta, const PairList* reuse_pl, const double2* reuse_utot, const double2* reuse_Z);
+                    double* d_gbeta, const PairList* reuse_pl, const double2* reuse_utot, const double2* reuse_Z,
+                    const double2** v_out = nullptr);
 
 // Graph mode of a whole force-matching training step (snap_train_step).
 constexpr int MODE_TRAIN = 100;
@@ -4284,9 +4285,13 @@ namespace {
 // reuse_pl / reuse_utot: the pair list and Utot of an evaluation of the same positions just
 // before (snap_eval's pl_out / utot_out), or null to build them here.
 // reuse_Z: Z [idxz_max][n] of the same positions (k_snap_yrows<YM_YZ>), or null to form it here.
+// v_out (optional): receives V [u_half][n] (V = sum_j (g_i - g_j) . d(sfac U_ij)/dr_ij) when the
+// chain path formed it in one chunk, else null.
 int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_species, int nconf,
                     const int64_t* h_atom_off, const double* h_L, const double* beta, double gE, const double* d_g,
-                    double* d_gbeta, const PairList* reuse_pl, const double2* reuse_utot, const double2* reuse_Z) {
+                    double* d_gbeta, const PairList* reuse_pl, const double2* reuse_utot, const double2* reuse_Z,
+                    const double2** v_out) {
+  if (v_out) *v_out = nullptr;
   ipg_ctx* ctx = s->ctx;
   SnapDev dev = s->dev;
   if (dev.chem || dev.quadratic) {
@@ -4371,6 +4376,7 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
       rows += gg;
     }
     IPG_LAUNCH(ctx, k_sum_partials, nblk((int64_t)nsp * K, 128), 128, 0, rows, nsp * K, gpart, d_gbeta, 0.0);
+    if (v_out && nchunk == 1) *v_out = V;
     return IPG_OK;
   }
   int threads = s->threads;
@@ -4428,7 +4434,12 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
   IPG_RET(check_common(s, n, pos, species, L));
   ipg_ctx* ctx = s->ctx;
   if (gpos && !beta) return ipg_fail(ctx, IPG_ERR_ARG, "the position pullback needs beta");
-  if (gbeta) IPG_RET(ipg_snap_vjp_beta(s, n, pos, species, L, gE, gF, gbeta, nullptr));
+  const SnapDev& d0 = s->dev;
+  // both pullbacks from one evaluation: its list, Utot and Z (Y kernel in its Y+Z mode) serve
+  // the beta pullback, whose V (gF contracted with dU/dr) is the Utot tangent of H gF
+  const bool fused = gbeta && gpos && gF && n > 0 && !d0.chem && !d0.quadratic && d0.J <= YR_MAX_J &&
+                     !s->generic_adjoint && !s->y_entries && s->h.yconst_ok && !s->generic_hvp;
+  if (gbeta && !fused) IPG_RET(ipg_snap_vjp_beta(s, n, pos, species, L, gE, gF, gbeta, nullptr));
   if (gbeta0) *gbeta0 = gE;
   if (!gpos || n == 0) return IPG_OK;
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
@@ -4447,10 +4458,20 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
   o.F = F0;
   PairList pl;
   o.pl_out = &pl;
-  const double2 *utot = nullptr, *yw = nullptr;
+  const double2 *utot = nullptr, *yw = nullptr, *Vg = nullptr;
   o.utot_out = &utot;
   o.yw_out = &yw;
+  double2* Z = nullptr;
+  bool zdone = false;
+  double* d_gb = nullptr;
+  if (fused) {
+    IPG_RET(scratch(ctx, "vjp_Z", (size_t)d0.idxz_max * n + 1, &Z));
+    IPG_RET(scratch(ctx, "snap_vjp_gb", (size_t)d0.nsp * d0.K, &d_gb));
+    o.zall = Z;
+    o.zall_done = &zdone;
+  }
   IPG_RET(snap_eval(s, n, d_pos, d_sp, 1, aoff, L, beta, 0.0, MODE_ADJ, o));
+  if (fused && !(zdone && utot && yw)) return ipg_fail(ctx, IPG_ERR_CUDA, "position pullback: evaluation without Z");
   if (gF) {
     // H gF: the tangent of the forces along gF, exact
     SnapDev dev = s->dev;
@@ -4463,6 +4484,10 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
     IPG_RET(scratch(ctx, "vjp_fdot", 3 * (size_t)pl.npairs + 3, &fd));
     IPG_RET(ipg_copy_h2d(ctx, d_v, gF, sizeof(double) * m));
     IPG_RET(ipg_side_join(ctx));
+    if (fused) {
+      IPG_RET(snap_vjp_device(s, n, d_pos, d_sp, 1, aoff, L, beta, gE, d_v, d_gb, &pl, utot, Z, &Vg));
+      IPG_RET(set_beta(s, beta, 0.0, dev));
+    }
     if (utot && yw && dev.J <= YR_MAX_J && !s->generic_hvp) {
       // register chains: Udot (k_snap_vsum), Ydot by polarization (two Y launches), the
       // second-order pair chains (k_snap_pair_hvp)
@@ -4479,11 +4504,14 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
       IPG_RET(scratch(ctx, "hvp_scale", (size_t)n, &sc));
       IPG_RET(scratch(ctx, "hvp_E", (size_t)n, &ebuf));
       IPG_RET(scratch(ctx, "snap_owner", (size_t)pl.npairs + 1, &owner));
-      IPG_RET(launch_vsum(ctx, dev, 0, n, pl.d_off, pl.d_j, pl.d_r, d_sp, d_v, V));
+      if (Vg)
+        V = const_cast<double2*>(Vg);
+      else
+        IPG_RET(launch_vsum(ctx, dev, 0, n, pl.d_off, pl.d_j, pl.d_r, d_sp, d_v, V));
       IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_hvp_split, nblk(32 * n, 256), 256, 0, dev, n, utot, V, Up, Um, sc);
       bool d1 = false, d2 = false;
-      IPG_RET(launch_y(s, dev, "snap_hvp", n, d_sp, Up, Yp, ebuf, nullptr, nullptr, &d1));
-      IPG_RET(launch_y(s, dev, "snap_hvp", n, d_sp, Um, Ym, ebuf, nullptr, nullptr, &d2));
+      IPG_RET(launch_y(s, dev, "snap_hvp_y", n, d_sp, Up, Yp, ebuf, nullptr, nullptr, &d1));
+      IPG_RET(launch_y(s, dev, "snap_hvp_y", n, d_sp, Um, Ym, ebuf, nullptr, nullptr, &d2));
       if (!d1 || !d2) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "position pullback: no atoms-in-lanes Y kernel");
       IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_hvp_ydot, nblk((int64_t)UH * n, 256), 256, 0, n, UH, Yp, Ym, sc, Yd);
       IPG_LAUNCH(ctx, k_pair_owner, nblk(32 * n, 256), 256, 0, n, pl.d_off, owner);
@@ -4516,6 +4544,8 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
                d_pos, Fd, (double*)nullptr);
   }
   IPG_LAUNCH(ctx, k_vjp_pos, nblk((int64_t)m, 256), 256, 0, (int64_t)m, F0, gE, Fd, gp);
+  if (fused)
+    CUDA_RET(ctx, cudaMemcpyAsync(gbeta, d_gb, sizeof(double) * d0.nsp * d0.K, cudaMemcpyDeviceToHost, ctx->stream));
   IPG_RET(ipg_copy_d2h(ctx, gpos, gp, sizeof(double) * m));
   return ipg_status_check(ctx, "ipg_snap_vjp");
 }
