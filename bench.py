@@ -198,7 +198,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="size of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and pair-workload lines")
-    ap.add_argument("--extras", default="skin,batch,plain,vjp,desc,pair",
+    ap.add_argument("--extras", default="skin,batch,plain,vjp,desc,pair,j6",
                     help="comma list of the extra measurements to run (skin, batch, plain, vjp, desc, pair)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-tune", action="store_true", help="skip the (untimed) autotuner and use the default kernel "
@@ -390,6 +390,9 @@ def main():
         ms_be, _, _ = timed(lambda: db.evaluate(beta_b, 0.0, graph=False), max(2, args.steps // 5))
         db.evaluate(beta_b, 0.0, graph=True)  # capture (untimed)
         ms_bg, _, _ = timed(lambda: db.evaluate(beta_b, 0.0, graph=True), max(2, args.steps // 5))
+        # the plain dB/dr path on the same batch (eager: its fused dB/dr kernel sizes its chunks
+        # from the exact pair count, which graph capture does not read back)
+        ms_bp, _, _ = timed(lambda: db.evaluate(beta_b, 0.0, mode="plain", graph=False), max(2, args.steps // 5))
         Fref_b = np.asarray(db.F.cpu().numpy()) * 1.01
         ms_bl, _, _ = timed(lambda: snap.batch_loss_grad(systems_b, beta_b, Fref_b), 2)
         ctx.set_stream(stream.cuda_stream)
@@ -405,6 +408,8 @@ def main():
         line["batch512"] = {"n_configs": len(systems_b), "n_atoms": nb_atoms,
                             "eager_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_be * 1e-3),
                             "graph_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_bg * 1e-3),
+                            "plain_eager_atom_steps_per_s": world * nb_atoms * max(2, args.steps // 5) / (ms_bp * 1e-3),
+                            "adjoint_over_plain_eager": ms_bp / ms_be, "adjoint_graph_over_plain_eager": ms_bp / ms_bg,
                             "ef_graph_ms": ms_bg / max(2, args.steps // 5),
                             "loss_grad_ms": ms_bl / 2,
                             "train_step_eager_ms": ms_te / nts, "train_step_graph_ms": ms_tg / nts,
@@ -448,6 +453,30 @@ def main():
         line["descriptors"] = {"ms_per_call": ms_d / max(2, args.steps // 5),
                                "kernel_ms_per_call": {k: v[0] / max(2, args.steps // 5) for k, v in ktd.items()
                                                       if v[1]}}
+    if "j6" in extras:
+        # SNAP single species, twojmax 6, 8,192 atoms (BCC 16^3, rcut 4.7 A): plain dB/dr path (the
+        # reference's route) and the adjoint path, device buffers, neighbor build included
+        s6, p6, b6 = W.snap_j6()
+        snap6 = ipg.SNAP(len(s6), p6["twojmax"], p6["species"], p6["rcutfac"], p6["rmin0"], p6["rfac0"], p6["radii"],
+                         p6["weight"], switch_flag=True, ctx=ctx)
+        n6 = len(s6)
+        b6b = snap6.beta_blocks(b6)
+        p6_d = torch.tensor(s6.positions, device=dev)
+        sp6_d = torch.tensor(snap6.species_ids(s6), device=dev)
+        F6_d = torch.zeros((n6, 3), dtype=torch.float64, device=dev)
+        L6 = s6.L
+
+        def step6(mode):
+            ctx.check(lib().ipg_snap_energy_forces_dev(snap6.handle, n6, vp(p6_d.data_ptr()), vp(sp6_d.data_ptr()),
+                                                       L6.ctypes.data_as(vp), b6b.ctypes.data_as(vp), 0.0, mode,
+                                                       vp(E_d.data_ptr()), vp(F6_d.data_ptr()), vp(W_d.data_ptr())))
+        k6 = max(2, args.steps // 2)
+        ms6p, _, _ = timed(lambda: step6(SNAP_PLAIN), k6)
+        ms6a, _, _ = timed(lambda: step6(SNAP_ADJOINT), k6)
+        line["snap_j6"] = {"n_atoms": n6, "twojmax": 6, "plain_atom_steps_per_s": world * n6 * k6 / (ms6p * 1e-3),
+                           "adjoint_atom_steps_per_s": world * n6 * k6 / (ms6a * 1e-3),
+                           "plain_ms_per_step": ms6p / k6, "adjoint_ms_per_step": ms6a / k6}
+        del snap6
     if "pair" in extras:
         pair = {}
         for name, (s2, p2) in (("lj1000", W.lj1000()), ("lc32000", W.lc32000()), ("lc_scaled", W.lc32000(cells=args.pair_cells))):
@@ -472,6 +501,18 @@ def main():
             term_pairs = pairs * len(terms)
             pair[name] = {"pairs_per_s": world * term_pairs * psteps / (ms_p * 1e-3), "ms_per_step":
                           ms_p / psteps, "n_atoms": len(s2), "half_pairs": pairs, "terms": len(terms)}
+            if len(s2) < 1_000_000:
+                # the same step as one CUDA-graph replay (IPG_PAIR_GRAPH: an MD loop with fixed
+                # buffers); the first call captures, outside the timed steps
+                def pstep_graph():
+                    ctx.check(lib().ipg_pair_eval_dev(ctx.handle, len(s2), vp(p_d.data_ptr()), vp(s_d.data_ptr()),
+                                                      L2.ctypes.data_as(vp), C.cast(arr, vp), len(terms),
+                                                      vp(E_d.data_ptr()), vp(f_d.data_ptr()), vp(W_d.data_ptr()),
+                                                      7 | 8))
+                pstep_graph()
+                ms_g, _, _ = timed(pstep_graph, psteps)
+                pair[name]["graph_pairs_per_s"] = world * term_pairs * psteps / (ms_g * 1e-3)
+                pair[name]["graph_ms_per_step"] = ms_g / psteps
             if name == "lc_scaled":
                 # HBM roofline of the pair path: algorithmic bytes per step = positions (24 B),
                 # species (4 B) and forces (24 B) per atom; no pair list is materialised.  The

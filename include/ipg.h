@@ -142,6 +142,12 @@ typedef struct ipg_pair_term {
 #define IPG_WANT_E 1u
 #define IPG_WANT_F 2u
 #define IPG_WANT_W 4u
+/* ipg_pair_eval_dev only: replay a CUDA graph of the whole evaluation (cell list, pair
+ * tiles, gather, reductions).  The first call with a given (n, L, terms, device buffers,
+ * flags) runs eagerly and captures the graph; later calls with the same key upload the cell
+ * grid and launch the graph once (an MD loop's step with fixed buffers).  Open boxes
+ * (L = inf) and failed captures run eagerly.  Results are those of the eager call. */
+#define IPG_PAIR_GRAPH 8u
 
 /* energy_and_force / potential_energy / force / virial_stress for an EmpiricalPotential
  * or a LinearCombinationPotential (empirical_potential.jl:49-77,

@@ -457,6 +457,8 @@ int ipg_destroy(ipg_ctx* ctx) {
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   ipg_copy_team_free(ctx);
+  for (auto& g : ctx->pair_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (int k = 0; k < ipg_ctx::PIN_SLOTS; k++) {
     if (ctx->pinned[k]) cudaFreeHost(ctx->pinned[k]);
     if (ctx->pinned_ev[k]) cudaEventDestroy(ctx->pinned_ev[k]);

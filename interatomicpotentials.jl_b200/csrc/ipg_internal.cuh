@@ -68,7 +68,23 @@ struct ipg_ctx {
   cudaEvent_t pinned_ev[PIN_SLOTS] = {};
   struct HostCopyTeam* copy_team = nullptr;
   int copy_threads = 0;  // threads per host memcpy, the caller included (0: chosen at first use)
+  // CUDA graphs of ipg_pair_eval_dev (IPG_PAIR_GRAPH), keyed by the call's inputs
+  struct PairGraph {
+    int64_t n = 0;
+    double L[3] = {0, 0, 0};
+    const void *pos = nullptr, *sp = nullptr, *E = nullptr, *F = nullptr, *W6 = nullptr;
+    uint32_t flags = 0;
+    std::vector<char> terms;        // the ipg_pair_term array, bytewise
+    std::vector<char> grid;         // the cell grid (ConfGrid) the replay uploads
+    int full_stencil = 0, minb = 0;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t gen = 0;               // scratch generation at capture
+  };
+  std::vector<PairGraph> pair_graphs;
+  int64_t pair_graph_replays = 0;
 };
+
+constexpr int IPG_ERR_NOT_CAPTURED = 1;  // internal: no CUDA graph for this key (not an API code)
 
 // Runs the launches between ipg_side_begin and ipg_side_end on the side stream (ctx->stream
 // points at it meanwhile), after everything already on the main stream; ipg_side_join makes

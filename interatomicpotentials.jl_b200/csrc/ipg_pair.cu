@@ -384,13 +384,14 @@ int prepare_terms(ipg_ctx* ctx, const ipg_pair_term* terms, int nterms, PairTerm
 
 int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
                      const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
-                     uint32_t flags) {
+                     uint32_t flags, std::vector<ConfGrid>* grid_out = nullptr) {
   PairTerms pt;
   IPG_RET(prepare_terms(ctx, terms, nterms, pt));
   IPG_RET(ipg_status_reset(ctx));
   int64_t aoff[2] = {0, n};
   CellList cl;
   IPG_RET(ipg_build_cells(ctx, "pair_", n, d_pos, d_species, 64, 1, aoff, L, pt.rcut_max, cl));
+  if (grid_out) *grid_out = cl.h_grid;
   const ConfGrid& g = cl.h_grid[0];
   bool half = n > 0 && !ctx->pair_full_stencil;
   for (int a = 0; a < 3; a++) half &= std::isinf(g.L[a]) || g.nc[a] >= 3;
@@ -428,6 +429,88 @@ int pair_eval_device(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t
   IPG_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, nb, 7, partial, (flags & IPG_WANT_E) ? d_E : nullptr,
              (flags & IPG_WANT_W) ? d_W6 : nullptr);
   return IPG_OK;
+}
+
+// ---- CUDA graphs of the device evaluation (IPG_PAIR_GRAPH) --------------------------------
+ipg_ctx::PairGraph* pair_graph_find(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species,
+                                    const double L[3], const ipg_pair_term* terms, int32_t nterms,
+                                    const double* d_E, const double* d_F, const double* d_W6, uint32_t flags) {
+  const size_t tb = sizeof(ipg_pair_term) * (size_t)nterms;
+  for (auto& g : ctx->pair_graphs)
+    if (g.n == n && g.L[0] == L[0] && g.L[1] == L[1] && g.L[2] == L[2] && g.pos == d_pos && g.sp == d_species &&
+        g.E == d_E && g.F == d_F && g.W6 == d_W6 && g.flags == flags && g.terms.size() == tb &&
+        memcmp(g.terms.data(), terms, tb) == 0 && g.full_stencil == (int)ctx->pair_full_stencil &&
+        g.minb == ctx->pair_minb)
+      return &g;
+  return nullptr;
+}
+
+// Uploads the cell grid the graph reads and launches it; IPG_ERR_NOT_CAPTURED when there is
+// no usable graph (none for this key, or a scratch buffer moved since the capture).
+int pair_graph_replay(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
+                      const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
+                      uint32_t flags) {
+  ipg_ctx::PairGraph* g = pair_graph_find(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags);
+  if (!g) return IPG_ERR_NOT_CAPTURED;
+  ConfGrid* d_grid = nullptr;
+  if (g->gen == ctx->scratch_gen) IPG_RET(scratch(ctx, "pair_grid", 1, &d_grid));
+  if (g->gen != ctx->scratch_gen) {
+    cudaGraphExecDestroy(g->exec);
+    ctx->pair_graphs.erase(ctx->pair_graphs.begin() + (g - ctx->pair_graphs.data()));
+    return IPG_ERR_NOT_CAPTURED;
+  }
+  CUDA_RET(ctx, cudaMemcpyAsync(d_grid, g->grid.data(), g->grid.size(), cudaMemcpyHostToDevice, ctx->stream));
+  IPG_RET(ipg_status_reset(ctx));
+  CUDA_RET(ctx, cudaGraphLaunch(g->exec, ctx->stream));
+  ctx->pair_graph_replays++;
+  return ipg_status_check(ctx, "ipg_pair_eval_dev (graph)");
+}
+
+// Captures the evaluation just run eagerly with the same inputs (every scratch buffer already
+// has its size).  A failure only means that later calls run eagerly.
+void pair_graph_capture(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_t* d_species, const double L[3],
+                        const ipg_pair_term* terms, int32_t nterms, double* d_E, double* d_F, double* d_W6,
+                        uint32_t flags) {
+  if (ctx->pair_graphs.size() >= 8) {
+    cudaGraphExecDestroy(ctx->pair_graphs.front().exec);
+    ctx->pair_graphs.erase(ctx->pair_graphs.begin());
+  }
+  ipg_ctx::PairGraph g;
+  g.n = n;
+  for (int a = 0; a < 3; a++) g.L[a] = L[a];
+  g.pos = d_pos;
+  g.sp = d_species;
+  g.E = d_E;
+  g.F = d_F;
+  g.W6 = d_W6;
+  g.flags = flags;
+  g.terms.assign(reinterpret_cast<const char*>(terms), reinterpret_cast<const char*>(terms) + sizeof(ipg_pair_term) * nterms);
+  g.full_stencil = ctx->pair_full_stencil;
+  g.minb = ctx->pair_minb;
+  const uint64_t gen0 = ctx->scratch_gen;
+  std::vector<ConfGrid> grid;
+  const bool timing = ctx->timing;
+  ctx->timing = false;
+  ctx->capturing = true;
+  cudaGraph_t graph = nullptr;
+  int st = IPG_OK;
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    st = IPG_ERR_CUDA;
+  } else {
+    st = pair_eval_device(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags, &grid);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st == IPG_OK && e != cudaSuccess) st = IPG_ERR_CUDA;
+  }
+  ctx->capturing = false;
+  ctx->timing = timing;
+  if (st == IPG_OK && graph && ctx->scratch_gen == gen0 && grid.size() == 1 &&
+      cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess) {
+    g.grid.assign(reinterpret_cast<const char*>(grid.data()), reinterpret_cast<const char*>(grid.data() + 1));
+    g.gen = ctx->scratch_gen;
+    ctx->pair_graphs.push_back(std::move(g));
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // a failed capture leaves no sticky error behind
 }
 
 int check_pair_args(ipg_ctx* ctx, int64_t n, const void* pos, const void* species, const double* L,
@@ -479,8 +562,16 @@ int ipg_pair_eval_dev(ipg_ctx* ctx, int64_t n, const double* d_pos, const int32_
                       uint32_t flags) {
   IPG_RET(check_pair_args(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags));
   CUDA_RET(ctx, cudaSetDevice(ctx->device));
+  const bool want_graph = (flags & IPG_PAIR_GRAPH) && n > 0 && !std::isinf(L[0]) && !std::isinf(L[1]) &&
+                          !std::isinf(L[2]);
+  flags &= IPG_WANT_E | IPG_WANT_F | IPG_WANT_W;
+  if (want_graph) {
+    const int st = pair_graph_replay(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags);
+    if (st != IPG_ERR_NOT_CAPTURED) return st;
+  }
   IPG_RET(pair_eval_device(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags));
   IPG_RET(ipg_status_check(ctx, "ipg_pair_eval_dev"));
+  if (want_graph) pair_graph_capture(ctx, n, d_pos, d_species, L, terms, nterms, d_E, d_F, d_W6, flags);
   return IPG_OK;
 }
 

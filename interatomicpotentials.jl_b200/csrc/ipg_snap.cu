@@ -3838,7 +3838,6 @@ int snap_train_step(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
 }
 
 // ---- CUDA-graph replay of batched evaluations -------------------------------------------
-constexpr int IPG_ERR_NOT_CAPTURED = 1;  // internal: no graph for this key (not an API code)
 
 // The device buffers of a force-matching training step (MODE_TRAIN graphs).
 struct TrainBufs {

@@ -20,6 +20,7 @@ STATUS = {
 
 PAIR_KIND = {"LJ": 1, "BM": 2, "COUL": 3, "MORSE": 4, "ZBL": 5, "MOCK_R2": 6}
 WANT_E, WANT_F, WANT_W = 1, 2, 4
+PAIR_GRAPH = 8  # ipg_pair_eval_dev: replay a CUDA graph of the evaluation
 DESC_B, DESC_DB, DESC_W = 1, 2, 4
 NLIST_HALF, NLIST_FULL, NLIST_LITERAL_SQRT = 0, 1, 0x100
 SNAP_PLAIN, SNAP_ADJOINT = 0, 1

@@ -190,3 +190,52 @@ def test_half_and_full_stencil_paths(case, full, monkeypatch):
     assert abs(e - eo) <= TOL * max(abs(eo), 1e-300), (e, eo)
     assert rel_err(f, fo) <= TOL
     assert rel_err(w, wo) <= TOL
+
+
+def test_dev_graph_replay():
+    """IPG_PAIR_GRAPH: the first call captures, later calls with the same buffers replay one
+    graph (no library launches) and give the eager results bit for bit, also after the
+    positions change in place; another box length captures anew."""
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    s, p = W.lc32000(cells=8)
+    ctx = ipg.Context(0)
+    idx = {sym: k for k, sym in enumerate(s.unique_symbols())}
+    terms = ipg.empirical.empirical_terms(p)
+    arr = (ipg._lib.PairTerm * len(terms))()
+    for q, (c, pp) in enumerate(terms):
+        arr[q] = pp.term(idx, c)
+    n = len(s)
+    pos = torch.tensor(s.positions, device="cuda")
+    sp = torch.tensor(np.array([idx[x] for x in s.symbols], np.int32), device="cuda")
+    out = [torch.zeros(k, dtype=torch.float64, device="cuda") for k in (1, 3 * n, 6)]
+    vp = C.c_void_p
+
+    def call(L, flags):
+        ctx.check(ipg._lib.lib().ipg_pair_eval_dev(ctx.handle, n, vp(pos.data_ptr()), vp(sp.data_ptr()),
+                                                   L.ctypes.data_as(vp), C.cast(arr, vp), len(terms),
+                                                   vp(out[0].data_ptr()), vp(out[1].data_ptr()),
+                                                   vp(out[2].data_ptr()), flags))
+        torch.cuda.synchronize()
+        return [t.cpu().numpy().copy() for t in out]
+
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        L = s.L.copy()
+        ref = call(L, 7)
+        call(L, 7 | 8)  # eager + capture
+        for step in range(3):
+            l0 = ctx.launch_count()
+            got = call(L, 7 | 8)
+            assert ctx.launch_count() == l0  # one graph launch, no library kernel launches
+            for a, b in zip(got, ref):
+                assert np.array_equal(a, b)
+            pos.add_(torch.tensor(np.random.default_rng(step).normal(0, 0.02, (n, 3)), device="cuda"))
+            ref = call(L, 7)
+        L2 = L * 1.01
+        r2 = call(L2, 7)
+        call(L2, 7 | 8)
+        l0 = ctx.launch_count()
+        assert all(np.array_equal(a, b) for a, b in zip(call(L2, 7 | 8), r2)) and ctx.launch_count() == l0
+    finally:
+        ctx.set_stream(None)
