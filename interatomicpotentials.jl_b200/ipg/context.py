@@ -3,6 +3,7 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import weakref
 
 from ._lib import check, lib
 
@@ -15,6 +16,13 @@ class Context:
         check(lib().ipg_create(int(device), C.byref(h)))
         self._h = h
         self.device = device
+        # handles created on this context (SNAP objects): closed before the context itself, so
+        # that finalizers running in any order (a reference cycle collected at exit) never
+        # reach a destroyed context
+        self._dependents = weakref.WeakSet()
+
+    def _register(self, obj):
+        self._dependents.add(obj)
 
     @property
     def handle(self):
@@ -45,6 +53,8 @@ class Context:
 
     def close(self):
         if getattr(self, "_h", None):
+            for d in list(getattr(self, "_dependents", ())):
+                d.close()
             lib().ipg_destroy(self._h)
             self._h = None
 

@@ -81,6 +81,7 @@ class SNAP:
         h = C.c_void_p()
         self.ctx.check(lib().ipg_snap_create(self.ctx.handle, C.byref(p), C.byref(h)))
         self._h = h
+        self.ctx._register(self)
         K = C.c_int32()
         self.ctx.check(lib().ipg_snap_ncoeff(h, C.byref(K)))
         self.K = K.value
@@ -108,7 +109,8 @@ class SNAP:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().ipg_snap_destroy(self._h)
+            if getattr(self.ctx, "_h", None):  # a closed context has closed its SNAP handles
+                lib().ipg_snap_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -121,3 +121,37 @@ def test_flop_counts_consistent():
     from ipg import flops as F
     assert F.snap_atom_kernel(8, 1, 26, "plain") > F.snap_atom_kernel(8, 1, 26, "adjoint") > 0
     assert F.z_atom(8) > F.z_atom(6)
+
+
+def test_context_closes_its_snap_handles_first(monkeypatch):
+    """Finalizers of a context and its SNAP objects may run in any order (a reference cycle
+    collected at exit): closing the context closes the SNAP handles first, and a SNAP whose
+    context is gone does not call into the library."""
+    import weakref
+    import ipg.context as ctxmod
+    import ipg.snap as snapmod
+    calls = []
+
+    class FakeLib:
+        def ipg_destroy(self, h):
+            calls.append(("ctx", h))
+
+        def ipg_snap_destroy(self, h):
+            calls.append(("snap", h))
+
+    monkeypatch.setattr(ctxmod, "lib", lambda: FakeLib())
+    monkeypatch.setattr(snapmod, "lib", lambda: FakeLib())
+    ctx = object.__new__(ctxmod.Context)  # no device here: only the handle bookkeeping
+    ctx._h, ctx._dependents = "c", weakref.WeakSet()
+    snap = object.__new__(snapmod.SNAP)
+    snap._h, snap.ctx = "s", ctx
+    ctx._register(snap)
+    ctx.close()
+    assert calls == [("snap", "s"), ("ctx", "c")]
+    snap.close()  # already closed: nothing more
+    ctx2 = object.__new__(ctxmod.Context)
+    ctx2._h, ctx2._dependents = None, weakref.WeakSet()  # a context finalized first
+    snap2 = object.__new__(snapmod.SNAP)
+    snap2._h, snap2.ctx = "s2", ctx2
+    snap2.close()
+    assert calls == [("snap", "s"), ("ctx", "c")] and snap2._h is None
