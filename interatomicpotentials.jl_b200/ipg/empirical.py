@@ -225,7 +225,7 @@ def pair_eval(system, terms, flags=WANT_E | WANT_F | WANT_W, ctx=None):
     idx = _symbol_index(system)
     if len(idx) > 64:
         raise ValueError("at most 64 distinct species")
-    sp = np.ascontiguousarray([idx[s] for s in system.symbols], dtype=np.int32)
+    sp = system.species_index(list(idx))
     arr = (PairTerm * max(1, len(terms)))()
     for k, (c, p) in enumerate(terms):
         arr[k] = p.term(idx, c)

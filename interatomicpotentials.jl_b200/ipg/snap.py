@@ -101,9 +101,8 @@ class SNAP:
 
     def species_ids(self, system):
         """0-based species ids of the system's atoms, by their position in snap.species."""
-        lut = {s: k for k, s in enumerate(self.species)}
         try:
-            return np.fromiter((lut[s] for s in system.symbols), dtype=np.int32, count=len(system.symbols))
+            return system.species_index(self.species)
         except KeyError as e:
             raise ValueError(f"system has a species not in snap.species: {e}") from None
 

@@ -14,7 +14,7 @@ class System:
         """positions: (n, 3); symbols: n atomic symbols (str) or ints; box: 3 lengths or a
         3x3 matrix of which only the diagonal is used; periodic: 3 booleans."""
         self.positions = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
-        self.symbols = list(symbols)
+        self.symbols = tuple(symbols)  # immutable, so that the per-species index below can be cached
         if len(self.symbols) != len(self.positions):
             raise ValueError("one symbol per atom is required")
         b = np.asarray(box, dtype=np.float64)
@@ -33,11 +33,24 @@ class System:
         return list(self.symbols)
 
     def unique_symbols(self):
-        seen = []
-        for s in self.symbols:
-            if s not in seen:
-                seen.append(s)
-        return seen
+        """The distinct symbols in order of first appearance."""
+        u = getattr(self, "_unique", None)
+        if u is None:
+            u = self._unique = list(dict.fromkeys(self.symbols))
+        return list(u)
+
+    def species_index(self, species):
+        """int32 index of each atom's symbol in `species` (KeyError for a symbol not in it),
+        computed once per species list."""
+        key = tuple(species)
+        cache = self.__dict__.setdefault("_species_index", {})
+        arr = cache.get(key)
+        if arr is None:
+            lut = {s: k for k, s in enumerate(key)}
+            arr = np.fromiter((lut[s] for s in self.symbols), dtype=np.int32, count=len(self.symbols))
+            arr.flags.writeable = False
+            cache[key] = arr
+        return arr
 
 
 def periodic_system(positions, symbols, box):
