@@ -453,6 +453,19 @@ def main():
         line["descriptors"] = {"ms_per_call": ms_d / max(2, args.steps // 5),
                                "kernel_ms_per_call": {k: v[0] / max(2, args.steps // 5) for k, v in ktd.items()
                                                       if v[1]}}
+        # compute_all_descriptors (B, dB and W: the fitting inputs; dB is 142 MB at 54,000 atoms)
+        dB_h = np.zeros((n, K * nsp, 3))
+        Wd_h = np.zeros((K * nsp, 6))
+
+        def desc_all_call():
+            ctx.check(lib().ipg_snap_descriptors(snap.handle, n, pos_np.ctypes.data_as(vp), sp_np.ctypes.data_as(vp),
+                                                 L.ctypes.data_as(vp), B_h.ctypes.data_as(vp),
+                                                 dB_h.ctypes.data_as(vp), Wd_h.ctypes.data_as(vp), 7))
+        nda = 2
+        ms_da, _, ktda = timed(desc_all_call, nda, kernel_timing=True)
+        ctx.set_stream(stream.cuda_stream)
+        line["all_descriptors"] = {"ms_per_call": ms_da / nda, "dB_bytes": dB_h.nbytes,
+                                   "kernel_ms_per_call": {k: v[0] / nda for k, v in ktda.items() if v[1]}}
     if "j6" in extras:
         # SNAP single species, twojmax 6, 8,192 atoms (BCC 16^3, rcut 4.7 A): plain dB/dr path (the
         # reference's route) and the adjoint path, device buffers, neighbor build included
