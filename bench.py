@@ -45,8 +45,9 @@ WORKLOAD = ("snap_j8: SNAP twojmax=8 (55 components), 2 species (weights 1.0/0.5
 
 
 # timing name -> kernel
+PAIR_KERNEL = "tangent" if os.environ.get("IPG_PAIR_TANGENT", "0") == "1" else "lie"
 KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot_all<8>",
-                "snap_pair": "k_snap_pair_adj_all<8>"}
+                "snap_pair": "k_snap_pair_adj_all<8>" if PAIR_KERNEL == "tangent" else "k_snap_pair_lie<8>"}
 # DRAM bytes (read + write) per atom of one launch, from the ncu --set full captures on the
 # 16,000-atom case summarised in profiles/k_snap_{yrows,pair_adj_all,utot_all}_snap_j8.md;
 # scaled by atoms (pairs per atom are the same).
@@ -335,7 +336,7 @@ def main():
     tf = C.c_double()
     probe.ipg_probe_fp64_peak(local, 5, C.byref(tf), None)
     fp64_peak = tf.value
-    kflops = FL.adjoint_kernels(prm["twojmax"], n, npairs)
+    kflops = FL.adjoint_kernels(prm["twojmax"], n, npairs, PAIR_KERNEL)
     per_kernel = {}
     for k, fl in kflops.items():
         k_ms, k_n = kt.get(k, (0.0, 0))

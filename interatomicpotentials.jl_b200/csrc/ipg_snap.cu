@@ -1494,6 +1494,7 @@ __device__ __forceinline__ double2 zitem_lanes(const ZDev& z, const double* __re
 // compute_yi.jl:23-121), then writes Y'_h = w_h Y_h to yout[h][atom] and adds
 // Re(conj(U_h) Y'_h) to the atom's energy: E_i = (2/3) sum_h Re(conj(U_h) Y'_h) - beta.bzero
 // (B is cubic in U).
+static_assert(SNAP_MAX_J + 1 <= 13, "k_snap_yatoms covers Z entries of up to 13 terms");
 __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yatoms(const __grid_constant__ SnapDev S, int64_t n,
                                                                   const int32_t* __restrict__ species,
                                                                   const double2* __restrict__ utot,
@@ -1527,7 +1528,9 @@ __global__ void __launch_bounds__(YS_WARPS * 32, 2) k_snap_yatoms(const __grid_c
   case NA:                                                                                                \
     zz = zitem_lanes<NA>(z, S.cglist + z.cgoff, us + lane, S.half_block, mb1min, ma1min, mb2max, ma2max); \
     break;
+          // na <= j1 + 1 <= SNAP_MAX_J + 1 (j1 = j2 = twojmax, j = 0 reaches it)
           IPG_NA(1) IPG_NA(2) IPG_NA(3) IPG_NA(4) IPG_NA(5) IPG_NA(6) IPG_NA(7) IPG_NA(8) IPG_NA(9) IPG_NA(10)
+          IPG_NA(11) IPG_NA(12) IPG_NA(13)
 #undef IPG_NA
           default:
             zz = make_double2(0.0, 0.0);
@@ -2612,6 +2615,110 @@ int launch_pair_adj_all(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_
   }
 }
 
+// Adjoint forces of every directed pair from U alone (snapchain::all_chains_lie: the
+// derivative of U along r_ij is U times a Lie-algebra generator, so the three tangent chains
+// of k_snap_pair_adj_all are not needed).  The block's pairs are sorted by owner; the owners'
+// weighted Y and the two generator-shifted copies Y2, Y3 (per atom, from Yw) are staged in
+// shared memory for up to PAIR_LIE_ATOMS atoms at a time; a block whose pairs span more
+// atoms stages them group by group.
+constexpr int PAIR_LIE_T = 128;
+constexpr int PAIR_LIE_ATOMS = 8;
+__host__ __device__ constexpr size_t pair_lie_smem(int uh) { return (size_t)3 * uh * PAIR_LIE_ATOMS * sizeof(double2); }
+template <int J>
+__global__ void __launch_bounds__(PAIR_LIE_T) k_snap_pair_lie(const __grid_constant__ SnapDev S,
+                                                              const int64_t* __restrict__ d_np, int64_t natoms,
+                                                              const int32_t* __restrict__ owner,
+                                                              const int32_t* __restrict__ nbr,
+                                                              const double* __restrict__ rij,
+                                                              const int32_t* __restrict__ species,
+                                                              const double2* __restrict__ Yw,
+                                                              double* __restrict__ part) {
+  extern __shared__ double2 ylie[];  // [3][u_half][PAIR_LIE_ATOMS]: Yw, Y2, Y3 of a group of owners
+  const int64_t np = *d_np;          // the live count (capacity mode sizes the grid larger)
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
+  if (p0 >= np) return;  // block-uniform
+  const int first = owner[p0];
+  const int lastat = owner[(p0 + blockDim.x < np ? p0 + blockDim.x : np) - 1];
+  const int UH = S.u_half;
+  const int i = p < np ? owner[p] : -1;
+  // per direction k: F_k = c0_k S0 + cT_k . T (the generator coefficients times sfac)
+  double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);
+  double c0[3] = {0.0, 0.0, 0.0}, cT[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  if (p < np) {
+    const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[nbr[p]], S.nsp);
+    const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+    PairGeom PG;
+    geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+    a = PG.a;
+    b = PG.b;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double2 da = PG.da[k], db = PG.db[k];
+      c0[k] = 2.0 * PG.dsfac * PG.u[k];
+      const double f = 2.0 * PG.sfac;
+      cT[k][0] = f * (a.y * da.x - a.x * da.y + b.x * db.y - b.y * db.x);  // Im(a conj(da) + conj(b) db)
+      cT[k][1] = f * (b.x * da.x + b.y * da.y - a.x * db.x - a.y * db.y);  // Re(conj(b) da - a conj(db))
+      cT[k][2] = f * (b.x * da.y - b.y * da.x - a.y * db.x + a.x * db.y);  // Im(conj(b) da - a conj(db))
+    }
+  }
+  double S0 = 0.0, T[3] = {0.0, 0.0, 0.0};
+  for (int g0 = first; g0 <= lastat; g0 += PAIR_LIE_ATOMS) {  // block-uniform bounds
+    const int nat = lastat - g0 + 1 < PAIR_LIE_ATOMS ? lastat - g0 + 1 : PAIR_LIE_ATOMS;
+    if (g0 > first) __syncthreads();  // the previous group's readers are done
+    for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
+      const int h = idx / nat, a = idx - h * nat;
+      int j = 0;
+      while (j < S.J && S.half_block[j + 1] <= h) j++;
+      const int q = h - S.half_block[j], mb = q / (j + 1), m = q - mb * (j + 1);
+      const int last = (2 * mb == j) ? mb : j;  // weighted entries of the row
+      const double2* yr = Yw + (size_t)(S.half_block[j] + mb * (j + 1)) * natoms + g0 + a;
+      const double2 z = make_double2(0.0, 0.0);
+      const double2 w = m <= last ? yr[(size_t)m * natoms] : z;
+      const double2 wp = m + 1 <= last ? yr[(size_t)(m + 1) * natoms] : z;
+      const double2 wm = (m >= 1 && m - 1 <= last) ? yr[(size_t)(m - 1) * natoms] : z;
+      const double sp = m < j ? sqrt((double)((m + 1) * (j - m))) : 0.0;   // s_m
+      const double sm = m >= 1 ? sqrt((double)(m * (j - m + 1))) : 0.0;    // s_{m-1}
+      const double2 A = make_double2(sp * wp.x, sp * wp.y), B = make_double2(sm * wm.x, sm * wm.y);
+      ylie[(size_t)h * PAIR_LIE_ATOMS + a] = w;
+      ylie[(size_t)(UH + h) * PAIR_LIE_ATOMS + a] = make_double2(A.x - B.x, A.y - B.y);
+      ylie[(size_t)(2 * UH + h) * PAIR_LIE_ATOMS + a] = make_double2(A.y + B.y, -(A.x + B.x));
+    }
+    __syncthreads();
+    if (i >= g0 && i < g0 + nat)
+      snapchain::all_chains_lie<J>(a, b, ylie + (i - g0), PAIR_LIE_ATOMS, UH, S0, T);
+  }
+  if (p >= np) return;
+  double* out = part + (size_t)p * 3;
+#pragma unroll
+  for (int k = 0; k < 3; k++) out[k] = c0[k] * S0 + (cT[k][0] * T[0] + cT[k][1] * T[1] + cT[k][2] * T[2]);
+}
+
+template <int J>
+int launch_pair_lie_t(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms,
+                      const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species,
+                      const double2* Yw, double* part) {
+  const size_t sm = pair_lie_smem(S.u_half);
+  if (sm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_pair_lie<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  IPG_TIMED_LAUNCH(ctx, "snap_pair", k_snap_pair_lie<J>, nblk(np, PAIR_LIE_T), PAIR_LIE_T, sm, S, d_np, natoms, owner,
+                   nbr, rij, species, Yw, part);
+  return IPG_OK;
+}
+
+int launch_pair_lie(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms, const int32_t* owner,
+                    const int32_t* nbr, const double* rij, const int32_t* species, const double2* Yw, double* part) {
+  if (np == 0) return IPG_OK;
+  switch (S.J) {
+#define IPG_J(JJ) \
+  case JJ:        \
+    return launch_pair_lie_t<JJ>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, Yw, part);
+    IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8) IPG_J(9) IPG_J(10)
+#undef IPG_J
+    default:
+      return IPG_ERR_UNSUPPORTED;
+  }
+}
+
 // ---- exact Hessian-vector product on the register chains -------------------------------
 // The position pullback needs Hv, the tangent of the forces along a displacement v of the
 // atoms.  dE_i/dr_ij = 2 sum_h w Re(conj(D_k,h) Y_h), D_k = dsfac uhat_k U + sfac dU/dr_k,
@@ -3191,6 +3298,7 @@ struct ipg_snap {
   bool generic_adjoint = false;  // force the in-block per-neighbor adjoint (testing)
   std::vector<int64_t> chunk_tab;  // per-configuration reduction chunks (host staging)
   bool pair_split = false;  // adjoint pair kernel: one thread per (pair, chain) instead of per pair
+  bool pair_tangent = false;  // adjoint pair kernel: forward tangent chains instead of the generator identity
   bool y_entries = false;   // Y kernel: one Z entry at a time (k_snap_yatoms) even where rows fit
   int utot_warps = 4;       // atoms (warps) per block of the per-chain Utot kernels
   bool utot_split = false;  // Utot: one launch per chain (k_snap_utot) instead of k_snap_utot_all
@@ -3674,8 +3782,10 @@ int snap_eval(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* d_spec
       if (out.yw_out) *out.yw_out = yout;
       if (s->pair_split)
         IPG_RET(launch_pair_adj(ctx, dev, np, pl.d_np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
-      else
+      else if (s->pair_tangent)
         IPG_RET(launch_pair_adj_all(ctx, dev, np, pl.d_np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
+      else
+        IPG_RET(launch_pair_lie(ctx, dev, np, pl.d_np, n, owner, pl.d_j, pl.d_r, d_species, yout, fvec));
     }
   } else if (mode == MODE_ADJ) {
     IPG_RET(scratch(ctx, "snap_fvec", 3 * (size_t)np + 3, &fvec));
@@ -4092,6 +4202,7 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
   }
   if (const char* g = getenv("IPG_GENERIC_ADJOINT")) s->generic_adjoint = g[0] == '1';
   if (const char* g = getenv("IPG_PAIR_SPLIT")) s->pair_split = g[0] == '1';
+  if (const char* g = getenv("IPG_PAIR_TANGENT")) s->pair_tangent = g[0] == '1';
   if (const char* g = getenv("IPG_Y_ENTRIES")) s->y_entries = g[0] == '1';
   if (const char* g = getenv("IPG_UTOT_SPLIT")) s->utot_split = g[0] == '1';
   if (const char* g = getenv("IPG_VJP_CHUNK")) s->vjp_chunk = std::max<int64_t>(0, atoll(g));

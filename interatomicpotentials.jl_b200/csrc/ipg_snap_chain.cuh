@@ -623,6 +623,102 @@ __device__ __forceinline__ void all_chains_utot(double2 a, double2 b, double sw,
   st.flush();
 }
 
+// ---- adjoint forces from U alone (the SU(2) derivative identity) ------------------------
+// U^j(r) is the spin-j/2 representation of the unit quaternion (a, b), g = [[conj a, -conj b],
+// [b, a]] (the level-1 matrix of the recursion), so its derivative along r_k is U^j times
+// the representation of the Lie-algebra element g^-1 dg/dr_k = [[i al_k, be_k], [-conj be_k,
+// -i al_k]], acting on the column index ma:
+//   dU/dr_k = U (al_k D1 + Re(be_k) D2 + Im(be_k) D3),
+//   D1 = diag(i (j - 2 ma)),  D2[m][m+1] = s_m = -D2[m+1][m],  D3[m][m+1] = D3[m+1][m] = i s_m,
+//   s_m = sqrt((m + 1)(j - m)),
+//   al_k = Im(a conj(da_k) + conj(b) db_k),  be_k = conj(b) da_k - a conj(db_k).
+// So the adjoint sums S_k = sum_e Re(conj(dU_e/dr_k) Yw_e) over the half plane are
+//   S_k = al_k T1 + Re(be_k) T2 + Im(be_k) T3,
+//   T1 = sum_e (j - 2 ma) Im(conj(U_e) Yw_e),  T2 = sum_e Re(conj(U_e) Y2_e),  T3 = sum_e Re(conj(U_e) Y3_e),
+// with, within each row (Yw zero beyond a row's weighted entries),
+//   Y2[m] = s_m Yw[m+1] - s_{m-1} Yw[m-1],  Y3[m] = -i (s_m Yw[m+1] + s_{m-1} Yw[m-1]),
+// which depend on the centre atom only.  A pair then needs U alone, without the three
+// tangent chains: about a quarter of the FP64 work of all_chains_adjoint, same result up to
+// rounding.  y: the staged Yw, Y2, Y3 of the pair's atom, entry h of array g at
+// y[(g ya + h) ys]; acc: S0, T1, T2, T3 for even ma, then for odd ma (shorter FMA chains).
+template <int J, int j>
+__device__ __forceinline__ void contract_lie(const ChainU<J>& s, const double2* __restrict__ y, int ys, int ya,
+                                             int mb, double (&acc)[8]) {
+  // the middle row of an even level: Yw ends at ma = mb, Y2 and Y3 one entry later
+  const int lim = (2 * mb == j) ? (mb < j ? mb + 1 : j) : j;
+  const double2* y0 = y + (half_block(j) + mb * (j + 1)) * ys;
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > lim) break;
+    const int q = 4 * (ma & 1);  // a compile-time index once the loop is unrolled
+    const double2 u = s.u[ma];
+    const double2 w = y0[ma * ys], w2 = y0[(ya + ma) * ys], w3 = y0[(2 * ya + ma) * ys];
+    acc[q] = fma(u.x, w.x, fma(u.y, w.y, acc[q]));
+    if (j != 2 * ma) acc[q + 1] = fma((double)(j - 2 * ma), fma(u.x, w.y, -(u.y * w.x)), acc[q + 1]);
+    acc[q + 2] = fma(u.x, w2.x, fma(u.y, w2.y, acc[q + 2]));
+    acc[q + 3] = fma(u.x, w3.x, fma(u.y, w3.y, acc[q + 3]));
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level_lie_rt(ChainU<J>& s, double2 a, double2 b, int mb, const double2* y, int ys,
+                                             int ya, double (&acc)[8], double2 (&sv)[J + 1]) {
+  if constexpr (j <= J) {
+    advance_u_rt<J, j>(s, a, b, mb);
+    contract_lie<J, j>(s, y, ys, ya, mb, acc);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2) {
+      if (j == 2 * mb + 1) {  // start row of chain mb+1: the mirror of this row
+        constexpr int R = (j + 1) / 2;
+#pragma unroll
+        for (int c = 0; c <= j; c++) {
+          const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+          sv[c] = make_double2(sg * s.u[j - c].x, -sg * s.u[j - c].y);
+        }
+      }
+    }
+  }
+}
+
+// All chains of one neighbor, U only, contracted with the centre atom's Yw, Y2, Y3.
+template <int J>
+__device__ __forceinline__ void all_chains_lie(double2 a, double2 b, const double2* __restrict__ y, int ys, int ya,
+                                               double& S0, double (&T)[3]) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
+  ChainU<J> s;
+  double2 sv[J + 1];
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+    sv[c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);
+  double acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) acc[q] = 0.0;
+  contract_lie<J, 0>(s, y, ys, ya, 0, acc);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+#pragma unroll
+      for (int c = 0; c <= J; c++)
+        if (c < 2 * mb) s.u[c] = sv[c];
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {  // chain mb runs levels 2mb (1 for chain 0) .. J
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level_lie_rt<J, JJ>(s, a, b, mb, y, ys, ya, acc, sv);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
+  S0 = acc[0] + acc[4];
+#pragma unroll
+  for (int g = 0; g < 3; g++) T[g] = acc[1 + g] + acc[5 + g];
+}
+
 }  // namespace snapchain
 
 namespace snapchain {

@@ -129,10 +129,30 @@ def chain_adjoint_pair(J):
     return du_pair(J) + 16 * _n_contract(J) + 12
 
 
-def adjoint_kernels(J, natoms, npairs):
-    """Flops per launch of each kernel of the adjoint step, keyed like the library's timing names."""
+def lie_pair(J):
+    """k_snap_pair_lie, one directed pair: the U recursion of the half plane (no tangents), its
+    contraction with the staged Yw, Y2, Y3 (S0: 4 flops, T1: 5, T2 and T3: 4 each per contracted
+    entry; T1 vanishes where j = 2 ma; the middle row of an even level runs to ma = mb + 1), the
+    generator coefficients (30 flops per direction) and F_k (8 flops per direction)."""
+    f = 0
+    for j, mb, ma in _levels(J):
+        if j == 0:
+            continue
+        t = _terms(j, ma)
+        f += 8 * t + (2 if t == 2 else 0)
+    for j, mb, ma in _levels(J):
+        lim = min(mb + 1, j) if 2 * mb == j else j
+        if ma <= lim:
+            f += 12 + (5 if j != 2 * ma else 0)
+    return f + 3 * (30 + 8)
+
+
+def adjoint_kernels(J, natoms, npairs, pair_kernel="lie"):
+    """Flops per launch of each kernel of the adjoint step, keyed like the library's timing names.
+    pair_kernel: "lie" (k_snap_pair_lie, the default) or "tangent" (k_snap_pair_adj_all)."""
+    pair = lie_pair(J) if pair_kernel == "lie" else chain_adjoint_pair(J)
     return {"snap_atom": natoms * yatoms_atom(J), "snap_utot": npairs * utot_pair(J),
-            "snap_pair": npairs * chain_adjoint_pair(J)}
+            "snap_pair": npairs * pair}
 
 
 def snap_atom_kernel(J, natoms, npairs, mode):

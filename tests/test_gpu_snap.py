@@ -227,7 +227,7 @@ def test_lbasis_potential_api():
     assert rel_err(ipg.virial_stress(s, lbp), Wd @ beta) <= TOL
 
 
-@pytest.mark.parametrize("J", [4, 7, 8, 11])
+@pytest.mark.parametrize("J", [4, 7, 8, 9, 10, 11])
 def test_adjoint_paths_agree(J, monkeypatch):
     """twojmax <= 10 runs the register-chain kernel, larger twojmax (or IPG_GENERIC_ADJOINT=1)
     the in-block per-neighbor loop; both must equal the plain dB/dr path and the oracle."""
@@ -497,3 +497,30 @@ def test_y_kernel_variants_agree(env, monkeypatch):
     assert abs(e - e0) <= 1e-13 * abs(e0) and rel_err(f, f0) <= 1e-13 and rel_err(w, w0) <= 1e-13
     eo, fo, _ = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.1)
     assert abs(e - eo) <= TOL * abs(eo) and rel_err(f, fo) <= TOL
+
+
+@pytest.mark.parametrize("J", [2, 5, 6, 8, 10])
+@pytest.mark.parametrize("density", ["dense", "dilute"])
+def test_pair_generator_identity_vs_tangent_chains(J, density, monkeypatch):
+    """The adjoint pair kernel contracts U alone with the Lie-generator-shifted copies of Y
+    (dU/dr = U times a generator of SU(2)); IPG_PAIR_TANGENT=1 runs the forward tangent chains
+    instead.  Both give the same forces to rounding and the oracle's to 1e-10.  "dilute" gives
+    atoms a few neighbors or none, so a block of pairs spans more atoms than it stages at once
+    (its owners are staged group by group)."""
+    rng = np.random.default_rng(700 + J)
+    n, box = (60, 7.5) if density == "dense" else (90, 30.0)
+    pos = rng.uniform(0, box, (n, 3))
+    s = ipg.System(pos, list(np.where(rng.random(n) < 0.5, "A", "B")), [box] * 3)
+    prm = dict(twojmax=J, species=["A", "B"], rcutfac=2.4, rmin0=0.05, rfac0=0.97, radii=[1.0, 0.85],
+               weight=[1.0, 0.6], switch_flag=True)
+    snap, orc = make(prm)
+    beta = rng.normal(0, 1e-2, (2, len(snap)))
+    e0, f0, w0 = snap.energy_forces(s, beta, 0.0, mode="adjoint")
+    monkeypatch.setenv("IPG_PAIR_TANGENT", "1")
+    snap_t, _ = make(prm)
+    e1, f1, w1 = snap_t.energy_forces(s, beta, 0.0, mode="adjoint")
+    assert e1 == e0  # the energy does not go through the pair kernel
+    assert rel_err(f0, f1) <= 1e-12 and rel_err(w0, w1) <= 1e-12
+    eo, fo, wo = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.0)
+    assert abs(e0 - eo) <= TOL * abs(eo)
+    assert rel_err(f0, fo) <= TOL and rel_err(w0, wo) <= TOL
