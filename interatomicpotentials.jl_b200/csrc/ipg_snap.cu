@@ -2038,9 +2038,71 @@ __global__ void __launch_bounds__(VS_WARPS * 32) k_snap_vsum(const __grid_consta
   }
 }
 
+// V from U alone (snapchain::all_chains_vlie: the generator identity of k_snap_pair_lie
+// applied to the derivative chains of k_snap_vsum).
+template <int J>
+__global__ void __launch_bounds__(VS_WARPS * 32) k_snap_vlie(const __grid_constant__ SnapDev S, int64_t a0, int64_t nc,
+                                                             const int64_t* __restrict__ off,
+                                                             const int32_t* __restrict__ nbr,
+                                                             const double* __restrict__ rij,
+                                                             const int32_t* __restrict__ species,
+                                                             const double* __restrict__ g, double2* __restrict__ V) {
+  extern __shared__ double2 vsh[];  // [VS_WARPS][UT_SLOTS 33]
+  __shared__ int dst[VS_WARPS][snapchain::UT_SLOTS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t li = (int64_t)blockIdx.x * VS_WARPS + w;
+  if (li >= nc) return;  // warp-uniform; the kernel synchronises only within a warp
+  const int64_t i = a0 + li;
+  const int si = clamp_sp(species[i], S.nsp);
+  const int64_t beg = off[i], end = off[i + 1];
+  const double gi0 = g[3 * i], gi1 = g[3 * i + 1], gi2 = g[3 * i + 2];
+  snapchain::UtStage st;
+  st.buf = vsh + w * snapchain::UT_SLOTS * 33;
+  st.dst = dst[w];
+  st.ut = reinterpret_cast<double*>(V + li);
+  st.stride = nc;
+  st.lane = lane;
+  st.nslot = 0;
+  st.wself = 0.0;
+  for (int64_t p0 = beg; p0 < (end > beg ? end : beg + 1); p0 += 32) {
+    const int64_t p = p0 + lane;
+    double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);  // idle lanes: zero weights
+    double A = 0.0, gm[3] = {0.0, 0.0, 0.0};
+    if (p < end) {
+      const int32_t jn = nbr[p];
+      const int sj = clamp_sp(species[jn], S.nsp);
+      const double rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+      PairGeom PG;
+      geom_du(S, rij[3 * p], rij[3 * p + 1], rij[3 * p + 2], rcut, S.weight[sj], PG);
+      a = PG.a;
+      b = PG.b;
+      const double gv[3] = {gi0 - g[3 * jn], gi1 - g[3 * jn + 1], gi2 - g[3 * jn + 2]};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const double2 da = PG.da[k], db = PG.db[k];
+        A += gv[k] * (PG.dsfac * PG.u[k]);
+        const double Bk = PG.sfac * gv[k];
+        gm[0] = fma(Bk, a.y * da.x - a.x * da.y + b.x * db.y - b.y * db.x, gm[0]);  // Im(a conj(da) + conj(b) db)
+        gm[1] = fma(Bk, b.x * da.x + b.y * da.y - a.x * db.x - a.y * db.y, gm[1]);  // Re(conj(b) da - a conj(db))
+        gm[2] = fma(Bk, b.x * da.y - b.y * da.x - a.y * db.x + a.x * db.y, gm[2]);  // Im(conj(b) da - a conj(db))
+      }
+    }
+    st.first = p0 == beg;
+    snapchain::all_chains_vlie<J>(a, b, A, gm[0], gm[1], gm[2], st);
+  }
+}
+
 template <int J>
 int launch_vsum_j(ipg_ctx* ctx, const SnapDev& S, int64_t a0, int64_t nc, const int64_t* off, const int32_t* nbr,
-                  const double* rij, const int32_t* species, const double* g, double2* V) {
+                  const double* rij, const int32_t* species, const double* g, double2* V, bool tangent) {
+  if (!tangent) {
+    const size_t sl = (size_t)VS_WARPS * snapchain::UT_SLOTS * 33 * sizeof(double2);
+    if (sl > 48 * 1024)
+      CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_vlie<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sl));
+    IPG_TIMED_LAUNCH(ctx, "snap_vsum", k_snap_vlie<J>, nblk(nc, VS_WARPS), VS_WARPS * 32, sl, S, a0, nc, off, nbr,
+                     rij, species, g, V);
+    return IPG_OK;
+  }
   const size_t sm = ((size_t)4 * (J + 1) * VS_WARPS * 32 + (size_t)VS_WARPS * snapchain::UT_SLOTS * 33) * sizeof(double2);
   if (sm > 48 * 1024)
     CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_vsum<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -2049,13 +2111,14 @@ int launch_vsum_j(ipg_ctx* ctx, const SnapDev& S, int64_t a0, int64_t nc, const 
   return IPG_OK;
 }
 
+// tangent: the forward tangent chains (k_snap_vsum) instead of the generator identity (k_snap_vlie)
 int launch_vsum(ipg_ctx* ctx, const SnapDev& S, int64_t a0, int64_t nc, const int64_t* off, const int32_t* nbr,
-                const double* rij, const int32_t* species, const double* g, double2* V) {
+                const double* rij, const int32_t* species, const double* g, double2* V, bool tangent) {
   if (nc == 0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return launch_vsum_j<JJ>(ctx, S, a0, nc, off, nbr, rij, species, g, V);
+    return launch_vsum_j<JJ>(ctx, S, a0, nc, off, nbr, rij, species, g, V, tangent);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
 #undef IPG_J
     default:
@@ -4194,6 +4257,13 @@ int ipg_snap_create(ipg_ctx* ctx, const ipg_snap_params* params, ipg_snap** out)
     for (int a = 1; a < R; a++)
       for (int b = 1; b < R; b++) t[a * R + b] = std::sqrt((double)a / (double)b);
     cudaError_t e = cudaMemcpyToSymbol(snapchain::c_rpq, t, sizeof(t));
+    // generator factors sqrt((m + 1)(j - m)) of the derivative identity
+    constexpr int NR = snapchain::SGEN_ROWS;
+    double t2[R * NR * R] = {};
+    for (int j = 1; j < R; j++)
+      for (int mb = 0; mb < NR; mb++)
+        for (int m = 0; m < j; m++) t2[(j * NR + mb) * R + m] = std::sqrt((double)((m + 1) * (j - m)));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(snapchain::c_sgen, t2, sizeof(t2));
     if (e != cudaSuccess) {
       cudaFree(s->d_tables);
       delete s;
@@ -4479,7 +4549,7 @@ int snap_vjp_device(ipg_snap* s, int64_t n, const double* d_pos, const int32_t* 
         IPG_TIMED_LAUNCH(ctx, "snap_zrows", k_snap_yrows<YM_Z>, (unsigned)yg, YS_WARPS * 32, ysm, dev, s->h.yconst,
                          nc, d_species + a0, io.utot_in + (size_t)a0 * dev.idxu_max, Z, (double*)nullptr,
                          (double2*)nullptr);
-      IPG_RET(launch_vsum(ctx, dev, a0, nc, pl.d_off, pl.d_j, pl.d_r, d_species, d_g, V));
+      IPG_RET(launch_vsum(ctx, dev, a0, nc, pl.d_off, pl.d_j, pl.d_r, d_species, d_g, V, s->pair_tangent));
       const int64_t gg = std::min(tiles, gmax);
       IPG_TIMED_LAUNCH(ctx, "snap_gbeta", k_snap_gbeta, (unsigned)gg, GB_WARPS * 32, gsm, dev, a0, nc, d_species, Z,
                        V, io.utot_in, gE, gpart + (size_t)rows * nsp * K);
@@ -4617,7 +4687,7 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
       if (Vg)
         V = const_cast<double2*>(Vg);
       else
-        IPG_RET(launch_vsum(ctx, dev, 0, n, pl.d_off, pl.d_j, pl.d_r, d_sp, d_v, V));
+        IPG_RET(launch_vsum(ctx, dev, 0, n, pl.d_off, pl.d_j, pl.d_r, d_sp, d_v, V, s->pair_tangent));
       IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_hvp_split, nblk(32 * n, 256), 256, 0, dev, n, utot, V, Up, Um, sc);
       bool d1 = false, d2 = false;
       IPG_RET(launch_y(s, dev, "snap_hvp_y", n, d_sp, Up, Yp, ebuf, nullptr, nullptr, &d1));

@@ -791,6 +791,100 @@ __device__ __forceinline__ void all_chains_v(const Geom& G, double A, const doub
   st.flush();
 }
 
+// ---- V from U alone (the generator identity of all_chains_lie) --------------------------
+// sum_k B_k dU/dr_k = U (g1 D1 + g2 D2 + g3 D3) with g = sum_k B_k (al_k, Re be_k, Im be_k),
+// so within a row (s_m = c_sgen[j][mb][m])
+//   v[ma] = A u[ma] + g1 (j - 2 ma) i u[ma] + s_{ma-1} (g2 + i g3) u[ma-1] + s_ma (i g3 - g2) u[ma+1]:
+// the same V as all_chains_v without the three tangent chains.
+// [j][mb][m] = sqrt((m + 1)(j - m)), 0 <= m < j, the same for every row mb <= j/2: indexed by the
+// runtime row so that the compiler loads the factors where they are used instead of hoisting
+// all of them into registers for the whole neighbor loop (which spilled)
+constexpr int SGEN_ROWS = SNAP_MAX_J / 2 + 1;
+__constant__ double c_sgen[RPQ_STRIDE * SGEN_ROWS * RPQ_STRIDE];
+
+template <int J, int j>
+__device__ __forceinline__ void stage_vlie(const ChainU<J>& s, double A, double g1, double g2, double g3, int mb,
+                                           UtStage& st) {
+  const int last = (2 * mb == j) ? mb : j;
+  const int hb = half_block(j) + mb * (j + 1);
+  st.room(last + 1);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > last) break;
+    const double2 u = s.u[ma];
+    const double c1 = g1 * (double)(j - 2 * ma);  // i u = (-u.y, u.x)
+    double vx = fma(A, u.x, -(c1 * u.y)), vy = fma(A, u.y, c1 * u.x);
+    if (ma > 0) {  // s_{ma-1} (g2 + i g3) u[ma-1]
+      const double sg = c_sgen[(j * SGEN_ROWS + mb) * RPQ_STRIDE + ma - 1];
+      const double2 w = s.u[ma - 1];
+      const double px = sg * g2, py = sg * g3;
+      vx = fma(px, w.x, fma(-py, w.y, vx));
+      vy = fma(px, w.y, fma(py, w.x, vy));
+    }
+    if (ma < j) {  // s_ma (-g2 + i g3) u[ma+1]
+      const double sg = c_sgen[(j * SGEN_ROWS + mb) * RPQ_STRIDE + ma];
+      const double2 w = s.u[ma + 1];
+      const double px = -sg * g2, py = sg * g3;
+      vx = fma(px, w.x, fma(-py, w.y, vx));
+      vy = fma(px, w.y, fma(py, w.x, vy));
+    }
+    st.push(make_double2(vx, vy), hb + ma);  // packed: entry only (no mirror, no diagonal)
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level_vlie(ChainU<J>& s, double2 a, double2 b, double A, double g1, double g2,
+                                           double g3, int mb, UtStage& st, double2 (&sv)[J + 1]) {
+  if constexpr (j <= J) {
+    advance_u_rt<J, j>(s, a, b, mb);
+    stage_vlie<J, j>(s, A, g1, g2, g3, mb, st);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2) {
+      if (j == 2 * mb + 1) {  // start row of chain mb+1: the mirror of this row
+        constexpr int R = (j + 1) / 2;
+#pragma unroll
+        for (int c = 0; c <= j; c++) {
+          const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+          sv[c] = make_double2(sg * s.u[j - c].x, -sg * s.u[j - c].y);
+        }
+      }
+    }
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void all_chains_vlie(double2 a, double2 b, double A, double g1, double g2, double g3,
+                                                UtStage& st) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
+  ChainU<J> s;
+  double2 sv[J + 1];
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+    sv[c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);
+  stage_vlie<J, 0>(s, A, g1, g2, g3, 0, st);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+#pragma unroll
+      for (int c = 0; c <= J; c++)
+        if (c < 2 * mb) s.u[c] = sv[c];
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level_vlie<J, JJ>(s, a, b, A, g1, g2, g3, mb, st, sv);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
+  st.flush();
+}
+
 }  // namespace snapchain
 
 

@@ -524,3 +524,15 @@ def test_pair_generator_identity_vs_tangent_chains(J, density, monkeypatch):
     eo, fo, wo = orc.energy_forces(s.positions, snap.species_ids(s), s.L, beta, 0.0)
     assert abs(e0 - eo) <= TOL * abs(eo)
     assert rel_err(f0, fo) <= TOL and rel_err(w0, wo) <= TOL
+    # the beta pullback's V = sum_j g_ij . dU_ij/dr (and the Utot tangent of the position
+    # pullback) go through the same identity
+    gF = rng.normal(size=(n, 3))
+    gb0, g00 = snap.vjp_beta(s, 0.3, gF)
+    gb1, g01 = snap_t.vjp_beta(s, 0.3, gF)
+    assert rel_err(gb0, gb1) <= 1e-12 and g00 == g01
+    ob, _ = orc.vjp_beta(s.positions, snap.species_ids(s), s.L, 0.3, gF)
+    assert rel_err(gb0, ob) <= TOL
+    if J <= 8:  # the position pullback covers twojmax <= 8 (its shared memory beyond)
+        pb0, _, gp0 = snap.vjp(s, beta, 0.3, gF)
+        pb1, _, gp1 = snap_t.vjp(s, beta, 0.3, gF)
+        assert rel_err(pb0, pb1) <= 1e-12 and rel_err(gp0, gp1) <= 1e-12
