@@ -553,8 +553,10 @@ struct UtStage {
 };
 
 // Stages row mb of level j (the half-plane part) with its destinations in the full Utot.
+// The chain carries sw U (the recursion is linear and sw real, so starting it from sw instead
+// of 1 scales every entry, the mirrored rows included): the staged values need no multiply.
 template <int J, int j>
-__device__ __forceinline__ void stage_row(const ChainU<J>& s, double sw, int mb, UtStage& st) {
+__device__ __forceinline__ void stage_row(const ChainU<J>& s, int mb, UtStage& st) {
   static_assert(j + 1 <= UT_SLOTS, "a row must fit the staging buffer");
   const int last = (2 * mb == j) ? mb : j;  // middle row: entries beyond ma = mb are mirrors
   const int ub = u_block(j);
@@ -566,16 +568,16 @@ __device__ __forceinline__ void stage_row(const ChainU<J>& s, double sw, int mb,
     const bool self_mirror = (2 * mb == j) && ma == mb;
     const int em = ub + (j - mb) * (j + 1) + (j - ma);
     const int packed = e | (em << 12) | (((ma + mb) & 1) << 24) | ((ma == mb) << 25) | ((!self_mirror) << 26);
-    st.push(make_double2(sw * s.u[ma].x, sw * s.u[ma].y), packed);
+    st.push(s.u[ma], packed);
   }
 }
 
 template <int J, int j>
-__device__ __forceinline__ void level_u_rt(ChainU<J>& s, double2 a, double2 b, double sw, int mb, UtStage& st,
+__device__ __forceinline__ void level_u_rt(ChainU<J>& s, double2 a, double2 b, int mb, UtStage& st,
                                            double2 (&sv)[J + 1]) {
   if constexpr (j <= J) {
     advance_u_rt<J, j>(s, a, b, mb);
-    stage_row<J, j>(s, sw, mb, st);
+    stage_row<J, j>(s, mb, st);
     if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2) {
       if (j == 2 * mb + 1) {  // start row of chain mb+1: the mirror of this row
         constexpr int R = (j + 1) / 2;
@@ -600,8 +602,8 @@ __device__ __forceinline__ void all_chains_utot(double2 a, double2 b, double sw,
     s.u[c] = make_double2(0.0, 0.0);
     sv[c] = make_double2(0.0, 0.0);
   }
-  s.u[0] = make_double2(1.0, 0.0);
-  stage_row<J, 0>(s, sw, 0, st);
+  s.u[0] = make_double2(sw, 0.0);
+  stage_row<J, 0>(s, 0, st);
 #pragma unroll 1
   for (int mb = 0; mb <= J / 2; mb++) {
     if (mb > 0) {
@@ -612,7 +614,7 @@ __device__ __forceinline__ void all_chains_utot(double2 a, double2 b, double sw,
     switch (mb == 0 ? 1 : 2 * mb) {  // chain mb runs levels 2mb (1 for chain 0) .. J
 #define IPG_LEVEL(JJ) \
   case JJ:            \
-    level_u_rt<J, JJ>(s, a, b, sw, mb, st, sv);
+    level_u_rt<J, JJ>(s, a, b, mb, st, sv);
       IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
       IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
 #undef IPG_LEVEL
