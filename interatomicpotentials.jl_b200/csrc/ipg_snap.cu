@@ -2728,21 +2728,22 @@ __global__ void __launch_bounds__(PAIR_LIE_T) k_snap_pair_lie(const __grid_const
   for (int g0 = first; g0 <= lastat; g0 += PAIR_LIE_ATOMS) {  // block-uniform bounds
     const int nat = lastat - g0 + 1 < PAIR_LIE_ATOMS ? lastat - g0 + 1 : PAIR_LIE_ATOMS;
     if (g0 > first) __syncthreads();  // the previous group's readers are done
+    // Yw of the group, zero beyond each row's weighted entries (the Y kernel leaves those unset)
     for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
       const int h = idx / nat, a = idx - h * nat;
-      int j = 0;
-      while (j < S.J && S.half_block[j + 1] <= h) j++;
-      const int q = h - S.half_block[j], mb = q / (j + 1), m = q - mb * (j + 1);
-      const int last = (2 * mb == j) ? mb : j;  // weighted entries of the row
-      const double2* yr = Yw + (size_t)(S.half_block[j] + mb * (j + 1)) * natoms + g0 + a;
+      ylie[(size_t)h * PAIR_LIE_ATOMS + a] =
+          (S.h_info[h] >> 16) ? Yw[(size_t)h * natoms + g0 + a] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    // Y2, Y3 from the row neighbours of each entry
+    for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
+      const int h = idx / nat, a = idx - h * nat;
+      const int inf = S.h_info[h], m = inf & 255, j = (inf >> 8) & 255;
+      const double2 sg = S.h_sgen[h];  // (s_m, s_{m-1}), zero where the neighbour is off the row
       const double2 z = make_double2(0.0, 0.0);
-      const double2 w = m <= last ? yr[(size_t)m * natoms] : z;
-      const double2 wp = m + 1 <= last ? yr[(size_t)(m + 1) * natoms] : z;
-      const double2 wm = (m >= 1 && m - 1 <= last) ? yr[(size_t)(m - 1) * natoms] : z;
-      const double sp = m < j ? sqrt((double)((m + 1) * (j - m))) : 0.0;   // s_m
-      const double sm = m >= 1 ? sqrt((double)(m * (j - m + 1))) : 0.0;    // s_{m-1}
-      const double2 A = make_double2(sp * wp.x, sp * wp.y), B = make_double2(sm * wm.x, sm * wm.y);
-      ylie[(size_t)h * PAIR_LIE_ATOMS + a] = w;
+      const double2 wp = m < j ? ylie[(size_t)(h + 1) * PAIR_LIE_ATOMS + a] : z;
+      const double2 wm = m >= 1 ? ylie[(size_t)(h - 1) * PAIR_LIE_ATOMS + a] : z;
+      const double2 A = make_double2(sg.x * wp.x, sg.x * wp.y), B = make_double2(sg.y * wm.x, sg.y * wm.y);
       ylie[(size_t)(UH + h) * PAIR_LIE_ATOMS + a] = make_double2(A.x - B.x, A.y - B.y);
       ylie[(size_t)(2 * UH + h) * PAIR_LIE_ATOMS + a] = make_double2(A.y + B.y, -(A.x + B.x));
     }
@@ -3432,7 +3433,9 @@ int upload_tables(ipg_snap* s) {
   size_t o_ysh = o_yso + pad(h.ysched_off.size() * 4);
   size_t o_ysw = o_ysh + pad(h.ysched_h.size() * 4);
   size_t o_uoh = o_ysw + pad(h.ysched_w.size() * 8);
-  size_t o_yrows = o_uoh + pad(h.u_of_h.size() * 4);
+  size_t o_hinfo = o_uoh + pad(h.u_of_h.size() * 4);
+  size_t o_hsgen = o_hinfo + pad(h.h_info.size() * 4);
+  size_t o_yrows = o_hsgen + pad(h.h_sgen.size() * 8);
   size_t o_yit = o_yrows + pad(h.yrows.size() * sizeof(YRowDev));
   size_t o_yca = o_yit + pad(h.yitems.size() * sizeof(YItemDev));
   size_t o_ytj = o_yca + pad(h.yca.size() * 8);
@@ -3453,6 +3456,8 @@ int upload_tables(ipg_snap* s) {
   memcpy(hostbuf.data() + o_ysh, h.ysched_h.data(), h.ysched_h.size() * 4);
   memcpy(hostbuf.data() + o_ysw, h.ysched_w.data(), h.ysched_w.size() * 8);
   memcpy(hostbuf.data() + o_uoh, h.u_of_h.data(), h.u_of_h.size() * 4);
+  memcpy(hostbuf.data() + o_hinfo, h.h_info.data(), h.h_info.size() * 4);
+  memcpy(hostbuf.data() + o_hsgen, h.h_sgen.data(), h.h_sgen.size() * 8);
   memcpy(hostbuf.data() + o_yrows, h.yrows.data(), h.yrows.size() * sizeof(YRowDev));
   memcpy(hostbuf.data() + o_yit, h.yitems.data(), h.yitems.size() * sizeof(YItemDev));
   memcpy(hostbuf.data() + o_yca, h.yca.data(), h.yca.size() * 8);
@@ -3501,6 +3506,8 @@ int upload_tables(ipg_snap* s) {
   d.ysched_h = reinterpret_cast<const int32_t*>(b + o_ysh);
   d.ysched_w = reinterpret_cast<const double*>(b + o_ysw);
   d.u_of_h = reinterpret_cast<const int32_t*>(b + o_uoh);
+  d.h_info = reinterpret_cast<const int32_t*>(b + o_hinfo);
+  d.h_sgen = reinterpret_cast<const double2*>(b + o_hsgen);
   d.n_yrows = (int)h.yrows.size();
   d.yrows = reinterpret_cast<const YRowDev*>(b + o_yrows);
   d.yitems = reinterpret_cast<const YItemDev*>(b + o_yit);

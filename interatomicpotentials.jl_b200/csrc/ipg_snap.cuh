@@ -80,6 +80,8 @@ struct SnapDev {
   const int32_t* ysched_h;
   const double* ysched_w;
   const int32_t* u_of_h;      // [u_half] index of half-plane entry h in the full Utot
+  const int32_t* h_info;      // [u_half] m | j << 8 | (m within the row's weighted entries) << 16, m = column ma
+  const double2* h_sgen;      // [u_half] the generator factors (s_m, s_{m-1}), s_m = sqrt((m+1)(j-m)), 0 off the row
   // row-blocked Y kernel (twojmax <= YR_MAX_J): n_yrows target rows, longest first
   const YRowDev* yrows;
   const YItemDev* yitems;
@@ -106,7 +108,8 @@ struct SnapHost {
   std::vector<int32_t> y_jjb;     // component whose beta scales each Z entry in Y
   std::vector<double> y_mult;     // multiplicity * (j1+1)/(j+1) factor of each Z entry
   std::vector<int32_t> zperm;     // Z entries sorted by (nb, na): equal trip counts per warp
-  std::vector<int32_t> ysched_off, ysched_h, u_of_h;
+  std::vector<int32_t> ysched_off, ysched_h, u_of_h, h_info;
+  std::vector<double> h_sgen;  // 2 per half-plane entry
   std::vector<double> ysched_w;
   std::vector<YRowDev> yrows;
   std::vector<YItemDev> yitems;

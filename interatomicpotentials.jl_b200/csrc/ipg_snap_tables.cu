@@ -69,6 +69,16 @@ int snap_build_tables(const ipg_snap_params& p, SnapHost& h) {
   }
   h.half_block[jd] = cnt;
   h.u_half = cnt;
+  h.h_info.clear();
+  h.h_sgen.clear();
+  for (int j = 0; j <= J; j++)
+    for (int mb = 0; 2 * mb <= j; mb++)
+      for (int m = 0; m <= j; m++) {
+        const int last = (2 * mb == j) ? mb : j;  // the middle row of an even level is weighted up to mb
+        h.h_info.push_back(m | (j << 8) | ((m <= last ? 1 : 0) << 16));
+        h.h_sgen.push_back(m < j ? std::sqrt((double)((m + 1) * (j - m))) : 0.0);
+        h.h_sgen.push_back(m >= 1 ? std::sqrt((double)(m * (j - m + 1))) : 0.0);
+      }
 
   h.idxb.clear();
   for (int j1 = 0; j1 <= J; j1++)
