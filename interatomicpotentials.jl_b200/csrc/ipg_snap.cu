@@ -2927,6 +2927,109 @@ __global__ void __launch_bounds__(HVP_T) k_snap_pair_hvp(const __grid_constant__
                            PG.sfac.v * T[5]);
 }
 
+// The Hessian-vector product of the pair forces from U and one tangent chain
+// (snapchain::all_chains_hvp_lie), one thread per pair for all three directions: Yw and Ydot
+// of up to HVP_LIE_ATOMS owners staged in shared memory (zero beyond each row's weighted
+// entries), the start rows of U and its tangent saved per thread.  The pair geometry with its
+// tangent is computed before the chains for (a, b) and again after them for the force
+// coefficients, so that none of it is held in registers across the chains.
+constexpr int HVP_LIE_T = 128;
+constexpr int HVP_LIE_ATOMS = 8;
+__host__ __device__ constexpr size_t hvp_lie_smem(int J, int uh) {
+  return ((size_t)2 * (J + 1) * HVP_LIE_T + (size_t)2 * uh * HVP_LIE_ATOMS) * sizeof(double2);
+}
+__device__ __forceinline__ double opaque(double x) {  // the same value, not recognised as such
+  double y;
+  asm volatile("mov.b64 %0, %1;" : "=d"(y) : "d"(x));
+  return y;
+}
+template <int J>
+__global__ void __launch_bounds__(HVP_LIE_T) k_snap_pair_hvp_lie(const __grid_constant__ SnapDev S,
+                                                                 const int64_t* __restrict__ d_np, int64_t natoms,
+                                                                 const int32_t* __restrict__ owner,
+                                                                 const int32_t* __restrict__ nbr,
+                                                                 const double* __restrict__ rij,
+                                                                 const int32_t* __restrict__ species,
+                                                                 const double* __restrict__ v,
+                                                                 const double2* __restrict__ Yw,
+                                                                 const double2* __restrict__ Yd,
+                                                                 double* __restrict__ fdot) {
+  extern __shared__ double2 hsm[];  // save [2 (J+1)][HVP_LIE_T], then Yw, Yd [2][u_half][HVP_LIE_ATOMS]
+  const int64_t np = *d_np;
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x, p = p0 + threadIdx.x;
+  if (p0 >= np) return;  // block-uniform
+  const int first = owner[p0];
+  const int lastat = owner[(p0 + blockDim.x < np ? p0 + blockDim.x : np) - 1];
+  const int UH = S.u_half;
+  double2* ysm = hsm + 2 * (J + 1) * HVP_LIE_T;
+  double2* ydm = ysm + UH * HVP_LIE_ATOMS;
+  const int i = p < np ? owner[p] : -1;
+  int32_t jn = 0;
+  double rcut = 1.0, wj = 0.0, x = 1.0, y = 0.0, z = 0.0, tx = 0.0, ty = 0.0, tz = 0.0;
+  double2 a = make_double2(1.0, 0.0), at = make_double2(0.0, 0.0), b = at, bt = at;
+  if (p < np) {
+    jn = nbr[p];
+    const int si = clamp_sp(species[i], S.nsp), sj = clamp_sp(species[jn], S.nsp);
+    rcut = (S.radii[si] + S.radii[sj]) * S.rcutfac;
+    wj = S.weight[sj];
+    x = rij[3 * p];
+    y = rij[3 * p + 1];
+    z = rij[3 * p + 2];
+    tx = v[3 * jn] - v[3 * i];
+    ty = v[3 * jn + 1] - v[3 * i + 1];
+    tz = v[3 * jn + 2] - v[3 * i + 2];
+    PairGeomD PG;
+    geom_hvp(S, x, y, z, tx, ty, tz, rcut, wj, PG);
+    a = make_double2(PG.ar.v, PG.ai.v);
+    at = make_double2(PG.ar.t, PG.ai.t);
+    b = make_double2(PG.br.v, PG.bi.v);
+    bt = make_double2(PG.br.t, PG.bi.t);
+  }
+  double acc[12];
+#pragma unroll
+  for (int q = 0; q < 12; q++) acc[q] = 0.0;
+  for (int g0 = first; g0 <= lastat; g0 += HVP_LIE_ATOMS) {  // block-uniform bounds
+    const int nat = lastat - g0 + 1 < HVP_LIE_ATOMS ? lastat - g0 + 1 : HVP_LIE_ATOMS;
+    if (g0 > first) __syncthreads();  // the previous group's readers are done
+    for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
+      const int h = idx / nat, at_ = idx - h * nat;
+      const bool wt = (S.h_info[h] >> 16) != 0;  // the Y kernels leave the unweighted entries unset
+      const size_t gi = (size_t)h * natoms + g0 + at_;
+      ysm[h * HVP_LIE_ATOMS + at_] = wt ? Yw[gi] : make_double2(0.0, 0.0);
+      ydm[h * HVP_LIE_ATOMS + at_] = wt ? Yd[gi] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (i >= g0 && i < g0 + nat)
+      snapchain::all_chains_hvp_lie<J>(a, at, b, bt, ysm + (i - g0), ydm + (i - g0), HVP_LIE_ATOMS, acc, hsm,
+                                       HVP_LIE_T, threadIdx.x);
+  }
+  if (p >= np) return;
+  PairGeomD G;
+  geom_hvp(S, opaque(x), opaque(y), opaque(z), opaque(tx), opaque(ty), opaque(tz), rcut, wj, G);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const Dual c0 = 2.0 * (G.dsfac * G.u[k]);
+    const Dual f = 2.0 * G.sfac;
+    const Dual c1 = f * (G.ai * G.dar[k] - G.ar * G.dai[k] + G.br * G.dbi[k] - G.bi * G.dbr[k]);
+    const Dual c2 = f * (G.br * G.dar[k] + G.bi * G.dai[k] - G.ar * G.dbr[k] - G.ai * G.dbi[k]);
+    const Dual c3 = f * (G.br * G.dai[k] - G.bi * G.dar[k] - G.ai * G.dbr[k] + G.ar * G.dbi[k]);
+    fdot[3 * p + k] = c0.t * acc[0] + c0.v * (acc[1] + acc[2]) + (c1.t * acc[3] + c1.v * (acc[4] + acc[5])) +
+                      (c2.t * acc[6] + c2.v * (acc[7] + acc[8])) + (c3.t * acc[9] + c3.v * (acc[10] + acc[11]));
+  }
+}
+
+template <int J>
+int launch_pair_hvp_lie_j(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms,
+                          const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species,
+                          const double* v, const double2* Yw, const double2* Yd, double* fdot) {
+  const size_t sm = hvp_lie_smem(J, S.u_half);
+  if (sm > 48 * 1024)
+    CUDA_RET(ctx, cudaFuncSetAttribute(k_snap_pair_hvp_lie<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_snap_pair_hvp_lie<J>, nblk(np, HVP_LIE_T), HVP_LIE_T, sm, S, d_np, natoms, owner,
+                   nbr, rij, species, v, Yw, Yd, fdot);
+  return IPG_OK;
+}
+
 template <int J>
 int launch_pair_hvp_j(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms,
                       const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species,
@@ -2943,14 +3046,17 @@ int launch_pair_hvp_j(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t*
   return IPG_OK;
 }
 
+// tangent: the second-order tangent chains (k_snap_pair_hvp) instead of U and one tangent chain with
+// the generator identity (k_snap_pair_hvp_lie)
 int launch_pair_hvp(ipg_ctx* ctx, const SnapDev& S, int64_t np, const int64_t* d_np, int64_t natoms,
                     const int32_t* owner, const int32_t* nbr, const double* rij, const int32_t* species,
-                    const double* v, const double2* Yw, const double2* Yd, double* fdot) {
+                    const double* v, const double2* Yw, const double2* Yd, double* fdot, bool tangent) {
   if (np == 0) return IPG_OK;
   switch (S.J) {
 #define IPG_J(JJ) \
   case JJ:        \
-    return launch_pair_hvp_j<JJ>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, v, Yw, Yd, fdot);
+    return tangent ? launch_pair_hvp_j<JJ>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, v, Yw, Yd, fdot) \
+                   : launch_pair_hvp_lie_j<JJ>(ctx, S, np, d_np, natoms, owner, nbr, rij, species, v, Yw, Yd, fdot);
     IPG_J(0) IPG_J(1) IPG_J(2) IPG_J(3) IPG_J(4) IPG_J(5) IPG_J(6) IPG_J(7) IPG_J(8)
 #undef IPG_J
     default:
@@ -4702,7 +4808,8 @@ int ipg_snap_vjp(ipg_snap* s, int64_t n, const double* pos, const int32_t* speci
       if (!d1 || !d2) return ipg_fail(ctx, IPG_ERR_UNSUPPORTED, "position pullback: no atoms-in-lanes Y kernel");
       IPG_TIMED_LAUNCH(ctx, "snap_hvp", k_hvp_ydot, nblk((int64_t)UH * n, 256), 256, 0, n, UH, Yp, Ym, sc, Yd);
       IPG_LAUNCH(ctx, k_pair_owner, nblk(32 * n, 256), 256, 0, n, pl.d_off, owner);
-      IPG_RET(launch_pair_hvp(ctx, dev, pl.npairs, pl.d_np, n, owner, pl.d_j, pl.d_r, d_sp, d_v, yw, Yd, fd));
+      IPG_RET(launch_pair_hvp(ctx, dev, pl.npairs, pl.d_np, n, owner, pl.d_j, pl.d_r, d_sp, d_v, yw, Yd, fd,
+                              s->pair_tangent));
     } else {
       // one block per atom, every phase in forward mode (k_snap_hvp)
       const int nw = 8;

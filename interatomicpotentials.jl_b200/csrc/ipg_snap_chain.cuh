@@ -887,6 +887,158 @@ __device__ __forceinline__ void all_chains_vlie(double2 a, double2 b, double A, 
   st.flush();
 }
 
+// ---- the Hessian-vector product of the pair forces from U and one tangent ---------------
+// The pair force of all_chains_lie, F_k = c0_k S0 + sum_g cT_kg T_g, has along the pair
+// displacement tangent rdot the tangent
+//   Fdot_k = c0dot_k S0 + c0_k (S0a + S0b) + sum_g [cTdot_kg T_g + cT_kg (T_g,a + T_g,b)],
+// where the a-terms contract the tangent Udot of U (one tangent chain along rdot) with Yw and
+// the b-terms contract U with the centre atom's Ydot (Yd).  The generator rows U D_g are
+// formed from the row of U in registers ((U D1)[m] = i (j - 2m) U[m], (U D2)[m] = s_{m-1}
+// U[m-1] - s_m U[m+1], (U D3)[m] = i (s_{m-1} U[m-1] + s_m U[m+1])), so only Yw and Yd are
+// read.  acc: S0, S0a, S0b, then T_g, T_g,a, T_g,b for g = 1, 2, 3.
+template <int J>
+struct ChainT {
+  double2 u[J + 1];
+  double2 t[J + 1];  // the tangent of u along rdot
+};
+
+template <int J, int j>
+__device__ __forceinline__ void advance_t_rt(ChainT<J>& s, double2 a, double2 at, double2 b, double2 bt, int mb) {
+  const int col = j - mb;
+#pragma unroll
+  for (int ma = j; ma >= 0; --ma) {
+    double2 nu = make_double2(0.0, 0.0), nt = make_double2(0.0, 0.0);
+    if (ma > 0) {  // - rootpq[ma][j-mb] conj(b) u[ma-1]
+      const double rp = -c_rpq[ma * RPQ_STRIDE + col];
+      const double bx = rp * b.x, by = rp * b.y, btx = rp * bt.x, bty = rp * bt.y;
+      const double2 v = s.u[ma - 1], vt = s.t[ma - 1];
+      nu.x = fma(bx, v.x, by * v.y);
+      nu.y = fma(bx, v.y, -(by * v.x));
+      nt.x = fma(btx, v.x, fma(bty, v.y, fma(bx, vt.x, by * vt.y)));
+      nt.y = fma(btx, v.y, fma(-bty, v.x, fma(bx, vt.y, -(by * vt.x))));
+    }
+    if (ma < j) {  // + rootpq[j-ma][j-mb] conj(a) u[ma]
+      const double rp = c_rpq[(j - ma) * RPQ_STRIDE + col];
+      const double ax = rp * a.x, ay = rp * a.y, atx = rp * at.x, aty = rp * at.y;
+      const double2 v = s.u[ma], vt = s.t[ma];
+      nu.x = fma(ax, v.x, fma(ay, v.y, nu.x));
+      nu.y = fma(ax, v.y, fma(-ay, v.x, nu.y));
+      nt.x = fma(atx, v.x, fma(aty, v.y, fma(ax, vt.x, fma(ay, vt.y, nt.x))));
+      nt.y = fma(atx, v.y, fma(-aty, v.x, fma(ax, vt.y, fma(-ay, vt.x, nt.y))));
+    }
+    s.u[ma] = nu;
+    s.t[ma] = nt;
+  }
+}
+
+__device__ __forceinline__ double re_cm(double2 x, double2 y) { return fma(x.x, y.x, x.y * y.y); }   // Re(conj(x) y)
+__device__ __forceinline__ double im_cm(double2 x, double2 y) { return fma(x.x, y.y, -(x.y * y.x)); }  // Im(conj(x) y)
+
+template <int J, int j>
+__device__ __forceinline__ void contract_hvp_lie(const ChainT<J>& s, const double2* __restrict__ yw,
+                                                 const double2* __restrict__ yd, int ys, int mb, double (&acc)[12]) {
+  const int last = (2 * mb == j) ? mb : j;  // the weighted entries of the row
+  const int h0 = half_block(j) + mb * (j + 1);
+#pragma unroll
+  for (int ma = 0; ma <= j; ma++) {
+    if (ma > last) break;
+    const double2 w = yw[(h0 + ma) * ys], wd = yd[(h0 + ma) * ys];
+    const double2 u = s.u[ma], ut = s.t[ma];
+    acc[0] += re_cm(u, w);
+    acc[1] += re_cm(ut, w);
+    acc[2] += re_cm(u, wd);
+    if (j != 2 * ma) {
+      const double c = (double)(j - 2 * ma);
+      acc[3] = fma(c, im_cm(u, w), acc[3]);
+      acc[4] = fma(c, im_cm(ut, w), acc[4]);
+      acc[5] = fma(c, im_cm(u, wd), acc[5]);
+    }
+    // P = s_{ma-1} U[ma-1], Q = s_ma U[ma+1] (and their tangents)
+    double2 P = make_double2(0.0, 0.0), Q = P, Pt = P, Qt = P;
+    if (ma > 0) {
+      const double sg = c_sgen[(j * SGEN_ROWS + mb) * RPQ_STRIDE + ma - 1];
+      P = make_double2(sg * s.u[ma - 1].x, sg * s.u[ma - 1].y);
+      Pt = make_double2(sg * s.t[ma - 1].x, sg * s.t[ma - 1].y);
+    }
+    if (ma < j) {
+      const double sg = c_sgen[(j * SGEN_ROWS + mb) * RPQ_STRIDE + ma];
+      Q = make_double2(sg * s.u[ma + 1].x, sg * s.u[ma + 1].y);
+      Qt = make_double2(sg * s.t[ma + 1].x, sg * s.t[ma + 1].y);
+    }
+    const double2 X = make_double2(P.x - Q.x, P.y - Q.y), Xt = make_double2(Pt.x - Qt.x, Pt.y - Qt.y);
+    const double2 Z = make_double2(P.x + Q.x, P.y + Q.y), Zt = make_double2(Pt.x + Qt.x, Pt.y + Qt.y);
+    acc[6] += re_cm(X, w);
+    acc[7] += re_cm(Xt, w);
+    acc[8] += re_cm(X, wd);
+    acc[9] += im_cm(Z, w);   // Re(conj(i Z) w) = Im(conj(Z) w)
+    acc[10] += im_cm(Zt, w);
+    acc[11] += im_cm(Z, wd);
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void save_mirror_t(const ChainT<J>& s, double2* __restrict__ save, int nt, int tid) {
+  constexpr int R = (j + 1) / 2;
+#pragma unroll
+  for (int c = 0; c <= j; c++) {
+    const double sg = ((c + R) & 1) ? -1.0 : 1.0;
+    const double2 u = s.u[j - c], t = s.t[j - c];
+    save[c * nt + tid] = make_double2(sg * u.x, -sg * u.y);
+    save[((J + 1) + c) * nt + tid] = make_double2(sg * t.x, -sg * t.y);
+  }
+}
+
+template <int J, int j>
+__device__ __forceinline__ void level_hvp_lie(ChainT<J>& s, double2 a, double2 at, double2 b, double2 bt, int mb,
+                                              const double2* yw, const double2* yd, int ys, double (&acc)[12],
+                                              double2* save, int nt, int tid) {
+  if constexpr (j <= J) {
+    advance_t_rt<J, j>(s, a, at, b, bt, mb);
+    contract_hvp_lie<J, j>(s, yw, yd, ys, mb, acc);
+    if constexpr (j % 2 == 1 && (j + 1) / 2 <= J / 2)
+      if (j == 2 * mb + 1) save_mirror_t<J, j>(s, save, nt, tid);  // start row of chain mb+1
+  }
+}
+
+template <int J>
+__device__ __forceinline__ void all_chains_hvp_lie(double2 a, double2 at, double2 b, double2 bt,
+                                                   const double2* __restrict__ yw, const double2* __restrict__ yd,
+                                                   int ys, double (&acc)[12], double2* save, int nt, int tid) {
+  static_assert(J <= 12, "level switch covers twojmax <= 12");
+  ChainT<J> s;
+#pragma unroll
+  for (int c = 0; c <= J; c++) {
+    s.u[c] = make_double2(0.0, 0.0);
+    s.t[c] = make_double2(0.0, 0.0);
+  }
+  s.u[0] = make_double2(1.0, 0.0);
+#pragma unroll
+  for (int q = 0; q < 12; q++) acc[q] = 0.0;
+  contract_hvp_lie<J, 0>(s, yw, yd, ys, 0, acc);
+#pragma unroll 1
+  for (int mb = 0; mb <= J / 2; mb++) {
+    if (mb > 0) {
+      asm volatile("" ::: "memory");  // this chain's loads stay after the previous chain's saves
+#pragma unroll
+      for (int c = 0; c <= J; c++) {
+        if (c >= 2 * mb) break;
+        s.u[c] = save[c * nt + tid];
+        s.t[c] = save[((J + 1) + c) * nt + tid];
+      }
+    }
+    switch (mb == 0 ? 1 : 2 * mb) {  // chain mb runs levels 2mb (1 for chain 0) .. J
+#define IPG_LEVEL(JJ) \
+  case JJ:            \
+    level_hvp_lie<J, JJ>(s, a, at, b, bt, mb, yw, yd, ys, acc, save, nt, tid);
+      IPG_LEVEL(1) IPG_LEVEL(2) IPG_LEVEL(3) IPG_LEVEL(4) IPG_LEVEL(5) IPG_LEVEL(6)
+      IPG_LEVEL(7) IPG_LEVEL(8) IPG_LEVEL(9) IPG_LEVEL(10) IPG_LEVEL(11) IPG_LEVEL(12)
+#undef IPG_LEVEL
+      default:
+        break;
+    }
+  }
+}
+
 }  // namespace snapchain
 
 
