@@ -49,10 +49,11 @@ PAIR_KERNEL = "tangent" if os.environ.get("IPG_PAIR_TANGENT", "0") == "1" else "
 KERNEL_NAMES = {"snap_atom": "k_snap_yrows", "snap_utot": "k_snap_utot_all<8>",
                 "snap_pair": "k_snap_pair_adj_all<8>" if PAIR_KERNEL == "tangent" else "k_snap_pair_lie<8>"}
 # DRAM bytes (read + write) per atom of one launch, from the ncu --set full captures on the
-# 16,000-atom case summarised in profiles/k_snap_{yrows,pair_adj_all,utot_all}_snap_j8.md;
+# 16,000-atom case summarised in profiles/k_snap_{yrows,pair_lie,pair_adj_all,utot_all}_snap_j8.md;
 # scaled by atoms (pairs per atom are the same).
 NCU_DRAM_BYTES_PER_ATOM = {"snap_atom": (51.886336e6 + 2.899200e6) / 16000,
-                           "snap_pair": (52.742144e6 + 0.953088e6) / 16000,
+                           "snap_pair": ((52.742144e6 + 0.953088e6) if PAIR_KERNEL == "tangent"
+                                         else (50.157056e6 + 0.847360e6)) / 16000,
                            "snap_utot": (11.558912e6 + 16.316928e6) / 16000}
 
 

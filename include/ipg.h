@@ -81,8 +81,8 @@ IPG_API int ipg_launch_count(const ipg_ctx* ctx, int64_t* out);
  * "snap_bdesc" (B), "snap_dbfused" (plain dB/dr), "snap_contract" (plain-path contraction),
  * "snap_vsum" and "snap_gbeta" (beta pullback; "snap_vsum" also carries the Utot tangent of
  * the position pullback), "snap_hvp_y" (its two polarized Y evaluations), "snap_hvp" (the
- * rest of the exact Hessian-vector product: the second-order pair chains, or the per-atom
- * forward-mode kernel).  Unknown names read as zero. */
+ * rest of the exact Hessian-vector product: the pair part, or the per-atom forward-mode
+ * kernel).  Unknown names read as zero. */
 IPG_API int ipg_timing_enable(ipg_ctx* ctx, int on);
 IPG_API int ipg_timing_read(ipg_ctx* ctx, const char* kernel, double* total_ms, int64_t* launches);
 

@@ -2704,6 +2704,19 @@ __global__ void __launch_bounds__(PAIR_LIE_T) k_snap_pair_lie(const __grid_const
   const int lastat = owner[(p0 + blockDim.x < np ? p0 + blockDim.x : np) - 1];
   const int UH = S.u_half;
   const int i = p < np ? owner[p] : -1;
+  // the first group's Y' goes to shared memory by asynchronous copies (zero-filled beyond each
+  // row's weighted entries, which the Y kernel leaves unset) while the pair geometry is computed
+  auto stage = [&](int g0, int nat) {
+    for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
+      const int h = idx / nat, at = idx - h * nat;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(ylie + (size_t)h * PAIR_LIE_ATOMS + at);
+      const double2* src = Yw + (size_t)h * natoms + g0 + at;
+      const int bytes = (S.h_info[h] >> 16) ? 16 : 0;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  stage(first, lastat - first + 1 < PAIR_LIE_ATOMS ? lastat - first + 1 : PAIR_LIE_ATOMS);
   // per direction k: F_k = c0_k S0 + cT_k . T (the generator coefficients times sfac)
   double2 a = make_double2(1.0, 0.0), b = make_double2(0.0, 0.0);
   double c0[3] = {0.0, 0.0, 0.0}, cT[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
@@ -2727,13 +2740,11 @@ __global__ void __launch_bounds__(PAIR_LIE_T) k_snap_pair_lie(const __grid_const
   double S0 = 0.0, T[3] = {0.0, 0.0, 0.0};
   for (int g0 = first; g0 <= lastat; g0 += PAIR_LIE_ATOMS) {  // block-uniform bounds
     const int nat = lastat - g0 + 1 < PAIR_LIE_ATOMS ? lastat - g0 + 1 : PAIR_LIE_ATOMS;
-    if (g0 > first) __syncthreads();  // the previous group's readers are done
-    // Yw of the group, zero beyond each row's weighted entries (the Y kernel leaves those unset)
-    for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
-      const int h = idx / nat, a = idx - h * nat;
-      ylie[(size_t)h * PAIR_LIE_ATOMS + a] =
-          (S.h_info[h] >> 16) ? Yw[(size_t)h * natoms + g0 + a] : make_double2(0.0, 0.0);
+    if (g0 > first) {
+      __syncthreads();  // the previous group's readers are done
+      stage(g0, nat);
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     // Y2, Y3 from the row neighbours of each entry
     for (int idx = threadIdx.x; idx < UH * nat; idx += blockDim.x) {
